@@ -1,0 +1,247 @@
+"""B200 per-step hot path of the axisymmetric compressible jet solver (nataraj2/AxisymmetricJet).
+
+The compute path is libaxj.so (hand-written sm_100a CUDA behind the C-ABI in
+include/axj.h). This module is the host-side mirror of the reference's call
+interface for that path -- ComputeTimeStep / RK4 / ComputeRHS and the operator
+routines -- over ctypes. There is no CPU fallback: if the library or a CUDA
+device is missing, every call raises.
+
+Array convention: a field is a numpy float64 array of shape (Nr, Nz) (z fastest,
+the reference's column-major (Nz, Nr) layout); a solution pv is (5, Nr, Nz)
+holding rho, V_r, V_theta, V_z, T (pv(Nz,Nr,1,5) of ModuleVariables.f90:39).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._ffi import (AXJ_OK, STATUS, AxjBcRecord, AxjParams, AxjPatch, default_params, dptr, patch_array,
+                   patches_to_tuples, record_array)
+
+__all__ = ["AxiJetSolver", "AxjError", "default_params", "load_library", "read_bc_file", "patches_from_records",
+           "library_path"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def library_path():
+    return os.path.join(_HERE, "libaxj.so")
+
+
+class AxjError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load_library():
+    """Load the in-tree libaxj.so (built by axisymmetricjet_b200.build). Raises if absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m axisymmetricjet_b200.build` "
+                           "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    dp = C.POINTER(C.c_double)
+    i64 = C.c_int64
+    h = C.c_void_p
+    sig = {
+        "axj_default_params": (None, [C.POINTER(AxjParams)]),
+        "axj_create": (C.c_int, [C.POINTER(AxjParams), i64, i64, dp, dp, dp, C.POINTER(AxjPatch), i64,
+                                 C.POINTER(h)]),
+        "axj_set_state": (C.c_int, [h, dp, dp, i64, C.c_double]),
+        "axj_get_state": (C.c_int, [h, dp]),
+        "axj_get_time": (C.c_int, [h, C.POINTER(i64), dp]),
+        "axj_compute_dt": (C.c_int, [h, dp]),
+        "axj_rk4_step": (C.c_int, [h, C.c_double]),
+        "axj_run": (C.c_int, [h, i64, i64, C.c_void_p, C.c_void_p, dp]),
+        "axj_run_timed": (C.c_int, [h, i64, dp]),
+        "axj_profile_steps": (C.c_int, [h, i64, dp, C.POINTER(i64)]),
+        "axj_rhs": (C.c_int, [h, dp, dp]),
+        "axj_deriv1": (C.c_int, [h, dp, i64, dp]),
+        "axj_deriv2": (C.c_int, [h, dp, i64, dp, dp]),
+        "axj_tgfilter": (C.c_int, [h, dp, i64, i64, dp]),
+        "axj_sensor": (C.c_int, [h, dp, dp, dp, dp]),
+        "axj_last_error": (C.c_char_p, [h]),
+        "axj_destroy": (None, [h]),
+        "axj_read_bc_file": (C.c_int, [C.c_char_p, C.POINTER(AxjBcRecord), i64, C.POINTER(i64)]),
+        "axj_patches_from_records": (C.c_int, [C.POINTER(AxjBcRecord), i64, i64, i64, C.POINTER(AxjPatch),
+                                               C.POINTER(i64)]),
+        "axj_version": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+OUTPUT_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_double))
+
+
+def _check(lib, h, rc):
+    if rc != AXJ_OK:
+        msg = lib.axj_last_error(h)
+        raise AxjError(rc, msg.decode() if msg else "")
+
+
+def read_bc_file(path):
+    """Rows of a bc file (ModPatch.f90:30-63) as (bc, bc_dir, istart, iend, jstart, jend) tuples."""
+    lib = load_library()
+    n = C.c_int64(0)
+    _check(lib, None, lib.axj_read_bc_file(path.encode(), None, 0, C.byref(n)))
+    arr = (AxjBcRecord * max(n.value, 1))()
+    _check(lib, None, lib.axj_read_bc_file(path.encode(), arr, n.value, C.byref(n)))
+    return [(arr[k].bc, arr[k].bc_dir, arr[k].istart, arr[k].iend, arr[k].jstart, arr[k].jend)
+            for k in range(n.value)]
+
+
+def patches_from_records(records, Nz, Nr):
+    """PatchCreation for one block holding the whole grid (ModPatch.f90:117-309)."""
+    lib = load_library()
+    rec = record_array(records)
+    out = (AxjPatch * max(len(records), 1))()
+    n = C.c_int64(0)
+    _check(lib, None, lib.axj_patches_from_records(rec, len(records), Nz, Nr, out, C.byref(n)))
+    return patches_to_tuples(out, n.value)
+
+
+class AxiJetSolver:
+    """One device-resident block of the jet solver.
+
+    Mirrors the reference's per-step interface: compute_time_step() is
+    ComputeTimeStep (ModInputOutput.f90:389-438), rk4(delt) is RK4
+    (ModRungeKutta.f90:5-171), compute_rhs(pv) is AssignValues + ComputeRHS
+    (ModRHS.f90:5-258); deriv1/deriv2/tgfilter/sensor are the operator routines.
+    """
+
+    def __init__(self, params, zvec, rvec, ibval, patches):
+        self.lib = load_library()
+        zvec = np.ascontiguousarray(zvec, dtype=np.float64)
+        rvec = np.ascontiguousarray(rvec, dtype=np.float64)
+        ibval = np.ascontiguousarray(ibval, dtype=np.float64)
+        self.Nr, self.Nz = zvec.shape
+        assert rvec.shape == zvec.shape and ibval.shape == zvec.shape
+        self.params = params
+        pa = patch_array(patches)
+        h = C.c_void_p()
+        rc = self.lib.axj_create(C.byref(params), self.Nz, self.Nr, dptr(zvec), dptr(rvec), dptr(ibval), pa,
+                                 len(patches), C.byref(h))
+        _check(self.lib, None, rc)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.axj_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _chk(self, rc):
+        _check(self.lib, self.h, rc)
+
+    def _field(self):
+        return np.empty((self.Nr, self.Nz), dtype=np.float64)
+
+    def set_state(self, pv, pv_target, iteration=0, time=0.0):
+        pv = np.ascontiguousarray(pv, dtype=np.float64)
+        tg = np.ascontiguousarray(pv_target, dtype=np.float64)
+        assert pv.shape == (5, self.Nr, self.Nz) and tg.shape == pv.shape
+        self._chk(self.lib.axj_set_state(self.h, dptr(pv), dptr(tg), int(iteration), float(time)))
+
+    def get_state(self, out=None):
+        if out is None:
+            out = np.empty((5, self.Nr, self.Nz), dtype=np.float64)
+        self._chk(self.lib.axj_get_state(self.h, dptr(out)))
+        return out
+
+    def get_time(self):
+        it = C.c_int64(0)
+        t = C.c_double(0.0)
+        self._chk(self.lib.axj_get_time(self.h, C.byref(it), C.byref(t)))
+        return it.value, t.value
+
+    def compute_time_step(self):
+        d = C.c_double(0.0)
+        self._chk(self.lib.axj_compute_dt(self.h, C.byref(d)))
+        return d.value
+
+    def rk4(self, delt):
+        self._chk(self.lib.axj_rk4_step(self.h, float(delt)))
+
+    def run(self, nsteps, out_every=0, callback=None):
+        """nsteps x (ComputeTimeStep + RK4) on the device; returns the last dt."""
+        cb = None
+        if callback is not None and out_every > 0:
+            n = 5 * self.Nr * self.Nz
+            shape = (5, self.Nr, self.Nz)
+
+            def _cb(user, iteration, time, pv):
+                arr = np.ctypeslib.as_array(pv, shape=(n,)).reshape(shape).copy()
+                callback(iteration, time, arr)
+
+            cb = OUTPUT_CB(_cb)
+        d = C.c_double(0.0)
+        self._chk(self.lib.axj_run(self.h, int(nsteps), int(out_every), C.cast(cb, C.c_void_p) if cb else None,
+                                   None, C.byref(d)))
+        return d.value
+
+    def run_timed(self, nsteps):
+        """nsteps graph-replayed steps; returns their device time in ms (CUDA events)."""
+        ms = C.c_double(0.0)
+        self._chk(self.lib.axj_run_timed(self.h, int(nsteps), C.byref(ms)))
+        return ms.value
+
+    def profile_steps(self, nsteps):
+        """nsteps eager steps with CUDA events around each launch group.
+        Returns ({dt, sensor, stage, step}: ms summed, {dt, sensor, stage}: launches)."""
+        ms = (C.c_double * 4)()
+        nl = (C.c_int64 * 3)()
+        self._chk(self.lib.axj_profile_steps(self.h, int(nsteps), ms, nl))
+        keys = ("dt", "sensor", "stage", "step")
+        return dict(zip(keys, list(ms))), dict(zip(keys[:3], list(nl)))
+
+    def compute_rhs(self, pv):
+        pv = np.ascontiguousarray(pv, dtype=np.float64)
+        out = np.empty_like(pv)
+        self._chk(self.lib.axj_rhs(self.h, dptr(pv), dptr(out)))
+        return out
+
+    def deriv1(self, var, dirn):
+        var = np.ascontiguousarray(var, dtype=np.float64)
+        out = self._field()
+        self._chk(self.lib.axj_deriv1(self.h, dptr(var), int(dirn), dptr(out)))
+        return out
+
+    def deriv2(self, var, dirn, first):
+        var = np.ascontiguousarray(var, dtype=np.float64)
+        first = np.ascontiguousarray(first, dtype=np.float64)
+        out = self._field()
+        self._chk(self.lib.axj_deriv2(self.h, dptr(var), int(dirn), dptr(first), dptr(out)))
+        return out
+
+    def tgfilter(self, var, dirn, out, inplace=False):
+        out = np.array(out, dtype=np.float64, order="C", copy=True)
+        v = None if inplace else dptr(np.ascontiguousarray(var, dtype=np.float64))
+        self._chk(self.lib.axj_tgfilter(self.h, v, int(dirn), int(bool(inplace)), dptr(out)))
+        return out
+
+    def sensor(self, pv):
+        pv = np.ascontiguousarray(pv, dtype=np.float64)
+        mu, beta, kappa = self._field(), self._field(), self._field()
+        self._chk(self.lib.axj_sensor(self.h, dptr(pv), dptr(mu), dptr(beta), dptr(kappa)))
+        return mu, beta, kappa

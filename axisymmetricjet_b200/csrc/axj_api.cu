@@ -1,0 +1,904 @@
+// axj_api.cu -- the extern "C" boundary of libaxj.so (declared in include/axj.h):
+// handle lifetime, set-up of the stencil maps, face lists, tile classes and 1-D
+// metrics, host<->device copies, and the step sequence (plain calls or a CUDA graph).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/axj.h"
+#include "axj_common.cuh"
+#include "axj_kernels.cuh"
+
+using namespace axj;
+
+namespace {
+
+std::string g_create_error;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct axj_handle {
+  int device = 0;
+  int Nz = 0, Nr = 0;
+  long long P = 0, plane = 0;
+  axj_params params{};
+  Consts c{};
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::vector<void*> allocs;
+  // state and RK4 work buffers (5 planes each)
+  double *U0 = nullptr, *Ua = nullptr, *Ub = nullptr, *A = nullptr, *B = nullptr, *target = nullptr;
+  // shock-capturing buffers
+  double *S = nullptr, *dil = nullptr, *fsw = nullptr, *d2 = nullptr, *Q = nullptr, *Qz = nullptr, *star = nullptr;
+  uint32_t* desc = nullptr;
+  int* faces = nullptr;
+  double *dxidz = nullptr, *ddxidxidz = nullptr, *detadr = nullptr, *ddetadetadr = nullptr;
+  double *zc = nullptr, *rc = nullptr, *dzv = nullptr, *drv = nullptr, *ramp = nullptr, *forcing = nullptr;
+  double *dt = nullptr, *staleT = nullptr, *partial = nullptr, *time = nullptr;
+  int* flags = nullptr;
+  unsigned int* counter = nullptr;
+  int2 *tiles_int = nullptr, *tiles_gen = nullptr;
+  int ntiles_int = 0, ntiles_gen = 0;
+  int dt_blocks = 0;
+  int iT = 0, jT = 0;
+  int64_t iteration = 0;
+  double time_host = 0.0;
+  bool state_set = false;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  std::vector<double> host_out;  // output-callback staging
+};
+
+namespace {
+
+int fail(axj_handle* h, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (h) h->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+#define AXJ_CUDA(h, call)                                                                                 \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess) return fail((h), AXJ_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+// SBP_operator (ModOperator.f90:5-121). The truncated-Gaussian boundary rows are
+// default-kind (single-precision) literals in the reference, so they are rounded
+// to float before widening, exactly as the Fortran assignment does.
+void build_tables(double S1[9][6], double S2[9][6], double G[9][11]) {
+  std::memset(S1, 0, sizeof(double) * 54);
+  std::memset(S2, 0, sizeof(double) * 54);
+  std::memset(G, 0, sizeof(double) * 99);
+  const double s1[4][6] = {{-24.0 / 17.0, 59.0 / 34.0, -4.0 / 17.0, -3.0 / 34.0, 0.0, 0.0},
+                           {-1.0 / 2.0, 0.0, 1.0 / 2.0, 0.0, 0.0, 0.0},
+                           {4.0 / 43.0, -59.0 / 86.0, 0.0, 59.0 / 86.0, -4.0 / 43.0, 0.0},
+                           {3.0 / 98.0, 0.0, -59.0 / 98.0, 0.0, 32.0 / 49.0, -4.0 / 49.0}};
+  const double s2[4][6] = {{2.0, -5.0, 4.0, -1.0, 0.0, 0.0},
+                           {1.0, -2.0, 1.0, 0.0, 0.0, 0.0},
+                           {-4.0 / 43.0, 59.0 / 43.0, -110.0 / 43.0, 59.0 / 43.0, -4.0 / 43.0, 0.0},
+                           {-1.0 / 49.0, 0.0, 59.0 / 49.0, -118.0 / 49.0, 64.0 / 49.0, -4.0 / 49.0}};
+  for (int r = 0; r < 4; ++r)
+    for (int m = 0; m < 6; ++m) {
+      S1[r][m] = s1[r][m];
+      S2[r][m] = s2[r][m];
+      S1[8 - r][5 - m] = -1.0 * s1[r][m];  // bottom block = -mirror (:32-38)
+      S2[8 - r][5 - m] = 1.0 * s2[r][m];   // bottom block = +mirror (:68-74)
+    }
+  const double i1[5] = {1.0 / 12.0, -2.0 / 3.0, 0.0, 2.0 / 3.0, -1.0 / 12.0};
+  const double i2[5] = {-1.0 / 12.0, 4.0 / 3.0, -5.0 / 2.0, 4.0 / 3.0, -1.0 / 12.0};
+  for (int m = 0; m < 5; ++m) { S1[4][m] = i1[m]; S2[4][m] = i2[m]; }
+  const float g1[7] = {0.085777408970000f, 0.722371828476000f, 0.356848072173000f, -0.223119093072000f,
+                       0.057347064865000f, 0.000747264596000f, 0.000027453993000f};
+  const float g2[7] = {-0.032649010764000f, 0.143339502575000f, 0.726678822020000f, 0.294622121167000f,
+                       -0.186711738069000f, 0.062038376258000f, -0.007318073189000f};
+  const float g3[11] = {0.000054596010000f, -0.042124772446000f, 0.173103107841000f, 0.700384128648000f,
+                        0.276543612935000f, -0.131223506571000f, 0.023424966418000f, -0.013937561779000f,
+                        0.024565095706000f, -0.013098287852000f, 0.002308621090000f};
+  G[0][0] = 1.0;
+  for (int m = 0; m < 7; ++m) { G[1][m] = (double)g1[m]; G[2][m] = (double)g2[m]; }
+  for (int m = 0; m < 11; ++m) G[3][m] = (double)g3[m];
+  for (int r = 0; r < 4; ++r)
+    for (int m = 0; m < 11; ++m) G[8 - r][10 - m] = 1.0 * G[r][m];
+  const double gi[9] = {107.0 / 103680.0, 149.0 / 12960.0, 1997.0 / 25920.0, 3091.0 / 12960.0, 3565.0 / 10368.0,
+                        3091.0 / 12960.0, 1997.0 / 25920.0, 149.0 / 12960.0, 107.0 / 103680.0};
+  for (int m = 0; m < 9; ++m) G[4][m] = gi[m];
+}
+
+// ComputeMetric (ModDeriv.f90:241-382) on a 1-D coordinate line with closures at
+// both ends (single block: every neighbour is MPI_PROC_NULL). Sums start from 0.
+void metric_1d(const double S1[9][6], const std::vector<double>& v, std::vector<double>& out) {
+  const int n = (int)v.size();
+  out.assign(n, 0.0);
+  for (int i = 5; i <= n - 4; ++i) {
+    double s = 0.0;
+    for (int m = 0; m < 5; ++m) s = s + S1[4][m] * v[i - 2 + m - 1];
+    out[i - 1] = s;
+  }
+  for (int i = 1; i <= 4; ++i) {
+    double s = 0.0;
+    for (int m = 0; m < 6; ++m) s = s + S1[i - 1][m] * v[m];
+    out[i - 1] = s;
+  }
+  for (int i = n - 3; i <= n; ++i) {
+    double s = 0.0;
+    for (int m = 0; m < 6; ++m) s = s + S1[8 - n + i][m] * v[n - 6 + m];
+    out[i - 1] = s;
+  }
+}
+
+template <class T>
+T* dalloc(axj_handle* h, size_t count, int* rc) {
+  void* p = nullptr;
+  if (*rc != AXJ_OK) return nullptr;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 16);
+  if (e != cudaSuccess) {
+    *rc = fail(h, AXJ_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    return nullptr;
+  }
+  cudaMemset(p, 0, count * sizeof(T) + 16);
+  h->allocs.push_back(p);
+  return static_cast<T*>(p);
+}
+
+Grid grid_of(const axj_handle* h) {
+  Grid g;
+  g.Nz = h->Nz;
+  g.Nr = h->Nr;
+  g.P = h->P;
+  g.plane = h->plane;
+  return g;
+}
+
+// host (Nz x Nr x nf, z fastest) <-> device (pitch P) copies
+cudaError_t h2d(axj_handle* h, double* dst, const double* src, int nf) {
+  return cudaMemcpy2DAsync(dst, (size_t)h->P * sizeof(double), src, (size_t)h->Nz * sizeof(double),
+                           (size_t)h->Nz * sizeof(double), (size_t)h->Nr * nf, cudaMemcpyHostToDevice, h->stream);
+}
+cudaError_t d2h(axj_handle* h, double* dst, const double* src, int nf) {
+  return cudaMemcpy2DAsync(dst, (size_t)h->Nz * sizeof(double), src, (size_t)h->P * sizeof(double),
+                           (size_t)h->Nz * sizeof(double), (size_t)h->Nr * nf, cudaMemcpyDeviceToHost, h->stream);
+}
+
+SensorArgs sensor_args(axj_handle* h, const double* U) {
+  SensorArgs s;
+  s.g = grid_of(h);
+  s.U = U;
+  s.desc = h->desc;
+  s.dxidz = h->dxidz;
+  s.detadr = h->detadr;
+  s.zc = h->zc;
+  s.rc = h->rc;
+  s.dz = h->dzv;
+  s.dr = h->drv;
+  s.ramp = h->ramp;
+  s.S = h->S;
+  s.dil = h->dil;
+  s.fsw = h->fsw;
+  s.d2 = h->d2;
+  s.Q = h->Q;
+  s.Qz = h->Qz;
+  s.star = h->star;
+  s.c = h->c;
+  return s;
+}
+
+StageArgs stage_args(axj_handle* h, const double* Uin, double* Uout, int stage) {
+  StageArgs a;
+  a.g = grid_of(h);
+  a.Uin = Uin;
+  a.U0 = h->U0;
+  a.A = h->A;
+  a.B = h->B;
+  a.Uout = Uout;
+  a.target = h->target;
+  a.mustar = h->star;
+  a.betastar = h->star + h->plane;
+  a.kappastar = h->star + 2 * h->plane;
+  a.desc = h->desc;
+  a.faces = h->faces;
+  a.tiles = nullptr;
+  a.dxidz = h->dxidz;
+  a.ddxidxidz = h->ddxidxidz;
+  a.detadr = h->detadr;
+  a.ddetadetadr = h->ddetadetadr;
+  a.zc = h->zc;
+  a.rc = h->rc;
+  a.forcing = h->forcing;
+  a.dt = h->dt;
+  a.staleT = h->staleT;
+  a.flags = h->flags;
+  a.stage = stage;
+  a.iT = h->iT;
+  a.jT = h->jT;
+  a.c = h->c;
+  return a;
+}
+
+// One RK stage: the sensor chain on the stage input (if enabled), then the fused
+// stage kernel over both tile classes.
+int enqueue_stage(axj_handle* h, const double* Uin, double* Uout, int stage) {
+  if (h->c.shock_capturing) {
+    SensorArgs s = sensor_args(h, Uin);
+    AXJ_CUDA(h, launch_sensor(s, h->stream));
+  }
+  StageArgs a = stage_args(h, Uin, Uout, stage);
+  AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, h->ntiles_gen, h->tiles_gen, h->stream));
+  return AXJ_OK;
+}
+
+// ComputeTimeStep on the device; with advance != 0 the kernel also performs
+// time = time + delt for the step this dt is used by (ModRungeKutta.f90:152-155).
+int enqueue_dt(axj_handle* h, int advance) {
+  DtArgs d;
+  d.g = grid_of(h);
+  d.U = h->U0;
+  d.desc = h->desc;
+  d.dxidz = h->dxidz;
+  d.detadr = h->detadr;
+  d.staleT = h->staleT;
+  d.partial = h->partial;
+  d.counter = h->counter;
+  d.dt = h->dt;
+  d.flags = h->flags;
+  d.time = h->time;
+  d.advance = advance;
+  d.c = h->c;
+  AXJ_CUDA(h, launch_dt(d, h->dt_blocks, h->stream));
+  return AXJ_OK;
+}
+
+// RK4 (ModRungeKutta.f90:5-171) on the device dt: U0 -> Ua -> Ub -> Ua -> U0.
+int enqueue_rk4(axj_handle* h) {
+  int rc;
+  if ((rc = enqueue_stage(h, h->U0, h->Ua, 1)) != AXJ_OK) return rc;
+  if ((rc = enqueue_stage(h, h->Ua, h->Ub, 2)) != AXJ_OK) return rc;
+  if ((rc = enqueue_stage(h, h->Ub, h->Ua, 3)) != AXJ_OK) return rc;
+  if ((rc = enqueue_stage(h, h->Ua, h->U0, 4)) != AXJ_OK) return rc;
+  return AXJ_OK;
+}
+
+int check_flags(axj_handle* h) {
+  int f = 0;
+  AXJ_CUDA(h, cudaMemcpyAsync(&f, h->flags, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (f & 2) return fail(h, AXJ_ERR_DT_BLOWUP, "Time step blow up (every point blanked, dt == 100)");
+  if (f & 1) return fail(h, AXJ_ERR_NONFINITE, "non-finite value in the solution or time step");
+  return AXJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void axj_default_params(axj_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->gam = 1.4;
+  p->Re = 1000.0;
+  p->Pr = 0.72;
+  p->CFL = 0.5;
+  p->sponge_start_top = 12.5;
+  p->sponge_A_top = 0.5;
+  p->sponge_end_left = 6.0;
+  p->sponge_A_left = 5.0;
+  p->C_mu = 0.0;
+  p->C_beta = 0.0;
+  p->C_kappa = 0.0;
+  p->forcing_alpha = 6.0;
+  p->forcing_lz = 1.0;
+  p->forcing_lr = 1.0;
+  p->do_viscous_terms = 1;
+  p->shock_capturing = 0;
+  p->control_forcing = 0;
+  p->dt_mode = AXJ_DT_REFERENCE;
+  p->precision = AXJ_FP64;
+  p->sensor = AXJ_SENSOR_PLAIN;
+  p->judge_every = 50;
+  p->judge_threshold = 0.1;
+}
+
+const char* axj_version(void) { return "axj 0.1 sm_100a fp64"; }
+
+int axj_read_bc_file(const char* path, axj_bc_record* rec, int64_t max_records, int64_t* nrecords) {
+  if (!path || !nrecords) return fail(nullptr, AXJ_ERR_ARG, "null argument");
+  FILE* f = std::fopen(path, "r");
+  if (!f) return fail(nullptr, AXJ_ERR_ARG, "cannot open bc file %s", path);
+  int64_t n = 0;
+  char line[1024];
+  int rc = AXJ_OK;
+  while (std::fgets(line, sizeof(line), f)) {
+    long long v[9];
+    int k = std::sscanf(line, "%lld %lld %lld %lld %lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4],
+                        &v[5], &v[6], &v[7], &v[8]);
+    if (k <= 0) continue;  // blank line
+    if (k < 7) { rc = fail(nullptr, AXJ_ERR_BADPATCH, "bc file %s: short record %lld", path, (long long)n + 1); break; }
+    if (n < max_records && rec) {
+      rec[n].bc = v[1];
+      rec[n].bc_dir = v[2];
+      rec[n].istart = v[3];
+      rec[n].iend = v[4];
+      rec[n].jstart = v[5];
+      rec[n].jend = v[6];
+    }
+    ++n;
+  }
+  std::fclose(f);
+  *nrecords = n;
+  if (rc == AXJ_OK && rec && n > max_records)
+    return fail(nullptr, AXJ_ERR_ARG, "bc file has %lld records, buffer holds %lld", (long long)n,
+                (long long)max_records);
+  return rc;
+}
+
+int axj_patches_from_records(const axj_bc_record* rec, int64_t nrec, int64_t Nzg, int64_t Nrg, axj_patch* out,
+                             int64_t* npatch) {
+  if (!rec || !out || !npatch) return fail(nullptr, AXJ_ERR_ARG, "null argument");
+  int64_t n = 0;
+  for (int64_t k = 0; k < nrec; ++k) {
+    int64_t is = rec[k].istart, ie = rec[k].iend, js = rec[k].jstart, je = rec[k].jend, dir = rec[k].bc_dir;
+    if (is == -1) is = Nzg;
+    if (js == -1) js = Nrg;
+    if (ie == -1) ie = Nzg;
+    if (je == -1) je = Nrg;
+    int64_t pis, pie, pjs, pje;  // the 4-wide strip (ModPatch.f90:159-179)
+    if (dir == 1) { pis = is; pie = is + 3; pjs = js; pje = je; }
+    else if (dir == -1) { pis = ie - 3; pie = ie; pjs = js; pje = je; }
+    else if (dir == 2) { pis = is; pie = ie; pjs = js; pje = js + 3; }
+    else if (dir == -2) { pis = is; pie = ie; pjs = je - 3; pje = je; }
+    else return fail(nullptr, AXJ_ERR_BADPATCH, "record %lld: bc_dir %lld", (long long)k + 1, (long long)dir);
+    // the first/last block point inside the strip in the i-outer, j-inner scan
+    // (CreateAllPatches :154-197), for one block holding the whole grid
+    int64_t ci0 = std::max<int64_t>(pis, 1), ci1 = std::min<int64_t>(pie, Nzg);
+    int64_t cj0 = std::max<int64_t>(pjs, 1), cj1 = std::min<int64_t>(pje, Nrg);
+    if (pis > pie || pjs > pje || ci0 > ci1 || cj0 > cj1) continue;  // no point of this block: patch dropped
+    const int64_t sI = ci0, sJ = cj0, eI = ci1, eJ = cj1;
+    axj_patch p;
+    p.bc = rec[k].bc;
+    p.bc_dir = dir;
+    // PatchCreation (:264-309)
+    if (dir == 1) { p.i_start = sI; p.i_end = sI + 3; p.j_start = sJ; p.j_end = eJ; }
+    else if (dir == -1) { p.i_start = eI - 3; p.i_end = eI; p.j_start = sJ; p.j_end = eJ; }
+    else if (dir == 2) { p.i_start = sI; p.i_end = eI; p.j_start = sJ; p.j_end = sJ + 3; }
+    else { p.i_start = sI; p.i_end = eI; p.j_start = eJ - 3; p.j_end = eJ; }
+    out[n++] = p;
+  }
+  *npatch = n;
+  return AXJ_OK;
+}
+
+const char* axj_last_error(const axj_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+void axj_destroy(axj_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec, const double* rvec,
+               const double* ibval, const axj_patch* patches, int64_t npatch, axj_handle** out) {
+  if (!prm || !zvec || !rvec || !ibval || !out || (npatch > 0 && !patches))
+    return fail(nullptr, AXJ_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (Nz < 12 || Nr < 12 || Nz > (1 << 20) || Nr > (1 << 20))
+    return fail(nullptr, AXJ_ERR_BADGRID, "grid %lld x %lld outside 12..2^20", (long long)Nz, (long long)Nr);
+  if (npatch > MAX_PATCHES) return fail(nullptr, AXJ_ERR_BADPATCH, "more than %d patches", MAX_PATCHES);
+  if (prm->precision != AXJ_FP64) return fail(nullptr, AXJ_ERR_UNSUPPORTED, "precision %lld not built", (long long)prm->precision);
+  if (prm->shock_capturing && prm->sensor != AXJ_SENSOR_PLAIN)
+    return fail(nullptr, AXJ_ERR_UNSUPPORTED, "sensor %lld not built", (long long)prm->sensor);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, AXJ_ERR_NODEVICE, "no CUDA device available");
+  if (prm->device < 0 || prm->device >= ndev)
+    return fail(nullptr, AXJ_ERR_ARG, "device %lld not in 0..%d", (long long)prm->device, ndev - 1);
+  {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, (int)prm->device) != cudaSuccess || prop.major != 10)
+      return fail(nullptr, AXJ_ERR_NODEVICE, "device %lld is not an sm_100 (B200) GPU", (long long)prm->device);
+    if (cudaSetDevice((int)prm->device) != cudaSuccess)
+      return fail(nullptr, AXJ_ERR_NODEVICE, "cudaSetDevice(%lld) failed", (long long)prm->device);
+  }
+  // tensor-product grid: z depends on i only, r on j only (the reference only
+  // carries dxi/dz and deta/dr, ModDeriv.f90:57,108)
+  for (int64_t j = 0; j < Nr; ++j)
+    for (int64_t i = 0; i < Nz; ++i) {
+      if (zvec[i + j * Nz] != zvec[i]) return fail(nullptr, AXJ_ERR_BADGRID, "z varies with j at (%lld,%lld)", (long long)i + 1, (long long)j + 1);
+      if (rvec[i + j * Nz] != rvec[j * Nz]) return fail(nullptr, AXJ_ERR_BADGRID, "r varies with i at (%lld,%lld)", (long long)i + 1, (long long)j + 1);
+    }
+  for (int64_t k = 0; k < npatch; ++k) {
+    const axj_patch& p = patches[k];
+    if (p.bc_dir != 1 && p.bc_dir != -1 && p.bc_dir != 2 && p.bc_dir != -2)
+      return fail(nullptr, AXJ_ERR_BADPATCH, "patch %lld: bc_dir %lld", (long long)k + 1, (long long)p.bc_dir);
+    if (p.i_start > p.i_end || p.j_start > p.j_end)
+      return fail(nullptr, AXJ_ERR_BADPATCH, "patch %lld: empty range", (long long)k + 1);
+    if (p.bc < 90 || p.bc > 95) return fail(nullptr, AXJ_ERR_BADPATCH, "patch %lld: bc %lld", (long long)k + 1, (long long)p.bc);
+  }
+
+  axj_handle* h = new axj_handle();
+  cudaGetDevice(&h->device);
+  h->Nz = (int)Nz;
+  h->Nr = (int)Nr;
+  h->P = (Nz + 31) / 32 * 32;
+  h->plane = h->P * Nr;
+  h->params = *prm;
+  Consts& c = h->c;
+  c.gam = prm->gam; c.Re = prm->Re; c.Pr = prm->Pr; c.CFL = prm->CFL;
+  c.sponge_start_top = prm->sponge_start_top; c.sponge_A_top = prm->sponge_A_top;
+  c.sponge_end_left = prm->sponge_end_left; c.sponge_A_left = prm->sponge_A_left;
+  c.C_mu_Re = prm->C_mu * prm->Re;
+  c.C_beta_Re = prm->C_beta * prm->Re;
+  c.C_kappa_Re_Pr = prm->C_kappa * prm->Re * prm->Pr;
+  c.forcing_alpha = prm->forcing_alpha; c.forcing_z0 = prm->forcing_z0; c.forcing_r0 = prm->forcing_r0;
+  c.forcing_lz = prm->forcing_lz; c.forcing_lr = prm->forcing_lr;
+  c.r_top = rvec[(Nr - 1) * Nz];
+  c.do_viscous = prm->do_viscous_terms == 1;
+  c.shock_capturing = prm->shock_capturing == 1;
+  c.control_forcing = prm->control_forcing == 1;
+  c.dt_mode = (int)prm->dt_mode;
+  c.npatch = (int)npatch;
+
+  // ---- operator tables and 1-D metrics (ModSolver.f90:57-76)
+  double S1[9][6], S2[9][6], G[9][11];
+  build_tables(S1, S2, G);
+  std::vector<double> z(Nz), r(Nr);
+  for (int64_t i = 0; i < Nz; ++i) z[i] = zvec[i];
+  for (int64_t j = 0; j < Nr; ++j) r[j] = rvec[j * Nz];
+  std::vector<double> dzdxi, drdeta, dxidz(Nz), detadr(Nr), ddxidxidz, ddetadetadr;
+  metric_1d(S1, z, dzdxi);
+  metric_1d(S1, r, drdeta);
+  for (int64_t i = 0; i < Nz; ++i) dxidz[i] = 1.0 / dzdxi[i];
+  for (int64_t j = 0; j < Nr; ++j) detadr[j] = 1.0 / drdeta[j];
+  metric_1d(S1, dxidz, ddxidxidz);
+  metric_1d(S1, detadr, ddetadetadr);
+  // deltaz, deltar and the z ramp of the sensor (ModShockCapturing.f90:171-189, :85)
+  std::vector<double> dzv(Nz), drv(Nr), ramp(Nz);
+  for (int64_t i = 0; i < Nz; ++i) {
+    if (i >= 1 && i <= Nz - 2) dzv[i] = (z[i + 1] - z[i - 1]) / 2.0;
+    if (i == 0) dzv[i] = z[1] - z[0];
+    if (i == Nz - 1) dzv[i] = z[Nz - 1] - z[Nz - 2];
+    ramp[i] = (1.0 + std::tanh(5.0 * (z[i] - 10.0))) / 2.0;
+  }
+  for (int64_t j = 0; j < Nr; ++j) {
+    if (j >= 1 && j <= Nr - 2) drv[j] = (r[j + 1] - r[j - 1]) / 2.0;
+    if (j == 0) drv[j] = r[1] - r[0];
+    if (j == Nr - 1) drv[j] = r[Nr - 1] - r[Nr - 2];
+  }
+
+  // ---- stencil maps (CreateAllPatches, ModPatch.f90:214-242) -> per-point descriptors
+  const size_t npt = (size_t)Nz * Nr;
+  std::vector<int> which_i(npt, 0), which_j(npt, 0);  // 1-based patch number, 0 = none
+  for (int64_t k = 0; k < npatch; ++k) {
+    const axj_patch& p = patches[k];
+    for (int64_t i = std::max<int64_t>(p.i_start, 1); i <= std::min<int64_t>(p.i_end, Nz); ++i)
+      for (int64_t j = std::max<int64_t>(p.j_start, 1); j <= std::min<int64_t>(p.j_end, Nr); ++j) {
+        const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
+        if (p.bc_dir == 1 || p.bc_dir == -1) which_i[x] = (int)k + 1;
+        if (p.bc_dir == 2 || p.bc_dir == -2) which_j[x] = (int)k + 1;
+      }
+  }
+  // face-operation lists in patch order (BoundaryConditions loop, ModBC.f90:25-274)
+  std::vector<std::vector<int>> ops(npt);
+  int64_t iT = Nz, jT = Nr;  // stale T: last point of the RHS loops (ModRHS.f90:76,145)
+  for (int64_t k = 0; k < npatch; ++k) {
+    const axj_patch& p = patches[k];
+    if (p.bc == AXJ_BC_AXIS) continue;
+    int64_t is, ie, js, je;
+    if (p.bc_dir == 1) { is = ie = p.i_start; js = p.j_start; je = p.j_end; }
+    else if (p.bc_dir == -1) { is = ie = p.i_end; js = p.j_start; je = p.j_end; }
+    else if (p.bc_dir == 2) { is = p.i_start; ie = p.i_end; js = je = p.j_start; }
+    else { is = p.i_start; ie = p.i_end; js = je = p.j_end; }
+    for (int64_t i = is; i <= ie; ++i)
+      for (int64_t j = js; j <= je; ++j) {
+        if (i < 1 || i > Nz || j < 1 || j > Nr) continue;
+        const bool j1 = (j == 1);
+        const int adir = (int)(p.bc_dir < 0 ? -p.bc_dir : p.bc_dir);
+        bool active = false;
+        if (p.bc == AXJ_BC_SAT_FARFIELD) active = !j1 && adir == 1;
+        else if (p.bc == AXJ_BC_SAT_NOSLIP_WALL || p.bc == AXJ_BC_NSCBC_NOSLIP_WALL) active = true;
+        else if (p.bc == AXJ_BC_NSCBC_NONREFLECTING) active = !j1;
+        if (!active) continue;
+        const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
+        ops[x].push_back((int)k);
+        if ((int)ops[x].size() > MAX_FACE_OPS) {
+          delete h;
+          return fail(nullptr, AXJ_ERR_BADPATCH, "more than %d face operations at (%lld,%lld)", MAX_FACE_OPS,
+                      (long long)i, (long long)j);
+        }
+        iT = i;
+        jT = j;
+      }
+  }
+  h->iT = (int)(iT - 1);
+  h->jT = (int)(jT - 1);
+  std::vector<int> faces(1, 0);
+  std::vector<uint32_t> desc((size_t)h->P * Nr, make_desc(ROW_NONE, ROW_NONE, false, 0));
+  for (int64_t j = 1; j <= Nr; ++j)
+    for (int64_t i = 1; i <= Nz; ++i) {
+      const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
+      int zr = 4, rw = 4;
+      if (which_i[x]) {
+        const axj_patch& p = patches[which_i[x] - 1];
+        zr = p.bc_dir == 1 ? (int)(i - p.i_start) : (int)(8 + i - p.i_end);
+      }
+      if (which_j[x]) {
+        const axj_patch& p = patches[which_j[x] - 1];
+        rw = p.bc_dir == 2 ? (int)(j - p.j_start) : (int)(8 + j - p.j_end);
+      }
+      uint32_t f = 0;
+      if (!ops[x].empty()) {
+        f = (uint32_t)faces.size();
+        faces.push_back((int)ops[x].size());
+        for (int id : ops[x]) faces.push_back(id);
+      }
+      desc[(size_t)(j - 1) * h->P + (i - 1)] = make_desc(zr, rw, ibval[x] == 0.0, f);
+    }
+  if (faces.size() >= (1u << 20)) { delete h; return fail(nullptr, AXJ_ERR_BADPATCH, "too many face points"); }
+
+  // ---- tile classes
+  std::vector<int2> tint, tgen;
+  auto dsc = [&](int64_t i, int64_t j) { return desc[(size_t)j * h->P + i]; };
+  for (int64_t j0 = 0; j0 < Nr; j0 += TR)
+    for (int64_t i0 = 0; i0 < Nz; i0 += TZ) {
+      bool interior = i0 - H_INT >= 0 && i0 + TZ + H_INT <= Nz && j0 - H_INT >= 0 && j0 + TR + H_INT <= Nr;
+      for (int64_t j = j0; interior && j < j0 + TR; ++j)
+        for (int64_t i = i0; interior && i < i0 + TZ; ++i) {
+          uint32_t d = dsc(i, j);
+          if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d) || desc_face(d) != 0) interior = false;
+        }
+      for (int64_t j = j0 - H_INT; interior && j < j0 + TR + H_INT; ++j) {
+        if (j >= j0 && j < j0 + TR) continue;
+        for (int64_t i = i0; interior && i < i0 + TZ; ++i) {
+          uint32_t d = dsc(i, j);
+          if (desc_zrow(d) != 4 || desc_blank(d)) interior = false;
+        }
+      }
+      (interior ? tint : tgen).push_back(make_int2((int)i0, (int)j0));
+    }
+  h->ntiles_int = (int)tint.size();
+  h->ntiles_gen = (int)tgen.size();
+
+  // ---- device buffers
+  cudaError_t ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) { delete h; return fail(nullptr, AXJ_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(ce)); }
+  int rc = AXJ_OK;
+  const size_t pl = (size_t)h->plane;
+  h->U0 = dalloc<double>(h, 5 * pl, &rc);
+  h->Ua = dalloc<double>(h, 5 * pl, &rc);
+  h->Ub = dalloc<double>(h, 5 * pl, &rc);
+  h->A = dalloc<double>(h, 5 * pl, &rc);
+  h->B = dalloc<double>(h, 5 * pl, &rc);
+  h->target = dalloc<double>(h, 5 * pl, &rc);
+  h->star = dalloc<double>(h, 3 * pl, &rc);
+  if (c.shock_capturing) {
+    h->S = dalloc<double>(h, pl, &rc);
+    h->dil = dalloc<double>(h, pl, &rc);
+    h->fsw = dalloc<double>(h, pl, &rc);
+    h->d2 = dalloc<double>(h, 6 * pl, &rc);
+    h->Q = dalloc<double>(h, 3 * pl, &rc);
+    h->Qz = dalloc<double>(h, 3 * pl, &rc);
+  }
+  h->desc = dalloc<uint32_t>(h, pl, &rc);
+  h->faces = dalloc<int>(h, faces.size(), &rc);
+  h->dxidz = dalloc<double>(h, Nz, &rc);
+  h->ddxidxidz = dalloc<double>(h, Nz, &rc);
+  h->detadr = dalloc<double>(h, Nr, &rc);
+  h->ddetadetadr = dalloc<double>(h, Nr, &rc);
+  h->zc = dalloc<double>(h, Nz, &rc);
+  h->rc = dalloc<double>(h, Nr, &rc);
+  h->dzv = dalloc<double>(h, Nz, &rc);
+  h->drv = dalloc<double>(h, Nr, &rc);
+  h->ramp = dalloc<double>(h, Nz, &rc);
+  h->forcing = dalloc<double>(h, 25, &rc);
+  h->dt = dalloc<double>(h, 1, &rc);
+  h->staleT = dalloc<double>(h, 1, &rc);
+  h->time = dalloc<double>(h, 1, &rc);
+  h->flags = dalloc<int>(h, 1, &rc);
+  h->counter = dalloc<unsigned int>(h, 1, &rc);
+  h->dt_blocks = 148 * 4;
+  h->partial = dalloc<double>(h, h->dt_blocks, &rc);
+  h->tiles_int = dalloc<int2>(h, std::max<size_t>(tint.size(), 1), &rc);
+  h->tiles_gen = dalloc<int2>(h, std::max<size_t>(tgen.size(), 1), &rc);
+  if (rc != AXJ_OK) {
+    g_create_error = h->err;
+    axj_destroy(h);
+    return rc;
+  }
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    if (rc == AXJ_OK && bytes) {
+      cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+      if (e != cudaSuccess) rc = fail(h, AXJ_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+    }
+  };
+  up(h->desc, desc.data(), desc.size() * sizeof(uint32_t));
+  up(h->faces, faces.data(), faces.size() * sizeof(int));
+  up(h->dxidz, dxidz.data(), Nz * sizeof(double));
+  up(h->ddxidxidz, ddxidxidz.data(), Nz * sizeof(double));
+  up(h->detadr, detadr.data(), Nr * sizeof(double));
+  up(h->ddetadetadr, ddetadetadr.data(), Nr * sizeof(double));
+  up(h->zc, z.data(), Nz * sizeof(double));
+  up(h->rc, r.data(), Nr * sizeof(double));
+  up(h->dzv, dzv.data(), Nz * sizeof(double));
+  up(h->drv, drv.data(), Nr * sizeof(double));
+  up(h->ramp, ramp.data(), Nz * sizeof(double));
+  up(h->forcing, prm->forcing_mat, 25 * sizeof(double));
+  up(h->tiles_int, tint.data(), tint.size() * sizeof(int2));
+  up(h->tiles_gen, tgen.data(), tgen.size() * sizeof(int2));
+  std::vector<PatchDev> pd(npatch > 0 ? npatch : 1);
+  for (int64_t k = 0; k < npatch; ++k) { pd[k].bc = (int)patches[k].bc; pd[k].dir = (int)patches[k].bc_dir; }
+  upload_tables(S1, S2, G, pd.data(), (int)npatch, h->stream);
+  if (rc == AXJ_OK) {
+    cudaError_t e = init_kernel_attributes();
+    if (e != cudaSuccess) rc = fail(h, AXJ_ERR_NODEVICE, "kernel set-up failed (no sm_100a device?): %s", cudaGetErrorString(e));
+  }
+  if (rc == AXJ_OK) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = fail(h, AXJ_ERR_CUDA, "set-up: %s", cudaGetErrorString(e));
+  }
+  if (rc != AXJ_OK) {
+    g_create_error = h->err;
+    axj_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return AXJ_OK;
+}
+
+int axj_set_state(axj_handle* h, const double* pv, const double* pv_target, int64_t iteration, double time) {
+  if (!h || !pv || !pv_target) return fail(h, AXJ_ERR_ARG, "null argument");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, h2d(h, h->U0, pv, 5));
+  AXJ_CUDA(h, h2d(h, h->target, pv_target, 5));
+  AXJ_CUDA(h, cudaMemcpyAsync(h->time, &time, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->iteration = iteration;
+  h->time_host = time;
+  h->state_set = true;
+  return AXJ_OK;
+}
+
+int axj_get_state(axj_handle* h, double* pv) {
+  if (!h || !pv) return fail(h, AXJ_ERR_ARG, "null argument");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, d2h(h, pv, h->U0, 5));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return AXJ_OK;
+}
+
+int axj_get_time(axj_handle* h, int64_t* iteration, double* time) {
+  if (!h) return fail(h, AXJ_ERR_ARG, "null handle");
+  if (iteration) *iteration = h->iteration;
+  if (time) *time = h->time_host;
+  return AXJ_OK;
+}
+
+int axj_compute_dt(axj_handle* h, double* delt) {
+  if (!h) return fail(h, AXJ_ERR_ARG, "null handle");
+  if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  int rc = enqueue_dt(h, 0);
+  if (rc != AXJ_OK) return rc;
+  double d = 0.0;
+  AXJ_CUDA(h, cudaMemcpyAsync(&d, h->dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  rc = check_flags(h);
+  if (delt) *delt = d;
+  return rc;
+}
+
+int axj_rk4_step(axj_handle* h, double delt) {
+  if (!h) return fail(h, AXJ_ERR_ARG, "null handle");
+  if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, cudaMemcpyAsync(h->dt, &delt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  int rc = enqueue_rk4(h);
+  if (rc != AXJ_OK) return rc;
+  rc = check_flags(h);
+  h->time_host = h->time_host + delt;
+  h->iteration += 1;
+  AXJ_CUDA(h, cudaMemcpyAsync(h->time, &h->time_host, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return rc;
+}
+
+int axj_run(axj_handle* h, int64_t nsteps, int64_t out_every, axj_output_cb cb, void* user, double* last_dt) {
+  if (!h) return fail(h, AXJ_ERR_ARG, "null handle");
+  if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called");
+  if (nsteps < 0) return fail(h, AXJ_ERR_ARG, "nsteps < 0");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  if (!h->graph_exec) {
+    AXJ_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_dt(h, 1);
+    if (rc == AXJ_OK) rc = enqueue_rk4(h);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc != AXJ_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(h, AXJ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    h->graph = g;
+    AXJ_CUDA(h, cudaGraphInstantiate(&h->graph_exec, g, 0));
+  }
+  for (int64_t s = 0; s < nsteps; ++s) {
+    AXJ_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+    h->iteration += 1;
+    if (out_every > 0 && cb && (h->iteration % out_every == 0)) {
+      int rc = check_flags(h);
+      if (rc != AXJ_OK) return rc;
+      h->host_out.resize((size_t)h->Nz * h->Nr * 5);
+      AXJ_CUDA(h, d2h(h, h->host_out.data(), h->U0, 5));
+      AXJ_CUDA(h, cudaMemcpyAsync(&h->time_host, h->time, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+      cb(user, h->iteration, h->time_host, h->host_out.data());
+    }
+  }
+  double dlast = 0.0;
+  AXJ_CUDA(h, cudaMemcpyAsync(&dlast, h->dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaMemcpyAsync(&h->time_host, h->time, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  int rc = check_flags(h);
+  if (last_dt) *last_dt = dlast;
+  return rc;
+}
+
+int axj_run_timed(axj_handle* h, int64_t nsteps, double* ms) {
+  if (!h || !ms) return fail(h, AXJ_ERR_ARG, "null argument");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  int rc = axj_run(h, 0, 0, nullptr, nullptr, nullptr);  // builds the graph
+  if (rc != AXJ_OK) return rc;
+  cudaEvent_t e0, e1;
+  AXJ_CUDA(h, cudaEventCreate(&e0));
+  AXJ_CUDA(h, cudaEventCreate(&e1));
+  AXJ_CUDA(h, cudaEventRecord(e0, h->stream));
+  for (int64_t s = 0; s < nsteps; ++s) AXJ_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+  AXJ_CUDA(h, cudaEventRecord(e1, h->stream));
+  AXJ_CUDA(h, cudaEventSynchronize(e1));
+  float t = 0.f;
+  AXJ_CUDA(h, cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t;
+  h->iteration += nsteps;
+  AXJ_CUDA(h, cudaMemcpyAsync(&h->time_host, h->time, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return check_flags(h);
+}
+
+int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launches) {
+  if (!h || !ms) return fail(h, AXJ_ERR_ARG, "null argument");
+  if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  cudaEvent_t ev[2];
+  AXJ_CUDA(h, cudaEventCreate(&ev[0]));
+  AXJ_CUDA(h, cudaEventCreate(&ev[1]));
+  double acc[4] = {0, 0, 0, 0};
+  int64_t nl[3] = {0, 0, 0};
+  auto timed = [&](int slot, auto&& body) -> int {
+    AXJ_CUDA(h, cudaEventRecord(ev[0], h->stream));
+    int rc = body();
+    if (rc != AXJ_OK) return rc;
+    AXJ_CUDA(h, cudaEventRecord(ev[1], h->stream));
+    AXJ_CUDA(h, cudaEventSynchronize(ev[1]));
+    float t = 0.f;
+    AXJ_CUDA(h, cudaEventElapsedTime(&t, ev[0], ev[1]));
+    acc[slot] += t;
+    return AXJ_OK;
+  };
+  const int stage_launches = (h->ntiles_gen > 0) + (h->ntiles_int > 0);
+  double* bufs[5] = {h->U0, h->Ua, h->Ub, h->Ua, h->U0};
+  int rc = AXJ_OK;
+  for (int64_t s = 0; s < nsteps && rc == AXJ_OK; ++s) {
+    rc = timed(0, [&] { return enqueue_dt(h, 1); });
+    nl[0] += 1;
+    for (int st = 1; st <= 4 && rc == AXJ_OK; ++st) {
+      if (h->c.shock_capturing) {
+        rc = timed(1, [&]() -> int {
+          SensorArgs sa = sensor_args(h, bufs[st - 1]);
+          AXJ_CUDA(h, launch_sensor(sa, h->stream));
+          return AXJ_OK;
+        });
+        nl[1] += 5;
+      }
+      if (rc != AXJ_OK) break;
+      rc = timed(2, [&]() -> int {
+        StageArgs a = stage_args(h, bufs[st - 1], bufs[st], st);
+        AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, h->ntiles_gen, h->tiles_gen, h->stream));
+        return AXJ_OK;
+      });
+      nl[2] += stage_launches;
+    }
+    h->iteration += 1;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (rc != AXJ_OK) return rc;
+  acc[3] = acc[0] + acc[1] + acc[2];
+  for (int k = 0; k < 4; ++k) ms[k] = acc[k];
+  if (launches)
+    for (int k = 0; k < 3; ++k) launches[k] = nl[k];
+  AXJ_CUDA(h, cudaMemcpyAsync(&h->time_host, h->time, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return check_flags(h);
+}
+
+int axj_rhs(axj_handle* h, const double* pv, double* rhs) {
+  if (!h || !pv || !rhs) return fail(h, AXJ_ERR_ARG, "null argument");
+  if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called (the target is needed)");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
+  int rc = enqueue_stage(h, h->Ua, h->Ub, 0);
+  if (rc != AXJ_OK) return rc;
+  AXJ_CUDA(h, d2h(h, rhs, h->Ub, 5));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return AXJ_OK;
+}
+
+int axj_deriv1(axj_handle* h, const double* var, int64_t dirn, double* out) {
+  if (!h || !var || !out || (dirn != 1 && dirn != 2)) return fail(h, AXJ_ERR_ARG, "bad argument");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, h2d(h, h->Ua, var, 1));
+  AXJ_CUDA(h, launch_deriv(grid_of(h), h->desc, h->Ua, nullptr, dirn == 1 ? h->dxidz : h->detadr, nullptr, (int)dirn,
+                           1, h->Ub, h->stream));
+  AXJ_CUDA(h, d2h(h, out, h->Ub, 1));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return AXJ_OK;
+}
+
+int axj_deriv2(axj_handle* h, const double* var, int64_t dirn, const double* first, double* out) {
+  if (!h || !var || !out || !first || (dirn != 1 && dirn != 2)) return fail(h, AXJ_ERR_ARG, "bad argument");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, h2d(h, h->Ua, var, 1));
+  AXJ_CUDA(h, h2d(h, h->Ua + h->plane, first, 1));
+  AXJ_CUDA(h, launch_deriv(grid_of(h), h->desc, h->Ua, h->Ua + h->plane, dirn == 1 ? h->dxidz : h->detadr,
+                           dirn == 1 ? h->ddxidxidz : h->ddetadetadr, (int)dirn, 2, h->Ub, h->stream));
+  AXJ_CUDA(h, d2h(h, out, h->Ub, 1));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return AXJ_OK;
+}
+
+int axj_tgfilter(axj_handle* h, const double* var, int64_t dirn, int64_t inplace, double* out) {
+  if (!h || !out || (dirn != 1 && dirn != 2) || (!inplace && !var)) return fail(h, AXJ_ERR_ARG, "bad argument");
+  if (inplace && dirn != 1) return fail(h, AXJ_ERR_UNSUPPORTED, "in-place filtering is only defined along z");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, h2d(h, h->Ub, out, 1));
+  if (inplace) {
+    AXJ_CUDA(h, launch_tgfilter_z_inplace(grid_of(h), h->desc, h->Ub, h->Ua, 1, h->stream));
+    AXJ_CUDA(h, d2h(h, out, h->Ua, 1));
+  } else {
+    AXJ_CUDA(h, h2d(h, h->Ua, var, 1));
+    AXJ_CUDA(h, launch_tgfilter(grid_of(h), h->desc, h->Ua, (int)dirn, h->Ub, h->stream));
+    AXJ_CUDA(h, d2h(h, out, h->Ub, 1));
+  }
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return AXJ_OK;
+}
+
+int axj_sensor(axj_handle* h, const double* pv, double* mustar, double* betastar, double* kappastar) {
+  if (!h || !pv || !mustar || !betastar || !kappastar) return fail(h, AXJ_ERR_ARG, "null argument");
+  if (!h->c.shock_capturing) return fail(h, AXJ_ERR_ARG, "handle created with shock_capturing = 0");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
+  SensorArgs s = sensor_args(h, h->Ua);
+  AXJ_CUDA(h, launch_sensor(s, h->stream));
+  AXJ_CUDA(h, d2h(h, mustar, h->star, 1));
+  AXJ_CUDA(h, d2h(h, betastar, h->star + h->plane, 1));
+  AXJ_CUDA(h, d2h(h, kappastar, h->star + 2 * h->plane, 1));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return AXJ_OK;
+}
+
+}  // extern "C"

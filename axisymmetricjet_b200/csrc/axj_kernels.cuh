@@ -1,0 +1,105 @@
+// axj_kernels.cuh -- kernel argument blocks and launch entry points shared by the
+// C-ABI layer (axj_api.cu) and the kernels (axj_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "axj_common.cuh"
+
+namespace axj {
+
+// Device view of one solver instance.
+struct Grid {
+  int Nz, Nr;
+  long long P;       // row pitch (doubles) of every device field
+  long long plane;   // P * Nr
+};
+
+// Arguments of the fused RK-stage kernel.
+struct StageArgs {
+  Grid g;
+  const double* Uin;     // stage input state (5 planes)
+  const double* U0;      // pv_old (5 planes)
+  double* A;             // running sum  pv_old + k1/6 (+ (k2+k3)/3)
+  double* B;             // k2
+  double* Uout;          // stage output (5 planes); rhs (5 planes) in stage 0
+  const double* target;  // pv_target (5 planes)
+  const double* mustar;  // shock-capturing coefficients (planes), or null
+  const double* betastar;
+  const double* kappastar;
+  const uint32_t* desc;  // per-point stencil descriptors (pitch P)
+  const int* faces;      // face-operation lists: faces[f] = n, faces[f+1..f+n] = patch ids
+  const int2* tiles;     // tile origins (i0, j0)
+  const double* dxidz;   // 1-D metrics and coordinates
+  const double* ddxidxidz;
+  const double* detadr;
+  const double* ddetadetadr;
+  const double* zc;
+  const double* rc;
+  const double* forcing;  // 25 doubles, row-major F(eqn,k)
+  const double* dt;       // device dt (read by stages 1-4)
+  double* staleT;         // stage 4: T(i*, j*) of its input, the next ComputeTimeStep's stale T
+  int* flags;             // bit 0: non-finite value produced
+  int stage;              // 0: write rhs only; 1..4: RK4 stage
+  int iT, jT;             // stale-T point (0-based)
+  Consts c;
+};
+
+struct DtArgs {
+  Grid g;
+  const double* U;
+  const uint32_t* desc;
+  const double* dxidz;
+  const double* detadr;
+  const double* staleT;
+  double* partial;       // one per block
+  unsigned int* counter; // last-block-done counter, left at 0
+  double* dt;            // result
+  int* flags;            // bit 1: dt blow-up (every point blanked), bit 0: non-finite dt
+  double* time;          // solution time, advanced by dt when advance != 0
+  int advance;
+  Consts c;
+};
+
+// Shock-capturing sensor chain (ModShockCapturing.f90:5-106).
+struct SensorArgs {
+  Grid g;
+  const double* U;       // stage input state
+  const uint32_t* desc;
+  const double* dxidz;
+  const double* detadr;
+  const double* zc;
+  const double* rc;
+  const double* dz;      // deltaz(i) (:171-179)
+  const double* dr;      // deltar(j) (:181-189)
+  const double* ramp;    // (1+tanh(5(z-10)))/2 (:85)
+  double* S;             // MgnStrRate
+  double* dil;           // dilvec
+  double* fsw;           // Ducros-type switch f_sw (:202)
+  double* d2;            // 6 planes: S_xi2, T_xi2, dil_xi2, S_eta2, T_eta2, dil_eta2
+  double* Q;             // 3 planes: mustarQuantity, betastarQuantity, kappastarQuantity
+  double* Qz;            // 3 planes: Q after the in-place z filter
+  double* star;          // 3 planes: mustar, betastar, kappastar
+  Consts c;
+};
+
+cudaError_t init_kernel_attributes();
+void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const double tg[9][11],
+                   const PatchDev* patches, int npatch, cudaStream_t s);
+
+cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, int ntiles_gen,
+                         const int2* tiles_gen, cudaStream_t s);
+cudaError_t launch_dt(const DtArgs& a, int nblocks, cudaStream_t s);
+cudaError_t launch_sensor(const SensorArgs& a, cudaStream_t s);
+
+// Unit entry points (one operator on one field, host-facing).
+cudaError_t launch_deriv(const Grid& g, const uint32_t* desc, const double* var, const double* first,
+                         const double* met, const double* met2, int dirn, int order, double* out, cudaStream_t s);
+cudaError_t launch_tgfilter(const Grid& g, const uint32_t* desc, const double* var, int dirn, double* out,
+                            cudaStream_t s);
+cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const double* q, double* out,
+                                      int nfield, cudaStream_t s);
+
+constexpr int DT_THREADS = 256;
+
+}  // namespace axj

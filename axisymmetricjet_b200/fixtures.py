@@ -1,0 +1,117 @@
+"""Synthetic jet cases: grid, iblank, initial condition, target and bc records.
+
+The reference ships no grid, restart or target file (only bc_4400x640_nozzle.dat),
+so cases are generated from their published shapes:
+
+* jet512x128  -- plain method, small: Nz=512 x Nr=128, z uniform on [0, 30D],
+  r_j = 10D sinh(3 j/(Nr-1))/sinh(3), gamma=1.4, Pr=0.72, Re=1000, M_j=0.9,
+  shock capturing off, 100 RK4 steps.
+* jet4400x640 -- production size: Nz=4400 x Nr=640, z on [0, 60D], r to 15D,
+  M_j=1.5, Re=5000, shock capturing on, 1000 RK4 steps.
+* small test cases of the same construction, and a nozzle case with a blanked
+  lip and no-slip wall patches laid out like the reference's own nozzle bc file
+  (bc_4400x640_nozzle.dat, WriteMeshAndSoln/write_soln_file.f90:223-257).
+
+Initial condition: V_z = U_j/2 (1 + tanh((0.5D - r)/(2*0.05D))), V_r = V_theta = 0,
+T from Crocco-Busemann (write_soln_file.f90:68-72), rho = 1/T (p = rho T = 1), plus a
+seeded Gaussian perturbation of amplitude 1e-3 U_j on V_r and V_z where |r-0.5D| < 0.2D.
+The target (pv_target) is the unperturbed profile.
+"""
+import numpy as np
+
+from ._ffi import AXIS, NSCBC_NONREFLECTING, NSCBC_NOSLIP_WALL, SAT_FARFIELD, SAT_NOSLIP_WALL, default_params
+
+# Artificial-diffusivity coefficients used when shock capturing is on. The reference
+# ships C_mu = C_beta = C_kappa = 0 (ModuleVariables.f90:164); these are the
+# Kawai-Lele-type values.
+SC_COEFFS = dict(C_mu=0.002, C_beta=1.75, C_kappa=0.01)
+
+JET_RECORDS = [
+    (SAT_FARFIELD, 1, 1, 1, 1, -1),           # inflow z = 0
+    (NSCBC_NONREFLECTING, -1, -1, -1, 1, -1),  # outflow z = z_max
+    (NSCBC_NONREFLECTING, -2, 1, -1, -1, -1),  # top r = r_max
+    (AXIS, 2, 1, -1, 1, 1),                    # axis r = 0
+]
+
+
+def grid(Nz, Nr, zmax, rmax):
+    z = zmax * np.arange(Nz, dtype=np.float64) / (Nz - 1)
+    r = rmax * np.sinh(3.0 * np.arange(Nr, dtype=np.float64) / (Nr - 1)) / np.sinh(3.0)
+    zvec = np.ascontiguousarray(np.broadcast_to(z[None, :], (Nr, Nz)))
+    rvec = np.ascontiguousarray(np.broadcast_to(r[:, None], (Nr, Nz)))
+    return z, r, zvec, rvec
+
+
+def jet_profile(r, Mj, Tj_Tinf=1.0, gam=1.4):
+    """(rho, V_z, T) of the tanh jet with Crocco-Busemann temperature."""
+    Uj = Mj * np.sqrt(Tj_Tinf)
+    ut = 0.5 * (1.0 + np.tanh((0.5 - r) / (2.0 * 0.05)))
+    T_Tj = 0.5 * (gam - 1.0) * ut * (1.0 - ut) * Mj ** 2 + ut + (1.0 - ut) / Tj_Tinf
+    T = Tj_Tinf * T_Tj
+    return 1.0 / T, Uj * ut, T, Uj
+
+
+def initial_condition(r, Nz, Mj, seed=12345, amp=1e-3, Tj_Tinf=1.0, gam=1.4):
+    Nr = r.shape[0]
+    rho, Vz, T, Uj = jet_profile(r, Mj, Tj_Tinf, gam)
+    tgt = np.zeros((5, Nr, Nz))
+    tgt[0] = rho[:, None]
+    tgt[3] = Vz[:, None]
+    tgt[4] = T[:, None]
+    pv = tgt.copy()
+    rng = np.random.default_rng(seed)
+    mask = (np.abs(r - 0.5) < 0.2)[:, None]
+    pv[1] += amp * Uj * rng.standard_normal((Nr, Nz)) * mask
+    pv[3] += amp * Uj * rng.standard_normal((Nr, Nz)) * mask
+    return np.ascontiguousarray(pv), np.ascontiguousarray(tgt)
+
+
+def make_case(Nz, Nr, zmax, rmax, Mj, Re, sc=False, seed=12345, records=None, ibval=None, **pkw):
+    z, r, zvec, rvec = grid(Nz, Nr, zmax, rmax)
+    kw = dict(Re=float(Re))
+    if sc:
+        kw.update(shock_capturing=1, **SC_COEFFS)
+    kw.update(pkw)
+    params = default_params(**kw)
+    pv, tgt = initial_condition(r, Nz, Mj, seed=seed)
+    if ibval is None:
+        ibval = np.ones((Nr, Nz))
+    return dict(Nz=Nz, Nr=Nr, z=z, r=r, zvec=zvec, rvec=rvec, ibval=np.ascontiguousarray(ibval),
+                records=list(records or JET_RECORDS), params=params, pv=pv, target=tgt, Mj=Mj)
+
+
+def nozzle_records(iw, jb, jt, wall=NSCBC_NOSLIP_WALL):
+    """A nozzle lip from z = 0 to i = iw between rows jb and jt (1-based), with the
+    record order of the reference's nozzle bc file."""
+    return [
+        (SAT_FARFIELD, 1, 1, 1, 1, jb),
+        (wall, -2, 1, iw, jb, jb),
+        (wall, 1, iw, iw, jb, jt),
+        (wall, 2, 1, iw, jt, jt),
+        (SAT_FARFIELD, 1, 1, 1, jt, -1),
+        (NSCBC_NONREFLECTING, -2, 1, -1, -1, -1),
+        (NSCBC_NONREFLECTING, -1, -1, -1, 1, -1),
+        (AXIS, 2, 1, -1, 1, 1),
+    ]
+
+
+def nozzle_case(Nz=96, Nr=64, zmax=30.0, rmax=15.0, Mj=0.9, Re=1000.0, iw=20, jb=24, jt=28, wall=NSCBC_NOSLIP_WALL,
+                sc=False, seed=12345, **pkw):
+    ib = np.ones((Nr, Nz))
+    ib[jb:jt - 1, :iw - 1] = 0.0  # rows jb+1..jt-1, columns 1..iw-1 (1-based) are inside the lip
+    return make_case(Nz, Nr, zmax, rmax, Mj, Re, sc=sc, seed=seed, records=nozzle_records(iw, jb, jt, wall),
+                     ibval=ib, **pkw)
+
+
+CASES = {
+    "jet512x128": dict(Nz=512, Nr=128, zmax=30.0, rmax=10.0, Mj=0.9, Re=1000.0, sc=False),
+    "jet4400x640": dict(Nz=4400, Nr=640, zmax=60.0, rmax=15.0, Mj=1.5, Re=5000.0, sc=True),
+    "jet96x64": dict(Nz=96, Nr=64, zmax=30.0, rmax=15.0, Mj=0.9, Re=1000.0, sc=False),
+    "jet96x64sc": dict(Nz=96, Nr=64, zmax=30.0, rmax=15.0, Mj=1.5, Re=5000.0, sc=True),
+}
+
+
+def case(name, **kw):
+    spec = dict(CASES[name])
+    spec.update(kw)
+    return make_case(**spec)

@@ -1,0 +1,308 @@
+"""Throughput of the per-step hot path: RK4 grid-point updates per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--case NAME]
+
+Workload (default): jet4400x640 -- Nz=4400 x Nr=640 axisymmetric jet, M_j=1.5, Re=5000,
+artificial-diffusivity shock capturing on, SAT/NSCBC faces, sponges, FP64 end to end,
+synthetic seeded initial condition. One step = ComputeTimeStep + one RK4 step
+(4 right-hand-side evaluations, each with the sensor chain).
+
+Multi-GPU: one process per GPU (torchrun); every rank advances its own jet (replicas,
+no data-path collective); the timed region is bracketed by barriers and the device
+time is the max over ranks; value = total updates of all ranks / that time.
+
+--impl reference times the CPU implementation of the same step on the host cores:
+the reference Fortran cannot be built in this image (no Fortran compiler), so it is
+the oracle's line-faithful C restatement (OpenMP over columns, all host threads).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK4 grid-pt updates/s"
+UNIT = "grid-pt updates/s"
+# Algorithmic bytes of the FP64 path: 680 B per grid point per RK4 step (5 fields x 8 B x
+# 17 state accesses), i.e. 170 B per point per RK stage launch.
+ALG_BYTES_PER_POINT_STEP = 680.0
+ALG_BYTES_PER_POINT_STAGE = ALG_BYTES_PER_POINT_STEP / 4.0
+NOUTPUT = 200  # WriteOutput period of the reference (ModuleVariables.f90:69)
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(case):
+    """dram bytes per stage-kernel launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"stage_kernel_{case}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_stage_launch"):
+                return float(line.split("=")[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_step_sample(case, threads, steps=1):
+    """Oracle (CPU restatement) on the full workload grid: seconds per RK4 step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle
+    from axisymmetricjet_b200 import fixtures
+    c = fixtures.case(case)
+    ora = oracle.Oracle(c["params"], c["zvec"], c["rvec"], c["ibval"],
+                        oracle.patches_from_records(c["records"], c["Nz"], c["Nr"]))
+    ora.set_state(c["pv"], c["target"])
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        d = ora.compute_time_step()
+        ora.rk4(d)
+    return (time.perf_counter() - t0) / steps, c["Nz"] * c["Nr"]
+
+
+def run_reference(args):
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from axisymmetricjet_b200 import fixtures
+    c = fixtures.case(args.case)
+    ora = oracle.Oracle(c["params"], c["zvec"], c["rvec"], c["ibval"],
+                        oracle.patches_from_records(c["records"], c["Nz"], c["Nr"]))
+    ora.set_state(c["pv"], c["target"])
+    for _ in range(args.warmup):
+        ora.rk4(ora.compute_time_step())
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ora.rk4(ora.compute_time_step())
+    sec = time.perf_counter() - t0
+    npts = c["Nz"] * c["Nr"]
+    value = npts * args.steps / sec
+    sample = f"{args.steps} full RK4 steps (ComputeTimeStep + RK4) of {args.case} after {args.warmup} warm-up steps"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args.case, c),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample + "; CPU restatement of the reference (oracle/axj_oracle.c, -O2 "
+                                            "-ffp-contract=off, OpenMP), not the Fortran binary: no Fortran "
+                                            "compiler in this image"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(name, c):
+    p = c["params"]
+    return {"workload": f"{name}: axisymmetric jet Nz={c['Nz']} x Nr={c['Nr']}, M_j={c['Mj']}, Re={p.Re:g}, "
+                        f"shock capturing {'on' if p.shock_capturing else 'off'}, SAT/NSCBC + sponges, FP64",
+            "Nz": c["Nz"], "Nr": c["Nr"], "shock_capturing": bool(p.shock_capturing),
+            "l2": "inputs larger than L2 (about 1.6 GB of state, RK and sensor buffers touched per step)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", default="jet4400x640")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import axisymmetricjet_b200 as axj
+    from axisymmetricjet_b200 import fixtures
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    c = fixtures.case(args.case, seed=12345 + rank)
+    c["params"].device = local
+    patches = axj.patches_from_records(c["records"], c["Nz"], c["Nr"])
+    npts = c["Nz"] * c["Nr"]
+    solver = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+    solver.set_state(c["pv"], c["target"])
+
+    # warm-up (also builds the CUDA graph)
+    solver.run(args.warmup)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    ms = solver.run_timed(args.steps)
+    barrier()
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms)
+    value = world * npts * args.steps / (ms_max / 1e3)
+
+    # per-kernel breakdown (same kernels launched one group at a time with CUDA events)
+    prof_steps = max(2, min(args.steps, 10))
+    pms, plaunch = solver.profile_steps(prof_steps)
+    stage_launch_ms = pms["stage"] / (4 * prof_steps)
+    peak, peak_kind = measured_peaks()
+    alg_bytes = ALG_BYTES_PER_POINT_STAGE * npts
+    achieved = alg_bytes / (stage_launch_ms / 1e3) / 1e9
+    traffic = profile_traffic(args.case)
+    launches_per_step = 1 + 4 * ((5 if c["params"].shock_capturing else 0) + (plaunch["stage"] // (4 * prof_steps)))
+
+    # end to end through the public API with host buffers: IC and target upload, every
+    # step ComputeTimeStep (dt to the host) + RK4(delt), the state downloaded every
+    # NOUTPUT steps and at the end (ModRungeKutta.f90:161-165)
+    e2e_solver = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+    pv_h = torch.from_numpy(c["pv"]).pin_memory().numpy()
+    tg_h = torch.from_numpy(c["target"]).pin_memory().numpy()
+    out_h = torch.empty(c["pv"].shape, dtype=torch.float64).pin_memory().numpy()
+    e2e_solver.set_state(pv_h, tg_h)
+    for _ in range(args.warmup):
+        e2e_solver.rk4(e2e_solver.compute_time_step())
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    e2e_solver.set_state(pv_h, tg_h)
+    nout = 0
+    for s in range(1, args.steps + 1):
+        e2e_solver.rk4(e2e_solver.compute_time_step())
+        if s % NOUTPUT == 0:
+            e2e_solver.get_state(out_h)
+            nout += 1
+    e2e_solver.get_state(out_h)
+    nout += 1
+    ev1.record()
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    state_bytes = 5 * npts * 8
+    e2e = {"value": world * npts * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": (2 * state_bytes + 8 * args.steps) / args.steps,
+           "d2h_bytes_per_step": (nout * state_bytes + 12 * args.steps) / args.steps}
+    e2e_solver.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sec, n = cpu_step_sample(args.case, threads, steps=1)
+        cpu = {"value": n / sec, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"1 full RK4 step (ComputeTimeStep + RK4) of {args.case} by the oracle's C restatement "
+                         f"of the reference (OpenMP, {threads} threads): {sec:.2f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload_config(args.case, c), parallelism=f"replicas x{world}"),
+            "roofline": {"bound": "hbm", "kernel": "stage_kernel (fused RK stage, both tile classes)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes, "launch_ms": stage_launch_ms},
+            "breakdown_ms_per_step": {k: v / prof_steps for k, v in pms.items()},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,215 @@
+/*
+ * axj.h -- C-ABI of the B200 per-step hot path of the axisymmetric compressible
+ * jet solver (nataraj2/AxisymmetricJet).
+ *
+ * The reference drives the hot path through argument-less Fortran module
+ * subroutines that work on module globals:
+ *     DO iteration = ...; CALL ComputeTimeStep; CALL RK4; ENDDO   (ModSolver.f90:122-125)
+ * This header replaces those calls with a handle-based C interface that a
+ * Fortran host binds through ISO_C_BINDING (BIND(C, name="axj_...")).
+ *
+ * Conventions
+ *  - Every host array is Fortran column-major with z (index i) fastest:
+ *    a field is Nz*Nr doubles, element (i,j) at offset (i-1) + (j-1)*Nz.
+ *    A solution array pv(Nz,Nr,1,5) is 5 such fields back to back
+ *    (rho, V_r, V_theta, V_z, T), exactly the reference's pv layout
+ *    (ModuleVariables.f90:39, ModAllocate.f90).
+ *  - Patch indices are 1-based, as produced by PatchCreation (ModPatch.f90:264-309).
+ *  - The library copies host arrays in and out and never keeps a host pointer
+ *    after a call returns. It owns all device memory of a handle.
+ *  - Every function returns an axj_status; 0 is success. The library never
+ *    exits, aborts or prints; the host decides what to do (e.g. StopTheCode).
+ *  - One host thread per handle; calls on one handle are not thread-safe.
+ */
+#ifndef AXJ_H
+#define AXJ_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+enum axj_status {
+  AXJ_OK = 0,
+  AXJ_ERR_ARG = 1,          /* bad argument (null pointer, size, enum value) */
+  AXJ_ERR_CUDA = 2,         /* a CUDA runtime call failed; see axj_last_error */
+  AXJ_ERR_NONFINITE = 3,    /* NaN/Inf found in the state after a step */
+  AXJ_ERR_DT_BLOWUP = 4,    /* every point blanked: dt == 100 (ModInputOutput.f90:424-429) */
+  AXJ_ERR_TIMEOUT = 5,      /* a bounded device wait gave up */
+  AXJ_ERR_BADPATCH = 6,     /* inconsistent patch / bc record */
+  AXJ_ERR_BADGRID = 7,      /* grid not supported (too small, not a tensor-product z(i), r(j) grid) */
+  AXJ_ERR_NOMEM = 8,        /* device allocation failed */
+  AXJ_ERR_NODEVICE = 9,     /* no CUDA device / library built without sm_100a code */
+  AXJ_ERR_UNSUPPORTED = 10  /* option combination not implemented */
+};
+
+/* Boundary-condition codes (ModuleVariables.f90:112-117). */
+enum axj_bc {
+  AXJ_BC_AXIS = 90,
+  AXJ_BC_SAT_FARFIELD = 91,
+  AXJ_BC_NSCBC_NONREFLECTING = 92,
+  AXJ_BC_SAT_NOSLIP_WALL = 93,
+  AXJ_BC_NSCBC_NOSLIP_WALL = 94,
+  AXJ_BC_SPONGE = 95
+};
+
+/* One boundary patch after PatchCreation: the 4-wide strip the SBP closure rows
+ * live in. Field order follows TYPE patch_type (ModuleVariables.f90:102-106). */
+typedef struct axj_patch {
+  int64_t i_start, i_end, j_start, j_end;
+  int64_t bc;      /* enum axj_bc */
+  int64_t bc_dir;  /* +1/-1: z-face at i_start/i_end; +2/-2: r-face at j_start/j_end */
+} axj_patch;
+
+/* One raw row of the bc file as read by CreateAllPatches (ModPatch.f90:132):
+ * "grid bc dir istart iend jstart jend k k"; -1 means the last index. */
+typedef struct axj_bc_record {
+  int64_t bc, bc_dir, istart, iend, jstart, jend;
+} axj_bc_record;
+
+/* dt_mode values. */
+enum axj_dt_mode {
+  AXJ_DT_REFERENCE = 0, /* sqrt of the stale module scalar T, as ModInputOutput.f90:405 does */
+  AXJ_DT_PHYSICAL = 1   /* sqrt of the local temperature T(i,j) */
+};
+
+/* precision values. */
+enum axj_precision {
+  AXJ_FP64 = 0,  /* plain FP64 end to end */
+  AXJ_MIXED = 1  /* FP32 stage states/stencils, FP64 accumulation, penalties, near-axis terms, dt */
+};
+
+/* sensor values (artificial-diffusivity sensor, used when shock_capturing = 1). */
+enum axj_sensor_kind {
+  AXJ_SENSOR_PLAIN = 0,   /* ModShockCapturing.f90:5-106 */
+  AXJ_SENSOR_LEARNED = 1  /* MLP stand-in, plain sensor as periodic judge */
+};
+
+/* Run parameters: the reference's compile-time module variables
+ * (ModuleVariables.f90:4-188) as a POD struct. Fill with axj_default_params. */
+typedef struct axj_params {
+  double gam;                 /* 1.4          ModuleVariables.f90:66 */
+  double Re;                  /* 1000         :73 */
+  double Pr;                  /* 0.72         :73 */
+  double CFL;                 /* 0.5          :177 */
+  double sponge_start_top;    /* 12.5         :12 */
+  double sponge_A_top;        /* 0.5          :12 */
+  double sponge_end_left;     /* 6.0          :13 */
+  double sponge_A_left;       /* 5.0          :13 */
+  double C_mu, C_beta, C_kappa; /* 0,0,0      :164 */
+  double forcing_alpha;       /* 6.0          :184 */
+  double forcing_z0, forcing_r0, forcing_lz, forcing_lr; /* Vz_Control_Vr_Feedback.dat */
+  double forcing_mat[25];     /* F(eqn,k) stored row-major: forcing_mat[(eqn-1)*5 + (k-1)] */
+  int64_t do_viscous_terms;   /* 1            :71 */
+  int64_t shock_capturing;    /* 0            :152 */
+  int64_t control_forcing;    /* 0            :185 */
+  int64_t dt_mode;            /* AXJ_DT_REFERENCE */
+  int64_t precision;          /* AXJ_FP64 */
+  int64_t sensor;             /* AXJ_SENSOR_PLAIN */
+  int64_t judge_every;        /* learned sensor: plain-sensor judge period in steps (50) */
+  double judge_threshold;     /* learned sensor: fallback where |pred-plain| > thr * local max (0.1) */
+  int64_t device;             /* CUDA device ordinal the handle lives on (0) */
+  int64_t reserved[7];
+} axj_params;
+
+typedef struct axj_handle axj_handle;
+
+/* Fill p with the reference defaults (ModuleVariables.f90). */
+void axj_default_params(axj_params* p);
+
+/* Create a solver instance for one Nz x Nr block.
+ * zvec, rvec, ibval: Nz*Nr each (AssignGridCoordinates, ModInputOutput.f90:69-89).
+ * patches: the patch list after CreateAllPatches (ModPatch.f90:117-262).
+ * Replaces: AllocateVariables, CreateAllPatches' stencil maps, SBP_operator and the
+ * ComputeMetric calls of ModSolver.f90:57-76. */
+int axj_create(const axj_params* params, int64_t Nz, int64_t Nr,
+               const double* zvec, const double* rvec, const double* ibval,
+               const axj_patch* patches, int64_t npatch, axj_handle** out);
+
+/* Upload the solution and the target (SolnRead, ModInputOutput.f90:91-148).
+ * iteration/time are tau(1)/tau(4) of the restart file (ModSolver.f90:103-106). */
+int axj_set_state(axj_handle* h, const double* pv, const double* pv_target,
+                  int64_t iteration, double time);
+
+/* Download the solution pv(Nz,Nr,1,5) (feeds WriteOutput, ModInputOutput.f90:201-263). */
+int axj_get_state(axj_handle* h, double* pv);
+
+/* Current iteration counter and time held by the handle. */
+int axj_get_time(axj_handle* h, int64_t* iteration, double* time);
+
+/* ComputeTimeStep (ModInputOutput.f90:389-438): global CFL/viscous dt. */
+int axj_compute_dt(axj_handle* h, double* delt);
+
+/* RK4 (ModRungeKutta.f90:5-171) with the given delt; advances iteration and time. */
+int axj_rk4_step(axj_handle* h, double delt);
+
+/* nsteps x (ComputeTimeStep + RK4) with dt kept on the device, no host sync
+ * inside; the step sequence is captured once in a CUDA graph and replayed.
+ * If out_every > 0 and cb != NULL, cb(user, iteration, time, pv) is called with a
+ * host copy of the state every out_every iterations (the noutput hook,
+ * ModRungeKutta.f90:161-165). last_dt (nullable) receives the last dt used. */
+typedef void (*axj_output_cb)(void* user, int64_t iteration, double time, const double* pv);
+int axj_run(axj_handle* h, int64_t nsteps, int64_t out_every, axj_output_cb cb, void* user,
+            double* last_dt);
+
+/* Measurement entry points (no counterpart in the reference, which has no timers).
+ * axj_run_timed: like axj_run without output, with *ms = device time of the nsteps
+ * graph replays between two CUDA events on the handle's stream.
+ * axj_profile_steps: nsteps steps launched one kernel at a time with a CUDA event
+ * pair around every launch group; ms[0] = dt kernel, ms[1] = sensor chain,
+ * ms[2] = fused stage kernels, ms[3] = whole steps (sums over the nsteps steps);
+ * launches[0..2] = kernel launches of each group. */
+int axj_run_timed(axj_handle* h, int64_t nsteps, double* ms);
+int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launches);
+
+/* AssignValues + ComputeRHS (ModRHS.f90:5-258) on pv (Nz*Nr*5, host) with the
+ * handle's target and delt-independent terms; rhs receives Nz*Nr*5 values. The
+ * handle's solution is not changed. */
+int axj_rhs(axj_handle* h, const double* pv, double* rhs);
+
+/* Compute1stDerivative(var, dirn, out) (ModDeriv.f90:5-120). dirn = 1 (z) or 2 (r). */
+int axj_deriv1(axj_handle* h, const double* var, int64_t dirn, double* out);
+
+/* Compute2ndDerivative(var, dirn, first_deriv, out) (ModDeriv.f90:123-238). */
+int axj_deriv2(axj_handle* h, const double* var, int64_t dirn, const double* first_deriv,
+               double* out);
+
+/* PerformTGfilter(var, dirn, out) (ModTGfilter.f90:5-95). out is read as well:
+ * blanked points keep its incoming value. If inplace != 0, var is ignored and the
+ * filter runs in place on out along z, i.e. PerformTGfilter(q, 1, q) as
+ * ModShockCapturing.f90:63 calls it (a recurrence along i). */
+int axj_tgfilter(axj_handle* h, const double* var, int64_t dirn, int64_t inplace, double* out);
+
+/* ComputeArtTransCoeffs' sensor (ModShockCapturing.f90:5-92) on pv: the artificial
+ * coefficients mustar, betastar, kappastar (Nz*Nr each) before they are added
+ * to mu/beta/lambda/kappa. */
+int axj_sensor(axj_handle* h, const double* pv, double* mustar, double* betastar,
+               double* kappastar);
+
+/* Last error message of the handle (or of the last failed axj_create if h is NULL). */
+const char* axj_last_error(const axj_handle* h);
+
+void axj_destroy(axj_handle* h);
+
+/* Host helpers (no device work). */
+
+/* Parse a bc file (ModPatch.f90:30-63): rows of 9 integers. Fills up to max_records
+ * records and sets *nrecords. */
+int axj_read_bc_file(const char* path, axj_bc_record* records, int64_t max_records,
+                     int64_t* nrecords);
+
+/* PatchCreation for a single block holding the whole grid (ModPatch.f90:117-309):
+ * resolve -1 to the last index and widen each face to its 4-wide strip. */
+int axj_patches_from_records(const axj_bc_record* records, int64_t nrecords, int64_t Nz_grid,
+                             int64_t Nr_grid, axj_patch* patches, int64_t* npatch);
+
+/* Library build information, e.g. "axj 0.1 sm_100a". */
+const char* axj_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AXJ_H */

@@ -1,0 +1,136 @@
+"""Parity of the CUDA path (libaxj.so through the C-ABI) against the CPU oracle.
+
+Tolerances: the FP64 device path differs from the oracle only by FMA contraction and
+libm ulps, so per-routine, per-RHS and per-RK4-step results must agree to 1e-12
+relative (max error over a field divided by the field's max magnitude).
+"""
+import numpy as np
+import pytest
+
+import axisymmetricjet_b200 as axj
+from axisymmetricjet_b200 import fixtures
+from axisymmetricjet_b200._ffi import NSCBC_NOSLIP_WALL, SAT_NOSLIP_WALL
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+
+
+def relerr(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    scale = np.abs(b).max()
+    return np.abs(a - b).max() / (scale if scale > 0 else 1.0)
+
+
+def field_relerr(a, b):
+    return [relerr(a[k], b[k]) for k in range(a.shape[0])]
+
+
+CASES = {
+    "jet": lambda: fixtures.case("jet96x64"),
+    "jet_sc": lambda: fixtures.case("jet96x64sc"),
+    "nozzle_nscbc_wall": lambda: fixtures.nozzle_case(wall=NSCBC_NOSLIP_WALL),
+    "nozzle_sat_wall_sc": lambda: fixtures.nozzle_case(wall=SAT_NOSLIP_WALL, sc=True, Mj=1.5, Re=5000.0),
+    "jet_forcing_physdt": lambda: fixtures.case(
+        "jet96x64", control_forcing=1, forcing_z0=3.0, forcing_r0=0.5, forcing_lz=1.0, forcing_lr=0.3,
+        forcing_mat=np.arange(25.0).reshape(5, 5) * 1e-3, dt_mode=1),
+    "jet_ragged": lambda: fixtures.make_case(77, 45, 30.0, 15.0, 0.9, 1000.0),
+}
+
+
+def pair(c, oracle_mod):
+    gp = axj.patches_from_records(c["records"], c["Nz"], c["Nr"])
+    op = oracle_mod.patches_from_records(c["records"], c["Nz"], c["Nr"])
+    assert gp == op
+    dev = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], gp)
+    ora = oracle_mod.Oracle(c["params"], c["zvec"], c["rvec"], c["ibval"], op)
+    dev.set_state(c["pv"], c["target"])
+    ora.set_state(c["pv"], c["target"])
+    return dev, ora
+
+
+@pytest.mark.parametrize("name", ["nozzle_nscbc_wall", "jet_ragged"])
+def test_operators(oracle_mod, name):
+    c = CASES[name]()
+    dev, ora = pair(c, oracle_mod)
+    rng = np.random.default_rng(7)
+    var = rng.standard_normal((c["Nr"], c["Nz"]))
+    first = rng.standard_normal((c["Nr"], c["Nz"]))
+    for dirn in (1, 2):
+        assert relerr(dev.deriv1(var, dirn), ora.deriv1(var, dirn)) < REL
+        assert relerr(dev.deriv2(var, dirn, first), ora.deriv2(var, dirn, first)) < REL
+        prior = rng.standard_normal((c["Nr"], c["Nz"]))
+        assert relerr(dev.tgfilter(var, dirn, prior), ora.tgfilter(var, dirn, prior)) < REL
+    prior = rng.standard_normal((c["Nr"], c["Nz"]))
+    assert relerr(dev.tgfilter(None, 1, prior, inplace=True), ora.tgfilter(None, 1, prior, inplace=True)) < REL
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_rhs(oracle_mod, name):
+    c = CASES[name]()
+    dev, ora = pair(c, oracle_mod)
+    rd = dev.compute_rhs(c["pv"])
+    ro = ora.compute_rhs(c["pv"])
+    errs = field_relerr(rd, ro)
+    assert max(errs) < REL, errs
+
+
+@pytest.mark.parametrize("name", ["jet_sc", "nozzle_sat_wall_sc"])
+def test_sensor(oracle_mod, name):
+    c = CASES[name]()
+    dev, ora = pair(c, oracle_mod)
+    for a, b in zip(dev.sensor(c["pv"]), ora.sensor(c["pv"])):
+        assert relerr(a, b) < 1e-11
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_rk4_steps(oracle_mod, name):
+    c = CASES[name]()
+    dev, ora = pair(c, oracle_mod)
+    for step in range(3):
+        dd = dev.compute_time_step()
+        do = ora.compute_time_step()
+        assert abs(dd - do) <= 1e-14 * abs(do), (step, dd, do)
+        dev.rk4(do)
+        ora.rk4(do)
+        errs = field_relerr(dev.get_state(), ora.get_state())
+        assert max(errs) < REL, (step, errs)
+    assert dev.get_time()[0] == ora.get_time()[0] == 3
+    assert abs(dev.get_time()[1] - ora.get_time()[1]) <= 1e-15
+
+
+def test_graph_run_equals_stepping(oracle_mod):
+    c = CASES["jet_sc"]()
+    dev, ora = pair(c, oracle_mod)
+    dev2, _ = pair(c, oracle_mod)
+    dlast = dev.run(5)
+    for _ in range(5):
+        d = dev2.compute_time_step()
+        dev2.rk4(d)
+    assert dlast == d
+    np.testing.assert_array_equal(dev.get_state(), dev2.get_state())
+    it, t = dev.get_time()
+    it2, t2 = dev2.get_time()
+    assert it == it2 == 5 and t == t2
+
+
+def test_run_output_callback(oracle_mod):
+    c = CASES["jet"]()
+    dev, _ = pair(c, oracle_mod)
+    seen = []
+    dev.run(6, out_every=2, callback=lambda it, t, pv: seen.append((it, t, pv[0, 3, 3])))
+    assert [s[0] for s in seen] == [2, 4, 6]
+    assert seen[-1][1] == dev.get_time()[1]
+
+
+def test_multistep_jet512x128(oracle_mod):
+    """configs[0]-sized run: 100 RK4 steps, relative L2 error per field."""
+    c = fixtures.case("jet512x128")
+    dev, ora = pair(c, oracle_mod)
+    dev.run(100)
+    ora.run(100)
+    a, b = dev.get_state(), ora.get_state()
+    for k in (0, 1, 3, 4):
+        l2 = np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k])
+        assert l2 < 1e-11, (k, l2)
