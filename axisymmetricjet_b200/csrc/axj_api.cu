@@ -40,7 +40,9 @@ struct axj_handle {
   // state and RK4 work buffers (5 planes each)
   double *U0 = nullptr, *Ua = nullptr, *Ub = nullptr, *A = nullptr, *B = nullptr, *target = nullptr;
   // shock-capturing buffers
-  double *S = nullptr, *dil = nullptr, *fsw = nullptr, *d2 = nullptr, *Q = nullptr, *Qz = nullptr, *star = nullptr;
+  double *Q = nullptr, *Qz = nullptr, *star = nullptr;
+  int2 *stiles_int = nullptr, *stiles_gen = nullptr;  // sensor tile classes
+  int nstiles_int = 0, nstiles_gen = 0;
   uint32_t* desc = nullptr;
   int* faces = nullptr;
   double *dxidz = nullptr, *ddxidxidz = nullptr, *detadr = nullptr, *ddetadetadr = nullptr;
@@ -188,10 +190,10 @@ SensorArgs sensor_args(axj_handle* h, const double* U) {
   s.dz = h->dzv;
   s.dr = h->drv;
   s.ramp = h->ramp;
-  s.S = h->S;
-  s.dil = h->dil;
-  s.fsw = h->fsw;
-  s.d2 = h->d2;
+  s.tiles_int = h->stiles_int;
+  s.tiles_gen = h->stiles_gen;
+  s.ntiles_int = h->nstiles_int;
+  s.ntiles_gen = h->nstiles_gen;
   s.Q = h->Q;
   s.Qz = h->Qz;
   s.star = h->star;
@@ -556,7 +558,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   if (faces.size() >= (1u << 20)) { delete h; return fail(nullptr, AXJ_ERR_BADPATCH, "too many face points"); }
 
   // ---- tile classes
-  std::vector<int2> tint, tgen;
+  std::vector<int2> tint, tgen, sti, stg;
   auto dsc = [&](int64_t i, int64_t j) { return desc[(size_t)j * h->P + i]; };
   for (int64_t j0 = 0; j0 < Nr; j0 += TR)
     for (int64_t i0 = 0; i0 < Nz; i0 += TZ) {
@@ -574,9 +576,23 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
         }
       }
       (interior ? tint : tgen).push_back(make_int2((int)i0, (int)j0));
+      // sensor classes: S, T and the dilatation are formed on a cross of halo
+      // SENS_HS_INT from V_r, V_z stencils of reach H_INT, so every point within
+      // SENS_HS_INT of the tile must use centred rows, and the V region must lie inside.
+      const int64_t hv = SENS_HS_INT + H_INT, hs = SENS_HS_INT;
+      bool sint = i0 - hz_of((int)hv) >= 0 && i0 + TZ + hz_of((int)hv) <= Nz && j0 - hv >= 0 &&
+                  j0 + TR + hv <= Nr;
+      for (int64_t j = j0 - hs; sint && j < j0 + TR + hs; ++j)
+        for (int64_t i = i0 - hs; sint && i < i0 + TZ + hs; ++i) {
+          uint32_t d = dsc(i, j);
+          if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d)) sint = false;
+        }
+      (sint ? sti : stg).push_back(make_int2((int)i0, (int)j0));
     }
   h->ntiles_int = (int)tint.size();
   h->ntiles_gen = (int)tgen.size();
+  h->nstiles_int = (int)sti.size();
+  h->nstiles_gen = (int)stg.size();
 
   // ---- device buffers
   cudaError_t ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
@@ -591,10 +607,6 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->target = dalloc<double>(h, 5 * pl, &rc);
   h->star = dalloc<double>(h, 3 * pl, &rc);
   if (c.shock_capturing) {
-    h->S = dalloc<double>(h, pl, &rc);
-    h->dil = dalloc<double>(h, pl, &rc);
-    h->fsw = dalloc<double>(h, pl, &rc);
-    h->d2 = dalloc<double>(h, 6 * pl, &rc);
     h->Q = dalloc<double>(h, 3 * pl, &rc);
     h->Qz = dalloc<double>(h, 3 * pl, &rc);
   }
@@ -619,6 +631,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->partial = dalloc<double>(h, h->dt_blocks, &rc);
   h->tiles_int = dalloc<int2>(h, std::max<size_t>(tint.size(), 1), &rc);
   h->tiles_gen = dalloc<int2>(h, std::max<size_t>(tgen.size(), 1), &rc);
+  h->stiles_int = dalloc<int2>(h, std::max<size_t>(sti.size(), 1), &rc);
+  h->stiles_gen = dalloc<int2>(h, std::max<size_t>(stg.size(), 1), &rc);
   if (rc != AXJ_OK) {
     g_create_error = h->err;
     axj_destroy(h);
@@ -644,6 +658,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   up(h->forcing, prm->forcing_mat, 25 * sizeof(double));
   up(h->tiles_int, tint.data(), tint.size() * sizeof(int2));
   up(h->tiles_gen, tgen.data(), tgen.size() * sizeof(int2));
+  up(h->stiles_int, sti.data(), sti.size() * sizeof(int2));
+  up(h->stiles_gen, stg.data(), stg.size() * sizeof(int2));
   std::vector<PatchDev> pd(npatch > 0 ? npatch : 1);
   for (int64_t k = 0; k < npatch; ++k) { pd[k].bc = (int)patches[k].bc; pd[k].dir = (int)patches[k].bc_dir; }
   upload_tables(S1, S2, G, pd.data(), (int)npatch, h->stream);

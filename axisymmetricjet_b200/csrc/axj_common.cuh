@@ -26,6 +26,10 @@ constexpr int STAGE_THREADS = 256;
 // points) use patch-selected closure rows whose windows reach 5 points.
 constexpr int H_INT = 2;
 constexpr int H_GEN = 5;
+// Halo of the strain-rate / temperature / dilatation fields in the sensor kernel:
+// two SBP2 reaches (fourth derivative as SBP2 of SBP2).
+constexpr int SENS_HS_INT = 2 * H_INT;
+constexpr int SENS_HS_GEN = 2 * H_GEN;
 // z halo rounded up to an even count so every smem row starts 16-byte aligned
 // relative to the global row.
 constexpr int hz_of(int h) { return (h + 1) & ~1; }

@@ -15,6 +15,8 @@
 //                        with the in-place z filter as a chunked recurrence.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "axj_kernels.cuh"
 #include "axj_point.cuh"
 
@@ -323,14 +325,6 @@ static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* ti
   return cudaGetLastError();
 }
 
-cudaError_t init_kernel_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<H_GEN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)StageSmem<H_GEN>::bytes(true));
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel<H_INT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)StageSmem<H_INT>::bytes(false));
-}
-
 cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, int ntiles_gen,
                          const int2* tiles_gen, cudaStream_t s) {
   cudaError_t e = launch_stage_t<H_GEN, true>(a, ntiles_gen, tiles_gen, s);
@@ -439,84 +433,176 @@ __device__ __forceinline__ int row_of(uint32_t dsc, int dirn) {
   return dirn == 1 ? desc_zrow(dsc) : desc_rrow(dsc);
 }
 
-// Sensor step 1 (ModShockCapturing.f90:108-159, :197-202): dilatation, strain-rate
-// magnitude and the switch f_sw from dV/dz, dV/dr of the stage input.
-__global__ void sensor_first_kernel(const SensorArgs a) {
-  const Grid g = a.g;
-  const long long n = (long long)g.Nz * g.Nr;
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const int j = (int)(p / g.Nz), i = (int)(p - (long long)j * g.Nz);
-  const long long o = (long long)j * g.P + i;
-  const uint32_t dsc = __ldg(a.desc + o);
-  const double* Vr = a.U + 1 * g.plane;
-  const double* Vz = a.U + 3 * g.plane;
-  const int zr = row_of(dsc, 1), rw = row_of(dsc, 2);
-  const double xz = __ldg(a.dxidz + i), er = __ldg(a.detadr + j);
-  const double dVrdz = gstencil6(cSBP1, zr, Vr, g, i, j, 1) * xz;
-  const double dVzdz = gstencil6(cSBP1, zr, Vz, g, i, j, 1) * xz;
-  const double dVrdr = gstencil6(cSBP1, rw, Vr, g, i, j, 2) * er;
-  const double dVzdr = gstencil6(cSBP1, rw, Vz, g, i, j, 2) * er;
-  const double vr = __ldg(Vr + o), r = __ldg(a.rc + j);
-  double dil;
-  if (j == 0) dil = 2.0 * dVrdr + dVzdz;
-  else dil = dVrdr + vr / r + dVzdz;
-  const double S11 = dVrdr - (1.0 / 3.0) * dil;
-  const double S13 = 0.5 * (dVrdz + dVzdr);
-  const double S31 = S13;
-  const double S33 = dVzdz - (1.0 / 3.0) * dil;
-  const double S22 = (j == 0) ? dVrdr - (1.0 / 3.0) * dil : vr / r - (1.0 / 3.0) * dil;
-  const double S = sqrt(S11 * S11 + S13 * S13 + S22 * S22 + S31 * S31 + S33 * S33);
-  const double vort = fabs(dVrdz - dVzdr);
-  const double Hm = (-1.0 * dil < 0.0) ? 0.0 : 1.0;
-  const double eps = (double)1e-15f;  // single-precision literal of the reference (:202)
-  const double fsw = Hm * (dil * dil) / (dil * dil + vort * vort + eps);
-  a.S[o] = S;
-  a.dil[o] = dil;
-  a.fsw[o] = fsw;
-}
+// ---------------------------------------------------------------------------
+// Fused sensor tile kernel (ModShockCapturing.f90:18-53, :108-222): strain-rate
+// magnitude S, dilatation and f_sw from the first derivatives of V_r, V_z; the
+// computational-space SBP2 of S, T and the dilatation twice over (fourth
+// derivatives); the three quantities to be filtered. HS is the halo of S/T/dil
+// (two SBP2 reaches), HF the reach of one stencil (2 interior, 5 with closures).
+// ---------------------------------------------------------------------------
+template <int HS, int HF>
+struct SensSmem {
+  static constexpr int HV = HS + HF;          // halo of V_r, V_z
+  static constexpr int HVZ = hz_of(HV);
+  static constexpr int VZ = TZ + 2 * HVZ, VR = TR + 2 * HV, NV = VZ * VR;
+  static constexpr int SZ = TZ + 2 * HS, SR = TR + 2 * HS, NS = SZ * SR;
+  static constexpr int DZ = TZ + 2 * HF;      // z-arm of the second derivatives: [TR][DZ]
+  static constexpr int DR = TR + 2 * HF;      // r-arm: [DR][TZ]
+  static constexpr size_t bytes(bool gen) {
+    return sizeof(double) * (size_t)(2 * NV + 3 * NS + TR * DZ + DR * TZ + TR * TZ) +
+           (gen ? sizeof(uint32_t) * NV : 0);
+  }
+};
 
-// Sensor step 2 (:27-33): Compute2ndDerivativeComputational of S, T, dilatation.
-__global__ void sensor_d2_kernel(const SensorArgs a) {
+template <int HS, int HF, bool GEN>
+__global__ void __launch_bounds__(STAGE_THREADS) sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles) {
+  using SM = SensSmem<HS, HF>;
+  constexpr int HV = SM::HV, HVZ = SM::HVZ, VZ = SM::VZ, NV = SM::NV;
+  constexpr int SZ = SM::SZ, NS = SM::NS, DZ = SM::DZ, DR = SM::DR;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* sVr = reinterpret_cast<double*>(smem_raw);  // [VR][VZ]
+  double* sVz = sVr + NV;
+  double* sS = sVz + NV;                               // [SR][SZ] x 3: S, T, dil
+  double* sT = sS + NS;
+  double* sD = sT + NS;
+  double* sd2z = sD + NS;                              // [TR][DZ]
+  double* sd2r = sd2z + TR * DZ;                       // [DR][TZ]
+  double* sFsw = sd2r + DR * TZ;                       // [TR][TZ]
+  uint32_t* sDesc = reinterpret_cast<uint32_t*>(sFsw + TR * TZ);
+
+  const int tid = threadIdx.x;
+  const int2 t0 = tiles[blockIdx.x];
+  const int i0 = t0.x, j0 = t0.y;
   const Grid g = a.g;
-  const long long n = (long long)g.Nz * g.Nr;
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const int j = (int)(p / g.Nz), i = (int)(p - (long long)j * g.Nz);
-  const long long o = (long long)j * g.P + i;
-  const uint32_t dsc = __ldg(a.desc + o);
-  const int zr = row_of(dsc, 1), rw = row_of(dsc, 2);
-  const double* T = a.U + 4 * g.plane;
-  const double* src[3] = {a.S, T, a.dil};
+  const int Nz = g.Nz, Nr = g.Nr;
+  auto inside = [&](int i, int j) { return i >= 0 && i < Nz && j >= 0 && j < Nr; };
+  auto vdesc = [&](int vidx) -> uint32_t { return GEN ? sDesc[vidx] : make_desc(4, 4, false, 0); };
+
+  // ---- phase 1: V_r, V_z (+ descriptors) on the V region, T on the S region
+  for (int idx = tid; idx < NV; idx += STAGE_THREADS) {
+    const int vr = idx / VZ, vz = idx - vr * VZ;
+    const int i = i0 - HVZ + vz, j = j0 - HV + vr;
+    double a1 = 0.0, a3 = 0.0;
+    uint32_t dsc = make_desc(ROW_NONE, ROW_NONE, false, 0);
+    if (!GEN || inside(i, j)) {
+      const long long o = (long long)j * g.P + i;
+      a1 = __ldg(a.U + 1 * g.plane + o);
+      a3 = __ldg(a.U + 3 * g.plane + o);
+      if (GEN) dsc = __ldg(a.desc + o);
+    }
+    sVr[idx] = a1;
+    sVz[idx] = a3;
+    if (GEN) sDesc[idx] = dsc;
+  }
+  for (int idx = tid; idx < NS; idx += STAGE_THREADS) {
+    const int sr = idx / SZ, sz = idx - sr * SZ;
+    const int i = i0 - HS + sz, j = j0 - HS + sr;
+    sT[idx] = (!GEN || inside(i, j)) ? __ldg(a.U + 4 * g.plane + (long long)j * g.P + i) : 0.0;
+  }
+  __syncthreads();
+
+  // ---- phase 2: S and dilatation on the cross of the S region; f_sw on the tile
+  for (int idx = tid; idx < NS; idx += STAGE_THREADS) {
+    const int sr = idx / SZ, sz = idx - sr * SZ;
+    const bool zarm = sr >= HS && sr < HS + TR;
+    const bool rarm = sz >= HS && sz < HS + TZ;
+    double S = 0.0, dil = 0.0;
+    const int i = i0 - HS + sz, j = j0 - HS + sr;
+    if ((zarm || rarm) && (!GEN || inside(i, j))) {
+      const int vidx = (sr + HV - HS) * VZ + (sz + HVZ - HS);
+      const uint32_t dsc = vdesc(vidx);
+      const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
+      const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
+      const double xz = __ldg(a.dxidz + i), er = __ldg(a.detadr + j);
+      const double dVrdz = d1<GEN>(zr, sVr + vidx, 1) * xz;
+      const double dVzdz = d1<GEN>(zr, sVz + vidx, 1) * xz;
+      const double dVrdr = d1<GEN>(rw, sVr + vidx, VZ) * er;
+      const double dVzdr = d1<GEN>(rw, sVz + vidx, VZ) * er;
+      const double vr = sVr[vidx];
+      const double r = __ldg(a.rc + j);
+      if (j == 0) dil = 2.0 * dVrdr + dVzdz;
+      else dil = dVrdr + vr / r + dVzdz;
+      const double S11 = dVrdr - (1.0 / 3.0) * dil;
+      const double S13 = 0.5 * (dVrdz + dVzdr);
+      const double S33 = dVzdz - (1.0 / 3.0) * dil;
+      const double S22 = (j == 0) ? dVrdr - (1.0 / 3.0) * dil : vr / r - (1.0 / 3.0) * dil;
+      S = sqrt(S11 * S11 + S13 * S13 + S22 * S22 + S13 * S13 + S33 * S33);
+      if (zarm && rarm) {
+        const double vort = fabs(dVrdz - dVzdr);
+        const double Hm = (-1.0 * dil < 0.0) ? 0.0 : 1.0;
+        const double eps = (double)1e-15f;  // single-precision literal of the reference (:202)
+        sFsw[(sr - HS) * TZ + (sz - HS)] = Hm * (dil * dil) / (dil * dil + vort * vort + eps);
+      }
+    }
+    sS[idx] = S;
+    sD[idx] = dil;
+  }
+  __syncthreads();
+
+  // ---- phases 3-4 per field: second derivatives on the arms, fourth derivatives at
+  // the tile points (kept in registers: 2 points per thread)
+  constexpr int PPT = (TZ * TR) / STAGE_THREADS;
+  double d4z[3][PPT], d4r[3][PPT];
+  const double* srcs[3] = {sS, sT, sD};
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
-    a.d2[(long long)f * g.plane + o] = gstencil6(cSBP2, zr, src[f], g, i, j, 1);
-    a.d2[(long long)(3 + f) * g.plane + o] = gstencil6(cSBP2, rw, src[f], g, i, j, 2);
+    const double* src = srcs[f];
+    for (int idx = tid; idx < TR * DZ + DR * TZ; idx += STAGE_THREADS) {
+      if (idx < TR * DZ) {
+        const int r = idx / DZ, c = idx - r * DZ;  // point (i0 - HF + c, j0 + r)
+        const int i = i0 - HF + c, j = j0 + r;
+        double v = 0.0;
+        if (!GEN || inside(i, j)) {
+          const int sidx = (HS + r) * SZ + (HS - HF + c);
+          const uint32_t dsc = vdesc((HV + r) * VZ + (HVZ - HF + c));
+          const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
+          v = d2<GEN>(zr, src + sidx, 1);
+        }
+        sd2z[idx] = v;
+      } else {
+        const int k = idx - TR * DZ;
+        const int r = k / TZ, c = k - r * TZ;      // point (i0 + c, j0 - HF + r)
+        const int i = i0 + c, j = j0 - HF + r;
+        double v = 0.0;
+        if (!GEN || inside(i, j)) {
+          const int sidx = (HS - HF + r) * SZ + (HS + c);
+          const uint32_t dsc = vdesc((HV - HF + r) * VZ + (HVZ + c));
+          const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
+          v = d2<GEN>(rw, src + sidx, SZ);
+        }
+        sd2r[k] = v;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+      const int pidx = tid + q * STAGE_THREADS;
+      const int r = pidx / TZ, c = pidx - r * TZ;
+      const uint32_t dsc = vdesc((HV + r) * VZ + (HVZ + c));
+      const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
+      const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
+      d4z[f][q] = d2<GEN>(zr, sd2z + r * DZ + HF + c, 1);
+      d4r[f][q] = d2<GEN>(rw, sd2r + (HF + r) * TZ + c, TZ);
+    }
+    __syncthreads();
   }
-}
 
-// Sensor step 3 (:45-51, :162-222): fourth derivatives as SBP2 of the second
-// derivatives, then the three quantities to be filtered.
-__global__ void sensor_q_kernel(const SensorArgs a) {
-  const Grid g = a.g;
-  const long long n = (long long)g.Nz * g.Nr;
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const int j = (int)(p / g.Nz), i = (int)(p - (long long)j * g.Nz);
-  const long long o = (long long)j * g.P + i;
-  const uint32_t dsc = __ldg(a.desc + o);
-  const int zr = row_of(dsc, 1), rw = row_of(dsc, 2);
-  const double d4Sz = gstencil6(cSBP2, zr, a.d2 + 0 * g.plane, g, i, j, 1);
-  const double d4Tz = gstencil6(cSBP2, zr, a.d2 + 1 * g.plane, g, i, j, 1);
-  const double d4Dz = gstencil6(cSBP2, zr, a.d2 + 2 * g.plane, g, i, j, 1);
-  const double d4Sr = gstencil6(cSBP2, rw, a.d2 + 3 * g.plane, g, i, j, 2);
-  const double d4Tr = gstencil6(cSBP2, rw, a.d2 + 4 * g.plane, g, i, j, 2);
-  const double d4Dr = gstencil6(cSBP2, rw, a.d2 + 5 * g.plane, g, i, j, 2);
-  const double dz = __ldg(a.dz + i), dr = __ldg(a.dr + j);
-  const double rho = __ldg(a.U + o), T = __ldg(a.U + 4 * g.plane + o), fsw = __ldg(a.fsw + o);
-  a.Q[o] = rho * fabs((d4Sz * (dz * dz) + d4Sr * (dr * dr)));
-  a.Q[g.plane + o] = rho * fsw * fabs((d4Dz * (dz * dz) + d4Dr * (dr * dr)));
-  a.Q[2 * g.plane + o] = rho / (a.c.gam * sqrt(T)) * fabs((d4Tz * dz + d4Tr * dr));
+  // ---- quantities to be filtered (ComputeTobeFilteredQuantities :204-215)
+#pragma unroll
+  for (int q = 0; q < PPT; ++q) {
+    const int pidx = tid + q * STAGE_THREADS;
+    const int r = pidx / TZ, c = pidx - r * TZ;
+    const int i = i0 + c, j = j0 + r;
+    if (GEN && !inside(i, j)) continue;
+    const long long o = (long long)j * g.P + i;
+    const double dz = __ldg(a.dz + i), dr = __ldg(a.dr + j);
+    const double rho = __ldg(a.U + o);
+    const double T = sT[(HS + r) * SZ + HS + c];
+    const double fsw = sFsw[r * TZ + c];
+    a.Q[o] = rho * fabs((d4z[0][q] * (dz * dz) + d4r[0][q] * (dr * dr)));
+    a.Q[g.plane + o] = rho * fsw * fabs((d4z[2][q] * (dz * dz) + d4r[2][q] * (dr * dr)));
+    a.Q[2 * g.plane + o] = rho / (a.c.gam * sqrt(T)) * fabs((d4z[1][q] * dz + d4r[1][q] * dr));
+  }
 }
 
 // In-place z filter PerformTGfilter(q, 1, q) (ModShockCapturing.f90:63,69,75) as a
@@ -599,17 +685,100 @@ cudaError_t launch_sensor(const SensorArgs& a, cudaStream_t s) {
   const long long n = (long long)a.g.Nz * a.g.Nr;
   const int bs = 256;
   const int nb = (int)((n + bs - 1) / bs);
-  sensor_first_kernel<<<nb, bs, 0, s>>>(a);
-  sensor_d2_kernel<<<nb, bs, 0, s>>>(a);
-  sensor_q_kernel<<<nb, bs, 0, s>>>(a);
+  if (a.ntiles_gen > 0)
+    sensor_tile_kernel<SENS_HS_GEN, H_GEN, true>
+        <<<a.ntiles_gen, STAGE_THREADS, SensSmem<SENS_HS_GEN, H_GEN>::bytes(true), s>>>(a, a.tiles_gen);
+  if (a.ntiles_int > 0)
+    sensor_tile_kernel<SENS_HS_INT, H_INT, false>
+        <<<a.ntiles_int, STAGE_THREADS, SensSmem<SENS_HS_INT, H_INT>::bytes(false), s>>>(a, a.tiles_int);
   cudaError_t e = launch_tgfilter_z_inplace(a.g, a.desc, a.Q, a.Qz, 3, s);
   if (e != cudaSuccess) return e;
   sensor_rfilter_kernel<<<nb, bs, 0, s>>>(a);
   return cudaGetLastError();
 }
 
+// Row-staged version of the same recurrence: one CTA per (row, field); the row of
+// unfiltered values and the z row codes sit in shared memory, each thread owns a
+// chunk of ZR_L points (odd, so lanes read shared memory without bank conflicts) and
+// keeps the last 10 filtered values in registers. Rows up to ZR_MAXNZ points.
+constexpr int ZR_L = 33;
+constexpr int ZR_W = 48;
+constexpr int ZR_MAXNZ = 12288;
+
+// One output of the recurrence for TG row ROW at point i. p[k] = filtered value at
+// i-k (or the unfiltered value / 0 left of the chunk's start), xs = unfiltered row.
+template <int ROW>
+__device__ __forceinline__ double zr_apply(const double (&p)[11], const double* __restrict__ xs, int i, int Nz) {
+  constexpr int W0 = ROW < 4 ? -ROW : (ROW == 4 ? -4 : -2 - ROW);
+  constexpr int N = ROW == 4 ? 9 : 11;
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m < N; ++m) {
+    const int o = W0 + m;
+    double v;
+    if (o < 0) v = p[o < 0 ? -o : 0];
+    else v = (i + o < Nz) ? xs[i + o] : 0.0;
+    s = (m == 0) ? cTG[ROW][0] * v : s + cTG[ROW][m] * v;
+  }
+  return s;
+}
+
+__global__ void tgfilter_z_rows_kernel(const Grid g, const uint32_t* __restrict__ desc,
+                                       const double* __restrict__ q, double* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char zr_smem[];
+  const int Nz = g.Nz;
+  double* xs = reinterpret_cast<double*>(zr_smem);
+  double* ys = xs + Nz;
+  unsigned char* rs = reinterpret_cast<unsigned char*>(ys + Nz);
+  const int j = blockIdx.x, f = blockIdx.y;
+  const double* x = q + (long long)f * g.plane + (long long)j * g.P;
+  double* y = out + (long long)f * g.plane + (long long)j * g.P;
+  const uint32_t* dr = desc + (long long)j * g.P;
+  for (int i = threadIdx.x; i < Nz; i += blockDim.x) {
+    xs[i] = __ldg(x + i);
+    rs[i] = (unsigned char)row_of(__ldg(dr + i), 1);
+  }
+  __syncthreads();
+  const int nchunk = (Nz + ZR_L - 1) / ZR_L;
+  for (int c = threadIdx.x; c < nchunk; c += blockDim.x) {
+    const int ib = c * ZR_L, ie = min(Nz, ib + ZR_L), is = max(0, ib - ZR_W);
+    double p[11];
+    p[0] = 0.0;
+#pragma unroll
+    for (int k = 1; k <= 10; ++k) p[k] = (is - k >= 0) ? xs[is - k] : 0.0;
+    for (int i = is; i < ie; ++i) {
+      double v;
+      switch (rs[i]) {
+        case 4: v = zr_apply<4>(p, xs, i, Nz); break;
+        case 0: v = zr_apply<0>(p, xs, i, Nz); break;
+        case 1: v = zr_apply<1>(p, xs, i, Nz); break;
+        case 2: v = zr_apply<2>(p, xs, i, Nz); break;
+        case 3: v = zr_apply<3>(p, xs, i, Nz); break;
+        case 5: v = zr_apply<5>(p, xs, i, Nz); break;
+        case 6: v = zr_apply<6>(p, xs, i, Nz); break;
+        case 7: v = zr_apply<7>(p, xs, i, Nz); break;
+        case 8: v = zr_apply<8>(p, xs, i, Nz); break;
+        default: v = xs[i]; break;  // blanked / no row: left unchanged in place
+      }
+#pragma unroll
+      for (int k = 10; k >= 2; --k) p[k] = p[k - 1];
+      p[1] = v;
+      if (i >= ib) ys[i] = v;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Nz; i += blockDim.x) y[i] = ys[i];
+}
+
 cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const double* q, double* out, int nfield,
                                       cudaStream_t s) {
+  if (g.Nz <= ZR_MAXNZ) {
+    const size_t sm = (size_t)g.Nz * (2 * sizeof(double) + 1);
+    const int nchunk = (g.Nz + ZR_L - 1) / ZR_L;
+    const int bs = std::min(1024, (nchunk + 31) / 32 * 32);
+    tgfilter_z_rows_kernel<<<dim3(g.Nr, nfield), bs, sm, s>>>(g, desc, q, out);
+    return cudaGetLastError();
+  }
   const int nchunk = (g.Nz + ZF_CHUNK - 1) / ZF_CHUNK;
   const long long total = (long long)nfield * g.Nr * nchunk;
   const int bs = 128;
@@ -673,6 +842,29 @@ cudaError_t launch_tgfilter(const Grid& g, const uint32_t* desc, const double* v
   const long long n = (long long)g.Nz * g.Nr;
   tgfilter_kernel<<<(int)((n + 255) / 256), 256, 0, s>>>(g, desc, var, dirn, out);
   return cudaGetLastError();
+}
+
+}  // namespace axj
+
+namespace axj {
+
+// Opt-in shared-memory sizes; called once per handle at creation (outside any
+// stream capture).
+cudaError_t init_kernel_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<H_GEN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)StageSmem<H_GEN>::bytes(true));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(stage_kernel<H_INT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)StageSmem<H_INT>::bytes(false));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(sensor_tile_kernel<SENS_HS_GEN, H_GEN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)SensSmem<SENS_HS_GEN, H_GEN>::bytes(true));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(sensor_tile_kernel<SENS_HS_INT, H_INT, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SensSmem<SENS_HS_INT, H_INT>::bytes(false));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(tgfilter_z_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)((size_t)ZR_MAXNZ * (2 * sizeof(double) + 1)));
 }
 
 }  // namespace axj

@@ -73,10 +73,9 @@ struct SensorArgs {
   const double* dz;      // deltaz(i) (:171-179)
   const double* dr;      // deltar(j) (:181-189)
   const double* ramp;    // (1+tanh(5(z-10)))/2 (:85)
-  double* S;             // MgnStrRate
-  double* dil;           // dilvec
-  double* fsw;           // Ducros-type switch f_sw (:202)
-  double* d2;            // 6 planes: S_xi2, T_xi2, dil_xi2, S_eta2, T_eta2, dil_eta2
+  const int2* tiles_int; // sensor tile classes: centred rows within reach 6 of the tile
+  const int2* tiles_gen; // everything else (closure rows, blanked points, domain edges)
+  int ntiles_int, ntiles_gen;
   double* Q;             // 3 planes: mustarQuantity, betastarQuantity, kappastarQuantity
   double* Qz;            // 3 planes: Q after the in-place z filter
   double* star;          // 3 planes: mustar, betastar, kappastar

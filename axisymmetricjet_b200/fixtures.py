@@ -108,6 +108,9 @@ CASES = {
     "jet4400x640": dict(Nz=4400, Nr=640, zmax=60.0, rmax=15.0, Mj=1.5, Re=5000.0, sc=True),
     "jet96x64": dict(Nz=96, Nr=64, zmax=30.0, rmax=15.0, Mj=0.9, Re=1000.0, sc=False),
     "jet96x64sc": dict(Nz=96, Nr=64, zmax=30.0, rmax=15.0, Mj=1.5, Re=5000.0, sc=True),
+    # profiling case: the production physics on fewer z points (state 52 MB, larger than L2
+    # once the RK work buffers are counted, about 0.8 GB on the device)
+    "jet2048x640": dict(Nz=2048, Nr=640, zmax=60.0, rmax=15.0, Mj=1.5, Re=5000.0, sc=True),
 }
 
 

@@ -184,6 +184,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default="jet4400x640")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=10)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -233,7 +235,7 @@ def main():
     value = world * npts * args.steps / (ms_max / 1e3)
 
     # per-kernel breakdown (same kernels launched one group at a time with CUDA events)
-    prof_steps = max(2, min(args.steps, 10))
+    prof_steps = max(1, args.profile_steps)
     pms, plaunch = solver.profile_steps(prof_steps)
     stage_launch_ms = pms["stage"] / (4 * prof_steps)
     peak, peak_kind = measured_peaks()
@@ -242,36 +244,7 @@ def main():
     traffic = profile_traffic(args.case)
     launches_per_step = 1 + 4 * ((5 if c["params"].shock_capturing else 0) + (plaunch["stage"] // (4 * prof_steps)))
 
-    # end to end through the public API with host buffers: IC and target upload, every
-    # step ComputeTimeStep (dt to the host) + RK4(delt), the state downloaded every
-    # NOUTPUT steps and at the end (ModRungeKutta.f90:161-165)
-    e2e_solver = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
-    pv_h = torch.from_numpy(c["pv"]).pin_memory().numpy()
-    tg_h = torch.from_numpy(c["target"]).pin_memory().numpy()
-    out_h = torch.empty(c["pv"].shape, dtype=torch.float64).pin_memory().numpy()
-    e2e_solver.set_state(pv_h, tg_h)
-    for _ in range(args.warmup):
-        e2e_solver.rk4(e2e_solver.compute_time_step())
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    e2e_solver.set_state(pv_h, tg_h)
-    nout = 0
-    for s in range(1, args.steps + 1):
-        e2e_solver.rk4(e2e_solver.compute_time_step())
-        if s % NOUTPUT == 0:
-            e2e_solver.get_state(out_h)
-            nout += 1
-    e2e_solver.get_state(out_h)
-    nout += 1
-    ev1.record()
-    barrier()
-    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    state_bytes = 5 * npts * 8
-    e2e = {"value": world * npts * args.steps / (e2e_ms / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": (2 * state_bytes + 8 * args.steps) / args.steps,
-           "d2h_bytes_per_step": (nout * state_bytes + 12 * args.steps) / args.steps}
-    e2e_solver.close()
+    e2e = run_e2e(args, c, patches, npts, world, barrier, max_over_ranks) if not args.no_e2e else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -302,6 +275,43 @@ def main():
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def run_e2e(args, c, patches, npts, world, barrier, max_over_ranks):
+    """End to end through the public API with host buffers: IC and target upload, every
+    step ComputeTimeStep (dt to the host) + RK4(delt), the state downloaded every
+    NOUTPUT steps and at the end (ModRungeKutta.f90:161-165)."""
+    import torch
+
+    import axisymmetricjet_b200 as axj
+    e2e_solver = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+    pv_h = torch.from_numpy(c["pv"]).pin_memory().numpy()
+    tg_h = torch.from_numpy(c["target"]).pin_memory().numpy()
+    out_h = torch.empty(c["pv"].shape, dtype=torch.float64).pin_memory().numpy()
+    e2e_solver.set_state(pv_h, tg_h)
+    for _ in range(args.warmup):
+        e2e_solver.rk4(e2e_solver.compute_time_step())
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    e2e_solver.set_state(pv_h, tg_h)
+    nout = 0
+    for s in range(1, args.steps + 1):
+        e2e_solver.rk4(e2e_solver.compute_time_step())
+        if s % NOUTPUT == 0:
+            e2e_solver.get_state(out_h)
+            nout += 1
+    e2e_solver.get_state(out_h)
+    nout += 1
+    ev1.record()
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    state_bytes = 5 * npts * 8
+    e2e = {"value": world * npts * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": (2 * state_bytes + 8 * args.steps) / args.steps,
+           "d2h_bytes_per_step": (nout * state_bytes + 12 * args.steps) / args.steps}
+    e2e_solver.close()
+    return e2e
 
 
 if __name__ == "__main__":
