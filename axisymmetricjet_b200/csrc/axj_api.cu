@@ -35,6 +35,7 @@ struct axj_handle {
   axj_params params{};
   Consts c{};
   cudaStream_t stream = nullptr;
+  SideStream side{nullptr, nullptr, nullptr};  // general-tile launches run here, joined back
   std::string err;
   std::vector<void*> allocs;
   // state and RK4 work buffers (5 planes each)
@@ -44,6 +45,7 @@ struct axj_handle {
   int2 *stiles_int = nullptr, *stiles_gen = nullptr;  // sensor tile classes
   int nstiles_int = 0, nstiles_gen = 0;
   uint32_t* desc = nullptr;
+  unsigned char* zcode = nullptr;  // z stencil code per point for the z filter (9 = blanked)
   int* faces = nullptr;
   double *dxidz = nullptr, *ddxidxidz = nullptr, *detadr = nullptr, *ddetadetadr = nullptr;
   double *zc = nullptr, *rc = nullptr, *dzv = nullptr, *drv = nullptr, *ramp = nullptr, *forcing = nullptr;
@@ -60,6 +62,14 @@ struct axj_handle {
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   std::vector<double> host_out;  // output-callback staging
+  // TMA descriptors: stage-input halo boxes for U0/Ua/Ub x {interior, general} tiles,
+  // coefficient halo boxes, and tile boxes of pv_old and the running sum A
+  CUtensorMap map_state[3][2];
+  CUtensorMap map_star[2];
+  CUtensorMap map_u0_tile, map_acc_tile;
+  CUtensorMap map_sens[3][2];  // sensor V boxes of U0/Ua/Ub x {interior, general}
+  CUtensorMap map_sensT[3][2]; // sensor temperature boxes
+  CUtensorMap map_rho[3];      // density tile boxes
 };
 
 namespace {
@@ -182,6 +192,12 @@ SensorArgs sensor_args(axj_handle* h, const double* U) {
   SensorArgs s;
   s.g = grid_of(h);
   s.U = U;
+  const int b = U == h->U0 ? 0 : (U == h->Ua ? 1 : 2);
+  s.mv_int = &h->map_sens[b][0];
+  s.mv_gen = &h->map_sens[b][1];
+  s.mt_int = &h->map_sensT[b][0];
+  s.mt_gen = &h->map_sensT[b][1];
+  s.mrho = &h->map_rho[b];
   s.desc = h->desc;
   s.dxidz = h->dxidz;
   s.detadr = h->detadr;
@@ -194,6 +210,8 @@ SensorArgs sensor_args(axj_handle* h, const double* U) {
   s.tiles_gen = h->stiles_gen;
   s.ntiles_int = h->nstiles_int;
   s.ntiles_gen = h->nstiles_gen;
+  s.zcode = h->zcode;
+  s.flags = h->flags;
   s.Q = h->Q;
   s.Qz = h->Qz;
   s.star = h->star;
@@ -223,6 +241,7 @@ StageArgs stage_args(axj_handle* h, const double* Uin, double* Uout, int stage) 
   a.zc = h->zc;
   a.rc = h->rc;
   a.forcing = h->forcing;
+  a.ramp = h->ramp;
   a.dt = h->dt;
   a.staleT = h->staleT;
   a.flags = h->flags;
@@ -233,16 +252,100 @@ StageArgs stage_args(axj_handle* h, const double* Uin, double* Uout, int stage) 
   return a;
 }
 
+// cuTensorMapEncodeTiled, resolved from the driver at run time (no link-time libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 3-D map over nplanes planes of (Nz, Nr) doubles with pitch P; out-of-range
+// elements of a box read as zero.
+int make_map(axj_handle* h, CUtensorMap* m, const double* base, int nplanes, int bw, int bh, int bp) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return fail(h, AXJ_ERR_NODEVICE, "cuTensorMapEncodeTiled is not available from the driver");
+  const cuuint64_t dims[3] = {(cuuint64_t)h->Nz, (cuuint64_t)h->Nr, (cuuint64_t)nplanes};
+  const cuuint64_t strides[2] = {(cuuint64_t)h->P * sizeof(double), (cuuint64_t)h->plane * sizeof(double)};
+  const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, (cuuint32_t)bp};
+  const cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(h, AXJ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return AXJ_OK;
+}
+
+int build_maps(axj_handle* h) {
+  const double* st[3] = {h->U0, h->Ua, h->Ub};
+  for (int cls = 0; cls < 2; ++cls) {
+    int hw, hh, qh, tw, th;
+    stage_boxes(cls == 1, &hw, &hh, &qh, &tw, &th);
+    for (int b = 0; b < 3; ++b) {
+      int rc = make_map(h, &h->map_state[b][cls], st[b], 5, hw, hh, 5);
+      if (rc != AXJ_OK) return rc;
+    }
+    // z-filtered coefficient quantities (never loaded without shock capturing)
+    int rc = make_map(h, &h->map_star[cls], h->Qz ? h->Qz : h->star, 3, hw, qh, 3);
+    if (rc != AXJ_OK) return rc;
+    int vw, vh, tw2, th2;
+    sensor_boxes(cls == 1, &vw, &vh, &tw2, &th2);
+    for (int b = 0; b < 3; ++b) {
+      rc = make_map(h, &h->map_sens[b][cls], st[b], 5, vw, vh, 1);
+      if (rc != AXJ_OK) return rc;
+      rc = make_map(h, &h->map_sensT[b][cls], st[b], 5, tw2, th2, 1);
+      if (rc != AXJ_OK) return rc;
+    }
+  }
+  {
+    int hw, hh, qh, tw, th;
+    stage_boxes(false, &hw, &hh, &qh, &tw, &th);
+    for (int b = 0; b < 3; ++b) {
+      int rc = make_map(h, &h->map_rho[b], st[b], 5, tw, th, 1);
+      if (rc != AXJ_OK) return rc;
+    }
+  }
+  int hw, hh, qh, tw, th;
+  stage_boxes(false, &hw, &hh, &qh, &tw, &th);
+  int rc = make_map(h, &h->map_u0_tile, h->U0, 5, tw, th, 5);
+  if (rc != AXJ_OK) return rc;
+  return make_map(h, &h->map_acc_tile, h->A, 5, tw, th, 5);
+}
+
+StageMaps stage_maps(axj_handle* h, const double* Uin, int cls) {
+  const int b = Uin == h->U0 ? 0 : (Uin == h->Ua ? 1 : 2);
+  StageMaps m;
+  m.state = &h->map_state[b][cls];
+  m.star = &h->map_star[cls];
+  m.u0 = &h->map_u0_tile;
+  m.acc = &h->map_acc_tile;
+  return m;
+}
+
+int launch_stage_kernels(axj_handle* h, const double* Uin, double* Uout, int stage) {
+  StageArgs a = stage_args(h, Uin, Uout, stage);
+  StageMaps mi = stage_maps(h, Uin, 0), mg = stage_maps(h, Uin, 1);
+  AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, mi, h->ntiles_gen, h->tiles_gen, mg, h->side, h->stream));
+  return AXJ_OK;
+}
+
 // One RK stage: the sensor chain on the stage input (if enabled), then the fused
 // stage kernel over both tile classes.
 int enqueue_stage(axj_handle* h, const double* Uin, double* Uout, int stage) {
   if (h->c.shock_capturing) {
     SensorArgs s = sensor_args(h, Uin);
-    AXJ_CUDA(h, launch_sensor(s, h->stream));
+    AXJ_CUDA(h, launch_sensor(s, false, h->side, h->stream));
   }
-  StageArgs a = stage_args(h, Uin, Uout, stage);
-  AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, h->ntiles_gen, h->tiles_gen, h->stream));
-  return AXJ_OK;
+  return launch_stage_kernels(h, Uin, Uout, stage);
 }
 
 // ComputeTimeStep on the device; with advance != 0 the kernel also performs
@@ -280,6 +383,7 @@ int check_flags(axj_handle* h) {
   int f = 0;
   AXJ_CUDA(h, cudaMemcpyAsync(&f, h->flags, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (f & 4) return fail(h, AXJ_ERR_TIMEOUT, "a bounded wait on a TMA transfer gave up");
   if (f & 2) return fail(h, AXJ_ERR_DT_BLOWUP, "Time step blow up (every point blanked, dt == 100)");
   if (f & 1) return fail(h, AXJ_ERR_NONFINITE, "non-finite value in the solution or time step");
   return AXJ_OK;
@@ -394,6 +498,10 @@ void axj_destroy(axj_handle* h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   for (void* p : h->allocs) cudaFree(p);
+  if (h->side.stream) cudaStreamSynchronize(h->side.stream);
+  if (h->side.fork) cudaEventDestroy(h->side.fork);
+  if (h->side.join) cudaEventDestroy(h->side.join);
+  if (h->side.stream) cudaStreamDestroy(h->side.stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -556,6 +664,9 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
       desc[(size_t)(j - 1) * h->P + (i - 1)] = make_desc(zr, rw, ibval[x] == 0.0, f);
     }
   if (faces.size() >= (1u << 20)) { delete h; return fail(nullptr, AXJ_ERR_BADPATCH, "too many face points"); }
+  std::vector<unsigned char> zcode(desc.size());
+  for (size_t x = 0; x < desc.size(); ++x)
+    zcode[x] = (unsigned char)(desc_blank(desc[x]) ? ROW_NONE : (uint32_t)desc_zrow(desc[x]));
 
   // ---- tile classes
   std::vector<int2> tint, tgen, sti, stg;
@@ -568,13 +679,22 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
           uint32_t d = dsc(i, j);
           if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d) || desc_face(d) != 0) interior = false;
         }
+      // r-halo points on the tile columns: dV/dz there feeds the mixed derivatives, and
+      // the r filter of the coefficients runs there with the centred row
       for (int64_t j = j0 - H_INT; interior && j < j0 + TR + H_INT; ++j) {
         if (j >= j0 && j < j0 + TR) continue;
         for (int64_t i = i0; interior && i < i0 + TZ; ++i) {
           uint32_t d = dsc(i, j);
-          if (desc_zrow(d) != 4 || desc_blank(d)) interior = false;
+          if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d)) interior = false;
         }
       }
+      // z-halo points on the tile rows: the r filter of the coefficients
+      for (int64_t j = j0; interior && j < j0 + TR; ++j)
+        for (int64_t i = i0 - H_INT; interior && i < i0 + TZ + H_INT; ++i) {
+          if (i >= i0 && i < i0 + TZ) continue;
+          uint32_t d = dsc(i, j);
+          if (desc_rrow(d) != 4 || desc_blank(d)) interior = false;
+        }
       (interior ? tint : tgen).push_back(make_int2((int)i0, (int)j0));
       // sensor classes: S, T and the dilatation are formed on a cross of halo
       // SENS_HS_INT from V_r, V_z stencils of reach H_INT, so every point within
@@ -597,6 +717,13 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   // ---- device buffers
   cudaError_t ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (ce != cudaSuccess) { delete h; return fail(nullptr, AXJ_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(ce)); }
+  if (cudaStreamCreateWithFlags(&h->side.stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->side.fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->side.join, cudaEventDisableTiming) != cudaSuccess) {
+    g_create_error = "side stream / event creation failed";
+    axj_destroy(h);
+    return AXJ_ERR_CUDA;
+  }
   int rc = AXJ_OK;
   const size_t pl = (size_t)h->plane;
   h->U0 = dalloc<double>(h, 5 * pl, &rc);
@@ -611,6 +738,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     h->Qz = dalloc<double>(h, 3 * pl, &rc);
   }
   h->desc = dalloc<uint32_t>(h, pl, &rc);
+  h->zcode = dalloc<unsigned char>(h, pl, &rc);
   h->faces = dalloc<int>(h, faces.size(), &rc);
   h->dxidz = dalloc<double>(h, Nz, &rc);
   h->ddxidxidz = dalloc<double>(h, Nz, &rc);
@@ -645,6 +773,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     }
   };
   up(h->desc, desc.data(), desc.size() * sizeof(uint32_t));
+  up(h->zcode, zcode.data(), zcode.size());
   up(h->faces, faces.data(), faces.size() * sizeof(int));
   up(h->dxidz, dxidz.data(), Nz * sizeof(double));
   up(h->ddxidxidz, ddxidxidz.data(), Nz * sizeof(double));
@@ -667,6 +796,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     cudaError_t e = init_kernel_attributes();
     if (e != cudaSuccess) rc = fail(h, AXJ_ERR_NODEVICE, "kernel set-up failed (no sm_100a device?): %s", cudaGetErrorString(e));
   }
+  if (rc == AXJ_OK) rc = build_maps(h);
   if (rc == AXJ_OK) {
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) rc = fail(h, AXJ_ERR_CUDA, "set-up: %s", cudaGetErrorString(e));
@@ -825,17 +955,13 @@ int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launch
       if (h->c.shock_capturing) {
         rc = timed(1, [&]() -> int {
           SensorArgs sa = sensor_args(h, bufs[st - 1]);
-          AXJ_CUDA(h, launch_sensor(sa, h->stream));
+          AXJ_CUDA(h, launch_sensor(sa, false, h->side, h->stream));
           return AXJ_OK;
         });
-        nl[1] += 5;
+        nl[1] += (h->nstiles_int > 0) + (h->nstiles_gen > 0) + 1;
       }
       if (rc != AXJ_OK) break;
-      rc = timed(2, [&]() -> int {
-        StageArgs a = stage_args(h, bufs[st - 1], bufs[st], st);
-        AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, h->ntiles_gen, h->tiles_gen, h->stream));
-        return AXJ_OK;
-      });
+      rc = timed(2, [&]() -> int { return launch_stage_kernels(h, bufs[st - 1], bufs[st], st); });
       nl[2] += stage_launches;
     }
     h->iteration += 1;
@@ -892,7 +1018,7 @@ int axj_tgfilter(axj_handle* h, const double* var, int64_t dirn, int64_t inplace
   AXJ_CUDA(h, cudaSetDevice(h->device));
   AXJ_CUDA(h, h2d(h, h->Ub, out, 1));
   if (inplace) {
-    AXJ_CUDA(h, launch_tgfilter_z_inplace(grid_of(h), h->desc, h->Ub, h->Ua, 1, h->stream));
+    AXJ_CUDA(h, launch_tgfilter_z_inplace(grid_of(h), h->desc, h->zcode, h->Ub, h->Ua, 1, h->flags, h->stream));
     AXJ_CUDA(h, d2h(h, out, h->Ua, 1));
   } else {
     AXJ_CUDA(h, h2d(h, h->Ua, var, 1));
@@ -909,7 +1035,7 @@ int axj_sensor(axj_handle* h, const double* pv, double* mustar, double* betastar
   AXJ_CUDA(h, cudaSetDevice(h->device));
   AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
   SensorArgs s = sensor_args(h, h->Ua);
-  AXJ_CUDA(h, launch_sensor(s, h->stream));
+  AXJ_CUDA(h, launch_sensor(s, true, h->side, h->stream));
   AXJ_CUDA(h, d2h(h, mustar, h->star, 1));
   AXJ_CUDA(h, d2h(h, betastar, h->star + h->plane, 1));
   AXJ_CUDA(h, d2h(h, kappastar, h->star + 2 * h->plane, 1));

@@ -92,27 +92,92 @@ __device__ __forceinline__ double d1_p(int row, const double* rho, const double*
 // ---------------------------------------------------------------------------
 // Fused RK-stage kernel.
 // ---------------------------------------------------------------------------
+// ---- TMA / mbarrier helpers (inline PTX, sm_90+ forms valid on sm_100a) ----------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after about a second instead of spinning forever.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 20); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it > 32) __nanosleep(256);
+  }
+  return false;
+}
+// 3-D tiled TMA load (x = z index, y = r index, z = field plane) into shared memory;
+// out-of-range elements are filled with zeros.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
+
 template <int H>
 struct StageSmem {
   static constexpr int HZ = hz_of(H);
   static constexpr int RZ = TZ + 2 * HZ;
   static constexpr int RR = TR + 2 * H;
   static constexpr int NPT = RZ * RR;
-  // doubles: 5 state fields, mu_eff, kappa_eff, 2 dz-derivative fields
-  static constexpr size_t bytes_main = sizeof(double) * (size_t)(7 * NPT + 2 * RR * TZ);
-  static constexpr size_t bytes(bool gen) { return bytes_main + (gen ? sizeof(uint32_t) * NPT : 0); }
+  static constexpr int NTP = TZ * TR;
+  // r reach of the truncated-Gaussian filter rows: 4 for the centred row, 10 for the
+  // 11-point boundary rows (ModTGfilter.f90:31-44)
+  static constexpr int HT = (H == H_INT) ? 4 : 10;
+  static constexpr int RQ = RR + 2 * HT;  // rows of the z-filtered coefficient box
+  // byte offsets: state box [5][RR][RZ]; coefficient box [3][RQ][RZ] holding the
+  // z-filtered quantities on arrival and mu_eff, beta*, kappa_eff (rows HT..HT+RR) after
+  // the r filter (without shock capturing plane 0 rows HT.. hold mu); plain mu on the
+  // tile [TR][TZ]; pv_old tile [5][TR][TZ]; running-sum tile [5][TR][TZ]; dV/dz
+  // [2][RR][TZ]; descriptors [RR][RZ]
+  static constexpr size_t oU = 0;
+  static constexpr size_t oQ = align128(oU + sizeof(double) * 5 * NPT);
+  static constexpr size_t oMu0 = align128(oQ + sizeof(double) * 3 * RQ * RZ);
+  static constexpr size_t oP0 = align128(oMu0 + sizeof(double) * NTP);
+  static constexpr size_t oPA = align128(oP0 + sizeof(double) * 5 * NTP);
+  static constexpr size_t oDz = align128(oPA + sizeof(double) * 5 * NTP);
+  static constexpr size_t oDesc = align128(oDz + sizeof(double) * 2 * RR * TZ);
+  static constexpr size_t bytes(bool gen) { return align128(oDesc + (gen ? sizeof(uint32_t) * NPT : 0)); }
+  static constexpr uint32_t state_bytes = sizeof(double) * 5 * NPT;
+  static constexpr uint32_t q_bytes = sizeof(double) * 3 * RQ * RZ;
+  static constexpr uint32_t tile_bytes = sizeof(double) * 5 * NTP;
+  static constexpr int NPER = (NPT + STAGE_THREADS - 1) / STAGE_THREADS;
 };
 
 template <int H, bool GEN>
-__global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(const StageArgs a, const int2* __restrict__ tiles) {
+__global__ void __launch_bounds__(STAGE_THREADS)
+    stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
+                 const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
+                 const __grid_constant__ CUtensorMap mAcc) {
   using SM = StageSmem<H>;
-  constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* sU = reinterpret_cast<double*>(smem_raw);  // [5][RR][RZ]
-  double* sMu = sU + 5 * NPT;                        // [RR][RZ]
-  double* sKa = sMu + NPT;                           // [RR][RZ]
-  double* sDz = sKa + NPT;                           // [2][RR][TZ]
-  uint32_t* sDesc = reinterpret_cast<uint32_t*>(sDz + 2 * RR * TZ);
+  constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT, NTP = SM::NTP, HT = SM::HT, RQ = SM::RQ;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  double* sU = reinterpret_cast<double*>(smem_raw + SM::oU);      // [5][RR][RZ]
+  double* sQ = reinterpret_cast<double*>(smem_raw + SM::oQ);      // [3][RQ][RZ]
+  double* sMu = sQ + HT * RZ;                                      // [RR][RZ], row stride RZ
+  double* sBe = sQ + RQ * RZ + HT * RZ;
+  double* sKa = a.c.shock_capturing ? sQ + 2 * RQ * RZ + HT * RZ : sMu;
+  double* sMu0 = reinterpret_cast<double*>(smem_raw + SM::oMu0);  // [TR][TZ]
+  double* sP0 = reinterpret_cast<double*>(smem_raw + SM::oP0);    // [5][TR][TZ]
+  double* sPA = reinterpret_cast<double*>(smem_raw + SM::oPA);    // [5][TR][TZ]
+  double* sDz = reinterpret_cast<double*>(smem_raw + SM::oDz);    // [2][RR][TZ]
+  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
 
   const int tid = threadIdx.x;
   const int2 t0 = tiles[blockIdx.x];
@@ -120,36 +185,103 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(const StageArgs a,
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long P = a.g.P, PL = a.g.plane;
   const bool sc = a.c.shock_capturing != 0;
+  // pv_old is needed as a tile in stages 2 and 3 (stage 1 reads it from the state box),
+  // the running sum A in stages 3 and 4
+  const bool needU0 = a.stage == 2 || a.stage == 3;
+  const bool needA = a.stage == 3 || a.stage == 4;
 
-  // ---- phase 1: state + halo -> smem; mu = T**0.666 (AssignValues) on the cross
-  for (int idx = tid; idx < NPT; idx += STAGE_THREADS) {
-    const int rr = idx / RZ, rz = idx - rr * RZ;
-    const int i = i0 - HZ + rz, j = j0 - H + rr;
-    const bool in = (!GEN) || (i >= 0 && i < Nz && j >= 0 && j < Nr);
-    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    uint32_t dsc = make_desc(ROW_NONE, ROW_NONE, false, 0);
-    if (in) {
-      const long long o = (long long)j * P + i;
-#pragma unroll
-      for (int f = 0; f < 5; ++f) v[f] = __ldg(a.Uin + f * PL + o);
-      if (GEN) dsc = __ldg(a.desc + o);
+  // ---- phase 1: one thread issues the TMA loads; the RK operands complete on the
+  // second barrier while phases 1-2 run
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&bar[0], SM::state_bytes + (sc ? SM::q_bytes : 0u));
+    tma_load_3d(sU, &mState, i0 - HZ, j0 - H, 0, &bar[0]);
+    if (sc) tma_load_3d(sQ, &mQ, i0 - HZ, j0 - H - HT, 0, &bar[0]);
+    if (needU0 || needA) {
+      mbar_expect_tx(&bar[1], (needU0 ? SM::tile_bytes : 0u) + (needA ? SM::tile_bytes : 0u));
+      if (needU0) tma_load_3d(sP0, &mU0, i0, j0, 0, &bar[1]);
+      if (needA) tma_load_3d(sPA, &mAcc, i0, j0, 0, &bar[1]);
     }
+  }
+  if (GEN) {
+    for (int idx = tid; idx < NPT; idx += STAGE_THREADS) {
+      const int rr = idx / RZ, rz = idx - rr * RZ;
+      const int i = i0 - HZ + rz, j = j0 - H + rr;
+      sDesc[idx] = (i >= 0 && i < Nz && j >= 0 && j < Nr) ? __ldg(a.desc + (long long)j * P + i)
+                                                            : make_desc(ROW_NONE, ROW_NONE, false, 0);
+    }
+  }
+  if (!__syncthreads_and(mbar_wait_bounded(&bar[0], 0))) {
+    if (tid == 0) atomicOr(a.flags, 4);
+    return;
+  }
+  // mu = T**0.666 (AssignValues) on the cross of the region. With shock capturing the
+  // coefficient box holds the z-filtered quantities; the r filter PerformTGfilter(q, 2,
+  // star) (ModShockCapturing.f90:65,71,77), the C*Re(*Pr) scaling and the z ramp
+  // (:66-92) give mu*, beta*, kappa*, and mu_eff = mu + mu*, kappa_eff = mu + kappa*
+  // (UpdateTransportCoeffs :248-251). The results overwrite the box only after every
+  // thread has read its filter windows. Zero-filled points outside the block give
+  // mu = 0, as the never-written halo does; blanked points keep mu* = 0.
+  {
+    double vmu[SM::NPER], vbe[SM::NPER], vka[SM::NPER];
 #pragma unroll
-    for (int f = 0; f < 5; ++f) sU[f * NPT + idx] = v[f];
-    if (GEN) sDesc[idx] = dsc;
-    const bool cross = (rr >= H && rr < H + TR && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
-    double mu = 0.0, ka = 0.0;
-    if (in && cross) {
-      mu = pow(v[4], 0.666);
-      ka = mu;
+    for (int k = 0; k < SM::NPER; ++k) {
+      const int idx = tid + k * STAGE_THREADS;
+      vmu[k] = vbe[k] = vka[k] = 0.0;
+      if (idx >= NPT) continue;
+      const int rr = idx / RZ, rz = idx - rr * RZ;
+      const bool cross = (rr >= H && rr < H + TR && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
+      if (!cross) continue;
+      const double mu = pow(sU[4 * NPT + idx], 0.666);
+      vmu[k] = mu;
+      if (rr >= H && rr < H + TR && rz >= HZ && rz < HZ + TZ) sMu0[(rr - H) * TZ + (rz - HZ)] = mu;
       if (sc) {
-        const long long o = (long long)j * P + i;
-        mu = mu + __ldg(a.mustar + o);
-        ka = ka + __ldg(a.kappastar + o);
+        int rw = 4;
+        if (GEN) {
+          const uint32_t dsc = sDesc[idx];
+          rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
+          const int i = i0 - HZ + rz, j = j0 - H + rr;
+          if (!(i >= 0 && i < Nz && j >= 0 && j < Nr)) rw = (int)ROW_NONE;
+        }
+        double f[3] = {0.0, 0.0, 0.0};
+        if (rw < 9) {
+          const int w0 = GEN ? tg_w0(rw) : -4;
+          const int n = GEN ? tg_len(rw) : 9;
+          const int rowc = GEN ? rw : 4;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            const double* col = sQ + q * RQ * RZ + (rr + HT + w0) * RZ + rz;
+            double s = cTG[rowc][0] * col[0];
+            for (int m = 1; m < n; ++m) s = s + cTG[rowc][m] * col[m * RZ];
+            f[q] = s;
+          }
+        }
+        const int i = i0 - HZ + rz;
+        const double ramp = (i >= 0 && i < Nz) ? __ldg(a.ramp + i) : 0.0;
+        vmu[k] = mu + a.c.C_mu_Re * f[0] * ramp;
+        vbe[k] = a.c.C_beta_Re * f[1] * ramp;
+        vka[k] = mu + a.c.C_kappa_Re_Pr * f[2] * ramp;
       }
     }
-    sMu[idx] = mu;
-    sKa[idx] = ka;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < SM::NPER; ++k) {
+      const int idx = tid + k * STAGE_THREADS;
+      if (idx >= NPT) continue;
+      const int rr = idx / RZ, rz = idx - rr * RZ;
+      const bool cross = (rr >= H && rr < H + TR && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
+      if (!cross) continue;
+      sMu[idx] = vmu[k];
+      if (sc) {
+        sBe[idx] = vbe[k];
+        sKa[idx] = vka[k];
+      }
+    }
   }
   __syncthreads();
 
@@ -177,6 +309,12 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(const StageArgs a,
   __syncthreads();
 
   // ---- phase 3: one point per thread per pass
+  if (needU0 || needA) {
+    if (!__syncthreads_and(mbar_wait_bounded(&bar[1], 0))) {
+      if (tid == 0) atomicOr(a.flags, 4);
+      return;
+    }
+  }
   const double dtv = a.stage > 0 ? *a.dt : 0.0;
   for (int pidx = tid; pidx < TZ * TR; pidx += STAGE_THREADS) {
     const int r = pidx / TZ, c = pidx - r * TZ;
@@ -243,9 +381,9 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(const StageArgs a,
     {
       // lambda = beta - 2/3 mu with beta = 0.6 mu (+ betastar), ModAssign.f90:22-23,
       // ModShockCapturing.f90:248-251
-      const double mu0 = sc ? pow(q.T, 0.666) : q.mu;
+      const double mu0 = sMu0[r * TZ + c];
       double beta = (3.0 / 5.0) * mu0;
-      if (sc) beta = beta + __ldg(a.betastar + go);
+      if (sc) beta = beta + sBe[sidx];
       q.lambda = beta - (2.0 / 3.0) * q.mu;
     }
     const double rloc = __ldg(a.rc + j), zloc = __ldg(a.zc + i);
@@ -255,9 +393,14 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(const StageArgs a,
       rhs_inviscid(q, d, rloc, a.c.gam, rhs);
       if (a.c.do_viscous) rhs_viscous(q, d, rloc, a.c.gam, a.c.Re, a.c.Pr, sc, rhs);
     }
-    double tg[5];
+    // pv_target is read only where a term uses it: sponges, face operations, forcing
+    const bool need_tg = (rloc >= a.c.sponge_start_top) || (!j1 && zloc <= a.c.sponge_end_left) ||
+                         a.c.control_forcing || (GEN && face);
+    double tg[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (need_tg) {
 #pragma unroll
-    for (int f = 0; f < 5; ++f) tg[f] = __ldg(a.target + f * PL + go);
+      for (int f = 0; f < 5; ++f) tg[f] = __ldg(a.target + f * PL + go);
+    }
     const double pv[5] = {q.rho, q.Vr, q.Vt, q.Vz, q.T};
     if (a.c.control_forcing) control_forcing(zloc, rloc, a.c, a.forcing, pv, tg, rhs);
     if (GEN && face) {
@@ -276,25 +419,26 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(const StageArgs a,
     }
     // ---- RK4 stage update (ModRungeKutta.f90:32-51, :134-146)
     const double c6 = 1.0 / 6.0, c3 = 1.0 / 3.0;
+    const int tp = r * TZ + c;  // index in the tile boxes
     double un[5];
 #pragma unroll
     for (int f = 0; f < 5; ++f) {
       const double k = mul_rn(dtv, rhs[f]);
       const long long o = f * PL + go;
       if (a.stage == 1) {
-        const double u0 = __ldg(a.U0 + o);
+        const double u0 = pv[f];  // pv_old = stage-1 input
         un[f] = add_rn(u0, mul_rn(0.5, k));
         a.A[o] = add_rn(u0, mul_rn(c6, k));
       } else if (a.stage == 2) {
-        const double u0 = __ldg(a.U0 + o);
+        const double u0 = sP0[f * NTP + tp];
         un[f] = add_rn(u0, mul_rn(0.5, k));
         a.B[o] = k;
       } else if (a.stage == 3) {
-        const double u0 = __ldg(a.U0 + o);
+        const double u0 = sP0[f * NTP + tp];
         un[f] = add_rn(u0, k);
-        a.A[o] = add_rn(a.A[o], mul_rn(c3, add_rn(a.B[o], k)));
+        a.A[o] = add_rn(sPA[f * NTP + tp], mul_rn(c3, add_rn(__ldg(a.B + o), k)));
       } else {
-        un[f] = blank ? pv[f] : add_rn(a.A[o], mul_rn(c6, k));
+        un[f] = blank ? pv[f] : add_rn(sPA[f * NTP + tp], mul_rn(c6, k));
       }
     }
     if (j1) {
@@ -318,18 +462,47 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel(const StageArgs a,
 }
 
 template <int H, bool GEN>
-static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* tiles, cudaStream_t s) {
+static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* tiles, const StageMaps& m,
+                                  cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
   const size_t sm = StageSmem<H>::bytes(GEN);
-  stage_kernel<H, GEN><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles);
+  stage_kernel<H, GEN><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
   return cudaGetLastError();
 }
 
-cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, int ntiles_gen,
-                         const int2* tiles_gen, cudaStream_t s) {
-  cudaError_t e = launch_stage_t<H_GEN, true>(a, ntiles_gen, tiles_gen, s);
+// The general tiles (few, heavy, one CTA per SM) run on a side stream next to the
+// interior tiles so that they fill SMs the interior launch leaves idle.
+static cudaError_t fork(const SideStream& side, cudaStream_t s) {
+  if (!side.stream) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(side.fork, s);
   if (e != cudaSuccess) return e;
-  return launch_stage_t<H_INT, false>(a, ntiles_int, tiles_int, s);
+  return cudaStreamWaitEvent(side.stream, side.fork, 0);
+}
+static cudaError_t join(const SideStream& side, cudaStream_t s) {
+  if (!side.stream) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(side.join, side.stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamWaitEvent(s, side.join, 0);
+}
+
+cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, const StageMaps& mint,
+                         int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen, const SideStream& side,
+                         cudaStream_t s) {
+  cudaError_t e = fork(side, s);
+  if (e != cudaSuccess) return e;
+  e = launch_stage_t<H_GEN, true>(a, ntiles_gen, tiles_gen, mgen, side.stream ? side.stream : s);
+  if (e != cudaSuccess) return e;
+  e = launch_stage_t<H_INT, false>(a, ntiles_int, tiles_int, mint, s);
+  if (e != cudaSuccess) return e;
+  return join(side, s);
+}
+
+void stage_boxes(bool gen, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h) {
+  *halo_w = gen ? StageSmem<H_GEN>::RZ : StageSmem<H_INT>::RZ;
+  *halo_h = gen ? StageSmem<H_GEN>::RR : StageSmem<H_INT>::RR;
+  *q_h = gen ? StageSmem<H_GEN>::RQ : StageSmem<H_INT>::RQ;
+  *tile_w = TZ;
+  *tile_h = TR;
 }
 
 // ---------------------------------------------------------------------------
@@ -448,27 +621,40 @@ struct SensSmem {
   static constexpr int SZ = TZ + 2 * HS, SR = TR + 2 * HS, NS = SZ * SR;
   static constexpr int DZ = TZ + 2 * HF;      // z-arm of the second derivatives: [TR][DZ]
   static constexpr int DR = TR + 2 * HF;      // r-arm: [DR][TZ]
-  static constexpr size_t bytes(bool gen) {
-    return sizeof(double) * (size_t)(2 * NV + 3 * NS + TR * DZ + DR * TZ + TR * TZ) +
-           (gen ? sizeof(uint32_t) * NV : 0);
-  }
+  // byte offsets (every TMA destination 128-byte aligned): V_r, V_z [VR][VZ] each;
+  // T [SR][SZ] (TMA); S and dil [SR][SZ]; rho on the tile [TR][TZ] (TMA); arms; f_sw;
+  // descriptors
+  static constexpr size_t oVr = 0;
+  static constexpr size_t oVz = align128(sizeof(double) * NV);
+  static constexpr size_t oT = align128(oVz + sizeof(double) * NV);
+  static constexpr size_t oS = align128(oT + sizeof(double) * NS);
+  static constexpr size_t oD = align128(oS + sizeof(double) * NS);
+  static constexpr size_t oRho = align128(oD + sizeof(double) * NS);
+  static constexpr size_t oD2 = align128(oRho + sizeof(double) * TR * TZ);
+  static constexpr size_t oDesc = align128(oD2 + sizeof(double) * (TR * DZ + DR * TZ + TR * TZ));
+  static constexpr size_t bytes(bool gen) { return align128(oDesc + (gen ? sizeof(uint32_t) * NV : 0)); }
+  static constexpr uint32_t tx_bytes = sizeof(double) * (2 * NV + NS + TR * TZ);
 };
 
 template <int HS, int HF, bool GEN>
-__global__ void __launch_bounds__(STAGE_THREADS) sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles) {
+__global__ void __launch_bounds__(STAGE_THREADS)
+    sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mV,
+                       const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
   using SM = SensSmem<HS, HF>;
   constexpr int HV = SM::HV, HVZ = SM::HVZ, VZ = SM::VZ, NV = SM::NV;
   constexpr int SZ = SM::SZ, NS = SM::NS, DZ = SM::DZ, DR = SM::DR;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* sVr = reinterpret_cast<double*>(smem_raw);  // [VR][VZ]
-  double* sVz = sVr + NV;
-  double* sS = sVz + NV;                               // [SR][SZ] x 3: S, T, dil
-  double* sT = sS + NS;
-  double* sD = sT + NS;
-  double* sd2z = sD + NS;                              // [TR][DZ]
-  double* sd2r = sd2z + TR * DZ;                       // [DR][TZ]
-  double* sFsw = sd2r + DR * TZ;                       // [TR][TZ]
-  uint32_t* sDesc = reinterpret_cast<uint32_t*>(sFsw + TR * TZ);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  double* sVr = reinterpret_cast<double*>(smem_raw + SM::oVr);   // [VR][VZ]
+  double* sVz = reinterpret_cast<double*>(smem_raw + SM::oVz);   // [VR][VZ]
+  double* sT = reinterpret_cast<double*>(smem_raw + SM::oT);     // [SR][SZ]
+  double* sS = reinterpret_cast<double*>(smem_raw + SM::oS);     // [SR][SZ]
+  double* sD = reinterpret_cast<double*>(smem_raw + SM::oD);     // [SR][SZ]
+  double* sRho = reinterpret_cast<double*>(smem_raw + SM::oRho); // [TR][TZ]
+  double* sd2z = reinterpret_cast<double*>(smem_raw + SM::oD2);  // [TR][DZ]
+  double* sd2r = sd2z + TR * DZ;                                 // [DR][TZ]
+  double* sFsw = sd2r + DR * TZ;                                 // [TR][TZ]
+  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
 
   const int tid = threadIdx.x;
   const int2 t0 = tiles[blockIdx.x];
@@ -478,28 +664,31 @@ __global__ void __launch_bounds__(STAGE_THREADS) sensor_tile_kernel(const Sensor
   auto inside = [&](int i, int j) { return i >= 0 && i < Nz && j >= 0 && j < Nr; };
   auto vdesc = [&](int vidx) -> uint32_t { return GEN ? sDesc[vidx] : make_desc(4, 4, false, 0); };
 
-  // ---- phase 1: V_r, V_z (+ descriptors) on the V region, T on the S region
-  for (int idx = tid; idx < NV; idx += STAGE_THREADS) {
-    const int vr = idx / VZ, vz = idx - vr * VZ;
-    const int i = i0 - HVZ + vz, j = j0 - HV + vr;
-    double a1 = 0.0, a3 = 0.0;
-    uint32_t dsc = make_desc(ROW_NONE, ROW_NONE, false, 0);
-    if (!GEN || inside(i, j)) {
-      const long long o = (long long)j * g.P + i;
-      a1 = __ldg(a.U + 1 * g.plane + o);
-      a3 = __ldg(a.U + 3 * g.plane + o);
-      if (GEN) dsc = __ldg(a.desc + o);
-    }
-    sVr[idx] = a1;
-    sVz[idx] = a3;
-    if (GEN) sDesc[idx] = dsc;
-  }
-  for (int idx = tid; idx < NS; idx += STAGE_THREADS) {
-    const int sr = idx / SZ, sz = idx - sr * SZ;
-    const int i = i0 - HS + sz, j = j0 - HS + sr;
-    sT[idx] = (!GEN || inside(i, j)) ? __ldg(a.U + 4 * g.plane + (long long)j * g.P + i) : 0.0;
+  // ---- phase 1: V_r, V_z on the V region, T on the S region and rho on the tile by
+  // TMA (zero outside the block), descriptors by plain loads meanwhile
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
   }
   __syncthreads();
+  if (tid == 0) {
+    mbar_expect_tx(&bar, SM::tx_bytes);
+    tma_load_3d(sVr, &mV, i0 - HVZ, j0 - HV, 1, &bar);
+    tma_load_3d(sVz, &mV, i0 - HVZ, j0 - HV, 3, &bar);
+    tma_load_3d(sT, &mT, i0 - HS, j0 - HS, 4, &bar);
+    tma_load_3d(sRho, &mRho, i0, j0, 0, &bar);
+  }
+  if (GEN) {
+    for (int idx = tid; idx < NV; idx += STAGE_THREADS) {
+      const int vr = idx / VZ, vz = idx - vr * VZ;
+      const int i = i0 - HVZ + vz, j = j0 - HV + vr;
+      sDesc[idx] = inside(i, j) ? __ldg(a.desc + (long long)j * g.P + i) : make_desc(ROW_NONE, ROW_NONE, false, 0);
+    }
+  }
+  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0))) {
+    if (tid == 0) atomicOr(a.flags, 4);
+    return;
+  }
 
   // ---- phase 2: S and dilatation on the cross of the S region; f_sw on the tile
   for (int idx = tid; idx < NS; idx += STAGE_THREADS) {
@@ -596,7 +785,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) sensor_tile_kernel(const Sensor
     if (GEN && !inside(i, j)) continue;
     const long long o = (long long)j * g.P + i;
     const double dz = __ldg(a.dz + i), dr = __ldg(a.dr + j);
-    const double rho = __ldg(a.U + o);
+    const double rho = sRho[r * TZ + c];
     const double T = sT[(HS + r) * SZ + HS + c];
     const double fsw = sFsw[r * TZ + c];
     a.Q[o] = rho * fabs((d4z[0][q] * (dz * dz) + d4r[0][q] * (dr * dr)));
@@ -681,102 +870,208 @@ __global__ void sensor_rfilter_kernel(const SensorArgs a) {
   }
 }
 
-cudaError_t launch_sensor(const SensorArgs& a, cudaStream_t s) {
+cudaError_t launch_sensor(const SensorArgs& a, bool rfilter, const SideStream& side, cudaStream_t s) {
   const long long n = (long long)a.g.Nz * a.g.Nr;
   const int bs = 256;
   const int nb = (int)((n + bs - 1) / bs);
+  cudaError_t e = fork(side, s);
+  if (e != cudaSuccess) return e;
   if (a.ntiles_gen > 0)
     sensor_tile_kernel<SENS_HS_GEN, H_GEN, true>
-        <<<a.ntiles_gen, STAGE_THREADS, SensSmem<SENS_HS_GEN, H_GEN>::bytes(true), s>>>(a, a.tiles_gen);
+        <<<a.ntiles_gen, STAGE_THREADS, SensSmem<SENS_HS_GEN, H_GEN>::bytes(true), side.stream ? side.stream : s>>>(
+            a, a.tiles_gen, *a.mv_gen, *a.mt_gen, *a.mrho);
   if (a.ntiles_int > 0)
     sensor_tile_kernel<SENS_HS_INT, H_INT, false>
-        <<<a.ntiles_int, STAGE_THREADS, SensSmem<SENS_HS_INT, H_INT>::bytes(false), s>>>(a, a.tiles_int);
-  cudaError_t e = launch_tgfilter_z_inplace(a.g, a.desc, a.Q, a.Qz, 3, s);
+        <<<a.ntiles_int, STAGE_THREADS, SensSmem<SENS_HS_INT, H_INT>::bytes(false), s>>>(a, a.tiles_int, *a.mv_int, *a.mt_int,
+                                                                                     *a.mrho);
+  e = join(side, s);
   if (e != cudaSuccess) return e;
-  sensor_rfilter_kernel<<<nb, bs, 0, s>>>(a);
+  e = launch_tgfilter_z_inplace(a.g, a.desc, a.zcode, a.Q, a.Qz, 3, a.flags, s);
+  if (e != cudaSuccess) return e;
+  if (rfilter) sensor_rfilter_kernel<<<nb, bs, 0, s>>>(a);  // the stage kernel applies it on the fly
   return cudaGetLastError();
 }
 
-// Row-staged version of the same recurrence: one CTA per (row, field); the row of
-// unfiltered values and the z row codes sit in shared memory, each thread owns a
-// chunk of ZR_L points (odd, so lanes read shared memory without bank conflicts) and
-// keeps the last 10 filtered values in registers. Rows up to ZR_MAXNZ points.
-constexpr int ZR_L = 33;
-constexpr int ZR_W = 48;
-constexpr int ZR_MAXNZ = 12288;
+// Row-staged version of the same recurrence: one CTA per (row, field). The row of
+// unfiltered values and its z row codes are bulk-copied into shared memory with ZR_PADL
+// zeros (row code 4) on the left and ZR_PADR on the right, the never-written halo of
+// the reference; each thread owns a chunk of ZR_L points (odd: lanes read shared
+// memory without bank conflicts) and runs ZR_STEPS = ZR_W + ZR_L steps of the
+// recurrence, storing the last ZR_L. Left of a chunk's window it starts from
+// unfiltered values; for the first chunks that window begins inside the zero pad, so
+// they are exact. Chunks whose window holds only centred rows take an unrolled path
+// with the last 10 filtered values in a statically renamed register ring.
+constexpr int ZR_L = 31;
+constexpr int ZR_W = 49;
+constexpr int ZR_STEPS = ZR_L + ZR_W;  // 80 = 8 x 10
+constexpr int ZR_PADL = 64;            // >= ZR_W + 10, a multiple of 16 doubles
+constexpr int ZR_PADR = 48;            // >= ZR_L + 4 - 1: the unrolled path reads up to i+4 past the row
+constexpr int ZR_MAXNZ = 10240;  // the staged row, its output, codes and rings fit in 227 KB
 
-// One output of the recurrence for TG row ROW at point i. p[k] = filtered value at
-// i-k (or the unfiltered value / 0 left of the chunk's start), xs = unfiltered row.
+// One output of the recurrence for TG row ROW at point i (xs indexed with the pad).
+// p[k] = filtered value at i-k, xs = unfiltered row.
 template <int ROW>
-__device__ __forceinline__ double zr_apply(const double (&p)[11], const double* __restrict__ xs, int i, int Nz) {
+__device__ __forceinline__ double zr_apply(const double (&p)[11], const double* __restrict__ xs, int i) {
   constexpr int W0 = ROW < 4 ? -ROW : (ROW == 4 ? -4 : -2 - ROW);
   constexpr int N = ROW == 4 ? 9 : 11;
   double s = 0.0;
 #pragma unroll
   for (int m = 0; m < N; ++m) {
     const int o = W0 + m;
-    double v;
-    if (o < 0) v = p[o < 0 ? -o : 0];
-    else v = (i + o < Nz) ? xs[i + o] : 0.0;
+    const double v = (o < 0) ? p[o < 0 ? -o : 0] : xs[i + o];
     s = (m == 0) ? cTG[ROW][0] * v : s + cTG[ROW][m] * v;
   }
   return s;
 }
 
-__global__ void tgfilter_z_rows_kernel(const Grid g, const uint32_t* __restrict__ desc,
-                                       const double* __restrict__ q, double* __restrict__ out) {
-  extern __shared__ __align__(16) unsigned char zr_smem[];
-  const int Nz = g.Nz;
-  double* xs = reinterpret_cast<double*>(zr_smem);
-  double* ys = xs + Nz;
-  unsigned char* rs = reinterpret_cast<unsigned char*>(ys + Nz);
+// Bulk (non-tensor) global -> shared copy completing on an mbarrier; both addresses
+// 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__host__ __device__ constexpr int zr_pad(int nz) { return (nz + 15) & ~15; }
+__host__ __device__ constexpr int zr_xlen(int nz) { return ZR_PADL + zr_pad(nz) + ZR_PADR; }
+
+__global__ void tgfilter_z_rows_kernel(const Grid g, const unsigned char* __restrict__ zcode,
+                                       const double* __restrict__ q, double* __restrict__ out, int* flags) {
+  extern __shared__ __align__(128) unsigned char zr_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  const int Nz = g.Nz, P = (int)g.P;
+  const int nchunk = (Nz + ZR_L - 1) / ZR_L;
+  double* xs = reinterpret_cast<double*>(zr_smem);       // [ZR_PADL + Nz + pad]
+  unsigned char* rs = reinterpret_cast<unsigned char*>(xs + zr_xlen(Nz));  // [ZR_PADL + P + ZR_PADR]
+  unsigned char* gen = rs + ZR_PADL + P + ZR_PADR;       // [nchunk]: window holds a non-centred row
+  double* ring_s = reinterpret_cast<double*>(                                // [10][blockDim]
+      zr_smem + ((sizeof(double) * (size_t)zr_xlen(Nz) + ZR_PADL + P + ZR_PADR + nchunk + 15) & ~(size_t)15));
   const int j = blockIdx.x, f = blockIdx.y;
   const double* x = q + (long long)f * g.plane + (long long)j * g.P;
   double* y = out + (long long)f * g.plane + (long long)j * g.P;
-  const uint32_t* dr = desc + (long long)j * g.P;
-  for (int i = threadIdx.x; i < Nz; i += blockDim.x) {
-    xs[i] = __ldg(x + i);
-    rs[i] = (unsigned char)row_of(__ldg(dr + i), 1);
+  // the row of Q and its z stencil codes arrive by two bulk copies
+  const uint32_t xbytes = (uint32_t)(Nz / 2) * 16u;
+  const uint32_t rbytes = (uint32_t)P;  // P is a multiple of 32
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
   }
   __syncthreads();
-  const int nchunk = (Nz + ZR_L - 1) / ZR_L;
-  for (int c = threadIdx.x; c < nchunk; c += blockDim.x) {
-    const int ib = c * ZR_L, ie = min(Nz, ib + ZR_L), is = max(0, ib - ZR_W);
-    double p[11];
-    p[0] = 0.0;
-#pragma unroll
-    for (int k = 1; k <= 10; ++k) p[k] = (is - k >= 0) ? xs[is - k] : 0.0;
-    for (int i = is; i < ie; ++i) {
-      double v;
-      switch (rs[i]) {
-        case 4: v = zr_apply<4>(p, xs, i, Nz); break;
-        case 0: v = zr_apply<0>(p, xs, i, Nz); break;
-        case 1: v = zr_apply<1>(p, xs, i, Nz); break;
-        case 2: v = zr_apply<2>(p, xs, i, Nz); break;
-        case 3: v = zr_apply<3>(p, xs, i, Nz); break;
-        case 5: v = zr_apply<5>(p, xs, i, Nz); break;
-        case 6: v = zr_apply<6>(p, xs, i, Nz); break;
-        case 7: v = zr_apply<7>(p, xs, i, Nz); break;
-        case 8: v = zr_apply<8>(p, xs, i, Nz); break;
-        default: v = xs[i]; break;  // blanked / no row: left unchanged in place
-      }
-#pragma unroll
-      for (int k = 10; k >= 2; --k) p[k] = p[k - 1];
-      p[1] = v;
-      if (i >= ib) ys[i] = v;
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&bar, xbytes + rbytes);
+    bulk_g2s(xs + ZR_PADL, x, xbytes, &bar);
+    bulk_g2s(rs + ZR_PADL, zcode + (long long)j * g.P, rbytes, &bar);
+  }
+  // pads (disjoint from the bulk destinations)
+  for (int k = threadIdx.x; k < ZR_PADL; k += blockDim.x) {
+    xs[k] = 0.0;
+    rs[k] = 4;
+  }
+  for (int k = ZR_PADL + 2 * (Nz / 2) + threadIdx.x; k < zr_xlen(Nz); k += blockDim.x) xs[k] = 0.0;
+  for (int k = threadIdx.x; k < ZR_PADR; k += blockDim.x) rs[ZR_PADL + P + k] = 4;
+  for (int k = threadIdx.x; k < nchunk; k += blockDim.x) gen[k] = 0;
+  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0))) {
+    if (threadIdx.x == 0) atomicOr(flags, 4);
+    return;
+  }
+  if ((Nz & 1) && threadIdx.x == 0) xs[ZR_PADL + Nz - 1] = __ldg(x + Nz - 1);
+  // positions past Nz are not part of the row: treat them as centred (their outputs
+  // are never stored and only feed later, also unstored, positions)
+  for (int k = Nz + threadIdx.x; k < P; k += blockDim.x) rs[ZR_PADL + k] = 4;
+  __syncthreads();
+  // mark chunks whose window [c*L - W, c*L + L) contains a non-centred row
+  for (int i = threadIdx.x; i < Nz; i += blockDim.x) {
+    if (rs[ZR_PADL + i] != 4) {
+      const int c0 = max(0, (i - ZR_L + 1 + ZR_L - 1) / ZR_L), c1 = min(nchunk - 1, (i + ZR_W) / ZR_L);
+      for (int c = c0; c <= c1; ++c) gen[c] = 1;
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < Nz; i += blockDim.x) y[i] = ys[i];
+  const double* X = xs + ZR_PADL;  // X[i], i in [-ZR_PADL, Nz + pad)
+  const unsigned char* R = rs + ZR_PADL;
+  const double t0 = cTG[4][0], t1 = cTG[4][1], t2 = cTG[4][2], t3 = cTG[4][3], t4 = cTG[4][4];
+  const double t5 = cTG[4][5], t6 = cTG[4][6], t7 = cTG[4][7], t8 = cTG[4][8];
+  for (int c = threadIdx.x; c < nchunk; c += blockDim.x) {
+    const int ib = c * ZR_L, is = ib - ZR_W;
+    if (!gen[c]) {
+      double ring[10];
+#pragma unroll
+      for (int m = 1; m <= 10; ++m) ring[10 - m] = X[is - m];
+#pragma unroll
+      for (int s = 0; s < ZR_STEPS; ++s) {
+        const int i = is + s;
+        const double* xp = X + i;
+        // the feed-forward terms and the older feedback terms first, the newest
+        // filtered value last: one FMA of latency per step on the recurrence (the
+        // reference sums left to right; the two orders differ by rounding only)
+        const double ff = t4 * xp[0] + t5 * xp[1] + t6 * xp[2] + t7 * xp[3] + t8 * xp[4];
+        const double fb = t0 * ring[(s + 6) % 10] + t1 * ring[(s + 7) % 10] + t2 * ring[(s + 8) % 10];
+        const double v = (ff + fb) + t3 * ring[(s + 9) % 10];
+        ring[s % 10] = v;
+        if (s >= ZR_W && i < Nz) y[i] = v;
+      }
+    } else {
+      // general rows: the last 10 filtered values live in a per-thread ring in shared
+      // memory (slot = position mod 10, interleaved across threads). A window that
+      // begins in the left pad starts exactly at i = 0 from the zero halo.
+      const int bd = blockDim.x;
+      double* rg = ring_s + threadIdx.x;
+      const int i0c = max(is, 0);
+      const int ie = min(Nz, ib + ZR_L);
+      for (int k = 1; k <= 10; ++k) rg[((i0c - k + 1000) % 10) * bd] = X[i0c - k];
+      int slot = (i0c + 1000) % 10;
+      for (int i = i0c; i < ie; ++i) {
+        const int row = R[i];
+        double v;
+        if (row == 4) {
+          int s4 = slot - 4, s3 = slot - 3, s2 = slot - 2, s1 = slot - 1;
+          s4 += s4 < 0 ? 10 : 0;
+          s3 += s3 < 0 ? 10 : 0;
+          s2 += s2 < 0 ? 10 : 0;
+          s1 += s1 < 0 ? 10 : 0;
+          v = t0 * rg[s4 * bd] + t1 * rg[s3 * bd] + t2 * rg[s2 * bd] + t3 * rg[s1 * bd] + t4 * X[i] + t5 * X[i + 1] +
+              t6 * X[i + 2] + t7 * X[i + 3] + t8 * X[i + 4];
+        } else if (row < 9) {
+          const int w0 = tg_w0(row), n = tg_len(row);
+          double s = 0.0;
+          for (int m = 0; m < n; ++m) {
+            const int o = w0 + m;
+            double val;
+            if (o < 0) {
+              int sl = slot + o;
+              sl += sl < 0 ? 10 : 0;
+              val = rg[sl * bd];
+            } else {
+              val = X[i + o];
+            }
+            s = (m == 0) ? cTG[row][0] * val : s + cTG[row][m] * val;
+          }
+          v = s;
+        } else {
+          v = X[i];  // blanked / no row: left unchanged in place
+        }
+        rg[slot * bd] = v;
+        slot = (slot == 9) ? 0 : slot + 1;
+        if (i >= ib) y[i] = v;
+      }
+    }
+  }
 }
 
-cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const double* q, double* out, int nfield,
-                                      cudaStream_t s) {
+static size_t zr_smem_bytes(int Nz, long long P) {
+  const int nchunk = (Nz + ZR_L - 1) / ZR_L;
+  const int bs = std::min(1024, (nchunk + 31) / 32 * 32);
+  const size_t head = sizeof(double) * (size_t)zr_xlen(Nz) + (size_t)(ZR_PADL + P + ZR_PADR) + nchunk;
+  return ((head + 15) & ~(size_t)15) + sizeof(double) * 10 * (size_t)bs;
+}
+
+cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const unsigned char* zcode, const double* q,
+                                      double* out, int nfield, int* flags, cudaStream_t s) {
   if (g.Nz <= ZR_MAXNZ) {
-    const size_t sm = (size_t)g.Nz * (2 * sizeof(double) + 1);
     const int nchunk = (g.Nz + ZR_L - 1) / ZR_L;
     const int bs = std::min(1024, (nchunk + 31) / 32 * 32);
-    tgfilter_z_rows_kernel<<<dim3(g.Nr, nfield), bs, sm, s>>>(g, desc, q, out);
+    tgfilter_z_rows_kernel<<<dim3(g.Nr, nfield), bs, zr_smem_bytes(g.Nz, g.P), s>>>(g, zcode, q, out, flags);
     return cudaGetLastError();
   }
   const int nchunk = (g.Nz + ZF_CHUNK - 1) / ZF_CHUNK;
@@ -848,6 +1143,13 @@ cudaError_t launch_tgfilter(const Grid& g, const uint32_t* desc, const double* v
 
 namespace axj {
 
+void sensor_boxes(bool gen, int* vw, int* vh, int* tw, int* th) {
+  *vw = gen ? SensSmem<SENS_HS_GEN, H_GEN>::VZ : SensSmem<SENS_HS_INT, H_INT>::VZ;
+  *vh = gen ? SensSmem<SENS_HS_GEN, H_GEN>::VR : SensSmem<SENS_HS_INT, H_INT>::VR;
+  *tw = gen ? SensSmem<SENS_HS_GEN, H_GEN>::SZ : SensSmem<SENS_HS_INT, H_INT>::SZ;
+  *th = gen ? SensSmem<SENS_HS_GEN, H_GEN>::SR : SensSmem<SENS_HS_INT, H_INT>::SR;
+}
+
 // Opt-in shared-memory sizes; called once per handle at creation (outside any
 // stream capture).
 cudaError_t init_kernel_attributes() {
@@ -864,7 +1166,7 @@ cudaError_t init_kernel_attributes() {
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SensSmem<SENS_HS_INT, H_INT>::bytes(false));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(tgfilter_z_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)((size_t)ZR_MAXNZ * (2 * sizeof(double) + 1)));
+                              (int)zr_smem_bytes(ZR_MAXNZ, ZR_MAXNZ + 32));
 }
 
 }  // namespace axj

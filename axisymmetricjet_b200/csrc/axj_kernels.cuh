@@ -2,11 +2,22 @@
 // C-ABI layer (axj_api.cu) and the kernels (axj_kernels.cu).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the encoding call is resolved at run time)
 #include <cuda_runtime.h>
 
 #include "axj_common.cuh"
 
 namespace axj {
+
+// TMA descriptors of one fused-stage launch: the stage input with its halo box for
+// the tile class, the shock-capturing coefficient planes with the same box, and
+// the tile-sized boxes of pv_old and the running RK sum.
+struct StageMaps {
+  const CUtensorMap* state;
+  const CUtensorMap* star;
+  const CUtensorMap* u0;
+  const CUtensorMap* acc;
+};
 
 // Device view of one solver instance.
 struct Grid {
@@ -37,6 +48,7 @@ struct StageArgs {
   const double* zc;
   const double* rc;
   const double* forcing;  // 25 doubles, row-major F(eqn,k)
+  const double* ramp;     // shock-capturing z ramp (1+tanh(5(z-10)))/2
   const double* dt;       // device dt (read by stages 1-4)
   double* staleT;         // stage 4: T(i*, j*) of its input, the next ComputeTimeStep's stale T
   int* flags;             // bit 0: non-finite value produced
@@ -76,6 +88,13 @@ struct SensorArgs {
   const int2* tiles_int; // sensor tile classes: centred rows within reach 6 of the tile
   const int2* tiles_gen; // everything else (closure rows, blanked points, domain edges)
   int ntiles_int, ntiles_gen;
+  const CUtensorMap* mv_int;   // TMA maps of the stage input for the two sensor tile classes:
+  const CUtensorMap* mv_gen;   //   V_r / V_z boxes,
+  const CUtensorMap* mt_int;   //   temperature boxes,
+  const CUtensorMap* mt_gen;
+  const CUtensorMap* mrho;     //   and the density tile box
+  const unsigned char* zcode;  // z stencil code per point (9 = blanked), pitch P
+  int* flags;
   double* Q;             // 3 planes: mustarQuantity, betastarQuantity, kappastarQuantity
   double* Qz;            // 3 planes: Q after the in-place z filter
   double* star;          // 3 planes: mustar, betastar, kappastar
@@ -86,18 +105,36 @@ cudaError_t init_kernel_attributes();
 void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const double tg[9][11],
                    const PatchDev* patches, int npatch, cudaStream_t s);
 
-cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, int ntiles_gen,
-                         const int2* tiles_gen, cudaStream_t s);
+// Optional side stream for the general-tile launches (stream == null: one stream).
+struct SideStream {
+  cudaStream_t stream;
+  cudaEvent_t fork, join;
+};
+
+cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, const StageMaps& mint,
+                         int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen, const SideStream& side,
+                         cudaStream_t s);
+
+// Box sizes (doubles) the stage kernel expects in its tensor maps: state halo box
+// halo_w x halo_h, z-filtered coefficient box halo_w x q_h, tile box tile_w x tile_h.
+void stage_boxes(bool gen, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h);
+// Boxes (doubles, one plane deep) the sensor tile kernel expects for the stage input:
+// V_r / V_z box vw x vh, temperature box tw x th (rho uses the stage tile box).
+void sensor_boxes(bool gen, int* vw, int* vh, int* tw, int* th);
 cudaError_t launch_dt(const DtArgs& a, int nblocks, cudaStream_t s);
-cudaError_t launch_sensor(const SensorArgs& a, cudaStream_t s);
+// rfilter: also run the r filter into a.star (the stage kernel applies it itself; the
+// unit entry point axj_sensor needs the coefficients as output).
+cudaError_t launch_sensor(const SensorArgs& a, bool rfilter, const SideStream& side, cudaStream_t s);
 
 // Unit entry points (one operator on one field, host-facing).
 cudaError_t launch_deriv(const Grid& g, const uint32_t* desc, const double* var, const double* first,
                          const double* met, const double* met2, int dirn, int order, double* out, cudaStream_t s);
 cudaError_t launch_tgfilter(const Grid& g, const uint32_t* desc, const double* var, int dirn, double* out,
                             cudaStream_t s);
-cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const double* q, double* out,
-                                      int nfield, cudaStream_t s);
+// In-place z filter of nfield planes (q -> out). zcode: per-point z row code bytes
+// (9 = no filtering: blanked), pitch P; flags bit 2 is set if a bounded wait gives up.
+cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const unsigned char* zcode,
+                                      const double* q, double* out, int nfield, int* flags, cudaStream_t s);
 
 constexpr int DT_THREADS = 256;
 
