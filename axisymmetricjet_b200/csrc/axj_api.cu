@@ -391,6 +391,11 @@ int check_flags(axj_handle* h) {
 
 }  // namespace
 
+namespace axj {
+// Message returned by axj_last_error(NULL) (used by entry points without a handle).
+void set_global_error(const char* msg) { g_create_error = msg; }
+}  // namespace axj
+
 extern "C" {
 
 void axj_default_params(axj_params* p) {

@@ -138,4 +138,7 @@ cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const
 
 constexpr int DT_THREADS = 256;
 
+// Sets the message axj_last_error(NULL) returns.
+void set_global_error(const char* msg);
+
 }  // namespace axj

@@ -188,6 +188,30 @@ int axj_tgfilter(axj_handle* h, const double* var, int64_t dirn, int64_t inplace
 int axj_sensor(axj_handle* h, const double* pv, double* mustar, double* betastar,
                double* kappastar);
 
+/* ComputeTimeStep for callers that cannot allocate device memory. This entry point has
+ * no counterpart in the reference. The handle-based calls above allocate their buffers
+ * with cudaMalloc in axj_create; a host whose device memory is owned by someone else (a
+ * framework's caching allocator, a Fortran host passing its own device arrays, a process
+ * that may not grow its device footprint after start-up) cannot use them. This call
+ * allocates nothing: the caller passes every array, already on the device, and the
+ * reduction's scratch (per-block minima and a counter) lives in a fixed array inside the
+ * library, which every GPU that loads the library holds (about 512 KB) until exit.
+ *   d_pv     5 planes (rho, V_r, V_theta, V_z, T) of Nr rows, row pitch `pitch` doubles
+ *   d_dxidz  Nz values of dxi/dz, d_detadr Nr values of deta/dr (ComputeMetric's 1-D metrics)
+ *   d_ibval  Nz x Nr (pitch `pitch`) blanking values, or NULL for no blanked points
+ *   params   CFL, Re, Pr and dt_mode are read; stale_T is the module scalar T used when
+ *            dt_mode is AXJ_DT_REFERENCE
+ *   d_dt     receives dt on the device (100 if every point is blanked, NaN if any point
+ *            gives a non-finite dt); stream is a cudaStream_t (NULL: legacy default stream)
+ * At most 16,777,216 points (Nz*Nr); larger grids return AXJ_ERR_ARG with a message in
+ * axj_last_error(NULL). The call is asynchronous on `stream`. The first call on a device
+ * looks up the scratch array's device address with that device current; make that first
+ * call before any stream capture. Calls share the scratch, so calls that overlap on the
+ * GPU (different streams, no ordering) race with each other. */
+int axj_compute_dt_noalloc(const double* d_pv, int64_t pitch, int64_t Nz, int64_t Nr, const double* d_dxidz,
+                           const double* d_detadr, const double* d_ibval, const axj_params* params, double stale_T,
+                           double* d_dt, void* stream);
+
 /* Last error message of the handle (or of the last failed axj_create if h is NULL). */
 const char* axj_last_error(const axj_handle* h);
 
