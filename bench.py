@@ -168,6 +168,22 @@ def run_reference(args):
     return 0
 
 
+def reduce_max(x, world, device):
+    """Max of a per-rank time over all ranks (the device time of the slowest replica)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(npts, steps, world, ms_max):
+    """Whole-job updates/s: every rank advances its own jet of npts points."""
+    return world * npts * steps / (ms_max / 1e3)
+
+
 def workload_config(name, c):
     p = c["params"]
     return {"workload": f"{name}: axisymmetric jet Nz={c['Nz']} x Nr={c['Nr']}, M_j={c['Mj']}, Re={p.Re:g}, "
@@ -209,11 +225,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, world, "cuda")
 
     c = fixtures.case(args.case, seed=12345 + rank)
     c["params"].device = local
@@ -232,7 +244,7 @@ def main():
     barrier()
     clk = clocks.stop()
     ms_max = max_over_ranks(ms)
-    value = world * npts * args.steps / (ms_max / 1e3)
+    value = replica_throughput(npts, args.steps, world, ms_max)
 
     # per-kernel breakdown (same kernels launched one group at a time with CUDA events)
     prof_steps = max(1, args.profile_steps)
