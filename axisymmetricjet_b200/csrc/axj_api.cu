@@ -40,6 +40,10 @@ struct axj_handle {
   std::vector<void*> allocs;
   // state and RK4 work buffers (5 planes each)
   double *U0 = nullptr, *Ua = nullptr, *Ub = nullptr, *A = nullptr, *B = nullptr, *target = nullptr;
+  // mixed precision: the intermediate stage states as FP32 planes (pitch P) in the
+  // memory of Ua / Ub, which the unit entry points use as FP64 scratch
+  float *Uaf = nullptr, *Ubf = nullptr;
+  bool mixed = false;
   // shock-capturing buffers
   double *Q = nullptr, *Qz = nullptr, *star = nullptr;
   int2 *stiles_int = nullptr, *stiles_gen = nullptr;  // sensor tile classes
@@ -62,15 +66,30 @@ struct axj_handle {
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   std::vector<double> host_out;  // output-callback staging
-  // TMA descriptors: stage-input halo boxes for U0/Ua/Ub x {interior, general} tiles,
-  // coefficient halo boxes, and tile boxes of pv_old and the running sum A
-  CUtensorMap map_state[3][2];
+  // TMA descriptors: stage-input halo boxes for the stage buffers x {interior, general}
+  // tiles, coefficient halo boxes, and tile boxes of pv_old and the running sum A
+  CUtensorMap map_state[5][2];
   CUtensorMap map_star[2];
   CUtensorMap map_u0_tile, map_acc_tile;
-  CUtensorMap map_sens[3][2];  // sensor V boxes of U0/Ua/Ub x {interior, general}
-  CUtensorMap map_sensT[3][2]; // sensor temperature boxes
-  CUtensorMap map_rho[3];      // density tile boxes
+  CUtensorMap map_sens[5][2];  // sensor V boxes of the stage buffers x {interior, general}
+  CUtensorMap map_sensT[5][2]; // sensor temperature boxes
+  CUtensorMap map_rho[5];      // density tile boxes
 };
+
+namespace {
+// Stage buffers by id: U0, Ua, Ub in FP64; Ua, Ub as FP32 planes (mixed path only).
+enum { BU0 = 0, BUA = 1, BUB = 2, BUAF = 3, BUBF = 4, NBUF = 5 };
+inline bool buf_f32(int b) { return b >= BUAF; }
+inline void* buf_ptr(axj_handle* h, int b) {
+  switch (b) {
+    case BU0: return h->U0;
+    case BUA: return h->Ua;
+    case BUB: return h->Ub;
+    case BUAF: return h->Uaf;
+    default: return h->Ubf;
+  }
+}
+}  // namespace
 
 namespace {
 
@@ -188,11 +207,10 @@ cudaError_t d2h(axj_handle* h, double* dst, const double* src, int nf) {
                            (size_t)h->Nz * sizeof(double), (size_t)h->Nr * nf, cudaMemcpyDeviceToHost, h->stream);
 }
 
-SensorArgs sensor_args(axj_handle* h, const double* U) {
+SensorArgs sensor_args(axj_handle* h, int b) {
   SensorArgs s;
   s.g = grid_of(h);
-  s.U = U;
-  const int b = U == h->U0 ? 0 : (U == h->Ua ? 1 : 2);
+  s.U = buf_f32(b) ? nullptr : static_cast<const double*>(buf_ptr(h, b));
   s.mv_int = &h->map_sens[b][0];
   s.mv_gen = &h->map_sens[b][1];
   s.mt_int = &h->map_sensT[b][0];
@@ -215,18 +233,21 @@ SensorArgs sensor_args(axj_handle* h, const double* U) {
   s.Q = h->Q;
   s.Qz = h->Qz;
   s.star = h->star;
+  s.mixed = h->mixed;
+  s.in_f32 = buf_f32(b);
   s.c = h->c;
   return s;
 }
 
-StageArgs stage_args(axj_handle* h, const double* Uin, double* Uout, int stage) {
+StageArgs stage_args(axj_handle* h, int bin, int bout, int stage) {
   StageArgs a;
   a.g = grid_of(h);
-  a.Uin = Uin;
+  a.Uin = buf_f32(bin) ? nullptr : static_cast<const double*>(buf_ptr(h, bin));
   a.U0 = h->U0;
   a.A = h->A;
   a.B = h->B;
-  a.Uout = Uout;
+  a.Uout = buf_f32(bout) ? nullptr : static_cast<double*>(buf_ptr(h, bout));
+  a.Uout_f = buf_f32(bout) ? static_cast<float*>(buf_ptr(h, bout)) : nullptr;
   a.target = h->target;
   a.mustar = h->star;
   a.betastar = h->star + h->plane;
@@ -248,6 +269,9 @@ StageArgs stage_args(axj_handle* h, const double* Uin, double* Uout, int stage) 
   a.stage = stage;
   a.iT = h->iT;
   a.jT = h->jT;
+  a.mixed = h->mixed;
+  a.in_f32 = buf_f32(bin);
+  a.out_f32 = buf_f32(bout);
   a.c = h->c;
   return a;
 }
@@ -269,16 +293,18 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// 3-D map over nplanes planes of (Nz, Nr) doubles with pitch P; out-of-range
-// elements of a box read as zero.
-int make_map(axj_handle* h, CUtensorMap* m, const double* base, int nplanes, int bw, int bh, int bp) {
+// 3-D map over nplanes planes of (Nz, Nr) doubles (or floats) with pitch P;
+// out-of-range elements of a box read as zero.
+int make_map(axj_handle* h, CUtensorMap* m, const void* base, int nplanes, int bw, int bh, int bp, bool f32 = false) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return fail(h, AXJ_ERR_NODEVICE, "cuTensorMapEncodeTiled is not available from the driver");
+  const size_t es_bytes = f32 ? sizeof(float) : sizeof(double);
   const cuuint64_t dims[3] = {(cuuint64_t)h->Nz, (cuuint64_t)h->Nr, (cuuint64_t)nplanes};
-  const cuuint64_t strides[2] = {(cuuint64_t)h->P * sizeof(double), (cuuint64_t)h->plane * sizeof(double)};
+  const cuuint64_t strides[2] = {(cuuint64_t)h->P * es_bytes, (cuuint64_t)h->plane * es_bytes};
   const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, (cuuint32_t)bp};
   const cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, es,
+  CUresult r = fn(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                  const_cast<void*>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(h, AXJ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -286,43 +312,38 @@ int make_map(axj_handle* h, CUtensorMap* m, const double* base, int nplanes, int
 }
 
 int build_maps(axj_handle* h) {
-  const double* st[3] = {h->U0, h->Ua, h->Ub};
+  const int nb = h->mixed ? NBUF : BUAF;
   for (int cls = 0; cls < 2; ++cls) {
     int hw, hh, qh, tw, th;
-    stage_boxes(cls == 1, &hw, &hh, &qh, &tw, &th);
-    for (int b = 0; b < 3; ++b) {
-      int rc = make_map(h, &h->map_state[b][cls], st[b], 5, hw, hh, 5);
+    stage_boxes(cls == 1, h->mixed, &hw, &hh, &qh, &tw, &th);
+    for (int b = 0; b < nb; ++b) {
+      int rc = make_map(h, &h->map_state[b][cls], buf_ptr(h, b), 5, hw, hh, 5, buf_f32(b));
       if (rc != AXJ_OK) return rc;
     }
     // z-filtered coefficient quantities (never loaded without shock capturing)
     int rc = make_map(h, &h->map_star[cls], h->Qz ? h->Qz : h->star, 3, hw, qh, 3);
     if (rc != AXJ_OK) return rc;
     int vw, vh, tw2, th2;
-    sensor_boxes(cls == 1, &vw, &vh, &tw2, &th2);
-    for (int b = 0; b < 3; ++b) {
-      rc = make_map(h, &h->map_sens[b][cls], st[b], 5, vw, vh, 1);
+    sensor_boxes(cls == 1, h->mixed, &vw, &vh, &tw2, &th2);
+    for (int b = 0; b < nb; ++b) {
+      rc = make_map(h, &h->map_sens[b][cls], buf_ptr(h, b), 5, vw, vh, 1, buf_f32(b));
       if (rc != AXJ_OK) return rc;
-      rc = make_map(h, &h->map_sensT[b][cls], st[b], 5, tw2, th2, 1);
-      if (rc != AXJ_OK) return rc;
-    }
-  }
-  {
-    int hw, hh, qh, tw, th;
-    stage_boxes(false, &hw, &hh, &qh, &tw, &th);
-    for (int b = 0; b < 3; ++b) {
-      int rc = make_map(h, &h->map_rho[b], st[b], 5, tw, th, 1);
+      rc = make_map(h, &h->map_sensT[b][cls], buf_ptr(h, b), 5, tw2, th2, 1, buf_f32(b));
       if (rc != AXJ_OK) return rc;
     }
   }
   int hw, hh, qh, tw, th;
-  stage_boxes(false, &hw, &hh, &qh, &tw, &th);
+  stage_boxes(false, h->mixed, &hw, &hh, &qh, &tw, &th);
+  for (int b = 0; b < nb; ++b) {
+    int rc = make_map(h, &h->map_rho[b], buf_ptr(h, b), 5, tw, th, 1, buf_f32(b));
+    if (rc != AXJ_OK) return rc;
+  }
   int rc = make_map(h, &h->map_u0_tile, h->U0, 5, tw, th, 5);
   if (rc != AXJ_OK) return rc;
   return make_map(h, &h->map_acc_tile, h->A, 5, tw, th, 5);
 }
 
-StageMaps stage_maps(axj_handle* h, const double* Uin, int cls) {
-  const int b = Uin == h->U0 ? 0 : (Uin == h->Ua ? 1 : 2);
+StageMaps stage_maps(axj_handle* h, int b, int cls) {
   StageMaps m;
   m.state = &h->map_state[b][cls];
   m.star = &h->map_star[cls];
@@ -331,21 +352,27 @@ StageMaps stage_maps(axj_handle* h, const double* Uin, int cls) {
   return m;
 }
 
-int launch_stage_kernels(axj_handle* h, const double* Uin, double* Uout, int stage) {
-  StageArgs a = stage_args(h, Uin, Uout, stage);
-  StageMaps mi = stage_maps(h, Uin, 0), mg = stage_maps(h, Uin, 1);
+int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage) {
+  StageArgs a = stage_args(h, bin, bout, stage);
+  StageMaps mi = stage_maps(h, bin, 0), mg = stage_maps(h, bin, 1);
   AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, mi, h->ntiles_gen, h->tiles_gen, mg, h->side, h->stream));
   return AXJ_OK;
 }
 
 // One RK stage: the sensor chain on the stage input (if enabled), then the fused
 // stage kernel over both tile classes.
-int enqueue_stage(axj_handle* h, const double* Uin, double* Uout, int stage) {
+int enqueue_stage(axj_handle* h, int bin, int bout, int stage) {
   if (h->c.shock_capturing) {
-    SensorArgs s = sensor_args(h, Uin);
+    SensorArgs s = sensor_args(h, bin);
     AXJ_CUDA(h, launch_sensor(s, false, h->side, h->stream));
   }
-  return launch_stage_kernels(h, Uin, Uout, stage);
+  return launch_stage_kernels(h, bin, bout, stage);
+}
+
+// Stage input/output buffers of RK4: U0 -> Ua -> Ub -> Ua -> U0 (FP32 Ua, Ub when mixed).
+void rk4_buffers(const axj_handle* h, int b[5]) {
+  const int a = h->mixed ? BUAF : BUA, c = h->mixed ? BUBF : BUB;
+  b[0] = BU0; b[1] = a; b[2] = c; b[3] = a; b[4] = BU0;
 }
 
 // ComputeTimeStep on the device; with advance != 0 the kernel also performs
@@ -369,13 +396,14 @@ int enqueue_dt(axj_handle* h, int advance) {
   return AXJ_OK;
 }
 
-// RK4 (ModRungeKutta.f90:5-171) on the device dt: U0 -> Ua -> Ub -> Ua -> U0.
+// RK4 (ModRungeKutta.f90:5-171) on the device dt.
 int enqueue_rk4(axj_handle* h) {
-  int rc;
-  if ((rc = enqueue_stage(h, h->U0, h->Ua, 1)) != AXJ_OK) return rc;
-  if ((rc = enqueue_stage(h, h->Ua, h->Ub, 2)) != AXJ_OK) return rc;
-  if ((rc = enqueue_stage(h, h->Ub, h->Ua, 3)) != AXJ_OK) return rc;
-  if ((rc = enqueue_stage(h, h->Ua, h->U0, 4)) != AXJ_OK) return rc;
+  int b[5];
+  rk4_buffers(h, b);
+  for (int st = 1; st <= 4; ++st) {
+    const int rc = enqueue_stage(h, b[st - 1], b[st], st);
+    if (rc != AXJ_OK) return rc;
+  }
   return AXJ_OK;
 }
 
@@ -425,7 +453,7 @@ void axj_default_params(axj_params* p) {
   p->judge_threshold = 0.1;
 }
 
-const char* axj_version(void) { return "axj 0.1 sm_100a fp64"; }
+const char* axj_version(void) { return "axj 0.2 sm_100a fp64 mixed"; }
 
 int axj_read_bc_file(const char* path, axj_bc_record* rec, int64_t max_records, int64_t* nrecords) {
   if (!path || !nrecords) return fail(nullptr, AXJ_ERR_ARG, "null argument");
@@ -519,7 +547,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   if (Nz < 12 || Nr < 12 || Nz > (1 << 20) || Nr > (1 << 20))
     return fail(nullptr, AXJ_ERR_BADGRID, "grid %lld x %lld outside 12..2^20", (long long)Nz, (long long)Nr);
   if (npatch > MAX_PATCHES) return fail(nullptr, AXJ_ERR_BADPATCH, "more than %d patches", MAX_PATCHES);
-  if (prm->precision != AXJ_FP64) return fail(nullptr, AXJ_ERR_UNSUPPORTED, "precision %lld not built", (long long)prm->precision);
+  if (prm->precision != AXJ_FP64 && prm->precision != AXJ_MIXED)
+    return fail(nullptr, AXJ_ERR_UNSUPPORTED, "precision %lld not built", (long long)prm->precision);
   if (prm->shock_capturing && prm->sensor != AXJ_SENSOR_PLAIN)
     return fail(nullptr, AXJ_ERR_UNSUPPORTED, "sensor %lld not built", (long long)prm->sensor);
   int ndev = 0;
@@ -734,6 +763,11 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->U0 = dalloc<double>(h, 5 * pl, &rc);
   h->Ua = dalloc<double>(h, 5 * pl, &rc);
   h->Ub = dalloc<double>(h, 5 * pl, &rc);
+  h->mixed = prm->precision == AXJ_MIXED;
+  if (h->mixed) {
+    h->Uaf = reinterpret_cast<float*>(h->Ua);
+    h->Ubf = reinterpret_cast<float*>(h->Ub);
+  }
   h->A = dalloc<double>(h, 5 * pl, &rc);
   h->B = dalloc<double>(h, 5 * pl, &rc);
   h->target = dalloc<double>(h, 5 * pl, &rc);
@@ -951,7 +985,8 @@ int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launch
     return AXJ_OK;
   };
   const int stage_launches = (h->ntiles_gen > 0) + (h->ntiles_int > 0);
-  double* bufs[5] = {h->U0, h->Ua, h->Ub, h->Ua, h->U0};
+  int bufs[5];
+  rk4_buffers(h, bufs);
   int rc = AXJ_OK;
   for (int64_t s = 0; s < nsteps && rc == AXJ_OK; ++s) {
     rc = timed(0, [&] { return enqueue_dt(h, 1); });
@@ -987,7 +1022,7 @@ int axj_rhs(axj_handle* h, const double* pv, double* rhs) {
   if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called (the target is needed)");
   AXJ_CUDA(h, cudaSetDevice(h->device));
   AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
-  int rc = enqueue_stage(h, h->Ua, h->Ub, 0);
+  int rc = enqueue_stage(h, BUA, BUB, 0);
   if (rc != AXJ_OK) return rc;
   AXJ_CUDA(h, d2h(h, rhs, h->Ub, 5));
   AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1039,7 +1074,7 @@ int axj_sensor(axj_handle* h, const double* pv, double* mustar, double* betastar
   if (!h->c.shock_capturing) return fail(h, AXJ_ERR_ARG, "handle created with shock_capturing = 0");
   AXJ_CUDA(h, cudaSetDevice(h->device));
   AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
-  SensorArgs s = sensor_args(h, h->Ua);
+  SensorArgs s = sensor_args(h, BUA);
   AXJ_CUDA(h, launch_sensor(s, true, h->side, h->stream));
   AXJ_CUDA(h, d2h(h, mustar, h->star, 1));
   AXJ_CUDA(h, d2h(h, betastar, h->star + h->plane, 1));

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "axj_kernels.cuh"
 #include "axj_point.cuh"
@@ -25,6 +26,8 @@ namespace axj {
 __constant__ double cSBP1[9][6];
 __constant__ double cSBP2[9][6];
 __constant__ double cTG[9][11];
+__constant__ float cSBP1f[9][6];
+__constant__ float cSBP2f[9][6];
 __constant__ PatchDev cPatch[MAX_PATCHES];
 
 void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const double tg[9][11],
@@ -32,6 +35,16 @@ void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const doubl
   cudaMemcpyToSymbolAsync(cSBP1, sbp1, sizeof(double) * 54, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(cSBP2, sbp2, sizeof(double) * 54, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(cTG, tg, sizeof(double) * 99, 0, cudaMemcpyHostToDevice, s);
+  // FP32 copies of the SBP tables for the mixed-precision stencils (static: the
+  // asynchronous copies read them after this function returns)
+  static float f1[9][6], f2[9][6];
+  for (int r = 0; r < 9; ++r)
+    for (int m = 0; m < 6; ++m) {
+      f1[r][m] = (float)sbp1[r][m];
+      f2[r][m] = (float)sbp2[r][m];
+    }
+  cudaMemcpyToSymbolAsync(cSBP1f, f1, sizeof(float) * 54, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(cSBP2f, f2, sizeof(float) * 54, 0, cudaMemcpyHostToDevice, s);
   if (npatch > 0) cudaMemcpyToSymbolAsync(cPatch, patches, sizeof(PatchDev) * npatch, 0, cudaMemcpyHostToDevice, s);
 }
 
@@ -40,53 +53,57 @@ void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const doubl
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
-// Dot product of an SBP row with a window in shared memory (stride in doubles).
-// The sequence starts from the first product, as DOT_PRODUCT's 0 + a1*b1 does.
-template <int N>
-__device__ __forceinline__ double dotc(const double* __restrict__ c, const double* __restrict__ v, int stride) {
-  double s = c[0] * v[0];
+// SBP / TG tables in the arithmetic type of a stencil.
+template <typename R, int TAB>
+__device__ __forceinline__ R tabv(int row, int m);
+template <> __device__ __forceinline__ double tabv<double, 1>(int row, int m) { return cSBP1[row][m]; }
+template <> __device__ __forceinline__ double tabv<double, 2>(int row, int m) { return cSBP2[row][m]; }
+template <> __device__ __forceinline__ float tabv<float, 1>(int row, int m) { return cSBP1f[row][m]; }
+template <> __device__ __forceinline__ float tabv<float, 2>(int row, int m) { return cSBP2f[row][m]; }
+
+// Dot product of SBP row `row` of table TAB with N values at v (stride in elements),
+// evaluated in type R. The sequence starts from the first product, as DOT_PRODUCT's
+// 0 + a1*b1 does.
+template <typename R, int TAB, int N, typename S>
+__device__ __forceinline__ R dotc(int row, const S* __restrict__ v, int stride) {
+  R s = tabv<R, TAB>(row, 0) * R(v[0]);
 #pragma unroll
-  for (int m = 1; m < N; ++m) s = s + c[m] * v[m * stride];
+  for (int m = 1; m < N; ++m) s = s + tabv<R, TAB>(row, m) * R(v[m * stride]);
   return s;
 }
 
-// Derivative stencil of SBP row `row` (0..8; 9 = none) at p (pointer to the point's
-// own value), stride 1 along z or the smem row length along r.
-__device__ __forceinline__ double sbp_row_apply(const double (*tab)[6], int row, const double* p, int stride) {
-  if (row == 4) return dotc<5>(tab[4], p - 2 * stride, stride);
-  if (row >= 9) return 0.0;
-  const int w0 = sbp_w0(row);
-  return dotc<6>(tab[row], p + w0 * stride, stride);
+// Derivative stencil of table TAB with row code `row` (0..8; 9 = none) at p (pointer
+// to the point's own value), stride 1 along z or the row length along r. Interior
+// tiles (GEN = false) always use the centred row.
+template <typename R, int TAB, bool GEN, typename S>
+__device__ __forceinline__ R dst(int row, const S* p, int stride) {
+  if (!GEN || row == 4) return dotc<R, TAB, 5>(4, p - 2 * stride, stride);
+  if (row >= 9) return R(0);
+  return dotc<R, TAB, 6>(row, p + sbp_w0(row) * stride, stride);
 }
 
-template <bool GEN>
-__device__ __forceinline__ double d1(int row, const double* p, int stride) {
-  if (!GEN) return dotc<5>(cSBP1[4], p - 2 * stride, stride);
-  return sbp_row_apply(cSBP1, row, p, stride);
-}
-template <bool GEN>
-__device__ __forceinline__ double d2(int row, const double* p, int stride) {
-  if (!GEN) return dotc<5>(cSBP2[4], p - 2 * stride, stride);
-  return sbp_row_apply(cSBP2, row, p, stride);
-}
-
-// p = rho*T taps for dp/dz, dp/dr: the reference differentiates pvec = rhovec*Tvec.
-template <bool GEN>
-__device__ __forceinline__ double d1_p(int row, const double* rho, const double* T, int stride) {
-  double v[6];
-  int w0, n;
-  if (!GEN || row == 4) { w0 = -2; n = 5; }
-  else if (row >= 9) return 0.0;
-  else { w0 = sbp_w0(row); n = 6; }
-  const int r = GEN ? row : 4;
-#pragma unroll
-  for (int m = 0; m < 6; ++m)
-    if (m < n) v[m] = rho[(w0 + m) * stride] * T[(w0 + m) * stride];
-  double s = cSBP1[r][0] * v[0];
+// dp/dz, dp/dr: the reference differentiates pvec = rhovec*Tvec, so every tap is a product.
+template <typename R, bool GEN, typename S>
+__device__ __forceinline__ R dst_p(int row, const S* rho, const S* T, int stride) {
+  int w0, n, rw;
+  if (!GEN || row == 4) { w0 = -2; n = 5; rw = 4; }
+  else if (row >= 9) return R(0);
+  else { w0 = sbp_w0(row); n = 6; rw = row; }
+  R s = tabv<R, 1>(rw, 0) * (R(rho[w0 * stride]) * R(T[w0 * stride]));
 #pragma unroll
   for (int m = 1; m < 6; ++m)
-    if (m < n) s = s + cSBP1[r][m] * v[m];
+    if (m < n) s = s + tabv<R, 1>(rw, m) * (R(rho[(w0 + m) * stride]) * R(T[(w0 + m) * stride]));
   return s;
+}
+
+// axis_conditions (ModAxis.f90:14-16): f(1) = -DOT_PRODUCT(SBP1(0,1:5), f(2:6)) / SBP1(0,0),
+// with p pointing at row 2 of a column (stride = row length).
+template <typename S>
+__device__ __forceinline__ double axis_extrap(const S* p, int stride) {
+  double s = cSBP1[0][1] * double(p[0]);
+#pragma unroll
+  for (int m = 1; m < 5; ++m) s = s + cSBP1[0][m + 1] * double(p[m * stride]);
+  return -1.0 * s / cSBP1[0][0];
 }
 
 // ---------------------------------------------------------------------------
@@ -129,9 +146,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 
 constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
 
-template <int H>
+// z halo of a box in elements, rounded up so the box's x coordinate starts on a
+// 16-byte boundary (TMA requirement): even for doubles, a multiple of 4 for floats.
+__host__ __device__ constexpr int hz_t(int h, int esize) { return (h + 16 / esize - 1) / (16 / esize) * (16 / esize); }
+
+// HZ follows the arithmetic type: the mixed path rounds to 4 elements in every stage
+// (valid for its double stage-1 input too), so one coefficient-box map serves all stages.
+template <int H, typename SIN, typename R>
 struct StageSmem {
-  static constexpr int HZ = hz_of(H);
+  static constexpr int HZ = hz_t(H, (int)sizeof(R));
   static constexpr int RZ = TZ + 2 * HZ;
   static constexpr int RR = TR + 2 * H;
   static constexpr int NPT = RZ * RR;
@@ -140,35 +163,45 @@ struct StageSmem {
   // 11-point boundary rows (ModTGfilter.f90:31-44)
   static constexpr int HT = (H == H_INT) ? 4 : 10;
   static constexpr int RQ = RR + 2 * HT;  // rows of the z-filtered coefficient box
-  // byte offsets: state box [5][RR][RZ]; coefficient box [3][RQ][RZ] holding the
-  // z-filtered quantities on arrival and mu_eff, beta*, kappa_eff (rows HT..HT+RR) after
-  // the r filter (without shock capturing plane 0 rows HT.. hold mu); plain mu on the
-  // tile [TR][TZ]; pv_old tile [5][TR][TZ]; running-sum tile [5][TR][TZ]; dV/dz
-  // [2][RR][TZ]; descriptors [RR][RZ]
+  // byte offsets: state box [5][RR][RZ] of the stage-input type; coefficient box
+  // [3][RQ][RZ] (doubles) holding the z-filtered quantities on arrival and mu_eff,
+  // beta*, kappa_eff (rows HT..HT+RR) after the r filter (without shock capturing plane
+  // 0 rows HT.. hold mu); plain mu on the tile [TR][TZ]; pv_old tile [5][TR][TZ];
+  // running-sum tile [5][TR][TZ]; dV/dz [2][RR][TZ] (stencil type); descriptors [RR][RZ]
   static constexpr size_t oU = 0;
-  static constexpr size_t oQ = align128(oU + sizeof(double) * 5 * NPT);
+  static constexpr size_t oQ = align128(oU + sizeof(SIN) * 5 * NPT);
   static constexpr size_t oMu0 = align128(oQ + sizeof(double) * 3 * RQ * RZ);
   static constexpr size_t oP0 = align128(oMu0 + sizeof(double) * NTP);
   static constexpr size_t oPA = align128(oP0 + sizeof(double) * 5 * NTP);
   static constexpr size_t oDz = align128(oPA + sizeof(double) * 5 * NTP);
   static constexpr size_t oDesc = align128(oDz + sizeof(double) * 2 * RR * TZ);
   static constexpr size_t bytes(bool gen) { return align128(oDesc + (gen ? sizeof(uint32_t) * NPT : 0)); }
-  static constexpr uint32_t state_bytes = sizeof(double) * 5 * NPT;
+  static constexpr uint32_t state_bytes = sizeof(SIN) * 5 * NPT;
   static constexpr uint32_t q_bytes = sizeof(double) * 3 * RQ * RZ;
   static constexpr uint32_t tile_bytes = sizeof(double) * 5 * NTP;
   static constexpr int NPER = (NPT + STAGE_THREADS - 1) / STAGE_THREADS;
 };
 
-template <int H, bool GEN>
+template <typename R>
+__device__ __forceinline__ R pow0666(R T);
+template <> __device__ __forceinline__ double pow0666<double>(double T) { return pow(T, 0.666); }
+template <> __device__ __forceinline__ float pow0666<float>(float T) { return powf(T, 0.666f); }
+
+// Fused RK stage. SIN: storage type of the stage input (double, or float for the
+// mixed path's intermediate stages); R: arithmetic type of the stencils and, in
+// interior tiles, of the pointwise terms. General tiles (closure rows, faces, the axis
+// row) evaluate the pointwise terms, face penalties and sponges in double.
+template <int H, bool GEN, typename SIN, typename R>
 __global__ void __launch_bounds__(STAGE_THREADS)
     stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
                  const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
                  const __grid_constant__ CUtensorMap mAcc) {
-  using SM = StageSmem<H>;
+  using SM = StageSmem<H, SIN, R>;
+  using RP = typename std::conditional<GEN, double, R>::type;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT, NTP = SM::NTP, HT = SM::HT, RQ = SM::RQ;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
-  double* sU = reinterpret_cast<double*>(smem_raw + SM::oU);      // [5][RR][RZ]
+  SIN* sU = reinterpret_cast<SIN*>(smem_raw + SM::oU);            // [5][RR][RZ]
   double* sQ = reinterpret_cast<double*>(smem_raw + SM::oQ);      // [3][RQ][RZ]
   double* sMu = sQ + HT * RZ;                                      // [RR][RZ], row stride RZ
   double* sBe = sQ + RQ * RZ + HT * RZ;
@@ -176,7 +209,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   double* sMu0 = reinterpret_cast<double*>(smem_raw + SM::oMu0);  // [TR][TZ]
   double* sP0 = reinterpret_cast<double*>(smem_raw + SM::oP0);    // [5][TR][TZ]
   double* sPA = reinterpret_cast<double*>(smem_raw + SM::oPA);    // [5][TR][TZ]
-  double* sDz = reinterpret_cast<double*>(smem_raw + SM::oDz);    // [2][RR][TZ]
+  R* sDz = reinterpret_cast<R*>(smem_raw + SM::oDz);              // [2][RR][TZ]
   uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
 
   const int tid = threadIdx.x;
@@ -237,7 +270,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       const int rr = idx / RZ, rz = idx - rr * RZ;
       const bool cross = (rr >= H && rr < H + TR && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
       if (!cross) continue;
-      const double mu = pow(sU[4 * NPT + idx], 0.666);
+      const double mu = double(pow0666<R>(R(sU[4 * NPT + idx])));
       vmu[k] = mu;
       if (rr >= H && rr < H + TR && rz >= HZ && rz < HZ + TZ) sMu0[(rr - H) * TZ + (rz - HZ)] = mu;
       if (sc) {
@@ -290,7 +323,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   for (int idx = tid; idx < RR * TZ; idx += STAGE_THREADS) {
     const int rr = idx / TZ, c = idx - rr * TZ;
     const int i = i0 + c, j = j0 - H + rr;
-    double dvr = 0.0, dvz = 0.0;
+    R dvr = R(0), dvz = R(0);
     const bool in = (!GEN) || (i < Nz && j >= 0 && j < Nr);
     if (in) {
       const int sidx = rr * RZ + HZ + c;
@@ -299,9 +332,9 @@ __global__ void __launch_bounds__(STAGE_THREADS)
         const uint32_t dsc = sDesc[sidx];
         row = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
       }
-      const double m = __ldg(a.dxidz + i);
-      dvr = d1<GEN>(row, sU + 1 * NPT + sidx, 1) * m;
-      dvz = d1<GEN>(row, sU + 3 * NPT + sidx, 1) * m;
+      const R m = R(__ldg(a.dxidz + i));
+      dvr = dst<R, 1, GEN>(row, sU + 1 * NPT + sidx, 1) * m;
+      dvz = dst<R, 1, GEN>(row, sU + 3 * NPT + sidx, 1) * m;
     }
     sDz[idx] = dvr;
     sDz[RR * TZ + idx] = dvz;
@@ -332,51 +365,53 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       rw = blank ? (int)ROW_NONE : desc_rrow(dsc);
       face = desc_face(dsc);
     }
-    const double xz = __ldg(a.dxidz + i), xzz = __ldg(a.ddxidxidz + i);
-    const double er = __ldg(a.detadr + j), err = __ldg(a.ddetadetadr + j);
-    const double* pR = sU + 0 * NPT + sidx;
-    const double* pVr = sU + 1 * NPT + sidx;
-    const double* pVt = sU + 2 * NPT + sidx;
-    const double* pVz = sU + 3 * NPT + sidx;
-    const double* pT = sU + 4 * NPT + sidx;
+    const double xzd = __ldg(a.dxidz + i), erd = __ldg(a.detadr + j);
+    const R xz = R(xzd), xzz = R(__ldg(a.ddxidxidz + i));
+    const R er = R(erd), err = R(__ldg(a.ddetadetadr + j));
+    const SIN* pR = sU + 0 * NPT + sidx;
+    const SIN* pVr = sU + 1 * NPT + sidx;
+    const SIN* pVt = sU + 2 * NPT + sidx;
+    const SIN* pVz = sU + 3 * NPT + sidx;
+    const SIN* pT = sU + 4 * NPT + sidx;
     const double* pMu = sMu + sidx;
     const double* pKa = sKa + sidx;
     const int dzi = rr * TZ + c;
 
-    Deriv d;
+    DerivT<R> dr;
     // first derivatives (Compute1stDerivative: stencil, then * metric)
-    d.drhodz = d1<GEN>(zr, pR, 1) * xz;
-    d.dVrdz = sDz[dzi];
-    d.dVtdz = d1<GEN>(zr, pVt, 1) * xz;
-    d.dVzdz = sDz[RR * TZ + dzi];
-    d.dTdz = d1<GEN>(zr, pT, 1) * xz;
-    d.dpdz = d1_p<GEN>(zr, pR, pT, 1) * xz;
-    d.drhodr = d1<GEN>(rw, pR, RZ) * er;
-    d.dVrdr = d1<GEN>(rw, pVr, RZ) * er;
-    d.dVtdr = d1<GEN>(rw, pVt, RZ) * er;
-    d.dVzdr = d1<GEN>(rw, pVz, RZ) * er;
-    d.dTdr = d1<GEN>(rw, pT, RZ) * er;
-    d.dpdr = d1_p<GEN>(rw, pR, pT, RZ) * er;
+    dr.drhodz = dst<R, 1, GEN>(zr, pR, 1) * xz;
+    dr.dVrdz = sDz[dzi];
+    dr.dVtdz = dst<R, 1, GEN>(zr, pVt, 1) * xz;
+    dr.dVzdz = sDz[RR * TZ + dzi];
+    dr.dTdz = dst<R, 1, GEN>(zr, pT, 1) * xz;
+    dr.dpdz = dst_p<R, GEN>(zr, pR, pT, 1) * xz;
+    dr.drhodr = dst<R, 1, GEN>(rw, pR, RZ) * er;
+    dr.dVrdr = dst<R, 1, GEN>(rw, pVr, RZ) * er;
+    dr.dVtdr = dst<R, 1, GEN>(rw, pVt, RZ) * er;
+    dr.dVzdr = dst<R, 1, GEN>(rw, pVz, RZ) * er;
+    dr.dTdr = dst<R, 1, GEN>(rw, pT, RZ) * er;
+    dr.dpdr = dst_p<R, GEN>(rw, pR, pT, RZ) * er;
     // second derivatives (Compute2ndDerivative: out*metric**2 + f'*metric')
-    d.d2Vrdz2 = d2<GEN>(zr, pVr, 1) * (xz * xz) + d.dVrdz * xzz;
-    d.d2Vtdz2 = d2<GEN>(zr, pVt, 1) * (xz * xz) + d.dVtdz * xzz;
-    d.d2Vzdz2 = d2<GEN>(zr, pVz, 1) * (xz * xz) + d.dVzdz * xzz;
-    d.d2Tdz2 = d2<GEN>(zr, pT, 1) * (xz * xz) + d.dTdz * xzz;
-    d.d2Vrdr2 = d2<GEN>(rw, pVr, RZ) * (er * er) + d.dVrdr * err;
-    d.d2Vtdr2 = d2<GEN>(rw, pVt, RZ) * (er * er) + d.dVtdr * err;
-    d.d2Vzdr2 = d2<GEN>(rw, pVz, RZ) * (er * er) + d.dVzdr * err;
-    d.d2Tdr2 = d2<GEN>(rw, pT, RZ) * (er * er) + d.dTdr * err;
-    d.dmudz = d1<GEN>(zr, pMu, 1) * xz;
-    d.dkappadz = sc ? d1<GEN>(zr, pKa, 1) * xz : d.dmudz;
-    d.dmudr = d1<GEN>(rw, pMu, RZ) * er;
-    d.dkappadr = sc ? d1<GEN>(rw, pKa, RZ) * er : d.dmudr;
-    d.d2Vrdzdr = d1<GEN>(rw, sDz + dzi, TZ) * er;
-    d.d2Vzdzdr = d1<GEN>(rw, sDz + RR * TZ + dzi, TZ) * er;
+    dr.d2Vrdz2 = dst<R, 2, GEN>(zr, pVr, 1) * (xz * xz) + dr.dVrdz * xzz;
+    dr.d2Vtdz2 = dst<R, 2, GEN>(zr, pVt, 1) * (xz * xz) + dr.dVtdz * xzz;
+    dr.d2Vzdz2 = dst<R, 2, GEN>(zr, pVz, 1) * (xz * xz) + dr.dVzdz * xzz;
+    dr.d2Tdz2 = dst<R, 2, GEN>(zr, pT, 1) * (xz * xz) + dr.dTdz * xzz;
+    dr.d2Vrdr2 = dst<R, 2, GEN>(rw, pVr, RZ) * (er * er) + dr.dVrdr * err;
+    dr.d2Vtdr2 = dst<R, 2, GEN>(rw, pVt, RZ) * (er * er) + dr.dVtdr * err;
+    dr.d2Vzdr2 = dst<R, 2, GEN>(rw, pVz, RZ) * (er * er) + dr.dVzdr * err;
+    dr.d2Tdr2 = dst<R, 2, GEN>(rw, pT, RZ) * (er * er) + dr.dTdr * err;
+    dr.dmudz = dst<R, 1, GEN>(zr, pMu, 1) * xz;
+    dr.dkappadz = sc ? dst<R, 1, GEN>(zr, pKa, 1) * xz : dr.dmudz;
+    dr.dmudr = dst<R, 1, GEN>(rw, pMu, RZ) * er;
+    dr.dkappadr = sc ? dst<R, 1, GEN>(rw, pKa, RZ) * er : dr.dmudr;
+    dr.d2Vrdzdr = dst<R, 1, GEN>(rw, sDz + dzi, TZ) * er;
+    dr.d2Vzdzdr = dst<R, 1, GEN>(rw, sDz + RR * TZ + dzi, TZ) * er;
 
-    Prim q;
-    q.rho = *pR; q.Vr = *pVr; q.Vt = *pVt; q.Vz = *pVz; q.T = *pT;
-    q.mu = *pMu;
-    q.kappa = *pKa;
+    const double pv[5] = {double(*pR), double(*pVr), double(*pVt), double(*pVz), double(*pT)};
+    PrimT<RP> q;
+    q.rho = RP(*pR); q.Vr = RP(*pVr); q.Vt = RP(*pVt); q.Vz = RP(*pVz); q.T = RP(*pT);
+    q.mu = RP(*pMu);
+    q.kappa = RP(*pKa);
     const long long go = (long long)j * P + i;
     {
       // lambda = beta - 2/3 mu with beta = 0.6 mu (+ betastar), ModAssign.f90:22-23,
@@ -384,14 +419,18 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       const double mu0 = sMu0[r * TZ + c];
       double beta = (3.0 / 5.0) * mu0;
       if (sc) beta = beta + sBe[sidx];
-      q.lambda = beta - (2.0 / 3.0) * q.mu;
+      q.lambda = RP(beta - (2.0 / 3.0) * double(*pMu));
     }
+    const DerivT<RP> d = convert<RP>(dr);
     const double rloc = __ldg(a.rc + j), zloc = __ldg(a.zc + i);
     const bool j1 = (j == 0);
     double rhs[5] = {-0.0, -0.0, -0.0, -0.0, -0.0};
     if (!j1) {
-      rhs_inviscid(q, d, rloc, a.c.gam, rhs);
-      if (a.c.do_viscous) rhs_viscous(q, d, rloc, a.c.gam, a.c.Re, a.c.Pr, sc, rhs);
+      RP rp[5];
+      rhs_inviscid<RP>(q, d, RP(rloc), RP(a.c.gam), rp);
+      if (a.c.do_viscous) rhs_viscous<RP>(q, d, RP(rloc), RP(a.c.gam), RP(a.c.Re), RP(a.c.Pr), sc, rp);
+#pragma unroll
+      for (int f = 0; f < 5; ++f) rhs[f] = double(rp[f]);
     }
     // pv_target is read only where a term uses it: sponges, face operations, forcing
     const bool need_tg = (rloc >= a.c.sponge_start_top) || (!j1 && zloc <= a.c.sponge_end_left) ||
@@ -401,13 +440,14 @@ __global__ void __launch_bounds__(STAGE_THREADS)
 #pragma unroll
       for (int f = 0; f < 5; ++f) tg[f] = __ldg(a.target + f * PL + go);
     }
-    const double pv[5] = {q.rho, q.Vr, q.Vt, q.Vz, q.T};
     if (a.c.control_forcing) control_forcing(zloc, rloc, a.c, a.forcing, pv, tg, rhs);
     if (GEN && face) {
+      const Prim qd = convert<double>(q);
+      const Deriv dd = convert<double>(d);
       const int n = __ldg(a.faces + face);
       for (int k = 0; k < n; ++k) {
         const int pid = __ldg(a.faces + face + 1 + k);
-        face_op(cPatch[pid].bc, cPatch[pid].dir, j1, q, d, tg, xz, er, a.c.gam, rhs);
+        face_op(cPatch[pid].bc, cPatch[pid].dir, j1, qd, dd, tg, xzd, erd, a.c.gam, rhs);
       }
     }
     sponge(zloc, rloc, j1, a.c, pv, tg, rhs);
@@ -417,7 +457,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       for (int f = 0; f < 5; ++f) a.Uout[f * PL + go] = rhs[f];
       continue;
     }
-    // ---- RK4 stage update (ModRungeKutta.f90:32-51, :134-146)
+    // ---- RK4 stage update (ModRungeKutta.f90:32-51, :134-146), always in double
     const double c6 = 1.0 / 6.0, c3 = 1.0 / 3.0;
     const int tp = r * TZ + c;  // index in the tile boxes
     double un[5];
@@ -444,29 +484,33 @@ __global__ void __launch_bounds__(STAGE_THREADS)
     if (j1) {
       // axis_conditions (ModAxis.f90:14-29): rho, V_z, T at j = 1 from rows 2..6 of
       // the stage input (the vectors AssignValues filled before this stage).
-      const double s00 = cSBP1[0][0];
-      un[0] = -1.0 * dotc<5>(&cSBP1[0][1], pR + RZ, RZ) / s00;
-      un[3] = -1.0 * dotc<5>(&cSBP1[0][1], pVz + RZ, RZ) / s00;
-      un[4] = -1.0 * dotc<5>(&cSBP1[0][1], pT + RZ, RZ) / s00;
+      un[0] = axis_extrap(pR + RZ, RZ);
+      un[3] = axis_extrap(pVz + RZ, RZ);
+      un[4] = axis_extrap(pT + RZ, RZ);
     }
+    if (a.out_f32 && a.stage < 4) {
 #pragma unroll
-    for (int f = 0; f < 5; ++f) a.Uout[f * PL + go] = un[f];
+      for (int f = 0; f < 5; ++f) a.Uout_f[f * PL + go] = float(un[f]);
+    } else {
+#pragma unroll
+      for (int f = 0; f < 5; ++f) a.Uout[f * PL + go] = un[f];
+    }
     if (a.stage == 4) {
       bool bad = false;
 #pragma unroll
       for (int f = 0; f < 5; ++f) bad |= !isfinite(un[f]);
       if (bad) atomicOr(a.flags, 1);
-      if (i == a.iT && j == a.jT) *a.staleT = q.T;
+      if (i == a.iT && j == a.jT) *a.staleT = pv[4];
     }
   }
 }
 
-template <int H, bool GEN>
+template <int H, bool GEN, typename SIN, typename R>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* tiles, const StageMaps& m,
                                   cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
-  const size_t sm = StageSmem<H>::bytes(GEN);
-  stage_kernel<H, GEN><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+  const size_t sm = StageSmem<H, SIN, R>::bytes(GEN);
+  stage_kernel<H, GEN, SIN, R><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
   return cudaGetLastError();
 }
 
@@ -485,22 +529,39 @@ static cudaError_t join(const SideStream& side, cudaStream_t s) {
   return cudaStreamWaitEvent(s, side.join, 0);
 }
 
-cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, const StageMaps& mint,
-                         int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen, const SideStream& side,
-                         cudaStream_t s) {
+template <typename SIN, typename R>
+static cudaError_t launch_stage_pair(const StageArgs& a, int ntiles_int, const int2* tiles_int, const StageMaps& mint,
+                                     int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen,
+                                     const SideStream& side, cudaStream_t s) {
   cudaError_t e = fork(side, s);
   if (e != cudaSuccess) return e;
-  e = launch_stage_t<H_GEN, true>(a, ntiles_gen, tiles_gen, mgen, side.stream ? side.stream : s);
+  e = launch_stage_t<H_GEN, true, SIN, R>(a, ntiles_gen, tiles_gen, mgen, side.stream ? side.stream : s);
   if (e != cudaSuccess) return e;
-  e = launch_stage_t<H_INT, false>(a, ntiles_int, tiles_int, mint, s);
+  e = launch_stage_t<H_INT, false, SIN, R>(a, ntiles_int, tiles_int, mint, s);
   if (e != cudaSuccess) return e;
   return join(side, s);
 }
 
-void stage_boxes(bool gen, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h) {
-  *halo_w = gen ? StageSmem<H_GEN>::RZ : StageSmem<H_INT>::RZ;
-  *halo_h = gen ? StageSmem<H_GEN>::RR : StageSmem<H_INT>::RR;
-  *q_h = gen ? StageSmem<H_GEN>::RQ : StageSmem<H_INT>::RQ;
+// FP64 path: double state, double stencils. Mixed path: the stage-1 input is pv_old
+// (double), later inputs are FP32 stage states; stencils in FP32.
+cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, const StageMaps& mint,
+                         int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen, const SideStream& side,
+                         cudaStream_t s) {
+  if (!a.mixed)
+    return launch_stage_pair<double, double>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s);
+  if (!a.in_f32)
+    return launch_stage_pair<double, float>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s);
+  return launch_stage_pair<float, float>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s);
+}
+
+void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h) {
+  if (mixed) {
+    *halo_w = gen ? StageSmem<H_GEN, float, float>::RZ : StageSmem<H_INT, float, float>::RZ;
+  } else {
+    *halo_w = gen ? StageSmem<H_GEN, double, double>::RZ : StageSmem<H_INT, double, double>::RZ;
+  }
+  *halo_h = gen ? StageSmem<H_GEN, double, double>::RR : StageSmem<H_INT, double, double>::RR;
+  *q_h = gen ? StageSmem<H_GEN, double, double>::RQ : StageSmem<H_INT, double, double>::RQ;
   *tile_w = TZ;
   *tile_h = TR;
 }
@@ -613,47 +674,53 @@ __device__ __forceinline__ int row_of(uint32_t dsc, int dirn) {
 // derivatives); the three quantities to be filtered. HS is the halo of S/T/dil
 // (two SBP2 reaches), HF the reach of one stencil (2 interior, 5 with closures).
 // ---------------------------------------------------------------------------
-template <int HS, int HF>
+template <int HS, int HF, typename SIN, typename R>
 struct SensSmem {
   static constexpr int HV = HS + HF;          // halo of V_r, V_z
-  static constexpr int HVZ = hz_of(HV);
+  static constexpr int HVZ = hz_t(HV, (int)sizeof(R));
+  static constexpr int HSZ = hz_t(HS, (int)sizeof(R));  // z halo of the temperature box
   static constexpr int VZ = TZ + 2 * HVZ, VR = TR + 2 * HV, NV = VZ * VR;
-  static constexpr int SZ = TZ + 2 * HS, SR = TR + 2 * HS, NS = SZ * SR;
+  static constexpr int SZ = TZ + 2 * HSZ, SR = TR + 2 * HS, NS = SZ * SR;
   static constexpr int DZ = TZ + 2 * HF;      // z-arm of the second derivatives: [TR][DZ]
   static constexpr int DR = TR + 2 * HF;      // r-arm: [DR][TZ]
   // byte offsets (every TMA destination 128-byte aligned): V_r, V_z [VR][VZ] each;
   // T [SR][SZ] (TMA); S and dil [SR][SZ]; rho on the tile [TR][TZ] (TMA); arms; f_sw;
-  // descriptors
+  // descriptors. V, T, rho are in the stage-input type, the rest in the stencil type.
   static constexpr size_t oVr = 0;
-  static constexpr size_t oVz = align128(sizeof(double) * NV);
-  static constexpr size_t oT = align128(oVz + sizeof(double) * NV);
-  static constexpr size_t oS = align128(oT + sizeof(double) * NS);
-  static constexpr size_t oD = align128(oS + sizeof(double) * NS);
-  static constexpr size_t oRho = align128(oD + sizeof(double) * NS);
-  static constexpr size_t oD2 = align128(oRho + sizeof(double) * TR * TZ);
-  static constexpr size_t oDesc = align128(oD2 + sizeof(double) * (TR * DZ + DR * TZ + TR * TZ));
+  static constexpr size_t oVz = align128(sizeof(SIN) * NV);
+  static constexpr size_t oT = align128(oVz + sizeof(SIN) * NV);
+  static constexpr size_t oS = align128(oT + sizeof(SIN) * NS);
+  static constexpr size_t oD = align128(oS + sizeof(R) * NS);
+  static constexpr size_t oRho = align128(oD + sizeof(R) * NS);
+  static constexpr size_t oD2 = align128(oRho + sizeof(SIN) * TR * TZ);
+  static constexpr size_t oDesc = align128(oD2 + sizeof(R) * (TR * DZ + DR * TZ + TR * TZ));
   static constexpr size_t bytes(bool gen) { return align128(oDesc + (gen ? sizeof(uint32_t) * NV : 0)); }
-  static constexpr uint32_t tx_bytes = sizeof(double) * (2 * NV + NS + TR * TZ);
+  static constexpr uint32_t tx_bytes = sizeof(SIN) * (2 * NV + NS + TR * TZ);
 };
 
-template <int HS, int HF, bool GEN>
+template <typename R>
+__device__ __forceinline__ R sqrt_t(R x) { return sqrt(x); }
+template <>
+__device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
+
+template <int HS, int HF, bool GEN, typename SIN, typename R>
 __global__ void __launch_bounds__(STAGE_THREADS)
     sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mV,
                        const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
-  using SM = SensSmem<HS, HF>;
-  constexpr int HV = SM::HV, HVZ = SM::HVZ, VZ = SM::VZ, NV = SM::NV;
+  using SM = SensSmem<HS, HF, SIN, R>;
+  constexpr int HV = SM::HV, HVZ = SM::HVZ, HSZ = SM::HSZ, VZ = SM::VZ, NV = SM::NV;
   constexpr int SZ = SM::SZ, NS = SM::NS, DZ = SM::DZ, DR = SM::DR;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar;
-  double* sVr = reinterpret_cast<double*>(smem_raw + SM::oVr);   // [VR][VZ]
-  double* sVz = reinterpret_cast<double*>(smem_raw + SM::oVz);   // [VR][VZ]
-  double* sT = reinterpret_cast<double*>(smem_raw + SM::oT);     // [SR][SZ]
-  double* sS = reinterpret_cast<double*>(smem_raw + SM::oS);     // [SR][SZ]
-  double* sD = reinterpret_cast<double*>(smem_raw + SM::oD);     // [SR][SZ]
-  double* sRho = reinterpret_cast<double*>(smem_raw + SM::oRho); // [TR][TZ]
-  double* sd2z = reinterpret_cast<double*>(smem_raw + SM::oD2);  // [TR][DZ]
-  double* sd2r = sd2z + TR * DZ;                                 // [DR][TZ]
-  double* sFsw = sd2r + DR * TZ;                                 // [TR][TZ]
+  SIN* sVr = reinterpret_cast<SIN*>(smem_raw + SM::oVr);   // [VR][VZ]
+  SIN* sVz = reinterpret_cast<SIN*>(smem_raw + SM::oVz);   // [VR][VZ]
+  SIN* sT = reinterpret_cast<SIN*>(smem_raw + SM::oT);     // [SR][SZ]
+  R* sS = reinterpret_cast<R*>(smem_raw + SM::oS);         // [SR][SZ]
+  R* sD = reinterpret_cast<R*>(smem_raw + SM::oD);         // [SR][SZ]
+  SIN* sRho = reinterpret_cast<SIN*>(smem_raw + SM::oRho); // [TR][TZ]
+  R* sd2z = reinterpret_cast<R*>(smem_raw + SM::oD2);      // [TR][DZ]
+  R* sd2r = sd2z + TR * DZ;                                 // [DR][TZ]
+  R* sFsw = sd2r + DR * TZ;                                 // [TR][TZ]
   uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
 
   const int tid = threadIdx.x;
@@ -675,7 +742,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
     mbar_expect_tx(&bar, SM::tx_bytes);
     tma_load_3d(sVr, &mV, i0 - HVZ, j0 - HV, 1, &bar);
     tma_load_3d(sVz, &mV, i0 - HVZ, j0 - HV, 3, &bar);
-    tma_load_3d(sT, &mT, i0 - HS, j0 - HS, 4, &bar);
+    tma_load_3d(sT, &mT, i0 - HSZ, j0 - HS, 4, &bar);
     tma_load_3d(sRho, &mRho, i0, j0, 0, &bar);
   }
   if (GEN) {
@@ -690,37 +757,38 @@ __global__ void __launch_bounds__(STAGE_THREADS)
     return;
   }
 
-  // ---- phase 2: S and dilatation on the cross of the S region; f_sw on the tile
+  // ---- phase 2: S and dilatation on the cross of the S region (reach HS either way);
+  // f_sw on the tile
   for (int idx = tid; idx < NS; idx += STAGE_THREADS) {
     const int sr = idx / SZ, sz = idx - sr * SZ;
-    const bool zarm = sr >= HS && sr < HS + TR;
-    const bool rarm = sz >= HS && sz < HS + TZ;
-    double S = 0.0, dil = 0.0;
-    const int i = i0 - HS + sz, j = j0 - HS + sr;
+    const bool zarm = sr >= HS && sr < HS + TR && sz >= HSZ - HS && sz < HSZ + TZ + HS;
+    const bool rarm = sz >= HSZ && sz < HSZ + TZ;
+    R S = R(0), dil = R(0);
+    const int i = i0 - HSZ + sz, j = j0 - HS + sr;
     if ((zarm || rarm) && (!GEN || inside(i, j))) {
-      const int vidx = (sr + HV - HS) * VZ + (sz + HVZ - HS);
+      const int vidx = (sr + HV - HS) * VZ + (sz + HVZ - HSZ);
       const uint32_t dsc = vdesc(vidx);
       const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
       const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
-      const double xz = __ldg(a.dxidz + i), er = __ldg(a.detadr + j);
-      const double dVrdz = d1<GEN>(zr, sVr + vidx, 1) * xz;
-      const double dVzdz = d1<GEN>(zr, sVz + vidx, 1) * xz;
-      const double dVrdr = d1<GEN>(rw, sVr + vidx, VZ) * er;
-      const double dVzdr = d1<GEN>(rw, sVz + vidx, VZ) * er;
-      const double vr = sVr[vidx];
-      const double r = __ldg(a.rc + j);
-      if (j == 0) dil = 2.0 * dVrdr + dVzdz;
+      const R xz = R(__ldg(a.dxidz + i)), er = R(__ldg(a.detadr + j));
+      const R dVrdz = dst<R, 1, GEN>(zr, sVr + vidx, 1) * xz;
+      const R dVzdz = dst<R, 1, GEN>(zr, sVz + vidx, 1) * xz;
+      const R dVrdr = dst<R, 1, GEN>(rw, sVr + vidx, VZ) * er;
+      const R dVzdr = dst<R, 1, GEN>(rw, sVz + vidx, VZ) * er;
+      const R vr = R(sVr[vidx]);
+      const R r = R(__ldg(a.rc + j));
+      if (j == 0) dil = R(2.0) * dVrdr + dVzdz;
       else dil = dVrdr + vr / r + dVzdz;
-      const double S11 = dVrdr - (1.0 / 3.0) * dil;
-      const double S13 = 0.5 * (dVrdz + dVzdr);
-      const double S33 = dVzdz - (1.0 / 3.0) * dil;
-      const double S22 = (j == 0) ? dVrdr - (1.0 / 3.0) * dil : vr / r - (1.0 / 3.0) * dil;
-      S = sqrt(S11 * S11 + S13 * S13 + S22 * S22 + S13 * S13 + S33 * S33);
+      const R S11 = dVrdr - R(1.0 / 3.0) * dil;
+      const R S13 = R(0.5) * (dVrdz + dVzdr);
+      const R S33 = dVzdz - R(1.0 / 3.0) * dil;
+      const R S22 = (j == 0) ? dVrdr - R(1.0 / 3.0) * dil : vr / r - R(1.0 / 3.0) * dil;
+      S = sqrt_t<R>(S11 * S11 + S13 * S13 + S22 * S22 + S13 * S13 + S33 * S33);
       if (zarm && rarm) {
-        const double vort = fabs(dVrdz - dVzdr);
-        const double Hm = (-1.0 * dil < 0.0) ? 0.0 : 1.0;
-        const double eps = (double)1e-15f;  // single-precision literal of the reference (:202)
-        sFsw[(sr - HS) * TZ + (sz - HS)] = Hm * (dil * dil) / (dil * dil + vort * vort + eps);
+        const R vort = fabs(dVrdz - dVzdr);
+        const R Hm = (R(-1.0) * dil < R(0)) ? R(0) : R(1);
+        const R eps = R((double)1e-15f);  // single-precision literal of the reference (:202)
+        sFsw[(sr - HS) * TZ + (sz - HSZ)] = Hm * (dil * dil) / (dil * dil + vort * vort + eps);
       }
     }
     sS[idx] = S;
@@ -731,33 +799,31 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   // ---- phases 3-4 per field: second derivatives on the arms, fourth derivatives at
   // the tile points (kept in registers: 2 points per thread)
   constexpr int PPT = (TZ * TR) / STAGE_THREADS;
-  double d4z[3][PPT], d4r[3][PPT];
-  const double* srcs[3] = {sS, sT, sD};
+  R d4z[3][PPT], d4r[3][PPT];
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
-    const double* src = srcs[f];
     for (int idx = tid; idx < TR * DZ + DR * TZ; idx += STAGE_THREADS) {
       if (idx < TR * DZ) {
         const int r = idx / DZ, c = idx - r * DZ;  // point (i0 - HF + c, j0 + r)
         const int i = i0 - HF + c, j = j0 + r;
-        double v = 0.0;
+        R v = R(0);
         if (!GEN || inside(i, j)) {
-          const int sidx = (HS + r) * SZ + (HS - HF + c);
+          const int sidx = (HS + r) * SZ + (HSZ - HF + c);
           const uint32_t dsc = vdesc((HV + r) * VZ + (HVZ - HF + c));
           const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
-          v = d2<GEN>(zr, src + sidx, 1);
+          v = f == 1 ? dst<R, 2, GEN>(zr, sT + sidx, 1) : dst<R, 2, GEN>(zr, (f == 0 ? sS : sD) + sidx, 1);
         }
         sd2z[idx] = v;
       } else {
         const int k = idx - TR * DZ;
         const int r = k / TZ, c = k - r * TZ;      // point (i0 + c, j0 - HF + r)
         const int i = i0 + c, j = j0 - HF + r;
-        double v = 0.0;
+        R v = R(0);
         if (!GEN || inside(i, j)) {
-          const int sidx = (HS - HF + r) * SZ + (HS + c);
+          const int sidx = (HS - HF + r) * SZ + (HSZ + c);
           const uint32_t dsc = vdesc((HV - HF + r) * VZ + (HVZ + c));
           const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
-          v = d2<GEN>(rw, src + sidx, SZ);
+          v = f == 1 ? dst<R, 2, GEN>(rw, sT + sidx, SZ) : dst<R, 2, GEN>(rw, (f == 0 ? sS : sD) + sidx, SZ);
         }
         sd2r[k] = v;
       }
@@ -770,8 +836,8 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       const uint32_t dsc = vdesc((HV + r) * VZ + (HVZ + c));
       const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
       const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
-      d4z[f][q] = d2<GEN>(zr, sd2z + r * DZ + HF + c, 1);
-      d4r[f][q] = d2<GEN>(rw, sd2r + (HF + r) * TZ + c, TZ);
+      d4z[f][q] = dst<R, 2, GEN>(zr, sd2z + r * DZ + HF + c, 1);
+      d4r[f][q] = dst<R, 2, GEN>(rw, sd2r + (HF + r) * TZ + c, TZ);
     }
     __syncthreads();
   }
@@ -784,13 +850,13 @@ __global__ void __launch_bounds__(STAGE_THREADS)
     const int i = i0 + c, j = j0 + r;
     if (GEN && !inside(i, j)) continue;
     const long long o = (long long)j * g.P + i;
-    const double dz = __ldg(a.dz + i), dr = __ldg(a.dr + j);
-    const double rho = sRho[r * TZ + c];
-    const double T = sT[(HS + r) * SZ + HS + c];
-    const double fsw = sFsw[r * TZ + c];
-    a.Q[o] = rho * fabs((d4z[0][q] * (dz * dz) + d4r[0][q] * (dr * dr)));
-    a.Q[g.plane + o] = rho * fsw * fabs((d4z[2][q] * (dz * dz) + d4r[2][q] * (dr * dr)));
-    a.Q[2 * g.plane + o] = rho / (a.c.gam * sqrt(T)) * fabs((d4z[1][q] * dz + d4r[1][q] * dr));
+    const R dz = R(__ldg(a.dz + i)), dr = R(__ldg(a.dr + j));
+    const R rho = R(sRho[r * TZ + c]);
+    const R T = R(sT[(HS + r) * SZ + HSZ + c]);
+    const R fsw = sFsw[r * TZ + c];
+    a.Q[o] = double(rho * fabs((d4z[0][q] * (dz * dz) + d4r[0][q] * (dr * dr))));
+    a.Q[g.plane + o] = double(rho * fsw * fabs((d4z[2][q] * (dz * dz) + d4r[2][q] * (dr * dr))));
+    a.Q[2 * g.plane + o] = double(rho / (R(a.c.gam) * sqrt_t<R>(T)) * fabs((d4z[1][q] * dz + d4r[1][q] * dr)));
   }
 }
 
@@ -870,20 +936,28 @@ __global__ void sensor_rfilter_kernel(const SensorArgs a) {
   }
 }
 
+template <typename SIN, typename R>
+static void launch_sensor_tiles(const SensorArgs& a, const SideStream& side, cudaStream_t s) {
+  using SG = SensSmem<SENS_HS_GEN, H_GEN, SIN, R>;
+  using SI = SensSmem<SENS_HS_INT, H_INT, SIN, R>;
+  if (a.ntiles_gen > 0)
+    sensor_tile_kernel<SENS_HS_GEN, H_GEN, true, SIN, R><<<a.ntiles_gen, STAGE_THREADS, SG::bytes(true),
+                                                           side.stream ? side.stream : s>>>(a, a.tiles_gen, *a.mv_gen,
+                                                                                            *a.mt_gen, *a.mrho);
+  if (a.ntiles_int > 0)
+    sensor_tile_kernel<SENS_HS_INT, H_INT, false, SIN, R>
+        <<<a.ntiles_int, STAGE_THREADS, SI::bytes(false), s>>>(a, a.tiles_int, *a.mv_int, *a.mt_int, *a.mrho);
+}
+
 cudaError_t launch_sensor(const SensorArgs& a, bool rfilter, const SideStream& side, cudaStream_t s) {
   const long long n = (long long)a.g.Nz * a.g.Nr;
   const int bs = 256;
   const int nb = (int)((n + bs - 1) / bs);
   cudaError_t e = fork(side, s);
   if (e != cudaSuccess) return e;
-  if (a.ntiles_gen > 0)
-    sensor_tile_kernel<SENS_HS_GEN, H_GEN, true>
-        <<<a.ntiles_gen, STAGE_THREADS, SensSmem<SENS_HS_GEN, H_GEN>::bytes(true), side.stream ? side.stream : s>>>(
-            a, a.tiles_gen, *a.mv_gen, *a.mt_gen, *a.mrho);
-  if (a.ntiles_int > 0)
-    sensor_tile_kernel<SENS_HS_INT, H_INT, false>
-        <<<a.ntiles_int, STAGE_THREADS, SensSmem<SENS_HS_INT, H_INT>::bytes(false), s>>>(a, a.tiles_int, *a.mv_int, *a.mt_int,
-                                                                                     *a.mrho);
+  if (!a.mixed) launch_sensor_tiles<double, double>(a, side, s);
+  else if (!a.in_f32) launch_sensor_tiles<double, float>(a, side, s);
+  else launch_sensor_tiles<float, float>(a, side, s);
   e = join(side, s);
   if (e != cudaSuccess) return e;
   e = launch_tgfilter_z_inplace(a.g, a.desc, a.zcode, a.Q, a.Qz, 3, a.flags, s);
@@ -1143,27 +1217,49 @@ cudaError_t launch_tgfilter(const Grid& g, const uint32_t* desc, const double* v
 
 namespace axj {
 
-void sensor_boxes(bool gen, int* vw, int* vh, int* tw, int* th) {
-  *vw = gen ? SensSmem<SENS_HS_GEN, H_GEN>::VZ : SensSmem<SENS_HS_INT, H_INT>::VZ;
-  *vh = gen ? SensSmem<SENS_HS_GEN, H_GEN>::VR : SensSmem<SENS_HS_INT, H_INT>::VR;
-  *tw = gen ? SensSmem<SENS_HS_GEN, H_GEN>::SZ : SensSmem<SENS_HS_INT, H_INT>::SZ;
-  *th = gen ? SensSmem<SENS_HS_GEN, H_GEN>::SR : SensSmem<SENS_HS_INT, H_INT>::SR;
+void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th) {
+  using GD = SensSmem<SENS_HS_GEN, H_GEN, double, double>;
+  using ID = SensSmem<SENS_HS_INT, H_INT, double, double>;
+  using GF = SensSmem<SENS_HS_GEN, H_GEN, float, float>;
+  using IF = SensSmem<SENS_HS_INT, H_INT, float, float>;
+  if (mixed) {
+    *vw = gen ? GF::VZ : IF::VZ;
+    *vh = gen ? GF::VR : IF::VR;
+    *tw = gen ? GF::SZ : IF::SZ;
+    *th = gen ? GF::SR : IF::SR;
+  } else {
+    *vw = gen ? GD::VZ : ID::VZ;
+    *vh = gen ? GD::VR : ID::VR;
+    *tw = gen ? GD::SZ : ID::SZ;
+    *th = gen ? GD::SR : ID::SR;
+  }
+}
+
+template <int H, bool GEN, typename SIN, typename R>
+static cudaError_t stage_attr() {
+  return cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)StageSmem<H, SIN, R>::bytes(GEN));
+}
+template <int HS, int HF, bool GEN, typename SIN, typename R>
+static cudaError_t sensor_attr() {
+  return cudaFuncSetAttribute(sensor_tile_kernel<HS, HF, GEN, SIN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)SensSmem<HS, HF, SIN, R>::bytes(GEN));
+}
+template <typename SIN, typename R>
+static cudaError_t pair_attrs() {
+  cudaError_t e = stage_attr<H_GEN, true, SIN, R>();
+  if (e == cudaSuccess) e = stage_attr<H_INT, false, SIN, R>();
+  if (e == cudaSuccess) e = sensor_attr<SENS_HS_GEN, H_GEN, true, SIN, R>();
+  if (e == cudaSuccess) e = sensor_attr<SENS_HS_INT, H_INT, false, SIN, R>();
+  return e;
 }
 
 // Opt-in shared-memory sizes; called once per handle at creation (outside any
 // stream capture).
 cudaError_t init_kernel_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<H_GEN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)StageSmem<H_GEN>::bytes(true));
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(stage_kernel<H_INT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)StageSmem<H_INT>::bytes(false));
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(sensor_tile_kernel<SENS_HS_GEN, H_GEN, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)SensSmem<SENS_HS_GEN, H_GEN>::bytes(true));
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(sensor_tile_kernel<SENS_HS_INT, H_INT, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SensSmem<SENS_HS_INT, H_INT>::bytes(false));
+  cudaError_t e = pair_attrs<double, double>();
+  if (e == cudaSuccess) e = pair_attrs<double, float>();
+  if (e == cudaSuccess) e = pair_attrs<float, float>();
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(tgfilter_z_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)zr_smem_bytes(ZR_MAXNZ, ZR_MAXNZ + 32));

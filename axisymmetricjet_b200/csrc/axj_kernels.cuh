@@ -34,6 +34,7 @@ struct StageArgs {
   double* A;             // running sum  pv_old + k1/6 (+ (k2+k3)/3)
   double* B;             // k2
   double* Uout;          // stage output (5 planes); rhs (5 planes) in stage 0
+  float* Uout_f;         // FP32 stage output (mixed precision, stages 1-3)
   const double* target;  // pv_target (5 planes)
   const double* mustar;  // shock-capturing coefficients (planes), or null
   const double* betastar;
@@ -54,6 +55,9 @@ struct StageArgs {
   int* flags;             // bit 0: non-finite value produced
   int stage;              // 0: write rhs only; 1..4: RK4 stage
   int iT, jT;             // stale-T point (0-based)
+  int mixed;              // 1: FP32 stencils and interior pointwise terms
+  int in_f32;             // 1: the stage input (maps) is FP32
+  int out_f32;            // 1: stages 1-3 write Uout_f instead of Uout
   Consts c;
 };
 
@@ -98,6 +102,8 @@ struct SensorArgs {
   double* Q;             // 3 planes: mustarQuantity, betastarQuantity, kappastarQuantity
   double* Qz;            // 3 planes: Q after the in-place z filter
   double* star;          // 3 planes: mustar, betastar, kappastar
+  int mixed;             // 1: FP32 stencils
+  int in_f32;            // 1: the stage input (maps) is FP32
   Consts c;
 };
 
@@ -115,12 +121,13 @@ cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_i
                          int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen, const SideStream& side,
                          cudaStream_t s);
 
-// Box sizes (doubles) the stage kernel expects in its tensor maps: state halo box
+// Box sizes (elements) the stage kernel expects in its tensor maps: state halo box
 // halo_w x halo_h, z-filtered coefficient box halo_w x q_h, tile box tile_w x tile_h.
-void stage_boxes(bool gen, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h);
-// Boxes (doubles, one plane deep) the sensor tile kernel expects for the stage input:
+// The mixed path uses one set of box sizes for its FP64 and FP32 stage inputs.
+void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h);
+// Boxes (elements, one plane deep) the sensor tile kernel expects for the stage input:
 // V_r / V_z box vw x vh, temperature box tw x th (rho uses the stage tile box).
-void sensor_boxes(bool gen, int* vw, int* vh, int* tw, int* th);
+void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th);
 cudaError_t launch_dt(const DtArgs& a, int nblocks, cudaStream_t s);
 // rfilter: also run the r filter into a.star (the stage kernel applies it itself; the
 // unit entry point axj_sensor needs the coefficients as output).

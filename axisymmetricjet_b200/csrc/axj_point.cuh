@@ -11,58 +11,79 @@
 namespace axj {
 
 // Primitive state at a point (pv(i,j,1,1:5) = rho, V_r, V_theta, V_z, T) plus the
-// transport coefficients after AssignValues / UpdateTransportCoeffs.
-struct Prim {
-  double rho, Vr, Vt, Vz, T;
-  double mu, kappa, lambda;
+// transport coefficients after AssignValues / UpdateTransportCoeffs, in arithmetic
+// type R (double on the FP64 path; float for the interior of the mixed path).
+template <typename R>
+struct PrimT {
+  R rho, Vr, Vt, Vz, T;
+  R mu, kappa, lambda;
 };
 
 // The 26 derivative values ComputeRHS forms at a point (ModRHS.f90:29-41, :118-133).
-struct Deriv {
-  double drhodz, dVrdz, dVtdz, dVzdz, dTdz, dpdz, dmudz, dkappadz;
-  double drhodr, dVrdr, dVtdr, dVzdr, dTdr, dpdr, dmudr, dkappadr;
-  double d2Vrdz2, d2Vtdz2, d2Vzdz2, d2Tdz2;
-  double d2Vrdr2, d2Vtdr2, d2Vzdr2, d2Tdr2;
-  double d2Vrdzdr, d2Vzdzdr;
+template <typename R>
+struct DerivT {
+  R drhodz, dVrdz, dVtdz, dVzdz, dTdz, dpdz, dmudz, dkappadz;
+  R drhodr, dVrdr, dVtdr, dVzdr, dTdr, dpdr, dmudr, dkappadr;
+  R d2Vrdz2, d2Vtdz2, d2Vzdz2, d2Tdz2;
+  R d2Vrdr2, d2Vtdr2, d2Vzdr2, d2Tdr2;
+  R d2Vrdzdr, d2Vzdzdr;
 };
+using Prim = PrimT<double>;
+using Deriv = DerivT<double>;
+
+template <typename RO, typename RI>
+AXJ_HD PrimT<RO> convert(const PrimT<RI>& q) {
+  return PrimT<RO>{RO(q.rho), RO(q.Vr), RO(q.Vt), RO(q.Vz), RO(q.T), RO(q.mu), RO(q.kappa), RO(q.lambda)};
+}
+template <typename RO, typename RI>
+AXJ_HD DerivT<RO> convert(const DerivT<RI>& d) {
+  return DerivT<RO>{RO(d.drhodz),  RO(d.dVrdz),   RO(d.dVtdz),   RO(d.dVzdz),   RO(d.dTdz),    RO(d.dpdz),
+                    RO(d.dmudz),   RO(d.dkappadz), RO(d.drhodr),  RO(d.dVrdr),   RO(d.dVtdr),   RO(d.dVzdr),
+                    RO(d.dTdr),    RO(d.dpdr),    RO(d.dmudr),   RO(d.dkappadr), RO(d.d2Vrdz2), RO(d.d2Vtdz2),
+                    RO(d.d2Vzdz2), RO(d.d2Tdz2),  RO(d.d2Vrdr2), RO(d.d2Vtdr2), RO(d.d2Vzdr2), RO(d.d2Tdr2),
+                    RO(d.d2Vrdzdr), RO(d.d2Vzdzdr)};
+}
 
 // Inviscid part, already negated (ModRHS.f90:92-96 and :103-113).
-AXJ_HD void rhs_inviscid(const Prim& q, const Deriv& d, double r, double gam, double rhs[5]) {
-  const double rho = q.rho, Vr = q.Vr, Vt = q.Vt, Vz = q.Vz, T = q.T;
-  double r1 = Vr * d.drhodr + Vz * d.drhodz + rho * (d.dVrdr + Vr / r + d.dVzdz);
-  double r2 = Vr * d.dVrdr + Vz * d.dVrdz + 1.0 / (gam * rho) * d.dpdr;
-  double r3 = Vr * d.dVtdr + Vr * Vt / r + Vz * d.dVtdz;
-  double r4 = Vr * d.dVzdr + Vz * d.dVzdz + 1.0 / (gam * rho) * d.dpdz;
-  double r5 = Vr * d.dTdr + Vz * d.dTdz + (gam - 1.0) * T * (d.dVrdr + Vr / r + d.dVzdz);
-  rhs[0] = -1.0 * r1;
-  rhs[1] = -1.0 * r2;
-  rhs[2] = -1.0 * r3;
-  rhs[3] = -1.0 * r4;
-  rhs[4] = -1.0 * r5;
+template <typename R>
+AXJ_HD void rhs_inviscid(const PrimT<R>& q, const DerivT<R>& d, R r, R gam, R rhs[5]) {
+  const R one = R(1.0), mone = R(-1.0);
+  const R rho = q.rho, Vr = q.Vr, Vt = q.Vt, Vz = q.Vz, T = q.T;
+  R r1 = Vr * d.drhodr + Vz * d.drhodz + rho * (d.dVrdr + Vr / r + d.dVzdz);
+  R r2 = Vr * d.dVrdr + Vz * d.dVrdz + one / (gam * rho) * d.dpdr;
+  R r3 = Vr * d.dVtdr + Vr * Vt / r + Vz * d.dVtdz;
+  R r4 = Vr * d.dVzdr + Vz * d.dVzdz + one / (gam * rho) * d.dpdz;
+  R r5 = Vr * d.dTdr + Vz * d.dTdz + (gam - one) * T * (d.dVrdr + Vr / r + d.dVzdz);
+  rhs[0] = mone * r1;
+  rhs[1] = mone * r2;
+  rhs[2] = mone * r3;
+  rhs[3] = mone * r4;
+  rhs[4] = mone * r5;
 }
 
 // Viscous S_r, S_theta, S_z, S_T (ModRHS.f90:135-209). With shock capturing the
 // per-point constants come from lambda/mu (:180-188).
-AXJ_HD void rhs_viscous(const Prim& q, const Deriv& d, double r, double gam, double Re, double Pr, bool sc,
-                        double rhs[5]) {
-  double fourby3 = 29.0 / 15.0, oneby3 = 14.0 / 15.0, twoby3 = 1.0 / 15.0;
-  const double onebyr = 1.0 / r;
-  const double rho = q.rho, Vr = q.Vr, Vt = q.Vt, mu = q.mu, kappa = q.kappa;
+template <typename R>
+AXJ_HD void rhs_viscous(const PrimT<R>& q, const DerivT<R>& d, R r, R gam, R Re, R Pr, bool sc, R rhs[5]) {
+  const R one = R(1.0);
+  R fourby3 = R(29.0 / 15.0), oneby3 = R(14.0 / 15.0), twoby3 = R(1.0 / 15.0);
+  const R onebyr = one / r;
+  const R rho = q.rho, Vr = q.Vr, Vt = q.Vt, mu = q.mu, kappa = q.kappa;
   if (sc) {
-    double tmp = q.lambda / q.mu;
-    fourby3 = 2.0 + tmp;
-    oneby3 = 1.0 + tmp;
-    twoby3 = -1.0 * tmp;
+    R tmp = q.lambda / q.mu;
+    fourby3 = R(2.0) + tmp;
+    oneby3 = one + tmp;
+    twoby3 = R(-1.0) * tmp;
   }
-  rhs[1] = rhs[1] + 1.0 / (Re * rho) *
+  rhs[1] = rhs[1] + one / (Re * rho) *
                         (mu * (fourby3 * d.d2Vrdr2 + fourby3 * onebyr * d.dVrdr + oneby3 * d.d2Vzdzdr + d.d2Vrdz2 -
                                fourby3 * Vr * (onebyr * onebyr)) +
                          d.dmudr * (fourby3 * d.dVrdr - twoby3 * Vr * onebyr - twoby3 * d.dVzdz) +
                          d.dmudz * (d.dVrdz + d.dVzdr));
-  rhs[2] = rhs[2] + 1.0 / (Re * rho) *
+  rhs[2] = rhs[2] + one / (Re * rho) *
                         (mu * (d.d2Vtdr2 + d.d2Vtdz2 + onebyr * d.dVtdr - Vt * (onebyr * onebyr)) +
                          d.dmudr * (d.dVtdr - Vt * onebyr) + d.dmudz * d.dVtdz);
-  rhs[3] = rhs[3] + 1.0 / (Re * rho) *
+  rhs[3] = rhs[3] + one / (Re * rho) *
                         (mu * (d.d2Vzdr2 + fourby3 * d.d2Vzdz2 + oneby3 * d.d2Vrdzdr + onebyr * d.dVzdr +
                                oneby3 * onebyr * d.dVrdz) +
                          d.dmudr * (d.dVzdr + d.dVrdz) +
@@ -70,7 +91,7 @@ AXJ_HD void rhs_viscous(const Prim& q, const Deriv& d, double r, double gam, dou
   rhs[4] = rhs[4] +
            gam / (Re * Pr * rho) *
                (kappa * (d.d2Tdr2 + onebyr * d.dTdr + d.d2Tdz2) + d.dkappadr * d.dTdr + d.dkappadz * d.dTdz) +
-           gam * (gam - 1.0) / Re * mu / rho *
+           gam * (gam - one) / Re * mu / rho *
                (d.dVrdr * (fourby3 * d.dVrdr - twoby3 * Vr * onebyr - twoby3 * d.dVzdz) +
                 (d.dVtdr - Vt * onebyr) * (d.dVtdr - Vr * onebyr) +
                 Vr * onebyr * (fourby3 * Vr * onebyr - twoby3 * d.dVrdr - twoby3 * d.dVzdz) + d.dVtdz * d.dVtdz +

@@ -1,0 +1,125 @@
+"""Mixed precision (AXJ_MIXED) against the FP64 oracle and the FP64 device path.
+
+In the mixed path the three intermediate stage states are stored in FP32 and the SBP
+derivatives, viscous fluxes and filter windows of every interior tile are evaluated in
+FP32. The RK4 accumulation into the solution (pv, the running sum and k2), the SAT and
+NSCBC penalties, sponges, the pointwise terms of every tile that touches a boundary
+closure row (the first 16 rows off the axis among them, so the 1/r and 1/r^2 terms near
+the axis and the axis limits) and the CFL reduction stay in FP64.
+
+Tolerances, written per test: one RK4 step differs from the FP64 oracle by the FP32
+rounding of the stage states (6e-8 relative) carried through the stencils; after 1000
+steps of the production jet the relative L2 error of rho and p must stay at or below
+1e-5.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import axisymmetricjet_b200 as axj
+from axisymmetricjet_b200 import accuracy, fixtures
+from axisymmetricjet_b200._ffi import SAT_NOSLIP_WALL
+
+pytestmark = pytest.mark.gpu
+
+MIXED = 1
+STEP_REL = 2e-6   # per field, max error over the max magnitude, after 5 RK4 steps
+LONG_L2 = 1e-5    # rho and p, relative L2 after 1000 steps
+
+CASES = {
+    "jet": lambda **kw: fixtures.case("jet96x64", **kw),
+    "jet_sc": lambda **kw: fixtures.case("jet96x64sc", **kw),
+    "nozzle_sat_wall_sc": lambda **kw: fixtures.nozzle_case(wall=SAT_NOSLIP_WALL, sc=True, Mj=1.5, Re=5000.0, **kw),
+    "jet_ragged": lambda **kw: fixtures.make_case(77, 45, 30.0, 15.0, 0.9, 1000.0, **kw),
+}
+
+
+def velocity_scaled_errors(got, want):
+    """Max error per field over the field's max magnitude; the velocity components
+    share one scale, the largest velocity magnitude (V_r and V_theta are zero or
+    small perturbations, their FP32 error is set by the jet velocity)."""
+    vscale = max(np.abs(want[k]).max() for k in (1, 2, 3))
+    out = []
+    for k in range(5):
+        s = vscale if k in (1, 2, 3) else np.abs(want[k]).max()
+        out.append(float(np.abs(got[k] - want[k]).max() / s))
+    return out
+
+
+def solver(c):
+    patches = axj.patches_from_records(c["records"], c["Nz"], c["Nr"])
+    s = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+    s.set_state(c["pv"], c["target"])
+    return s
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_mixed_steps_vs_oracle(oracle_mod, name):
+    c = CASES[name](precision=MIXED)
+    dev = solver(c)
+    op = oracle_mod.patches_from_records(c["records"], c["Nz"], c["Nr"])
+    ora = oracle_mod.Oracle(c["params"], c["zvec"], c["rvec"], c["ibval"], op)
+    ora.set_state(c["pv"], c["target"])
+    for _ in range(5):
+        dt_d = dev.compute_time_step()
+        dt_o = ora.compute_time_step()
+        # dt comes from the FP64 solution; it moves only by the solution's difference
+        assert abs(dt_d - dt_o) <= 1e-6 * abs(dt_o)
+        dev.rk4(dt_o)
+        ora.rk4(dt_o)
+    got, want = dev.get_state(), ora.get_state()
+    errs = velocity_scaled_errors(got, want)
+    assert max(errs) < STEP_REL, errs
+    # and the mixed path is not bit-identical to FP64: the FP32 stages did run
+    assert max(errs) > 0.0
+    dev.close()
+
+
+def test_mixed_rhs_vs_oracle(oracle_mod):
+    c = CASES["nozzle_sat_wall_sc"](precision=MIXED)
+    dev = solver(c)
+    op = oracle_mod.patches_from_records(c["records"], c["Nz"], c["Nr"])
+    ora = oracle_mod.Oracle(c["params"], c["zvec"], c["rvec"], c["ibval"], op)
+    ora.set_state(c["pv"], c["target"])
+    rd, ro = dev.compute_rhs(c["pv"]), ora.compute_rhs(c["pv"])
+    # the rhs itself carries FP32 stencil error (rounding times the metric, about 1e-5
+    # of the rhs scale on this 96 x 64 grid)
+    errs = velocity_scaled_errors(rd, ro)
+    assert max(errs) < 1e-4, errs
+    dev.close()
+
+
+def test_mixed_1000_steps_production_jet():
+    """Nz=4400 x Nr=640, Mach 1.5, Re 5000, shock capturing on: mixed vs FP64 device
+    path (itself within 1e-12 per step of the oracle) after 1000 steps of the same dt
+    sequence taken from the FP64 run."""
+    base = fixtures.case("jet4400x640")
+    mixed = fixtures.case("jet4400x640", precision=MIXED)
+    ref, mix = solver(base), solver(mixed)
+    for _ in range(1000):
+        dt = ref.compute_time_step()
+        ref.rk4(dt)
+        mix.rk4(dt)
+    a, b = mix.get_state(), ref.get_state()
+    errs = accuracy.field_errors(a, b)
+    far = accuracy.farfield_pressure(a, b, base["target"], base["r"], 10.0)
+    near = accuracy.farfield_pressure(a, b, base["target"], base["r"], 2.0)
+    report = {"case": "jet4400x640", "steps": 1000, "fields": errs, "farfield_p_r10": far, "p_r2": near}
+    print("MIXED_ACCURACY " + json.dumps(report))
+    out = os.environ.get("AXJ_REPORT_DIR")
+    if out:
+        with open(os.path.join(out, "mixed_accuracy_jet4400x640.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    assert np.isfinite(a).all()
+    assert errs["rho"]["rel_l2"] <= LONG_L2, errs
+    assert errs["p"]["rel_l2"] <= LONG_L2, errs
+    assert errs["T"]["rel_l2"] <= LONG_L2, errs
+    for name in ("Vr", "Vz"):
+        assert errs[name]["rel_l2_vel"] <= LONG_L2, errs
+    # at r = 10 D the FP64 p' is still below double rounding after 1000 steps; the
+    # mixed path's p' there is FP32 stencil noise, bounded relative to p_inf
+    assert far["diff_rms_over_p_inf"] <= LONG_L2, far
+    ref.close()
+    mix.close()
