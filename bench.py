@@ -202,6 +202,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=10)
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the timing of the mixed-precision form of the same workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -258,6 +260,11 @@ def main():
 
     e2e = run_e2e(args, c, patches, npts, world, barrier, max_over_ranks) if not args.no_e2e else None
 
+    variants = None
+    if not args.no_variants:
+        variants = {"mixed": time_variant(args, c, patches, npts, world, barrier, max_over_ranks, precision=1)}
+        variants["mixed"]["speedup_vs_fp64"] = variants["mixed"]["value"] / value
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -281,12 +288,32 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clk,
+            "variants": variants,
         }
         print(json.dumps(line), flush=True)
     solver.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def time_variant(args, c, patches, npts, world, barrier, max_over_ranks, **pkw):
+    """The same workload and timing (graph-captured steps, CUDA events, max over ranks)
+    with changed solver parameters, e.g. precision = AXJ_MIXED."""
+    import axisymmetricjet_b200 as axj
+    from axisymmetricjet_b200._ffi import AxjParams
+    prm = AxjParams.from_buffer_copy(c["params"])
+    for k, v in pkw.items():
+        setattr(prm, k, v)
+    s = axj.AxiJetSolver(prm, c["zvec"], c["rvec"], c["ibval"], patches)
+    s.set_state(c["pv"], c["target"])
+    s.run(args.warmup)
+    barrier()
+    ms = max_over_ranks(s.run_timed(args.steps))
+    barrier()
+    s.close()
+    return {"params": dict(pkw), "value": replica_throughput(npts, args.steps, world, ms), "unit": UNIT,
+            "ms_per_step": ms / args.steps}
 
 
 def run_e2e(args, c, patches, npts, world, barrier, max_over_ranks):
