@@ -15,11 +15,11 @@ import os
 
 import numpy as np
 
-from ._ffi import (AXJ_OK, STATUS, AxjBcRecord, AxjParams, AxjPatch, default_params, dptr, patch_array,
-                   patches_to_tuples, record_array)
+from ._ffi import (AXJ_OK, STATUS, AxjBcRecord, AxjMlp, AxjParams, AxjPatch, AxjTrainCfg, default_params,
+                   default_train_cfg, dptr, patch_array, patches_to_tuples, record_array)
 
-__all__ = ["AxiJetSolver", "AxjError", "default_params", "load_library", "read_bc_file", "patches_from_records",
-           "library_path"]
+__all__ = ["AxiJetSolver", "AxjError", "AxjMlp", "default_params", "default_train_cfg", "load_library",
+           "read_bc_file", "patches_from_records", "library_path", "mlp_init"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -46,6 +46,7 @@ def load_library():
                            "(there is no CPU fallback)")
     lib = C.CDLL(path)
     dp = C.POINTER(C.c_double)
+    fp = C.POINTER(C.c_float)
     i64 = C.c_int64
     h = C.c_void_p
     sig = {
@@ -71,6 +72,19 @@ def load_library():
         "axj_patches_from_records": (C.c_int, [C.POINTER(AxjBcRecord), i64, i64, i64, C.POINTER(AxjPatch),
                                                C.POINTER(i64)]),
         "axj_version": (C.c_char_p, []),
+        "axj_default_train_cfg": (None, [C.POINTER(AxjTrainCfg)]),
+        "axj_mlp_init": (None, [C.POINTER(AxjMlp), i64]),
+        "axj_mlp_set": (C.c_int, [h, C.POINTER(AxjMlp)]),
+        "axj_mlp_get": (C.c_int, [h, C.POINTER(AxjMlp)]),
+        "axj_dataset_reserve": (C.c_int, [h, i64]),
+        "axj_dataset_add": (C.c_int, [h]),
+        "axj_dataset_size": (C.c_int, [h, C.POINTER(i64)]),
+        "axj_mlp_train": (C.c_int, [h, C.POINTER(AxjTrainCfg), fp]),
+        "axj_dataset_sample": (C.c_int, [h, i64, i64, i64, fp, fp]),
+        "axj_mlp_grad": (C.c_int, [h, fp, fp, i64, C.POINTER(AxjMlp), fp]),
+        "axj_mlp_features": (C.c_int, [h, dp, fp]),
+        "axj_mlp_predict": (C.c_int, [h, dp, dp, dp]),
+        "axj_learned_stats": (C.c_int, [h, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -245,3 +259,78 @@ class AxiJetSolver:
         mu, beta, kappa = self._field(), self._field(), self._field()
         self._chk(self.lib.axj_sensor(self.h, dptr(pv), dptr(mu), dptr(beta), dptr(kappa)))
         return mu, beta, kappa
+
+    # ---- learned sensor ----
+    def mlp_set(self, model):
+        """Install a model: an AxjMlp or a dict of its fields (see AxjMlp.to_dict)."""
+        m = model if isinstance(model, AxjMlp) else AxjMlp.from_dict(model)
+        self._chk(self.lib.axj_mlp_set(self.h, C.byref(m)))
+
+    def mlp_get(self):
+        m = AxjMlp()
+        self._chk(self.lib.axj_mlp_get(self.h, C.byref(m)))
+        return m.to_dict()
+
+    def dataset_reserve(self, nsnapshots):
+        self._chk(self.lib.axj_dataset_reserve(self.h, int(nsnapshots)))
+
+    def dataset_add(self):
+        self._chk(self.lib.axj_dataset_add(self.h))
+
+    def dataset_size(self):
+        n = C.c_int64(0)
+        self._chk(self.lib.axj_dataset_size(self.h, C.byref(n)))
+        return n.value
+
+    def mlp_train(self, cfg=None, **overrides):
+        """Adam training on the device; returns the per-step batch losses."""
+        cfg = cfg if cfg is not None else default_train_cfg(**overrides)
+        loss = np.zeros(max(int(cfg.steps), 1), dtype=np.float32)
+        self._chk(self.lib.axj_mlp_train(self.h, C.byref(cfg), _fptr(loss)))
+        return loss[:int(cfg.steps)]
+
+    def dataset_sample(self, batch, seed, step):
+        X = np.zeros((int(batch), 100), dtype=np.float32)
+        T = np.zeros((int(batch), 2), dtype=np.float32)
+        self._chk(self.lib.axj_dataset_sample(self.h, int(batch), int(seed), int(step), _fptr(X), _fptr(T)))
+        return X, T
+
+    def mlp_grad(self, X, T):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        g = AxjMlp()
+        loss = np.zeros(1, dtype=np.float32)
+        self._chk(self.lib.axj_mlp_grad(self.h, _fptr(X), _fptr(T), X.shape[0], C.byref(g), _fptr(loss)))
+        d = g.to_dict()
+        for k in ("feat_mean", "feat_scale", "out_scale"):
+            d.pop(k)
+        return d, float(loss[0])
+
+    def mlp_features(self, pv):
+        pv = np.ascontiguousarray(pv, dtype=np.float64)
+        out = np.zeros((4, self.Nr, self.Nz), dtype=np.float32)
+        self._chk(self.lib.axj_mlp_features(self.h, dptr(pv), _fptr(out)))
+        return out
+
+    def mlp_predict(self, pv):
+        pv = np.ascontiguousarray(pv, dtype=np.float64)
+        b, k = self._field(), self._field()
+        self._chk(self.lib.axj_mlp_predict(self.h, dptr(pv), dptr(b), dptr(k)))
+        return b, k
+
+    def learned_stats(self):
+        a, b, c = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        self._chk(self.lib.axj_learned_stats(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"judged_outputs": a.value, "fallbacks": b.value, "judges": c.value}
+
+
+def _fptr(a):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def mlp_init(seed):
+    """axj_mlp_init: the seeded initial model as a dict of float32 arrays."""
+    m = AxjMlp()
+    load_library().axj_mlp_init(C.byref(m), int(seed))
+    return m.to_dict()

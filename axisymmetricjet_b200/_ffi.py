@@ -62,6 +62,64 @@ class AxjBcRecord(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("bc", "bc_dir", "istart", "iend", "jstart", "jend")]
 
 
+MLP_CH, MLP_IN, MLP_HID, MLP_OUT = 4, 100, 64, 2
+
+
+class AxjMlp(C.Structure):
+    _fields_ = [
+        ("w1", C.c_float * (MLP_HID * MLP_IN)),
+        ("b1", C.c_float * MLP_HID),
+        ("w2", C.c_float * (MLP_HID * MLP_HID)),
+        ("b2", C.c_float * MLP_HID),
+        ("w3", C.c_float * (MLP_OUT * MLP_HID)),
+        ("b3", C.c_float * MLP_OUT),
+        ("feat_mean", C.c_float * MLP_CH),
+        ("feat_scale", C.c_float * MLP_CH),
+        ("out_scale", C.c_float * MLP_OUT),
+    ]
+    SHAPES = {"w1": (MLP_HID, MLP_IN), "b1": (MLP_HID,), "w2": (MLP_HID, MLP_HID), "b2": (MLP_HID,),
+              "w3": (MLP_OUT, MLP_HID), "b3": (MLP_OUT,), "feat_mean": (MLP_CH,), "feat_scale": (MLP_CH,),
+              "out_scale": (MLP_OUT,)}
+
+    def to_dict(self):
+        """float32 numpy copies of every field, weights as (out, in) matrices."""
+        return {k: np.ctypeslib.as_array(getattr(self, k)).reshape(shp).astype(np.float32).copy()
+                for k, shp in self.SHAPES.items()}
+
+    @classmethod
+    def from_dict(cls, d):
+        m = cls()
+        for k, shp in cls.SHAPES.items():
+            arr = np.ascontiguousarray(np.asarray(d[k], dtype=np.float32).reshape(-1))
+            assert arr.size == int(np.prod(shp)), k
+            C.memmove(getattr(m, k), arr.ctypes.data, arr.nbytes)
+        return m
+
+
+class AxjTrainCfg(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int64),
+        ("batch", C.c_int64),
+        ("lr", C.c_double),
+        ("beta1", C.c_double),
+        ("beta2", C.c_double),
+        ("eps", C.c_double),
+        ("seed", C.c_int64),
+        ("fit_normalization", C.c_int64),
+        ("reserved", C.c_int64 * 6),
+    ]
+
+
+def default_train_cfg(**overrides):
+    """The defaults of axj_default_train_cfg: 2000 Adam steps, batch 65536, lr 1e-3."""
+    c = AxjTrainCfg()
+    c.steps, c.batch, c.lr, c.beta1, c.beta2, c.eps, c.seed, c.fit_normalization = \
+        2000, 65536, 1e-3, 0.9, 0.999, 1e-8, 1, 1
+    for k, v in overrides.items():
+        setattr(c, k, v)
+    return c
+
+
 def default_params(**overrides):
     """The reference defaults of ModuleVariables.f90:4-188 (same as axj_default_params)."""
     p = AxjParams()

@@ -14,6 +14,7 @@
 #include "../../include/axj.h"
 #include "axj_common.cuh"
 #include "axj_kernels.cuh"
+#include "axj_mlp.cuh"
 
 using namespace axj;
 
@@ -65,11 +66,33 @@ struct axj_handle {
   bool state_set = false;
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_judge_exec = nullptr;  // learned sensor: the judge step
+  cudaGraph_t graph_judge = nullptr;
+  // learned sensor
+  double S1[9][6];              // SBP first-derivative rows (feature stencils)
+  bool learned = false;
+  bool judged = false;          // a judge step has run since the state or the model changed
+  int64_t judge_every = 50;
+  double judge_thr = 0.1;
+  float* mlp = nullptr;         // flat FP32 parameters (MLP_NPARAM)
+  MlpNorm norm{};
+  bool mlp_set = false;
+  float4* feat = nullptr;       // feature channels of the current stage input
+  double* pred = nullptr;       // 2 planes: predictions at the judge
+  double* held = nullptr;       // 2 planes: plain betastar, kappastar of the last judge
+  unsigned char* mask = nullptr;
+  unsigned long long* counts = nullptr;  // judged point-outputs, fallbacks
+  int64_t njudges = 0;
+  // training data set: features and plain targets of nsnap snapshots
+  float4* ds_feat = nullptr;
+  float2* ds_targ = nullptr;
+  int64_t ds_cap = 0, ds_n = 0;
   std::vector<double> host_out;  // output-callback staging
   // TMA descriptors: stage-input halo boxes for the stage buffers x {interior, general}
   // tiles, coefficient halo boxes, and tile boxes of pv_old and the running sum A
   CUtensorMap map_state[5][2];
   CUtensorMap map_star[2];
+  CUtensorMap map_starL[2];    // final mu*, beta*, kappa* planes (learned sensor)
   CUtensorMap map_u0_tile, map_acc_tile;
   CUtensorMap map_sens[5][2];  // sensor V boxes of the stage buffers x {interior, general}
   CUtensorMap map_sensT[5][2]; // sensor temperature boxes
@@ -235,6 +258,7 @@ SensorArgs sensor_args(axj_handle* h, int b) {
   s.star = h->star;
   s.mixed = h->mixed;
   s.in_f32 = buf_f32(b);
+  s.ramp_off = 0;
   s.c = h->c;
   return s;
 }
@@ -272,6 +296,7 @@ StageArgs stage_args(axj_handle* h, int bin, int bout, int stage) {
   a.mixed = h->mixed;
   a.in_f32 = buf_f32(bin);
   a.out_f32 = buf_f32(bout);
+  a.learned = 0;
   a.c = h->c;
   return a;
 }
@@ -315,13 +340,16 @@ int build_maps(axj_handle* h) {
   const int nb = h->mixed ? NBUF : BUAF;
   for (int cls = 0; cls < 2; ++cls) {
     int hw, hh, qh, tw, th;
-    stage_boxes(cls == 1, h->mixed, &hw, &hh, &qh, &tw, &th);
+    int qlh;
+    stage_boxes(cls == 1, h->mixed, &hw, &hh, &qh, &tw, &th, &qlh);
     for (int b = 0; b < nb; ++b) {
       int rc = make_map(h, &h->map_state[b][cls], buf_ptr(h, b), 5, hw, hh, 5, buf_f32(b));
       if (rc != AXJ_OK) return rc;
     }
     // z-filtered coefficient quantities (never loaded without shock capturing)
     int rc = make_map(h, &h->map_star[cls], h->Qz ? h->Qz : h->star, 3, hw, qh, 3);
+    if (rc != AXJ_OK) return rc;
+    rc = make_map(h, &h->map_starL[cls], h->star, 3, hw, qlh, 3);
     if (rc != AXJ_OK) return rc;
     int vw, vh, tw2, th2;
     sensor_boxes(cls == 1, h->mixed, &vw, &vh, &tw2, &th2);
@@ -333,7 +361,7 @@ int build_maps(axj_handle* h) {
     }
   }
   int hw, hh, qh, tw, th;
-  stage_boxes(false, h->mixed, &hw, &hh, &qh, &tw, &th);
+  stage_boxes(false, h->mixed, &hw, &hh, &qh, &tw, &th, nullptr);
   for (int b = 0; b < nb; ++b) {
     int rc = make_map(h, &h->map_rho[b], buf_ptr(h, b), 5, tw, th, 1, buf_f32(b));
     if (rc != AXJ_OK) return rc;
@@ -343,18 +371,19 @@ int build_maps(axj_handle* h) {
   return make_map(h, &h->map_acc_tile, h->A, 5, tw, th, 5);
 }
 
-StageMaps stage_maps(axj_handle* h, int b, int cls) {
+StageMaps stage_maps(axj_handle* h, int b, int cls, bool lrn) {
   StageMaps m;
   m.state = &h->map_state[b][cls];
-  m.star = &h->map_star[cls];
+  m.star = lrn ? &h->map_starL[cls] : &h->map_star[cls];
   m.u0 = &h->map_u0_tile;
   m.acc = &h->map_acc_tile;
   return m;
 }
 
-int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage) {
+int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage, bool lrn = false) {
   StageArgs a = stage_args(h, bin, bout, stage);
-  StageMaps mi = stage_maps(h, bin, 0), mg = stage_maps(h, bin, 1);
+  a.learned = lrn ? 1 : 0;
+  StageMaps mi = stage_maps(h, bin, 0, lrn), mg = stage_maps(h, bin, 1, lrn);
   AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, mi, h->ntiles_gen, h->tiles_gen, mg, h->side, h->stream));
   return AXJ_OK;
 }
@@ -367,6 +396,65 @@ int enqueue_stage(axj_handle* h, int bin, int bout, int stage) {
     AXJ_CUDA(h, launch_sensor(s, false, h->side, h->stream));
   }
   return launch_stage_kernels(h, bin, bout, stage);
+}
+
+FeatArgs feat_args(axj_handle* h, int b) {
+  FeatArgs f;
+  f.g = grid_of(h);
+  f.U = buf_ptr(h, b);
+  f.f32 = buf_f32(b);
+  f.desc = h->desc;
+  f.dxidz = h->dxidz;
+  f.detadr = h->detadr;
+  f.rc = h->rc;
+  f.dz = h->dzv;
+  f.dr = h->drv;
+  f.feat = h->feat;
+  for (int r = 0; r < 9; ++r)
+    for (int m = 0; m < 6; ++m) f.sbp1[r][m] = (float)h->S1[r][m];
+  return f;
+}
+
+InferArgs infer_args(axj_handle* h, int mode) {
+  InferArgs a;
+  a.g = grid_of(h);
+  a.feat = h->feat;
+  a.params = h->mlp;
+  a.norm = h->norm;
+  a.ramp = h->ramp;
+  a.mode = mode;
+  a.out = mode == 0 ? h->pred : h->star;
+  a.mask = h->mask;
+  a.held = h->held;
+  a.flags = h->flags;
+  a.ntiles_z = (h->Nz + 31) / 32;
+  a.ntiles = a.ntiles_z * ((h->Nr + 3) / 4);
+  return a;
+}
+
+// Learned-sensor stage. judge1: the first stage of a judge step (plain sensor with its
+// r filter into the coefficient planes, prediction on the same input, fallback mask and
+// held values); plain: a later stage of a judge step (the plain path).
+int enqueue_stage_learned(axj_handle* h, int bin, int bout, int stage, bool judge1, bool plain) {
+  if (plain) return enqueue_stage(h, bin, bout, stage);
+  AXJ_CUDA(h, launch_features(feat_args(h, bin), h->stream));
+  if (judge1) {
+    SensorArgs s = sensor_args(h, bin);
+    AXJ_CUDA(h, launch_sensor(s, true, h->side, h->stream));
+    AXJ_CUDA(h, launch_mlp_infer(infer_args(h, 0), h->stream));
+    JudgeArgs j;
+    j.g = grid_of(h);
+    j.pred = h->pred;
+    j.plain = h->star + h->plane;
+    j.thr = h->judge_thr;
+    j.mask = h->mask;
+    j.held = h->held;
+    j.counts = h->counts;
+    AXJ_CUDA(h, launch_judge(j, h->stream));
+  } else {
+    AXJ_CUDA(h, launch_mlp_infer(infer_args(h, 1), h->stream));
+  }
+  return launch_stage_kernels(h, bin, bout, stage, true);
 }
 
 // Stage input/output buffers of RK4: U0 -> Ua -> Ub -> Ua -> U0 (FP32 Ua, Ub when mixed).
@@ -396,14 +484,63 @@ int enqueue_dt(axj_handle* h, int advance) {
   return AXJ_OK;
 }
 
-// RK4 (ModRungeKutta.f90:5-171) on the device dt.
-int enqueue_rk4(axj_handle* h) {
+// RK4 (ModRungeKutta.f90:5-171) on the device dt. With the learned sensor, `judge`
+// makes this a judge step.
+int enqueue_rk4(axj_handle* h, bool judge = false) {
   int b[5];
   rk4_buffers(h, b);
   for (int st = 1; st <= 4; ++st) {
-    const int rc = enqueue_stage(h, b[st - 1], b[st], st);
+    const int rc = h->learned ? enqueue_stage_learned(h, b[st - 1], b[st], st, judge && st == 1, judge && st > 1)
+                              : enqueue_stage(h, b[st - 1], b[st], st);
     if (rc != AXJ_OK) return rc;
   }
+  return AXJ_OK;
+}
+
+// The learned sensor needs a model before any step.
+int check_model(axj_handle* h) {
+  if (h->learned && !h->mlp_set) return fail(h, AXJ_ERR_ARG, "learned sensor without a model (axj_mlp_set / axj_mlp_train)");
+  return AXJ_OK;
+}
+
+// The learned sensor judges on the first step after the state or the model changed
+// and every judge_every iterations.
+bool judge_due(const axj_handle* h) {
+  return h->learned && (!h->judged || (h->judge_every > 0 && h->iteration % h->judge_every == 0));
+}
+
+// Captured step graphs: dt + RK4, and (learned sensor) the judge step.
+int step_graph(axj_handle* h, bool judge, cudaGraphExec_t* out) {
+  cudaGraphExec_t* ge = judge ? &h->graph_judge_exec : &h->graph_exec;
+  cudaGraph_t* gr = judge ? &h->graph_judge : &h->graph;
+  if (!*ge) {
+    AXJ_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_dt(h, 1);
+    if (rc == AXJ_OK) rc = enqueue_rk4(h, judge);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc != AXJ_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(h, AXJ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    *gr = g;
+    AXJ_CUDA(h, cudaGraphInstantiate(ge, g, 0));
+  }
+  *out = *ge;
+  return AXJ_OK;
+}
+
+// One graph-launched step; advances the iteration counter.
+int launch_step(axj_handle* h) {
+  if (int rc = check_model(h)) return rc;
+  const bool judge = judge_due(h);
+  cudaGraphExec_t ge = nullptr;
+  int rc = step_graph(h, judge, &ge);
+  if (rc != AXJ_OK) return rc;
+  AXJ_CUDA(h, cudaGraphLaunch(ge, h->stream));
+  if (judge) {
+    h->judged = true;
+    h->njudges += 1;
+  }
+  h->iteration += 1;
   return AXJ_OK;
 }
 
@@ -530,7 +667,11 @@ void axj_destroy(axj_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->graph_judge_exec) cudaGraphExecDestroy(h->graph_judge_exec);
+  if (h->graph_judge) cudaGraphDestroy(h->graph_judge);
   for (void* p : h->allocs) cudaFree(p);
+  if (h->ds_feat) cudaFree(h->ds_feat);
+  if (h->ds_targ) cudaFree(h->ds_targ);
   if (h->side.stream) cudaStreamSynchronize(h->side.stream);
   if (h->side.fork) cudaEventDestroy(h->side.fork);
   if (h->side.join) cudaEventDestroy(h->side.join);
@@ -549,8 +690,12 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   if (npatch > MAX_PATCHES) return fail(nullptr, AXJ_ERR_BADPATCH, "more than %d patches", MAX_PATCHES);
   if (prm->precision != AXJ_FP64 && prm->precision != AXJ_MIXED)
     return fail(nullptr, AXJ_ERR_UNSUPPORTED, "precision %lld not built", (long long)prm->precision);
-  if (prm->shock_capturing && prm->sensor != AXJ_SENSOR_PLAIN)
-    return fail(nullptr, AXJ_ERR_UNSUPPORTED, "sensor %lld not built", (long long)prm->sensor);
+  if (prm->sensor != AXJ_SENSOR_PLAIN && prm->sensor != AXJ_SENSOR_LEARNED)
+    return fail(nullptr, AXJ_ERR_ARG, "sensor %lld unknown", (long long)prm->sensor);
+  if (prm->sensor == AXJ_SENSOR_LEARNED && !prm->shock_capturing)
+    return fail(nullptr, AXJ_ERR_ARG, "the learned sensor needs shock_capturing = 1");
+  if (prm->sensor == AXJ_SENSOR_LEARNED && (prm->judge_every < 1 || !(prm->judge_threshold >= 0.0)))
+    return fail(nullptr, AXJ_ERR_ARG, "judge_every must be >= 1 and judge_threshold >= 0");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(nullptr, AXJ_ERR_NODEVICE, "no CUDA device available");
@@ -605,6 +750,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   // ---- operator tables and 1-D metrics (ModSolver.f90:57-76)
   double S1[9][6], S2[9][6], G[9][11];
   build_tables(S1, S2, G);
+  std::memcpy(h->S1, S1, sizeof(S1));
   std::vector<double> z(Nz), r(Nr);
   for (int64_t i = 0; i < Nz; ++i) z[i] = zvec[i];
   for (int64_t j = 0; j < Nr; ++j) r[j] = rvec[j * Nz];
@@ -764,6 +910,18 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->Ua = dalloc<double>(h, 5 * pl, &rc);
   h->Ub = dalloc<double>(h, 5 * pl, &rc);
   h->mixed = prm->precision == AXJ_MIXED;
+  h->learned = prm->sensor == AXJ_SENSOR_LEARNED;
+  h->judge_every = prm->judge_every;
+  h->judge_thr = prm->judge_threshold;
+  if (c.shock_capturing) {
+    // learned-sensor buffers (also used by the feature/prediction entry points)
+    h->mlp = dalloc<float>(h, MLP_NPARAM, &rc);
+    h->feat = dalloc<float4>(h, pl, &rc);
+    h->pred = dalloc<double>(h, 2 * pl, &rc);
+    h->held = dalloc<double>(h, 2 * pl, &rc);
+    h->mask = dalloc<unsigned char>(h, pl, &rc);
+    h->counts = dalloc<unsigned long long>(h, 2, &rc);
+  }
   if (h->mixed) {
     h->Uaf = reinterpret_cast<float*>(h->Ua);
     h->Ubf = reinterpret_cast<float*>(h->Ub);
@@ -833,6 +991,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   upload_tables(S1, S2, G, pd.data(), (int)npatch, h->stream);
   if (rc == AXJ_OK) {
     cudaError_t e = init_kernel_attributes();
+    if (e == cudaSuccess) e = mlp_init_attributes();
     if (e != cudaSuccess) rc = fail(h, AXJ_ERR_NODEVICE, "kernel set-up failed (no sm_100a device?): %s", cudaGetErrorString(e));
   }
   if (rc == AXJ_OK) rc = build_maps(h);
@@ -859,6 +1018,7 @@ int axj_set_state(axj_handle* h, const double* pv, const double* pv_target, int6
   h->iteration = iteration;
   h->time_host = time;
   h->state_set = true;
+  h->judged = false;
   return AXJ_OK;
 }
 
@@ -895,8 +1055,14 @@ int axj_rk4_step(axj_handle* h, double delt) {
   if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called");
   AXJ_CUDA(h, cudaSetDevice(h->device));
   AXJ_CUDA(h, cudaMemcpyAsync(h->dt, &delt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  int rc = enqueue_rk4(h);
+  if (int rc0 = check_model(h)) return rc0;
+  const bool judge = judge_due(h);
+  int rc = enqueue_rk4(h, judge);
   if (rc != AXJ_OK) return rc;
+  if (judge) {
+    h->judged = true;
+    h->njudges += 1;
+  }
   rc = check_flags(h);
   h->time_host = h->time_host + delt;
   h->iteration += 1;
@@ -910,20 +1076,15 @@ int axj_run(axj_handle* h, int64_t nsteps, int64_t out_every, axj_output_cb cb, 
   if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called");
   if (nsteps < 0) return fail(h, AXJ_ERR_ARG, "nsteps < 0");
   AXJ_CUDA(h, cudaSetDevice(h->device));
-  if (!h->graph_exec) {
-    AXJ_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = enqueue_dt(h, 1);
-    if (rc == AXJ_OK) rc = enqueue_rk4(h);
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
-    if (rc != AXJ_OK) { if (g) cudaGraphDestroy(g); return rc; }
-    if (e != cudaSuccess) return fail(h, AXJ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-    h->graph = g;
-    AXJ_CUDA(h, cudaGraphInstantiate(&h->graph_exec, g, 0));
+  {
+    if (int rc = check_model(h)) return rc;
+    cudaGraphExec_t ge = nullptr;
+    int rc = step_graph(h, false, &ge);  // capture outside the step loop
+    if (rc != AXJ_OK) return rc;
   }
   for (int64_t s = 0; s < nsteps; ++s) {
-    AXJ_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
-    h->iteration += 1;
+    int rc = launch_step(h);
+    if (rc != AXJ_OK) return rc;
     if (out_every > 0 && cb && (h->iteration % out_every == 0)) {
       int rc = check_flags(h);
       if (rc != AXJ_OK) return rc;
@@ -950,8 +1111,16 @@ int axj_run_timed(axj_handle* h, int64_t nsteps, double* ms) {
   cudaEvent_t e0, e1;
   AXJ_CUDA(h, cudaEventCreate(&e0));
   AXJ_CUDA(h, cudaEventCreate(&e1));
+  if (judge_due(h)) {  // the judge graph is captured outside the timed region
+    cudaGraphExec_t ge = nullptr;
+    rc = step_graph(h, true, &ge);
+    if (rc != AXJ_OK) return rc;
+  }
   AXJ_CUDA(h, cudaEventRecord(e0, h->stream));
-  for (int64_t s = 0; s < nsteps; ++s) AXJ_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+  for (int64_t s = 0; s < nsteps; ++s) {
+    rc = launch_step(h);
+    if (rc != AXJ_OK) return rc;
+  }
   AXJ_CUDA(h, cudaEventRecord(e1, h->stream));
   AXJ_CUDA(h, cudaEventSynchronize(e1));
   float t = 0.f;
@@ -959,7 +1128,6 @@ int axj_run_timed(axj_handle* h, int64_t nsteps, double* ms) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *ms = t;
-  h->iteration += nsteps;
   AXJ_CUDA(h, cudaMemcpyAsync(&h->time_host, h->time, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   return check_flags(h);
 }
@@ -988,11 +1156,31 @@ int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launch
   int bufs[5];
   rk4_buffers(h, bufs);
   int rc = AXJ_OK;
+  if (rc == AXJ_OK) rc = check_model(h);
   for (int64_t s = 0; s < nsteps && rc == AXJ_OK; ++s) {
+    const bool judge = judge_due(h);
     rc = timed(0, [&] { return enqueue_dt(h, 1); });
     nl[0] += 1;
     for (int st = 1; st <= 4 && rc == AXJ_OK; ++st) {
-      if (h->c.shock_capturing) {
+      const bool lrn_plain = h->learned && judge && st > 1;
+      const bool lrn = h->learned && !lrn_plain;
+      if (lrn) {
+        // features + inference (+ plain sensor and judge at the first stage of a judge step)
+        rc = timed(1, [&]() -> int {
+          AXJ_CUDA(h, launch_features(feat_args(h, bufs[st - 1]), h->stream));
+          if (judge && st == 1) {
+            SensorArgs sa = sensor_args(h, bufs[st - 1]);
+            AXJ_CUDA(h, launch_sensor(sa, true, h->side, h->stream));
+            AXJ_CUDA(h, launch_mlp_infer(infer_args(h, 0), h->stream));
+            JudgeArgs j{grid_of(h), h->pred, h->star + h->plane, h->judge_thr, h->mask, h->held, h->counts};
+            AXJ_CUDA(h, launch_judge(j, h->stream));
+          } else {
+            AXJ_CUDA(h, launch_mlp_infer(infer_args(h, 1), h->stream));
+          }
+          return AXJ_OK;
+        });
+        nl[1] += 2 + ((judge && st == 1) ? (h->nstiles_int > 0) + (h->nstiles_gen > 0) + 4 : 0);
+      } else if (h->c.shock_capturing) {
         rc = timed(1, [&]() -> int {
           SensorArgs sa = sensor_args(h, bufs[st - 1]);
           AXJ_CUDA(h, launch_sensor(sa, false, h->side, h->stream));
@@ -1001,8 +1189,12 @@ int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launch
         nl[1] += (h->nstiles_int > 0) + (h->nstiles_gen > 0) + 1;
       }
       if (rc != AXJ_OK) break;
-      rc = timed(2, [&]() -> int { return launch_stage_kernels(h, bufs[st - 1], bufs[st], st); });
+      rc = timed(2, [&]() -> int { return launch_stage_kernels(h, bufs[st - 1], bufs[st], st, lrn); });
       nl[2] += stage_launches;
+    }
+    if (judge) {
+      h->judged = true;
+      h->njudges += 1;
     }
     h->iteration += 1;
   }
@@ -1076,10 +1268,400 @@ int axj_sensor(axj_handle* h, const double* pv, double* mustar, double* betastar
   AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
   SensorArgs s = sensor_args(h, BUA);
   AXJ_CUDA(h, launch_sensor(s, true, h->side, h->stream));
+  h->judged = false;  // the coefficient planes (the learned sensor's held mu*) were overwritten
   AXJ_CUDA(h, d2h(h, mustar, h->star, 1));
   AXJ_CUDA(h, d2h(h, betastar, h->star + h->plane, 1));
   AXJ_CUDA(h, d2h(h, kappastar, h->star + 2 * h->plane, 1));
   AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return AXJ_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Learned sensor: model, data set, training, checks
+// ---------------------------------------------------------------------------
+namespace {
+
+void mlp_to_flat(const axj_mlp* m, std::vector<float>& flat, MlpNorm* norm) {
+  flat.assign(MLP_NPARAM, 0.0f);
+  for (int n = 0; n < MLP_HID; ++n)
+    for (int k = 0; k < MLP_IN; ++k) flat[MLP_OFF_W1 + n * MLP_K1 + k] = m->w1[n * MLP_IN + k];
+  for (int n = 0; n < MLP_HID; ++n) flat[MLP_OFF_B1 + n] = m->b1[n];
+  for (int e = 0; e < MLP_HID * MLP_HID; ++e) flat[MLP_OFF_W2 + e] = m->w2[e];
+  for (int n = 0; n < MLP_HID; ++n) flat[MLP_OFF_B2 + n] = m->b2[n];
+  for (int e = 0; e < MLP_OUT * MLP_HID; ++e) flat[MLP_OFF_W3 + e] = m->w3[e];
+  for (int n = 0; n < MLP_OUT; ++n) flat[MLP_OFF_B3 + n] = m->b3[n];
+  if (norm) {
+    for (int c = 0; c < MLP_CH; ++c) {
+      norm->feat_mean[c] = m->feat_mean[c];
+      norm->feat_inv_scale[c] = 1.0f / m->feat_scale[c];
+    }
+    for (int k = 0; k < MLP_OUT; ++k) norm->out_scale[k] = m->out_scale[k];
+  }
+}
+
+void flat_to_mlp(const std::vector<float>& flat, const MlpNorm* norm, axj_mlp* m) {
+  std::memset(m, 0, sizeof(*m));
+  for (int n = 0; n < MLP_HID; ++n)
+    for (int k = 0; k < MLP_IN; ++k) m->w1[n * MLP_IN + k] = flat[MLP_OFF_W1 + n * MLP_K1 + k];
+  for (int n = 0; n < MLP_HID; ++n) m->b1[n] = flat[MLP_OFF_B1 + n];
+  for (int e = 0; e < MLP_HID * MLP_HID; ++e) m->w2[e] = flat[MLP_OFF_W2 + e];
+  for (int n = 0; n < MLP_HID; ++n) m->b2[n] = flat[MLP_OFF_B2 + n];
+  for (int e = 0; e < MLP_OUT * MLP_HID; ++e) m->w3[e] = flat[MLP_OFF_W3 + e];
+  for (int n = 0; n < MLP_OUT; ++n) m->b3[n] = flat[MLP_OFF_B3 + n];
+  if (norm) {
+    for (int c = 0; c < MLP_CH; ++c) {
+      m->feat_mean[c] = norm->feat_mean[c];
+      m->feat_scale[c] = 1.0f / norm->feat_inv_scale[c];
+    }
+    for (int k = 0; k < MLP_OUT; ++k) m->out_scale[k] = norm->out_scale[k];
+  }
+}
+
+int need_mlp_buffers(axj_handle* h) {
+  if (!h->mlp) return fail(h, AXJ_ERR_ARG, "handle created with shock_capturing = 0 (no sensor to learn)");
+  return AXJ_OK;
+}
+
+// Forward and backward workspace of one batch (row-major, batch-major).
+struct TrainWs {
+  int B = 0;
+  float *X = nullptr, *T = nullptr, *Z1 = nullptr, *H1 = nullptr, *Z2 = nullptr, *H2 = nullptr, *Y = nullptr,
+        *dY = nullptr, *dH2 = nullptr, *dH1 = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr, *loss = nullptr;
+  int* step = nullptr;
+  std::vector<void*> mem;
+  ~TrainWs() {
+    for (void* p : mem) cudaFree(p);
+  }
+  template <typename T_>
+  T_* get(size_t n, cudaError_t* e) {
+    void* p = nullptr;
+    if (*e == cudaSuccess) *e = cudaMalloc(&p, n * sizeof(T_) + 16);
+    if (*e == cudaSuccess) {
+      mem.push_back(p);
+      *e = cudaMemset(p, 0, n * sizeof(T_) + 16);
+    }
+    return static_cast<T_*>(p);
+  }
+  cudaError_t alloc(int B_, int nloss) {
+    B = B_;
+    cudaError_t e = cudaSuccess;
+    const size_t b = (size_t)B;
+    X = get<float>(b * MLP_K1, &e);
+    T = get<float>(b * MLP_OUT, &e);
+    Z1 = get<float>(b * MLP_HID, &e);
+    H1 = get<float>(b * MLP_HID, &e);
+    Z2 = get<float>(b * MLP_HID, &e);
+    H2 = get<float>(b * MLP_HID, &e);
+    Y = get<float>(b * MLP_OUT, &e);
+    dY = get<float>(b * MLP_OUT, &e);
+    dH2 = get<float>(b * MLP_HID, &e);
+    dH1 = get<float>(b * MLP_HID, &e);
+    grad = get<float>(MLP_NPARAM, &e);
+    m = get<float>(MLP_NPARAM, &e);
+    v = get<float>(MLP_NPARAM, &e);
+    loss = get<float>((size_t)(nloss > 0 ? nloss : 1), &e);
+    step = get<int>(1, &e);
+    return e;
+  }
+};
+
+// Forward and backward pass over ws.X / ws.T; gradients (all parameters) into ws.grad,
+// the batch loss added to ws.loss[*ws.step].
+int forward_backward(axj_handle* h, TrainWs& w) {
+  const int B = w.B;
+  const float* P = h->mlp;
+  float* G = w.grad;
+  cudaStream_t s = h->stream;
+  const int ks = B >= 2048 ? B / 1024 : 1;
+  AXJ_CUDA(h, launch_gemm(false, true, B, MLP_HID, MLP_K1, w.X, MLP_K1, P + MLP_OFF_W1, MLP_K1, w.Z1, MLP_HID, 1, s));
+  AXJ_CUDA(h, launch_bias_gelu(w.Z1, P + MLP_OFF_B1, w.H1, B, MLP_HID, s));
+  AXJ_CUDA(h, launch_gemm(false, true, B, MLP_HID, MLP_HID, w.H1, MLP_HID, P + MLP_OFF_W2, MLP_HID, w.Z2, MLP_HID, 1, s));
+  AXJ_CUDA(h, launch_bias_gelu(w.Z2, P + MLP_OFF_B2, w.H2, B, MLP_HID, s));
+  AXJ_CUDA(h, launch_gemm(false, true, B, MLP_OUT, MLP_HID, w.H2, MLP_HID, P + MLP_OFF_W3, MLP_HID, w.Y, MLP_OUT, 1, s));
+  AXJ_CUDA(h, launch_bias(w.Y, P + MLP_OFF_B3, B, MLP_OUT, s));
+  AXJ_CUDA(h, launch_loss(w.Y, w.T, w.dY, w.loss, w.step, B, s));
+  AXJ_CUDA(h, cudaMemsetAsync(G, 0, sizeof(float) * MLP_NPARAM, s));
+  AXJ_CUDA(h, launch_gemm(true, false, MLP_OUT, MLP_HID, B, w.dY, MLP_OUT, w.H2, MLP_HID, G + MLP_OFF_W3, MLP_HID, ks, s));
+  AXJ_CUDA(h, launch_colsum(w.dY, G + MLP_OFF_B3, B, MLP_OUT, s));
+  AXJ_CUDA(h, launch_gemm(false, false, B, MLP_HID, MLP_OUT, w.dY, MLP_OUT, P + MLP_OFF_W3, MLP_HID, w.dH2, MLP_HID, 1, s));
+  AXJ_CUDA(h, launch_gelu_bwd(w.dH2, w.Z2, B * MLP_HID, s));
+  AXJ_CUDA(h, launch_gemm(true, false, MLP_HID, MLP_HID, B, w.dH2, MLP_HID, w.H1, MLP_HID, G + MLP_OFF_W2, MLP_HID, ks, s));
+  AXJ_CUDA(h, launch_colsum(w.dH2, G + MLP_OFF_B2, B, MLP_HID, s));
+  AXJ_CUDA(h, launch_gemm(false, false, B, MLP_HID, MLP_HID, w.dH2, MLP_HID, P + MLP_OFF_W2, MLP_HID, w.dH1, MLP_HID, 1, s));
+  AXJ_CUDA(h, launch_gelu_bwd(w.dH1, w.Z1, B * MLP_HID, s));
+  AXJ_CUDA(h, launch_gemm(true, false, MLP_HID, MLP_K1, B, w.dH1, MLP_HID, w.X, MLP_K1, G + MLP_OFF_W1, MLP_K1, ks, s));
+  AXJ_CUDA(h, launch_colsum(w.dH1, G + MLP_OFF_B1, B, MLP_HID, s));
+  return AXJ_OK;
+}
+
+Dataset dataset_of(axj_handle* h) {
+  Dataset d;
+  d.feat = h->ds_feat;
+  d.targ = h->ds_targ;
+  d.S = (int)h->ds_n;
+  d.g = grid_of(h);
+  return d;
+}
+
+uint64_t host_mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace
+
+extern "C" {
+
+void axj_default_train_cfg(axj_train_cfg* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->steps = 2000;
+  c->batch = 65536;
+  c->lr = 1e-3;
+  c->beta1 = 0.9;
+  c->beta2 = 0.999;
+  c->eps = 1e-8;
+  c->seed = 1;
+  c->fit_normalization = 1;
+}
+
+void axj_mlp_init(axj_mlp* m, int64_t seed) {
+  if (!m) return;
+  std::memset(m, 0, sizeof(*m));
+  uint64_t state = (uint64_t)seed;
+  auto uni = [&](double bound) {
+    state = host_mix64(state);
+    const double u = (double)(state >> 11) * (1.0 / 9007199254740992.0);
+    return (float)((2.0 * u - 1.0) * bound);
+  };
+  const double b1 = 1.0 / std::sqrt((double)MLP_IN), b2 = 1.0 / std::sqrt((double)MLP_HID);
+  for (int e = 0; e < MLP_HID * MLP_IN; ++e) m->w1[e] = uni(b1);
+  for (int e = 0; e < MLP_HID; ++e) m->b1[e] = uni(b1);
+  for (int e = 0; e < MLP_HID * MLP_HID; ++e) m->w2[e] = uni(b2);
+  for (int e = 0; e < MLP_HID; ++e) m->b2[e] = uni(b2);
+  for (int e = 0; e < MLP_OUT * MLP_HID; ++e) m->w3[e] = uni(b2);
+  for (int e = 0; e < MLP_OUT; ++e) m->b3[e] = uni(b2);
+  for (int c = 0; c < MLP_CH; ++c) m->feat_scale[c] = 1.0f;
+  for (int k = 0; k < MLP_OUT; ++k) m->out_scale[k] = 1.0f;
+}
+
+int axj_mlp_set(axj_handle* h, const axj_mlp* m) {
+  if (!h || !m) return fail(h, AXJ_ERR_ARG, "null argument");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  for (int c = 0; c < MLP_CH; ++c)
+    if (!(m->feat_scale[c] > 0.0f) || !std::isfinite(m->feat_mean[c]))
+      return fail(h, AXJ_ERR_ARG, "feature normalisation of channel %d is not positive and finite", c);
+  for (int k = 0; k < MLP_OUT; ++k)
+    if (!std::isfinite(m->out_scale[k])) return fail(h, AXJ_ERR_ARG, "out_scale[%d] is not finite", k);
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  std::vector<float> flat;
+  mlp_to_flat(m, flat, &h->norm);
+  AXJ_CUDA(h, cudaMemcpyAsync(h->mlp, flat.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->mlp_set = true;
+  h->judged = false;
+  return AXJ_OK;
+}
+
+int axj_mlp_get(axj_handle* h, axj_mlp* m) {
+  if (!h || !m) return fail(h, AXJ_ERR_ARG, "null argument");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  std::vector<float> flat(MLP_NPARAM);
+  AXJ_CUDA(h, cudaMemcpyAsync(flat.data(), h->mlp, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  flat_to_mlp(flat, &h->norm, m);
+  return AXJ_OK;
+}
+
+int axj_dataset_reserve(axj_handle* h, int64_t nsnapshots) {
+  if (!h || nsnapshots < 1) return fail(h, AXJ_ERR_ARG, "bad argument");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (h->ds_feat) cudaFree(h->ds_feat);
+  if (h->ds_targ) cudaFree(h->ds_targ);
+  h->ds_feat = nullptr;
+  h->ds_targ = nullptr;
+  h->ds_cap = h->ds_n = 0;
+  const size_t n = (size_t)nsnapshots * (size_t)h->plane;
+  cudaError_t e = cudaMalloc(&h->ds_feat, n * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc(&h->ds_targ, n * sizeof(float2));
+  if (e != cudaSuccess) {
+    if (h->ds_feat) cudaFree(h->ds_feat);
+    h->ds_feat = nullptr;
+    h->ds_targ = nullptr;
+    return fail(h, AXJ_ERR_NOMEM, "data set of %lld snapshots: %s", (long long)nsnapshots, cudaGetErrorString(e));
+  }
+  h->ds_cap = nsnapshots;
+  return AXJ_OK;
+}
+
+int axj_dataset_add(axj_handle* h) {
+  if (!h) return fail(h, AXJ_ERR_ARG, "null handle");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called");
+  if (h->ds_n >= h->ds_cap) return fail(h, AXJ_ERR_ARG, "data set full (%lld snapshots)", (long long)h->ds_cap);
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  const size_t off = (size_t)h->ds_n * (size_t)h->plane;
+  FeatArgs f = feat_args(h, BU0);
+  f.feat = h->ds_feat + off;
+  AXJ_CUDA(h, launch_features(f, h->stream));
+  SensorArgs sa = sensor_args(h, BU0);
+  sa.ramp_off = 1;  // the network predicts the coefficients before the z ramp
+  AXJ_CUDA(h, launch_sensor(sa, true, h->side, h->stream));
+  AXJ_CUDA(h, launch_pack_targets(grid_of(h), h->star, h->ds_targ + off, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->ds_n += 1;
+  h->judged = false;  // the coefficient planes were overwritten
+  return check_flags(h);
+}
+
+int axj_dataset_size(axj_handle* h, int64_t* n) {
+  if (!h || !n) return fail(h, AXJ_ERR_ARG, "null argument");
+  *n = h->ds_n;
+  return AXJ_OK;
+}
+
+int axj_dataset_sample(axj_handle* h, int64_t batch, int64_t seed, int64_t step, float* X, float* T) {
+  if (!h || !X || !T || batch < 1 || step < 0) return fail(h, AXJ_ERR_ARG, "bad argument");
+  if (h->ds_n < 1) return fail(h, AXJ_ERR_ARG, "empty data set");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  TrainWs w;
+  AXJ_CUDA(h, w.alloc((int)batch, 1));
+  const int st = (int)step;
+  AXJ_CUDA(h, cudaMemcpyAsync(w.step, &st, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  AXJ_CUDA(h, launch_sample(dataset_of(h), h->norm, (unsigned long long)seed, w.step, (int)batch, w.X, w.T, h->stream));
+  std::vector<float> xb((size_t)batch * MLP_K1);
+  AXJ_CUDA(h, cudaMemcpyAsync(xb.data(), w.X, xb.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaMemcpyAsync(T, w.T, (size_t)batch * MLP_OUT * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (int64_t b = 0; b < batch; ++b)
+    for (int k = 0; k < MLP_IN; ++k) X[b * MLP_IN + k] = xb[b * MLP_K1 + k];
+  return AXJ_OK;
+}
+
+int axj_mlp_grad(axj_handle* h, const float* X, const float* T, int64_t batch, axj_mlp* grad, float* loss) {
+  if (!h || !X || !T || !grad || batch < 1) return fail(h, AXJ_ERR_ARG, "bad argument");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  TrainWs w;
+  AXJ_CUDA(h, w.alloc((int)batch, 1));
+  std::vector<float> xb((size_t)batch * MLP_K1, 0.0f);
+  for (int64_t b = 0; b < batch; ++b)
+    for (int k = 0; k < MLP_IN; ++k) xb[b * MLP_K1 + k] = X[b * MLP_IN + k];
+  AXJ_CUDA(h, cudaMemcpyAsync(w.X, xb.data(), xb.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  AXJ_CUDA(h, cudaMemcpyAsync(w.T, T, (size_t)batch * MLP_OUT * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  int rc = forward_backward(h, w);
+  if (rc != AXJ_OK) return rc;
+  std::vector<float> g(MLP_NPARAM);
+  float l = 0.0f;
+  AXJ_CUDA(h, cudaMemcpyAsync(g.data(), w.grad, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaMemcpyAsync(&l, w.loss, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  flat_to_mlp(g, nullptr, grad);
+  if (loss) *loss = l;
+  return AXJ_OK;
+}
+
+int axj_mlp_train(axj_handle* h, const axj_train_cfg* cfg, float* loss) {
+  if (!h || !cfg || cfg->steps < 0 || cfg->batch < 1 || cfg->batch > (1 << 24))
+    return fail(h, AXJ_ERR_ARG, "bad argument");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  if (h->ds_n < 1) return fail(h, AXJ_ERR_ARG, "empty data set (axj_dataset_add)");
+  if (!h->mlp_set) return fail(h, AXJ_ERR_ARG, "no initial model (axj_mlp_set)");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  if (cfg->fit_normalization) {
+    double* acc = nullptr;
+    AXJ_CUDA(h, cudaMalloc(&acc, 11 * sizeof(double)));
+    cudaMemsetAsync(acc, 0, 11 * sizeof(double), h->stream);
+    cudaError_t e = launch_dataset_stats(dataset_of(h), acc, h->stream);
+    double a[11];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a, acc, sizeof(a), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(acc);
+    if (e != cudaSuccess) return fail(h, AXJ_ERR_CUDA, "data set statistics: %s", cudaGetErrorString(e));
+    const double n = a[10];
+    for (int c = 0; c < MLP_CH; ++c) {
+      const double mean = a[c] / n;
+      const double var = std::max(a[4 + c] / n - mean * mean, 0.0);
+      const double sd = std::sqrt(var);
+      h->norm.feat_mean[c] = (float)mean;
+      h->norm.feat_inv_scale[c] = (float)(sd > 1e-30 ? 1.0 / sd : 1.0);
+    }
+    for (int k = 0; k < MLP_OUT; ++k) {
+      const double rms = std::sqrt(a[8 + k] / n);
+      h->norm.out_scale[k] = (float)(rms > 1e-30 ? rms : 1.0);
+    }
+  }
+  TrainWs w;
+  AXJ_CUDA(h, w.alloc((int)cfg->batch, (int)std::max<int64_t>(cfg->steps, 1)));
+  const Dataset d = dataset_of(h);
+  for (int64_t it = 0; it < cfg->steps; ++it) {
+    AXJ_CUDA(h, launch_sample(d, h->norm, (unsigned long long)cfg->seed, w.step, w.B, w.X, w.T, h->stream));
+    int rc = forward_backward(h, w);
+    if (rc != AXJ_OK) return rc;
+    AXJ_CUDA(h, launch_adam(h->mlp, w.grad, w.m, w.v, MLP_NPARAM, w.step, (float)cfg->lr, (float)cfg->beta1,
+                            (float)cfg->beta2, (float)cfg->eps, h->stream));
+    AXJ_CUDA(h, launch_step_inc(w.step, h->stream));
+  }
+  if (loss && cfg->steps > 0)
+    AXJ_CUDA(h, cudaMemcpyAsync(loss, w.loss, sizeof(float) * cfg->steps, cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->judged = false;
+  return AXJ_OK;
+}
+
+int axj_mlp_features(axj_handle* h, const double* pv, float* feat) {
+  if (!h || !pv || !feat) return fail(h, AXJ_ERR_ARG, "null argument");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
+  AXJ_CUDA(h, launch_features(feat_args(h, BUA), h->stream));
+  std::vector<float4> f((size_t)h->plane);
+  AXJ_CUDA(h, cudaMemcpyAsync(f.data(), h->feat, f.size() * sizeof(float4), cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  const size_t np = (size_t)h->Nz * h->Nr;
+  for (int j = 0; j < h->Nr; ++j)
+    for (int i = 0; i < h->Nz; ++i) {
+      const float4 v = f[(size_t)j * h->P + i];
+      const size_t o = (size_t)j * h->Nz + i;
+      feat[o] = v.x;
+      feat[np + o] = v.y;
+      feat[2 * np + o] = v.z;
+      feat[3 * np + o] = v.w;
+    }
+  return AXJ_OK;
+}
+
+int axj_mlp_predict(axj_handle* h, const double* pv, double* betastar, double* kappastar) {
+  if (!h || !pv || !betastar || !kappastar) return fail(h, AXJ_ERR_ARG, "null argument");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  if (!h->mlp_set) return fail(h, AXJ_ERR_ARG, "no model (axj_mlp_set)");
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
+  AXJ_CUDA(h, launch_features(feat_args(h, BUA), h->stream));
+  AXJ_CUDA(h, launch_mlp_infer(infer_args(h, 0), h->stream));
+  AXJ_CUDA(h, d2h(h, betastar, h->pred, 1));
+  AXJ_CUDA(h, d2h(h, kappastar, h->pred + h->plane, 1));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  return check_flags(h);
+}
+
+int axj_learned_stats(axj_handle* h, int64_t* judged, int64_t* fallback, int64_t* njudges) {
+  if (!h) return fail(h, AXJ_ERR_ARG, "null handle");
+  if (int rc = need_mlp_buffers(h)) return rc;
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  unsigned long long c[2] = {0, 0};
+  AXJ_CUDA(h, cudaMemcpyAsync(c, h->counts, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (judged) *judged = (int64_t)c[0];
+  if (fallback) *fallback = (int64_t)c[1];
+  if (njudges) *njudges = h->njudges;
   return AXJ_OK;
 }
 

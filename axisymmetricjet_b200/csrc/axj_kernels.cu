@@ -152,7 +152,9 @@ __host__ __device__ constexpr int hz_t(int h, int esize) { return (h + 16 / esiz
 
 // HZ follows the arithmetic type: the mixed path rounds to 4 elements in every stage
 // (valid for its double stage-1 input too), so one coefficient-box map serves all stages.
-template <int H, typename SIN, typename R>
+// LRN: the coefficient box holds the final mu*, beta*, kappa* planes (learned sensor),
+// so it has the state box's halo and no filter reach.
+template <int H, typename SIN, typename R, bool LRN = false>
 struct StageSmem {
   static constexpr int HZ = hz_t(H, (int)sizeof(R));
   static constexpr int RZ = TZ + 2 * HZ;
@@ -161,7 +163,7 @@ struct StageSmem {
   static constexpr int NTP = TZ * TR;
   // r reach of the truncated-Gaussian filter rows: 4 for the centred row, 10 for the
   // 11-point boundary rows (ModTGfilter.f90:31-44)
-  static constexpr int HT = (H == H_INT) ? 4 : 10;
+  static constexpr int HT = LRN ? 0 : ((H == H_INT) ? 4 : 10);
   static constexpr int RQ = RR + 2 * HT;  // rows of the z-filtered coefficient box
   // byte offsets: state box [5][RR][RZ] of the stage-input type; coefficient box
   // [3][RQ][RZ] (doubles) holding the z-filtered quantities on arrival and mu_eff,
@@ -191,12 +193,12 @@ template <> __device__ __forceinline__ float pow0666<float>(float T) { return po
 // mixed path's intermediate stages); R: arithmetic type of the stencils and, in
 // interior tiles, of the pointwise terms. General tiles (closure rows, faces, the axis
 // row) evaluate the pointwise terms, face penalties and sponges in double.
-template <int H, bool GEN, typename SIN, typename R>
+template <int H, bool GEN, typename SIN, typename R, bool LRN>
 __global__ void __launch_bounds__(STAGE_THREADS)
     stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
                  const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
                  const __grid_constant__ CUtensorMap mAcc) {
-  using SM = StageSmem<H, SIN, R>;
+  using SM = StageSmem<H, SIN, R, LRN>;
   using RP = typename std::conditional<GEN, double, R>::type;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT, NTP = SM::NTP, HT = SM::HT, RQ = SM::RQ;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -282,6 +284,17 @@ __global__ void __launch_bounds__(STAGE_THREADS)
           if (!(i >= 0 && i < Nz && j >= 0 && j < Nr)) rw = (int)ROW_NONE;
         }
         double f[3] = {0.0, 0.0, 0.0};
+        if (LRN) {
+          // final coefficients (ramp applied), zero at blanked points as the filter gives
+          if (rw < 9) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) f[q] = sQ[q * RQ * RZ + idx];
+          }
+          vmu[k] = mu + f[0];
+          vbe[k] = f[1];
+          vka[k] = mu + f[2];
+          continue;
+        }
         if (rw < 9) {
           const int w0 = GEN ? tg_w0(rw) : -4;
           const int n = GEN ? tg_len(rw) : 9;
@@ -509,8 +522,13 @@ template <int H, bool GEN, typename SIN, typename R>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* tiles, const StageMaps& m,
                                   cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
-  const size_t sm = StageSmem<H, SIN, R>::bytes(GEN);
-  stage_kernel<H, GEN, SIN, R><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+  if (a.learned) {
+    const size_t sm = StageSmem<H, SIN, R, true>::bytes(GEN);
+    stage_kernel<H, GEN, SIN, R, true><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+  } else {
+    const size_t sm = StageSmem<H, SIN, R, false>::bytes(GEN);
+    stage_kernel<H, GEN, SIN, R, false><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+  }
   return cudaGetLastError();
 }
 
@@ -554,7 +572,7 @@ cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_i
   return launch_stage_pair<float, float>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s);
 }
 
-void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h) {
+void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h, int* qlrn_h) {
   if (mixed) {
     *halo_w = gen ? StageSmem<H_GEN, float, float>::RZ : StageSmem<H_INT, float, float>::RZ;
   } else {
@@ -562,6 +580,7 @@ void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* 
   }
   *halo_h = gen ? StageSmem<H_GEN, double, double>::RR : StageSmem<H_INT, double, double>::RR;
   *q_h = gen ? StageSmem<H_GEN, double, double>::RQ : StageSmem<H_INT, double, double>::RQ;
+  if (qlrn_h) *qlrn_h = gen ? StageSmem<H_GEN, double, double, true>::RQ : StageSmem<H_INT, double, double, true>::RQ;
   *tile_w = TZ;
   *tile_h = TR;
 }
@@ -921,7 +940,7 @@ __global__ void sensor_rfilter_kernel(const SensorArgs a) {
   const uint32_t dsc = __ldg(a.desc + o);
   const int row = row_of(dsc, 2);
   const double scale[3] = {a.c.C_mu_Re, a.c.C_beta_Re, a.c.C_kappa_Re_Pr};
-  const double ramp = __ldg(a.ramp + i);
+  const double ramp = a.ramp_off ? 1.0 : __ldg(a.ramp + i);
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
     double v = 0.0;
@@ -1237,8 +1256,11 @@ void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th) {
 
 template <int H, bool GEN, typename SIN, typename R>
 static cudaError_t stage_attr() {
-  return cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)StageSmem<H, SIN, R>::bytes(GEN));
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)StageSmem<H, SIN, R, false>::bytes(GEN));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)StageSmem<H, SIN, R, true>::bytes(GEN));
 }
 template <int HS, int HF, bool GEN, typename SIN, typename R>
 static cudaError_t sensor_attr() {

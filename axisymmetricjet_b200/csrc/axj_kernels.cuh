@@ -58,6 +58,7 @@ struct StageArgs {
   int mixed;              // 1: FP32 stencils and interior pointwise terms
   int in_f32;             // 1: the stage input (maps) is FP32
   int out_f32;            // 1: stages 1-3 write Uout_f instead of Uout
+  int learned;            // 1: the coefficient maps hold final mu*, beta*, kappa* (learned sensor)
   Consts c;
 };
 
@@ -104,6 +105,7 @@ struct SensorArgs {
   double* star;          // 3 planes: mustar, betastar, kappastar
   int mixed;             // 1: FP32 stencils
   int in_f32;            // 1: the stage input (maps) is FP32
+  int ramp_off;          // 1: the r filter leaves out the z ramp (training targets)
   Consts c;
 };
 
@@ -124,7 +126,8 @@ cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_i
 // Box sizes (elements) the stage kernel expects in its tensor maps: state halo box
 // halo_w x halo_h, z-filtered coefficient box halo_w x q_h, tile box tile_w x tile_h.
 // The mixed path uses one set of box sizes for its FP64 and FP32 stage inputs.
-void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h);
+// qlrn_h (nullable): box height of the final-coefficient planes of the learned sensor.
+void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h, int* qlrn_h);
 // Boxes (elements, one plane deep) the sensor tile kernel expects for the stage input:
 // V_r / V_z box vw x vh, temperature box tw x th (rho uses the stage tile box).
 void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th);

@@ -212,6 +212,69 @@ int axj_compute_dt_noalloc(const double* d_pv, int64_t pitch, int64_t Nz, int64_
                            const double* d_detadr, const double* d_ibval, const axj_params* params, double stale_T,
                            double* d_dt, void* stream);
 
+/* ---- Learned artificial-diffusivity sensor (sensor = AXJ_SENSOR_LEARNED) ----------
+ * No counterpart in the reference. A small MLP stands in for the evaluation of
+ * betastar and kappastar (ModShockCapturing.f90:18-92): 100 inputs (4 channels x a
+ * 5 x 5 (z, r) window), two hidden layers of 64 with the tanh-form GELU, 2 outputs,
+ * BF16 weights and FP32 accumulation on the tensor cores at inference. mustar keeps
+ * the plain sensor's value of the last judge step. The plain sensor runs on the first
+ * stage of every judge_every-th step (and on the first step after axj_set_state,
+ * axj_mlp_set or training) as judge: wherever |prediction - plain| exceeds
+ * judge_threshold x the largest |plain| in the point's 5 x 5 window, the plain value
+ * of that judge step replaces the prediction until the next judge step. The other
+ * three stages of a judge step use the plain sensor throughout. */
+#define AXJ_MLP_CHANNELS 4  /* dilatation, |grad rho|, |vorticity|, sqrt(deltaz*deltar) */
+#define AXJ_MLP_IN 100      /* input index ch*25 + (dr+2)*5 + (dz+2), dz, dr in -2..2 */
+#define AXJ_MLP_HIDDEN 64
+#define AXJ_MLP_OUT 2       /* betastar, kappastar before the z ramp (1+tanh(5(z-10)))/2 */
+
+typedef struct axj_mlp {
+  float w1[AXJ_MLP_HIDDEN * AXJ_MLP_IN]; /* row-major [out][in] */
+  float b1[AXJ_MLP_HIDDEN];
+  float w2[AXJ_MLP_HIDDEN * AXJ_MLP_HIDDEN];
+  float b2[AXJ_MLP_HIDDEN];
+  float w3[AXJ_MLP_OUT * AXJ_MLP_HIDDEN];
+  float b3[AXJ_MLP_OUT];
+  float feat_mean[AXJ_MLP_CHANNELS];     /* input = (channel value - mean) / scale; 0 outside the grid */
+  float feat_scale[AXJ_MLP_CHANNELS];
+  float out_scale[AXJ_MLP_OUT];          /* coefficient = output * out_scale * ramp(z) */
+} axj_mlp;
+
+typedef struct axj_train_cfg {
+  int64_t steps;              /* Adam steps (2000) */
+  int64_t batch;              /* points per step (65536), drawn uniformly over the data set */
+  double lr, beta1, beta2, eps; /* 1e-3, 0.9, 0.999, 1e-8 */
+  int64_t seed;               /* batch-sampling seed */
+  int64_t fit_normalization;  /* 1: set the feature/output normalisation from the data set first */
+  int64_t reserved[6];
+} axj_train_cfg;
+
+void axj_default_train_cfg(axj_train_cfg* cfg);
+/* Seeded initial model: weights and biases uniform in +-1/sqrt(fan_in), unit normalisation. */
+void axj_mlp_init(axj_mlp* m, int64_t seed);
+/* Install / read the handle's model (the handle needs shock_capturing = 1). */
+int axj_mlp_set(axj_handle* h, const axj_mlp* m);
+int axj_mlp_get(axj_handle* h, axj_mlp* m);
+/* Training data on the device: room for nsnapshots snapshots (24 bytes per grid point
+ * each); axj_dataset_add appends the feature channels and the plain sensor's betastar,
+ * kappastar (before the ramp) of the handle's current solution. */
+int axj_dataset_reserve(axj_handle* h, int64_t nsnapshots);
+int axj_dataset_add(axj_handle* h);
+int axj_dataset_size(axj_handle* h, int64_t* nsnapshots);
+/* Train the installed model with Adam on the data set (FP32, on the device);
+ * loss (nullable) receives cfg->steps batch losses (mean squared error of the
+ * normalised outputs, summed over the two outputs). */
+int axj_mlp_train(axj_handle* h, const axj_train_cfg* cfg, float* loss);
+/* Checks: the normalised batch (X: batch x 100, T: batch x 2) that training step `step`
+ * with `seed` draws; the gradient (in model layout) and loss of the installed model on
+ * a given normalised batch; the feature channels of pv (4 planes of Nz*Nr); the
+ * tensor-core prediction (ramp applied) on pv; judge counters since creation. */
+int axj_dataset_sample(axj_handle* h, int64_t batch, int64_t seed, int64_t step, float* X, float* T);
+int axj_mlp_grad(axj_handle* h, const float* X, const float* T, int64_t batch, axj_mlp* grad, float* loss);
+int axj_mlp_features(axj_handle* h, const double* pv, float* feat);
+int axj_mlp_predict(axj_handle* h, const double* pv, double* betastar, double* kappastar);
+int axj_learned_stats(axj_handle* h, int64_t* judged_outputs, int64_t* fallbacks, int64_t* njudges);
+
 /* Last error message of the handle (or of the last failed axj_create if h is NULL). */
 const char* axj_last_error(const axj_handle* h);
 
