@@ -70,7 +70,8 @@ struct axj_handle {
   cudaGraph_t graph_judge = nullptr;
   // learned sensor
   double S1[9][6];              // SBP first-derivative rows (feature stencils)
-  bool learned = false;
+  bool learned = false;         // learned sensor (or its held-coefficient baseline)
+  bool held_only = false;       // AXJ_SENSOR_HELD: no network between judge steps
   bool judged = false;          // a judge step has run since the state or the model changed
   int64_t judge_every = 50;
   double judge_thr = 0.1;
@@ -437,6 +438,17 @@ InferArgs infer_args(axj_handle* h, int mode) {
 // held values); plain: a later stage of a judge step (the plain path).
 int enqueue_stage_learned(axj_handle* h, int bin, int bout, int stage, bool judge1, bool plain) {
   if (plain) return enqueue_stage(h, bin, bout, stage);
+  if (h->held_only) {
+    if (judge1) {
+      SensorArgs s = sensor_args(h, bin);
+      AXJ_CUDA(h, launch_sensor(s, true, h->side, h->stream));
+    }
+    return launch_stage_kernels(h, bin, bout, stage, true);
+  }
+  // the network runs once per step, on the first stage's input; its coefficients
+  // serve the step's four stages, as the judge's plain values serve the steps between
+  // judges
+  if (stage > 1) return launch_stage_kernels(h, bin, bout, stage, true);
   AXJ_CUDA(h, launch_features(feat_args(h, bin), h->stream));
   if (judge1) {
     SensorArgs s = sensor_args(h, bin);
@@ -499,7 +511,7 @@ int enqueue_rk4(axj_handle* h, bool judge = false) {
 
 // The learned sensor needs a model before any step.
 int check_model(axj_handle* h) {
-  if (h->learned && !h->mlp_set) return fail(h, AXJ_ERR_ARG, "learned sensor without a model (axj_mlp_set / axj_mlp_train)");
+  if (h->learned && !h->held_only && !h->mlp_set) return fail(h, AXJ_ERR_ARG, "learned sensor without a model (axj_mlp_set / axj_mlp_train)");
   return AXJ_OK;
 }
 
@@ -690,11 +702,11 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   if (npatch > MAX_PATCHES) return fail(nullptr, AXJ_ERR_BADPATCH, "more than %d patches", MAX_PATCHES);
   if (prm->precision != AXJ_FP64 && prm->precision != AXJ_MIXED)
     return fail(nullptr, AXJ_ERR_UNSUPPORTED, "precision %lld not built", (long long)prm->precision);
-  if (prm->sensor != AXJ_SENSOR_PLAIN && prm->sensor != AXJ_SENSOR_LEARNED)
+  if (prm->sensor != AXJ_SENSOR_PLAIN && prm->sensor != AXJ_SENSOR_LEARNED && prm->sensor != AXJ_SENSOR_HELD)
     return fail(nullptr, AXJ_ERR_ARG, "sensor %lld unknown", (long long)prm->sensor);
-  if (prm->sensor == AXJ_SENSOR_LEARNED && !prm->shock_capturing)
+  if (prm->sensor != AXJ_SENSOR_PLAIN && !prm->shock_capturing)
     return fail(nullptr, AXJ_ERR_ARG, "the learned sensor needs shock_capturing = 1");
-  if (prm->sensor == AXJ_SENSOR_LEARNED && (prm->judge_every < 1 || !(prm->judge_threshold >= 0.0)))
+  if (prm->sensor != AXJ_SENSOR_PLAIN && (prm->judge_every < 1 || !(prm->judge_threshold >= 0.0)))
     return fail(nullptr, AXJ_ERR_ARG, "judge_every must be >= 1 and judge_threshold >= 0");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -910,7 +922,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->Ua = dalloc<double>(h, 5 * pl, &rc);
   h->Ub = dalloc<double>(h, 5 * pl, &rc);
   h->mixed = prm->precision == AXJ_MIXED;
-  h->learned = prm->sensor == AXJ_SENSOR_LEARNED;
+  h->learned = prm->sensor != AXJ_SENSOR_PLAIN;
+  h->held_only = prm->sensor == AXJ_SENSOR_HELD;
   h->judge_every = prm->judge_every;
   h->judge_thr = prm->judge_threshold;
   if (c.shock_capturing) {
@@ -1164,7 +1177,18 @@ int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launch
     for (int st = 1; st <= 4 && rc == AXJ_OK; ++st) {
       const bool lrn_plain = h->learned && judge && st > 1;
       const bool lrn = h->learned && !lrn_plain;
-      if (lrn) {
+      if (lrn && h->held_only) {
+        if (judge && st == 1) {
+          rc = timed(1, [&]() -> int {
+            SensorArgs sa = sensor_args(h, bufs[st - 1]);
+            AXJ_CUDA(h, launch_sensor(sa, true, h->side, h->stream));
+            return AXJ_OK;
+          });
+          nl[1] += (h->nstiles_int > 0) + (h->nstiles_gen > 0) + 2;
+        }
+      } else if (lrn && st > 1) {
+        // the step's coefficients come from its first stage
+      } else if (lrn) {
         // features + inference (+ plain sensor and judge at the first stage of a judge step)
         rc = timed(1, [&]() -> int {
           AXJ_CUDA(h, launch_features(feat_args(h, bufs[st - 1]), h->stream));

@@ -104,14 +104,28 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// Two floats to a BF16 pair (a in the low half), one packed conversion.
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-  const __nv_bfloat16 x = __float2bfloat16_rn(a), y = __float2bfloat16_rn(b);
-  return (uint32_t)__bfloat16_as_ushort(x) | ((uint32_t)__bfloat16_as_ushort(y) << 16);
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  return r;
 }
 
 }  // namespace
 
 // GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), and its derivative.
+// Inference uses the hardware tanh approximation (one MUFU operation, relative error
+// about 2^-11, below the BF16 rounding of the activations it feeds); training uses tanhf.
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float gelu_fast(float x) {
+  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  const float hx = 0.5f * x;
+  return fmaf(hx, tanh_fast(u), hx);
+}
 __device__ __forceinline__ float gelu_f(float x) {
   const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
   return 0.5f * x * (1.0f + tanhf(u));
@@ -125,87 +139,104 @@ __device__ __forceinline__ float gelu_grad_f(float x) {
 // ---------------------------------------------------------------------------
 // Feature channels
 // ---------------------------------------------------------------------------
-template <typename SIN>
-__device__ __forceinline__ double dval(const SIN* f, const Grid& g, int i, int j) {
-  if (i < 0 || i >= g.Nz || j < 0 || j >= g.Nr) return 0.0;
-  return double(f[(long long)j * g.P + i]);
-}
+// Tile of 32 (z) x 8 (r) points per CTA (256 threads). rho, V_r, V_z of the tile and
+// a halo of 5 (the widest SBP boundary row reaches 5 points) are staged in shared
+// memory as FP32 (zero outside the grid, the never-written halo); each thread forms
+// its six first derivatives in FP32 on differences from its own value: every SBP row
+// sums to zero, so sum c_m (f_m - f_0) equals sum c_m f_m, and the differences of
+// nearby values are exact in FP32 (the network reads its inputs in BF16).
+constexpr int FT_Z = 32, FT_R = 8, FT_H = 5;
+constexpr int FB_Z = FT_Z + 2 * FT_H, FB_R = FT_R + 2 * FT_H;
 
-// SBP first-derivative stencil (row code `row`, 9 = none) along dirn at (i, j), in FP32
-// on differences from the point's own value: every SBP row sums to zero, so
-// sum c_m (f_m - f_0) equals sum c_m f_m, and the differences (formed in FP64) carry
-// no rounding of the field's common level.
-template <typename SIN>
-__device__ __forceinline__ float fd1(const FeatArgs& a, const SIN* f, int row, int i, int j, int dirn) {
+__device__ __forceinline__ float fd1s(const FeatArgs& a, const float* box, int row, int bz, int br, int dirn) {
   if (row >= 9) return 0.0f;
-  const int w0 = sbp_w0(row), n = sbp_len(row);
-  const int di = dirn == 1 ? 1 : 0, dj = dirn == 1 ? 0 : 1;
-  const double f0 = dval(f, a.g, i, j);
-  float s = a.sbp1[row][0] * (float)(dval(f, a.g, i + w0 * di, j + w0 * dj) - f0);
-  for (int m = 1; m < n; ++m)
-    s = s + a.sbp1[row][m] * (float)(dval(f, a.g, i + (w0 + m) * di, j + (w0 + m) * dj) - f0);
+  const int st = dirn == 1 ? 1 : FB_Z;
+  const float* p = box + br * FB_Z + bz;
+  const float f0 = p[0];
+  if (row == 4) {  // centred row
+    float s = a.sbp1[4][0] * (p[-2 * st] - f0);
+#pragma unroll
+    for (int m = 1; m < 5; ++m) s = s + a.sbp1[4][m] * (p[(m - 2) * st] - f0);
+    return s;
+  }
+  const int w0 = sbp_w0(row);
+  float s = a.sbp1[row][0] * (p[w0 * st] - f0);
+#pragma unroll
+  for (int m = 1; m < 6; ++m) s = s + a.sbp1[row][m] * (p[(w0 + m) * st] - f0);
   return s;
 }
 
 template <typename SIN>
-__global__ void features_kernel(const FeatArgs a) {
-  const long long n = (long long)a.g.Nz * a.g.Nr;
+__global__ void __launch_bounds__(256) features_kernel(const FeatArgs a) {
+  __shared__ float sb[3][FB_R * FB_Z];
+  const Grid g = a.g;
+  const int i0 = blockIdx.x * FT_Z, j0 = blockIdx.y * FT_R;
   const SIN* U = static_cast<const SIN*>(a.U);
-  const SIN* rho = U;
-  const SIN* Vr = U + a.g.plane;
-  const SIN* Vz = U + 3 * a.g.plane;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const int j = (int)(p / a.g.Nz), i = (int)(p - (long long)j * a.g.Nz);
-    const long long o = (long long)j * a.g.P + i;
-    const uint32_t dsc = __ldg(a.desc + o);
-    const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
-    const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
-    const float xz = (float)__ldg(a.dxidz + i), er = (float)__ldg(a.detadr + j);
-    const float dVrdz = fd1(a, Vr, zr, i, j, 1) * xz;
-    const float dVzdz = fd1(a, Vz, zr, i, j, 1) * xz;
-    const float drdz = fd1(a, rho, zr, i, j, 1) * xz;
-    const float dVrdr = fd1(a, Vr, rw, i, j, 2) * er;
-    const float dVzdr = fd1(a, Vz, rw, i, j, 2) * er;
-    const float drdr = fd1(a, rho, rw, i, j, 2) * er;
-    const float vr = float(Vr[o]);
-    const float r = (float)__ldg(a.rc + j);
-    const float dil = (j == 0) ? 2.0f * dVrdr + dVzdz : dVrdr + vr / r + dVzdz;
-    const float grad = sqrtf(drdz * drdz + drdr * drdr);
-    const float vort = fabsf(dVrdz - dVzdr);
-    const float h = sqrtf((float)(__ldg(a.dz + i) * __ldg(a.dr + j)));
-    a.feat[o] = make_float4(dil, grad, vort, h);
+  const int fld[3] = {0, 1, 3};  // rho, V_r, V_z
+  for (int e = threadIdx.x; e < 3 * FB_R * FB_Z; e += 256) {
+    const int f = e / (FB_R * FB_Z), q = e - f * (FB_R * FB_Z);
+    const int br = q / FB_Z, bz = q - br * FB_Z;
+    const int i = i0 - FT_H + bz, j = j0 - FT_H + br;
+    float v = 0.0f;
+    if (i >= 0 && i < g.Nz && j >= 0 && j < g.Nr) v = float(U[fld[f] * g.plane + (long long)j * g.P + i]);
+    sb[f][q] = v;
   }
+  __syncthreads();
+  const int tz = threadIdx.x & 31, tr = threadIdx.x >> 5;
+  const int i = i0 + tz, j = j0 + tr;
+  if (i >= g.Nz || j >= g.Nr) return;
+  const long long o = (long long)j * g.P + i;
+  const uint32_t dsc = __ldg(a.desc + o);
+  const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
+  const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
+  const int bz = tz + FT_H, br = tr + FT_H;
+  const float xz = (float)__ldg(a.dxidz + i), er = (float)__ldg(a.detadr + j);
+  const float drdz = fd1s(a, sb[0], zr, bz, br, 1) * xz;
+  const float dVrdz = fd1s(a, sb[1], zr, bz, br, 1) * xz;
+  const float dVzdz = fd1s(a, sb[2], zr, bz, br, 1) * xz;
+  const float drdr = fd1s(a, sb[0], rw, bz, br, 2) * er;
+  const float dVrdr = fd1s(a, sb[1], rw, bz, br, 2) * er;
+  const float dVzdr = fd1s(a, sb[2], rw, bz, br, 2) * er;
+  const float vr = sb[1][br * FB_Z + bz];
+  const float r = (float)__ldg(a.rc + j);
+  const float dil = (j == 0) ? 2.0f * dVrdr + dVzdz : dVrdr + vr / r + dVzdz;
+  const float grad = sqrtf(drdz * drdz + drdr * drdr);
+  const float vort = fabsf(dVrdz - dVzdr);
+  const float h = sqrtf((float)(__ldg(a.dz + i) * __ldg(a.dr + j)));
+  a.feat[o] = make_float4(dil, grad, vort, h);
 }
 
 cudaError_t launch_features(const FeatArgs& a, cudaStream_t s) {
-  const int bs = 256;
-  const long long n = (long long)a.g.Nz * a.g.Nr;
-  const int nb = (int)((n + bs - 1) / bs);
-  if (a.f32) features_kernel<float><<<nb, bs, 0, s>>>(a);
-  else features_kernel<double><<<nb, bs, 0, s>>>(a);
+  const dim3 grid((a.g.Nz + FT_Z - 1) / FT_Z, (a.g.Nr + FT_R - 1) / FT_R);
+  if (a.f32) features_kernel<float><<<grid, 256, 0, s>>>(a);
+  else features_kernel<double><<<grid, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
-// Inference on the tensor cores. One CTA of 128 threads owns TMEM columns [0, 128):
-// layer 1 accumulates in [0, 64), layer 2 in [64, 128). A tile is 32 (z) x 4 (r)
-// points, one point per thread, thread t = row t of the MMA (TMEM lane t).
-// Shared memory (bytes from a 1024-aligned base): W1 64x112 and W2 64x64 in BF16,
-// the A operands 128x112 and 128x64 in BF16, all in the no-swizzle K-major layout
-// with the K chunks outermost (chunk c of 8 K values at c * rows * 16, row group g at
-// g * 128, row r of the group at r * 16); the channel box 4 x 8 x 36 floats; biases
-// and layer 3 in FP32.
+// Inference on the tensor cores. A tile is 32 (z) x 4 (r) points, one point per
+// thread, thread t = row t of the MMA (TMEM lane t). One CTA of 128 threads owns 64
+// TMEM columns: layer 1 accumulates there, and once every thread has read its row,
+// layer 2 accumulates in the same columns. Shared memory (from a 128-aligned base):
+// W1 64x112 and W2 64x64 in BF16; one A operand region of 128x112 BF16 that holds the
+// layer-1 inputs and then (after the layer-1 MMAs completed) the layer-2 inputs, all
+// in the no-swizzle K-major layout with the K chunks outermost (chunk c of 8 K values
+// at c * rows * 16, row group g at g * 128, row r of the group at r * 16); the
+// normalised channel box 4 x 8 x 36 in BF16; biases and layer 3 in FP32. The next
+// tile's channel box is loaded into registers while this tile's MMAs run. About 54 KB
+// per CTA: 4 CTAs (16 warps, 256 TMEM columns) per SM.
 // ---------------------------------------------------------------------------
 constexpr int MT_Z = 32, MT_R = 4, MT_THREADS = 128;
-constexpr int MBOX_Z = MT_Z + 4, MBOX_R = MT_R + 4;
+constexpr int MBOX_Z = MT_Z + 4, MBOX_R = MT_R + 4, MBOX_N = MBOX_Z * MBOX_R;  // 288 points
+constexpr int MBOX_PER = (MBOX_N + MT_THREADS - 1) / MT_THREADS;              // 3
 constexpr uint32_t M_OW1 = 0;
 constexpr uint32_t M_OW2 = M_OW1 + MLP_HID * MLP_K1 * 2;      // 14336
-constexpr uint32_t M_OA1 = M_OW2 + MLP_HID * MLP_HID * 2;     // 22528
-constexpr uint32_t M_OA2 = M_OA1 + MT_THREADS * MLP_K1 * 2;   // 51200
-constexpr uint32_t M_OBOX = M_OA2 + MT_THREADS * MLP_HID * 2; // 67584
-constexpr uint32_t M_OP = M_OBOX + MLP_CH * MBOX_R * MBOX_Z * 4;
+constexpr uint32_t M_OA = M_OW2 + MLP_HID * MLP_HID * 2;      // 22528
+constexpr uint32_t M_OBOX = M_OA + MT_THREADS * MLP_K1 * 2;   // 51200
+constexpr uint32_t M_OP = M_OBOX + MLP_CH * MBOX_N * 2;       // 53504
 constexpr uint32_t M_NP = MLP_HID + MLP_HID + MLP_OUT * MLP_HID + MLP_OUT;
-constexpr size_t M_SMEM = M_OP + M_NP * 4 + 1024;  // + alignment slack
+constexpr size_t M_SMEM = M_OP + M_NP * 4 + 128;  // + alignment slack
+constexpr int M_CTAS_PER_SM = 4;
 
 // byte offset of (row, k) in a K-major operand of `rows` rows
 __device__ __forceinline__ uint32_t kmaj(int row, int k, int rows) {
@@ -216,26 +247,24 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
   extern __shared__ unsigned char m_raw[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
-  unsigned char* base =
-      m_raw + ((1024u - (smem_addr(m_raw) & 1023u)) & 1023u);  // 1024-aligned start of the layout
+  unsigned char* base = m_raw + ((128u - (smem_addr(m_raw) & 127u)) & 127u);  // 128-aligned start
   const uint32_t sb = smem_addr(base);
-  float* sBox = reinterpret_cast<float*>(base + M_OBOX);  // [4][8][36]
+  __nv_bfloat16* sBox = reinterpret_cast<__nv_bfloat16*>(base + M_OBOX);  // [4][8][36]
   float* sB1 = reinterpret_cast<float*>(base + M_OP);
   float* sB2 = sB1 + MLP_HID;
   float* sW3 = sB2 + MLP_HID;  // [2][64]
   float* sB3 = sW3 + MLP_OUT * MLP_HID;
   const int tid = threadIdx.x, warp = tid >> 5;
+  const Grid g = a.g;
 
   // weights in BF16, core-matrix layout
   for (int e = tid; e < MLP_HID * MLP_K1; e += MT_THREADS) {
     const int n = e / MLP_K1, k = e - n * MLP_K1;
-    const __nv_bfloat16 w = __float2bfloat16_rn(a.params[MLP_OFF_W1 + e]);
-    *reinterpret_cast<__nv_bfloat16*>(base + M_OW1 + kmaj(n, k, MLP_HID)) = w;
+    *reinterpret_cast<__nv_bfloat16*>(base + M_OW1 + kmaj(n, k, MLP_HID)) = __float2bfloat16_rn(a.params[MLP_OFF_W1 + e]);
   }
   for (int e = tid; e < MLP_HID * MLP_HID; e += MT_THREADS) {
     const int n = e / MLP_HID, k = e - n * MLP_HID;
-    const __nv_bfloat16 w = __float2bfloat16_rn(a.params[MLP_OFF_W2 + e]);
-    *reinterpret_cast<__nv_bfloat16*>(base + M_OW2 + kmaj(n, k, MLP_HID)) = w;
+    *reinterpret_cast<__nv_bfloat16*>(base + M_OW2 + kmaj(n, k, MLP_HID)) = __float2bfloat16_rn(a.params[MLP_OFF_W2 + e]);
   }
   for (int e = tid; e < MLP_HID; e += MT_THREADS) {
     sB1[e] = a.params[MLP_OFF_B1 + e];
@@ -244,7 +273,41 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
   for (int e = tid; e < MLP_OUT * MLP_HID; e += MT_THREADS) sW3[e] = a.params[MLP_OFF_W3 + e];
   if (tid < MLP_OUT) sB3[tid] = a.params[MLP_OFF_B3 + tid];
   if (tid == 0) bar_init(&bar);
-  if (warp == 0) tmem_alloc(&tmem_slot, 128);
+  if (warp == 0) tmem_alloc(&tmem_slot, 64);
+
+  // channel box of a tile: raw loads (zero outside the grid) into registers ...
+  auto load_box = [&](int t, float4* v) {
+    const int tz = t % a.ntiles_z, tr = t / a.ntiles_z;
+    const int i0 = tz * MT_Z - 2, j0 = tr * MT_R - 2;
+#pragma unroll
+    for (int q = 0; q < MBOX_PER; ++q) {
+      const int e = tid + q * MT_THREADS;
+      v[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (e < MBOX_N) {
+        const int br = e / MBOX_Z, bz = e - br * MBOX_Z;
+        const int i = i0 + bz, j = j0 + br;
+        if (i >= 0 && i < g.Nz && j >= 0 && j < g.Nr) v[q] = __ldg(a.feat + (long long)j * g.P + i);
+      }
+    }
+  };
+  // ... then normalised into the BF16 box
+  auto store_box = [&](const float4* v) {
+#pragma unroll
+    for (int q = 0; q < MBOX_PER; ++q) {
+      const int e = tid + q * MT_THREADS;
+      if (e < MBOX_N) {
+        sBox[0 * MBOX_N + e] = __float2bfloat16_rn((v[q].x - a.norm.feat_mean[0]) * a.norm.feat_inv_scale[0]);
+        sBox[1 * MBOX_N + e] = __float2bfloat16_rn((v[q].y - a.norm.feat_mean[1]) * a.norm.feat_inv_scale[1]);
+        sBox[2 * MBOX_N + e] = __float2bfloat16_rn((v[q].z - a.norm.feat_mean[2]) * a.norm.feat_inv_scale[2]);
+        sBox[3 * MBOX_N + e] = __float2bfloat16_rn((v[q].w - a.norm.feat_mean[3]) * a.norm.feat_inv_scale[3]);
+      }
+    }
+  };
+  float4 nxt[MBOX_PER];
+  if (blockIdx.x < a.ntiles) {
+    load_box(blockIdx.x, nxt);
+    store_box(nxt);
+  }
   fence_async_smem();
   tc_fence_before();
   __syncthreads();
@@ -252,45 +315,32 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
   const uint32_t tmem = tmem_slot;
   const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
 
-  const Grid g = a.g;
   const int c = tid & 31, rr = tid >> 5;  // this thread's point in the tile
   uint32_t phase = 0;
   bool ok = true;
   for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
     const int tz = t % a.ntiles_z, tr = t / a.ntiles_z;
     const int i0 = tz * MT_Z, j0 = tr * MT_R;
-    // channel box (z: i0-2 .. i0+33, r: j0-2 .. j0+5), zero outside the block, normalised
-    for (int e = tid; e < MBOX_R * MBOX_Z; e += MT_THREADS) {
-      const int br = e / MBOX_Z, bz = e - br * MBOX_Z;
-      const int i = i0 - 2 + bz, j = j0 - 2 + br;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (i >= 0 && i < g.Nz && j >= 0 && j < g.Nr) v = __ldg(a.feat + (long long)j * g.P + i);
-      sBox[(0 * MBOX_R + br) * MBOX_Z + bz] = (v.x - a.norm.feat_mean[0]) * a.norm.feat_inv_scale[0];
-      sBox[(1 * MBOX_R + br) * MBOX_Z + bz] = (v.y - a.norm.feat_mean[1]) * a.norm.feat_inv_scale[1];
-      sBox[(2 * MBOX_R + br) * MBOX_Z + bz] = (v.z - a.norm.feat_mean[2]) * a.norm.feat_inv_scale[2];
-      sBox[(3 * MBOX_R + br) * MBOX_Z + bz] = (v.w - a.norm.feat_mean[3]) * a.norm.feat_inv_scale[3];
-    }
-    __syncthreads();
-    // A1 row `tid`: feature k = ch*25 + (dr+2)*5 + (dz+2), zero for k >= 100
+    // A row `tid` of layer 1: feature k = ch*25 + (dr+2)*5 + (dz+2), zero for k >= 100
+    const unsigned short* bx = reinterpret_cast<const unsigned short*>(sBox);
 #pragma unroll
     for (int kc = 0; kc < MLP_K1 / 8; ++kc) {
       uint32_t pk[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        float f[2];
+        uint32_t hv[2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int k = kc * 8 + 2 * q + h;
-          float v = 0.0f;
+          hv[h] = 0u;
           if (k < MLP_IN) {
             const int ch = k / 25, w = k - ch * 25, dr = w / 5, dz = w - dr * 5;
-            v = sBox[(ch * MBOX_R + rr + dr) * MBOX_Z + c + dz];
+            hv[h] = bx[ch * MBOX_N + (rr + dr) * MBOX_Z + c + dz];
           }
-          f[h] = v;
         }
-        pk[q] = pack_bf16(f[0], f[1]);
+        pk[q] = hv[0] | (hv[1] << 16);
       }
-      *reinterpret_cast<uint4*>(base + M_OA1 + kmaj(tid, kc * 8, MT_THREADS)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      *reinterpret_cast<uint4*>(base + M_OA + kmaj(tid, kc * 8, MT_THREADS)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
     fence_async_smem();
     tc_fence_before();
@@ -299,28 +349,32 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
       tc_fence_after();
 #pragma unroll
       for (int s = 0; s < MLP_K1 / 16; ++s)
-        mma_bf16(tmem, mdesc(sb + M_OA1 + s * 2 * MT_THREADS * 16, MT_THREADS * 16, 128),
+        mma_bf16(tmem, mdesc(sb + M_OA + s * 2 * MT_THREADS * 16, MT_THREADS * 16, 128),
                  mdesc(sb + M_OW1 + s * 2 * MLP_HID * 16, MLP_HID * 16, 128), IDESC_BF16_M128_N64, s > 0);
       mma_commit(&bar);
     }
     __syncwarp();
+    // the next tile's channel values travel while the MMAs run
+    const int tn = t + gridDim.x;
+    if (tn < a.ntiles) load_box(tn, nxt);
     ok = __syncthreads_and(bar_wait(&bar, phase));
     phase ^= 1u;
     if (!ok) break;
     tc_fence_after();
-    // layer 1 epilogue: z1 + b1 -> GELU -> BF16 row of A2
+    // layer 1 epilogue: z1 + b1 -> GELU -> BF16 row of the layer-2 A operand, written
+    // over the layer-1 operand (its MMAs completed)
+    float z[MLP_HID];
 #pragma unroll
-    for (int q = 0; q < MLP_HID / 16; ++q) {
-      float v[16];
-      tmem_ld16(lane_base + q * 16, v);
-      tmem_wait_ld();
-      uint32_t pk[8];
+    for (int q = 0; q < MLP_HID / 16; ++q) tmem_ld16(lane_base + q * 16, z + q * 16);
+    tmem_wait_ld();
 #pragma unroll
-      for (int h = 0; h < 8; ++h)
-        pk[h] = pack_bf16(gelu_f(v[2 * h] + sB1[q * 16 + 2 * h]), gelu_f(v[2 * h + 1] + sB1[q * 16 + 2 * h + 1]));
-      *reinterpret_cast<uint4*>(base + M_OA2 + kmaj(tid, q * 16, MT_THREADS)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-      *reinterpret_cast<uint4*>(base + M_OA2 + kmaj(tid, q * 16 + 8, MT_THREADS)) =
-          make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    for (int q = 0; q < MLP_HID / 8; ++q) {
+      uint32_t pk[4];
+#pragma unroll
+      for (int h = 0; h < 4; ++h)
+        pk[h] = pack_bf16(gelu_fast(z[q * 8 + 2 * h] + sB1[q * 8 + 2 * h]),
+                          gelu_fast(z[q * 8 + 2 * h + 1] + sB1[q * 8 + 2 * h + 1]));
+      *reinterpret_cast<uint4*>(base + M_OA + kmaj(tid, q * 8, MT_THREADS)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
     fence_async_smem();
     tc_fence_before();
@@ -329,28 +383,27 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
       tc_fence_after();
 #pragma unroll
       for (int s = 0; s < MLP_HID / 16; ++s)
-        mma_bf16(tmem + 64, mdesc(sb + M_OA2 + s * 2 * MT_THREADS * 16, MT_THREADS * 16, 128),
+        mma_bf16(tmem, mdesc(sb + M_OA + s * 2 * MT_THREADS * 16, MT_THREADS * 16, 128),
                  mdesc(sb + M_OW2 + s * 2 * MLP_HID * 16, MLP_HID * 16, 128), IDESC_BF16_M128_N64, s > 0);
       mma_commit(&bar);
     }
     __syncwarp();
+    // the box of this tile is no longer read: the next tile's goes in while the MMAs run
+    if (tn < a.ntiles) store_box(nxt);
     ok = __syncthreads_and(bar_wait(&bar, phase));
     phase ^= 1u;
     if (!ok) break;
     tc_fence_after();
     // layer 2 epilogue and layer 3 (64 -> 2) in FP32
+#pragma unroll
+    for (int q = 0; q < MLP_HID / 16; ++q) tmem_ld16(lane_base + q * 16, z + q * 16);
+    tmem_wait_ld();
     float y0 = sB3[0], y1 = sB3[1];
 #pragma unroll
-    for (int q = 0; q < MLP_HID / 16; ++q) {
-      float v[16];
-      tmem_ld16(lane_base + 64 + q * 16, v);
-      tmem_wait_ld();
-#pragma unroll
-      for (int h = 0; h < 16; ++h) {
-        const float hv = gelu_f(v[h] + sB2[q * 16 + h]);
-        y0 = fmaf(sW3[q * 16 + h], hv, y0);
-        y1 = fmaf(sW3[MLP_HID + q * 16 + h], hv, y1);
-      }
+    for (int h = 0; h < MLP_HID; ++h) {
+      const float hv = gelu_fast(z[h] + sB2[h]);
+      y0 = fmaf(sW3[h], hv, y0);
+      y1 = fmaf(sW3[MLP_HID + h], hv, y1);
     }
     tc_fence_before();
     const int i = i0 + c, j = j0 + rr;
@@ -368,6 +421,7 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
         a.out[2 * g.plane + o] = (m & 2) ? __ldg(a.held + g.plane + o) : p1;
       }
     }
+    fence_async_smem();  // the next tile's box (generic writes) before its A operand is built
     __syncthreads();
   }
   if (!ok) {
@@ -379,7 +433,7 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tmem_dealloc(tmem, 128);
+  if (warp == 0) tmem_dealloc(tmem, 64);
 }
 
 cudaError_t mlp_init_attributes() {
@@ -390,8 +444,8 @@ cudaError_t launch_mlp_infer(const InferArgs& a, cudaStream_t s) {
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  // at most 3 CTAs per SM (shared memory), 3 x 128 of the 512 TMEM columns
-  const int grid = a.ntiles < 3 * nsm ? a.ntiles : 3 * nsm;
+  // at most 4 CTAs per SM (shared memory): 4 x 64 of the 512 TMEM columns
+  const int grid = a.ntiles < M_CTAS_PER_SM * nsm ? a.ntiles : M_CTAS_PER_SM * nsm;
   if (grid <= 0) return cudaSuccess;
   mlp_infer_kernel<<<grid, MT_THREADS, M_SMEM, s>>>(a);
   return cudaGetLastError();

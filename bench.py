@@ -262,8 +262,13 @@ def main():
 
     variants = None
     if not args.no_variants:
+        from axisymmetricjet_b200.train_sensor import MODEL_FILE, load_model
         variants = {"mixed": time_variant(args, c, patches, npts, world, barrier, max_over_ranks, precision=1)}
-        variants["mixed"]["speedup_vs_fp64"] = variants["mixed"]["value"] / value
+        if os.path.exists(MODEL_FILE):
+            variants["mixed_learned"] = time_variant(args, c, patches, npts, world, barrier, max_over_ranks,
+                                                     model=load_model(), precision=1, sensor=1)
+        for v in variants.values():
+            v["speedup_vs_fp64"] = v["value"] / value
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -297,15 +302,18 @@ def main():
     return 0
 
 
-def time_variant(args, c, patches, npts, world, barrier, max_over_ranks, **pkw):
+def time_variant(args, c, patches, npts, world, barrier, max_over_ranks, model=None, **pkw):
     """The same workload and timing (graph-captured steps, CUDA events, max over ranks)
-    with changed solver parameters, e.g. precision = AXJ_MIXED."""
+    with changed solver parameters, e.g. precision = AXJ_MIXED; `model` is installed for
+    the learned sensor (its judge steps are part of the timed steps)."""
     import axisymmetricjet_b200 as axj
     from axisymmetricjet_b200._ffi import AxjParams
     prm = AxjParams.from_buffer_copy(c["params"])
     for k, v in pkw.items():
         setattr(prm, k, v)
     s = axj.AxiJetSolver(prm, c["zvec"], c["rvec"], c["ibval"], patches)
+    if model is not None:
+        s.mlp_set(model)
     s.set_state(c["pv"], c["target"])
     s.run(args.warmup)
     barrier()

@@ -84,7 +84,9 @@ enum axj_precision {
 /* sensor values (artificial-diffusivity sensor, used when shock_capturing = 1). */
 enum axj_sensor_kind {
   AXJ_SENSOR_PLAIN = 0,   /* ModShockCapturing.f90:5-106 */
-  AXJ_SENSOR_LEARNED = 1  /* MLP stand-in, plain sensor as periodic judge */
+  AXJ_SENSOR_LEARNED = 1, /* MLP stand-in, plain sensor as periodic judge */
+  AXJ_SENSOR_HELD = 2     /* baseline of the learned sensor without the network: the plain
+                             sensor's coefficients of the last judge step are held between judges */
 };
 
 /* Run parameters: the reference's compile-time module variables
@@ -216,8 +218,9 @@ int axj_compute_dt_noalloc(const double* d_pv, int64_t pitch, int64_t Nz, int64_
  * No counterpart in the reference. A small MLP stands in for the evaluation of
  * betastar and kappastar (ModShockCapturing.f90:18-92): 100 inputs (4 channels x a
  * 5 x 5 (z, r) window), two hidden layers of 64 with the tanh-form GELU, 2 outputs,
- * BF16 weights and FP32 accumulation on the tensor cores at inference. mustar keeps
- * the plain sensor's value of the last judge step. The plain sensor runs on the first
+ * BF16 weights and FP32 accumulation on the tensor cores at inference. The network
+ * runs once per step on the first stage's input and its coefficients serve the
+ * step's four stages. mustar keeps the plain sensor's value of the last judge step. The plain sensor runs on the first
  * stage of every judge_every-th step (and on the first step after axj_set_state,
  * axj_mlp_set or training) as judge: wherever |prediction - plain| exceeds
  * judge_threshold x the largest |plain| in the point's 5 x 5 window, the plain value

@@ -2,7 +2,7 @@
 kernels and the judge, against the NumPy oracle (oracle/oracle_mlp.py) and the C oracle.
 
 Tolerances (written per test):
-  features        1e-5 of each channel's max (FP32 stencils vs the FP64 oracle)
+  features        1e-4 of each channel's max (FP32 inputs and stencils vs the FP64 oracle)
   gradients       1e-4 of each tensor's max (FP32 GEMMs with atomics vs FP64)
   Adam step       1e-5 of each tensor's max (same gradient, FP32 vs FP64 update)
   sampler         exact indices; features 1e-6, targets 1e-5 relative
@@ -98,7 +98,7 @@ def test_features_vs_oracle(oracle_mod, name):
     got = dev.mlp_features(pv)
     want = om.features(ora, pv, c["z"], c["r"])
     for ch in range(4):
-        assert _relmax(got[ch], want[ch]) < 1e-5, ch
+        assert _relmax(got[ch], want[ch]) < 1e-4, ch
     dev.close()
 
 
