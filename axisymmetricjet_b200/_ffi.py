@@ -50,7 +50,10 @@ class AxjParams(C.Structure):
         ("judge_every", C.c_int64),
         ("judge_threshold", C.c_double),
         ("device", C.c_int64),
-        ("reserved", C.c_int64 * 7),
+        ("harmonic_amp", C.c_double),
+        ("harmonic_st", C.c_double),
+        ("harmonic_uj", C.c_double),
+        ("reserved", C.c_int64 * 4),
     ]
 
 

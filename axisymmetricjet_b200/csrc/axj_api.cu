@@ -63,6 +63,7 @@ struct axj_handle {
   int iT = 0, jT = 0;
   int64_t iteration = 0;
   double time_host = 0.0;
+  double time_end = 0.0;  // staging for the device time upload of axj_rk4_step
   bool state_set = false;
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -290,6 +291,7 @@ StageArgs stage_args(axj_handle* h, int bin, int bout, int stage) {
   a.ramp = h->ramp;
   a.dt = h->dt;
   a.staleT = h->staleT;
+  a.time = h->time;
   a.flags = h->flags;
   a.stage = stage;
   a.iT = h->iT;
@@ -755,7 +757,9 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   c.r_top = rvec[(Nr - 1) * Nz];
   c.do_viscous = prm->do_viscous_terms == 1;
   c.shock_capturing = prm->shock_capturing == 1;
-  c.control_forcing = prm->control_forcing == 1;
+  c.control_forcing = (prm->control_forcing == 1 || prm->control_forcing == 2) ? (int)prm->control_forcing : 0;
+  c.harm_amp = prm->harmonic_amp;
+  c.harm_omega = 2.0 * 3.141592653589793 * prm->harmonic_st * prm->harmonic_uj;
   c.dt_mode = (int)prm->dt_mode;
   c.npatch = (int)npatch;
 
@@ -1069,6 +1073,9 @@ int axj_rk4_step(axj_handle* h, double delt) {
   AXJ_CUDA(h, cudaSetDevice(h->device));
   AXJ_CUDA(h, cudaMemcpyAsync(h->dt, &delt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
   if (int rc0 = check_model(h)) return rc0;
+  // the stages read the step's end time t_n + delt, as after the dt kernel of axj_run
+  h->time_end = h->time_host + delt;
+  AXJ_CUDA(h, cudaMemcpyAsync(h->time, &h->time_end, sizeof(double), cudaMemcpyHostToDevice, h->stream));
   const bool judge = judge_due(h);
   int rc = enqueue_rk4(h, judge);
   if (rc != AXJ_OK) return rc;

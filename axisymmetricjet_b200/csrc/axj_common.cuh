@@ -80,9 +80,10 @@ struct Consts {
   double C_mu_Re, C_beta_Re, C_kappa_Re_Pr;  // C_mu*Re, C_beta*Re, (C_kappa*Re)*Pr
   double forcing_alpha, forcing_z0, forcing_r0, forcing_lz, forcing_lr;
   double r_top;   // r(i, Nr): sponge normalisation (ModBC.f90:571)
+  double harm_amp, harm_omega;  // harmonic forcing (control_forcing == 2): A, 2 pi St U_j
   int do_viscous;
   int shock_capturing;
-  int control_forcing;
+  int control_forcing;  // 0 off, 1 feedback (ControlForcingTerms), 2 harmonic source
   int dt_mode;
   int npatch;
 };

@@ -362,6 +362,13 @@ __global__ void __launch_bounds__(STAGE_THREADS)
     }
   }
   const double dtv = a.stage > 0 ? *a.dt : 0.0;
+  // stage time t_n + c_s dt, c = (0, 1/2, 1/2, 1); the device time is t_n + dt in stages 1-4
+  double tstage = 0.0;
+  if (a.c.control_forcing == 2) {
+    const double tend = *a.time;
+    const double cs = a.stage == 1 ? 0.0 : (a.stage == 4 ? 1.0 : 0.5);
+    tstage = a.stage == 0 ? tend : (tend - dtv) + cs * dtv;
+  }
   for (int pidx = tid; pidx < TZ * TR; pidx += STAGE_THREADS) {
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
@@ -447,13 +454,14 @@ __global__ void __launch_bounds__(STAGE_THREADS)
     }
     // pv_target is read only where a term uses it: sponges, face operations, forcing
     const bool need_tg = (rloc >= a.c.sponge_start_top) || (!j1 && zloc <= a.c.sponge_end_left) ||
-                         a.c.control_forcing || (GEN && face);
+                         a.c.control_forcing == 1 || (GEN && face);
     double tg[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (need_tg) {
 #pragma unroll
       for (int f = 0; f < 5; ++f) tg[f] = __ldg(a.target + f * PL + go);
     }
-    if (a.c.control_forcing) control_forcing(zloc, rloc, a.c, a.forcing, pv, tg, rhs);
+    if (a.c.control_forcing == 1) control_forcing(zloc, rloc, a.c, a.forcing, pv, tg, rhs);
+    else if (a.c.control_forcing == 2) harmonic_forcing(zloc, rloc, tstage, a.c, rhs);
     if (GEN && face) {
       const Prim qd = convert<double>(q);
       const Deriv dd = convert<double>(d);

@@ -52,6 +52,7 @@ struct StageArgs {
   const double* ramp;     // shock-capturing z ramp (1+tanh(5(z-10)))/2
   const double* dt;       // device dt (read by stages 1-4)
   double* staleT;         // stage 4: T(i*, j*) of its input, the next ComputeTimeStep's stale T
+  const double* time;     // t_n + dt during stages 1-4 (advanced by the dt kernel); t_n in stage 0
   int* flags;             // bit 0: non-finite value produced
   int stage;              // 0: write rhs only; 1..4: RK4 stage
   int iT, jT;             // stale-T point (0-based)

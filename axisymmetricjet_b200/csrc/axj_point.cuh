@@ -287,6 +287,15 @@ AXJ_HD void control_forcing(double z, double r, const Consts& c, const double* F
     for (int k = 0; k < 5; ++k) rhs[e] = rhs[e] + c.forcing_alpha * F[e * 5 + k] * G * (pv[k] - tg[k]);
 }
 
+// Harmonic inflow forcing (control_forcing = 2, an extension; the reference's
+// ControlForcingTerms is the feedback above): rhs(V_z) += A omega G cos(omega t) in the
+// same Gaussian window, a V_z fluctuation of amplitude A G.
+AXJ_HD void harmonic_forcing(double z, double r, double t, const Consts& c, double rhs[5]) {
+  double dz = z - c.forcing_z0, dr = r - c.forcing_r0;
+  double G = exp(-((dz * dz) / (c.forcing_lz * c.forcing_lz)) - (dr * dr) / (c.forcing_lr * c.forcing_lr));
+  rhs[3] = rhs[3] + c.harm_amp * c.harm_omega * G * cos(c.harm_omega * t);
+}
+
 // Per-point dt of ComputeTimeStep (ModInputOutput.f90:395-416).
 AXJ_HD double dt_point(double Vz, double Vr, double Ts, double mu, double lambda, double kappa, double dxidz,
                        double detadr, const Consts& c) {

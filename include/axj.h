@@ -106,14 +106,23 @@ typedef struct axj_params {
   double forcing_mat[25];     /* F(eqn,k) stored row-major: forcing_mat[(eqn-1)*5 + (k-1)] */
   int64_t do_viscous_terms;   /* 1            :71 */
   int64_t shock_capturing;    /* 0            :152 */
-  int64_t control_forcing;    /* 0            :185 */
+  int64_t control_forcing;    /* 0 (:185); 1: ControlForcingTerms feedback; 2: harmonic source (below) */
   int64_t dt_mode;            /* AXJ_DT_REFERENCE */
   int64_t precision;          /* AXJ_FP64 */
   int64_t sensor;             /* AXJ_SENSOR_PLAIN */
   int64_t judge_every;        /* learned sensor: plain-sensor judge period in steps (50) */
   double judge_threshold;     /* learned sensor: fallback where |pred-plain| > thr * local max (0.1) */
   int64_t device;             /* CUDA device ordinal the handle lives on (0) */
-  int64_t reserved[7];
+  /* control_forcing = 2, an extension with no counterpart in the reference (whose
+   * ControlForcingTerms is steady linear feedback): azimuthal-mode-0 harmonic forcing in
+   * the same Gaussian window G(z,r) = exp(-(z-z0)^2/lz^2 - (r-r0)^2/lr^2). The source
+   * rhs(V_z) += A * omega * G * cos(omega * t), omega = 2 pi St U_j / D (D = 1), imposes
+   * a V_z fluctuation of amplitude A * G; t is the stage time t_n + c_s dt, c = (0, 1/2,
+   * 1/2, 1). */
+  double harmonic_amp;        /* A (velocity units) */
+  double harmonic_st;         /* Strouhal number St */
+  double harmonic_uj;         /* jet velocity U_j */
+  int64_t reserved[4];
 } axj_params;
 
 typedef struct axj_handle axj_handle;

@@ -58,6 +58,7 @@ typedef struct axo {
   I8 no_bcs;
   double T;       /* the module scalar T (ModuleVariables.f90:53) */
   double delt, time;
+  double t_stage;  /* time of the current RHS evaluation (harmonic forcing) */
   I8 iteration;
 } axo;
 
@@ -639,6 +640,21 @@ static void control_forcing(axo* o) {
     }
 }
 
+/* Harmonic inflow forcing (control_forcing = 2): an extension with no counterpart in the
+ * reference, rhs(V_z) += A omega G cos(omega t) in the ControlForcingTerms window. */
+static void harmonic_forcing(axo* o, double t) {
+  const axj_params* p = &o->p;
+  const double omega = 2.0 * 3.141592653589793 * p->harmonic_st * p->harmonic_uj;
+#pragma omp parallel for schedule(static)
+  for (I8 j = 1; j <= o->Nr; ++j)
+    for (I8 i = 1; i <= o->Nz; ++i) {
+      double zl = H(o, zvec, i, j), rl = H(o, rvec, i, j);
+      double dz = zl - p->forcing_z0, dr = rl - p->forcing_r0;
+      double G = exp(-((dz * dz) / (p->forcing_lz * p->forcing_lz)) - (dr * dr) / (p->forcing_lr * p->forcing_lr));
+      S5(o, rhs, i, j, 4) = S5(o, rhs, i, j, 4) + p->harmonic_amp * omega * G * cos(omega * t);
+    }
+}
+
 /* ComputeRHS (ModRHS.f90:5-258) */
 static void compute_rhs(axo* o) {
   const I8 Nz = o->Nz, Nr = o->Nr;
@@ -745,6 +761,7 @@ static void compute_rhs(axo* o) {
     if (Nr >= j0) o->T = H(o, Tvec, Nz, Nr);
   }
   if (o->p.control_forcing == 1) control_forcing(o);
+  else if (o->p.control_forcing == 2) harmonic_forcing(o, o->t_stage);
   boundary_conditions(o);
   sponge_bcs(o);
 }
@@ -896,8 +913,10 @@ int axo_rk4_step(axo* o, double delt) {
   memcpy(o->pv_old, o->pv, n * sizeof(double));
   double* ks[4] = {o->k1, o->k2, o->k3, o->k4};
   const double a[3] = {0.5, 0.5, 1.0};
+  const double cs[4] = {0.0, 0.5, 0.5, 1.0};
   for (int s = 0; s < 4; ++s) {
     assign_values(o);
+    o->t_stage = (o->time + delt) - delt + cs[s] * delt;
     compute_rhs(o);
     double* k = ks[s];
     for (size_t x = 0; x < n; ++x) k[x] = delt * o->rhs[x];
@@ -930,6 +949,7 @@ int axo_rhs(axo* o, const double* pv, double* rhs) {
   double Tsave = o->T;
   memcpy(o->pv, pv, n * sizeof(double));
   assign_values(o);
+  o->t_stage = o->time;
   compute_rhs(o);
   memcpy(rhs, o->rhs, n * sizeof(double));
   memcpy(o->pv, save, n * sizeof(double));

@@ -36,6 +36,10 @@ CASES = {
         "jet96x64", control_forcing=1, forcing_z0=3.0, forcing_r0=0.5, forcing_lz=1.0, forcing_lr=0.3,
         forcing_mat=np.arange(25.0).reshape(5, 5) * 1e-3, dt_mode=1),
     "jet_ragged": lambda: fixtures.make_case(77, 45, 30.0, 15.0, 0.9, 1000.0),
+    # harmonic inflow forcing (control_forcing = 2), the batched instances' forcing
+    "jet_harmonic": lambda: fixtures.case(
+        "jet96x64", control_forcing=2, forcing_z0=1.0, forcing_r0=0.5, forcing_lz=0.5, forcing_lr=0.2,
+        harmonic_amp=0.018, harmonic_st=0.4, harmonic_uj=0.9),
 }
 
 
@@ -100,8 +104,9 @@ def test_rk4_steps(oracle_mod, name):
     assert abs(dev.get_time()[1] - ora.get_time()[1]) <= 1e-15
 
 
-def test_graph_run_equals_stepping(oracle_mod):
-    c = CASES["jet_sc"]()
+@pytest.mark.parametrize("name", ["jet_sc", "jet_harmonic"])
+def test_graph_run_equals_stepping(oracle_mod, name):
+    c = CASES[name]()
     dev, ora = pair(c, oracle_mod)
     dev2, _ = pair(c, oracle_mod)
     dlast = dev.run(5)
