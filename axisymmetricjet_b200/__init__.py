@@ -15,10 +15,10 @@ import os
 
 import numpy as np
 
-from ._ffi import (AXJ_OK, STATUS, AxjBcRecord, AxjMlp, AxjParams, AxjPatch, AxjTrainCfg, default_params,
-                   default_train_cfg, dptr, patch_array, patches_to_tuples, record_array)
+from ._ffi import (AXJ_OK, STATUS, AxjBatchTuning, AxjBcRecord, AxjMlp, AxjParams, AxjPatch, AxjTrainCfg,
+                   default_params, default_train_cfg, dptr, patch_array, patches_to_tuples, record_array)
 
-__all__ = ["AxiJetSolver", "AxjError", "AxjMlp", "default_params", "default_train_cfg", "load_library",
+__all__ = ["AxiJetSolver", "AxjBatch", "AxjError", "AxjMlp", "default_params", "default_train_cfg", "load_library",
            "read_bc_file", "patches_from_records", "library_path", "mlp_init"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -85,6 +85,15 @@ def load_library():
         "axj_mlp_features": (C.c_int, [h, dp, fp]),
         "axj_mlp_predict": (C.c_int, [h, dp, dp, dp]),
         "axj_learned_stats": (C.c_int, [h, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]),
+        "axj_batch_default_tuning": (None, [C.POINTER(AxjBatchTuning)]),
+        "axj_batch_create": (C.c_int, [C.POINTER(h), i64, C.POINTER(h)]),
+        "axj_batch_run": (C.c_int, [h, i64]),
+        "axj_batch_run_timed": (C.c_int, [h, i64, dp]),
+        "axj_batch_set_tuning": (C.c_int, [h, C.POINTER(AxjBatchTuning)]),
+        "axj_batch_get_tuning": (C.c_int, [h, C.POINTER(AxjBatchTuning)]),
+        "axj_batch_autotune": (C.c_int, [h, i64, C.POINTER(AxjBatchTuning), dp, C.POINTER(i64)]),
+        "axj_batch_last_error": (C.c_char_p, [h]),
+        "axj_batch_destroy": (None, [h]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -322,6 +331,65 @@ class AxiJetSolver:
         a, b, c = C.c_int64(0), C.c_int64(0), C.c_int64(0)
         self._chk(self.lib.axj_learned_stats(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return {"judged_outputs": a.value, "fallbacks": b.value, "judges": c.value}
+
+
+class AxjBatch:
+    """Many AxiJetSolver instances advanced together (axj_batch_*): every kernel of the
+    step runs once for all instances, the step is graph-captured. The solvers keep their
+    state; close the batch before them."""
+
+    def __init__(self, solvers):
+        self.lib = load_library()
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s.h for s in self.solvers])
+        b = C.c_void_p()
+        rc = self.lib.axj_batch_create(arr, len(self.solvers), C.byref(b))
+        if rc != AXJ_OK:
+            raise AxjError(rc, self.lib.axj_batch_last_error(None).decode())
+        self.b = b
+
+    def _chk(self, rc):
+        if rc != AXJ_OK:
+            raise AxjError(rc, self.lib.axj_batch_last_error(self.b).decode())
+
+    def run(self, nsteps):
+        self._chk(self.lib.axj_batch_run(self.b, int(nsteps)))
+
+    def run_timed(self, nsteps):
+        ms = C.c_double(0.0)
+        self._chk(self.lib.axj_batch_run_timed(self.b, int(nsteps), C.byref(ms)))
+        return ms.value
+
+    def tuning(self):
+        t = AxjBatchTuning()
+        self._chk(self.lib.axj_batch_get_tuning(self.b, C.byref(t)))
+        return t.to_dict()
+
+    def set_tuning(self, **kw):
+        t = AxjBatchTuning()
+        self._chk(self.lib.axj_batch_get_tuning(self.b, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self._chk(self.lib.axj_batch_set_tuning(self.b, C.byref(t)))
+
+    def autotune(self, steps_per_trial=5):
+        """Time every candidate tuning, keep the fastest; returns (chosen, trial times in ms)."""
+        t = AxjBatchTuning()
+        ms = (C.c_double * 8)()
+        n = C.c_int64(0)
+        self._chk(self.lib.axj_batch_autotune(self.b, int(steps_per_trial), C.byref(t), ms, C.byref(n)))
+        return t.to_dict(), list(ms)[:n.value]
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.axj_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _fptr(a):

@@ -123,6 +123,15 @@ def default_train_cfg(**overrides):
     return c
 
 
+class AxjBatchTuning(C.Structure):
+    _fields_ = [("tile_order", C.c_int64), ("stage_ctas_per_sm", C.c_int64), ("sensor_ctas_per_sm", C.c_int64),
+                ("reserved", C.c_int64 * 5)]
+
+    def to_dict(self):
+        return {"tile_order": self.tile_order, "stage_ctas_per_sm": self.stage_ctas_per_sm,
+                "sensor_ctas_per_sm": self.sensor_ctas_per_sm}
+
+
 def default_params(**overrides):
     """The reference defaults of ModuleVariables.f90:4-188 (same as axj_default_params)."""
     p = AxjParams()

@@ -55,6 +55,7 @@ struct axj_handle {
   double *dxidz = nullptr, *ddxidxidz = nullptr, *detadr = nullptr, *ddetadetadr = nullptr;
   double *zc = nullptr, *rc = nullptr, *dzv = nullptr, *drv = nullptr, *ramp = nullptr, *forcing = nullptr;
   double *dt = nullptr, *staleT = nullptr, *partial = nullptr, *time = nullptr;
+  double* harm = nullptr;  // cos(omega t_s) of the harmonic forcing per stage
   int* flags = nullptr;
   unsigned int* counter = nullptr;
   int2 *tiles_int = nullptr, *tiles_gen = nullptr;
@@ -291,7 +292,7 @@ StageArgs stage_args(axj_handle* h, int bin, int bout, int stage) {
   a.ramp = h->ramp;
   a.dt = h->dt;
   a.staleT = h->staleT;
-  a.time = h->time;
+  a.harm = h->harm;
   a.flags = h->flags;
   a.stage = stage;
   a.iT = h->iT;
@@ -479,7 +480,7 @@ void rk4_buffers(const axj_handle* h, int b[5]) {
 
 // ComputeTimeStep on the device; with advance != 0 the kernel also performs
 // time = time + delt for the step this dt is used by (ModRungeKutta.f90:152-155).
-int enqueue_dt(axj_handle* h, int advance) {
+DtArgs dt_args(axj_handle* h, int advance) {
   DtArgs d;
   d.g = grid_of(h);
   d.U = h->U0;
@@ -494,7 +495,11 @@ int enqueue_dt(axj_handle* h, int advance) {
   d.time = h->time;
   d.advance = advance;
   d.c = h->c;
-  AXJ_CUDA(h, launch_dt(d, h->dt_blocks, h->stream));
+  return d;
+}
+
+int enqueue_dt(axj_handle* h, int advance) {
+  AXJ_CUDA(h, launch_dt(dt_args(h, advance), h->dt_blocks, h->stream));
   return AXJ_OK;
 }
 
@@ -503,6 +508,8 @@ int enqueue_dt(axj_handle* h, int advance) {
 int enqueue_rk4(axj_handle* h, bool judge = false) {
   int b[5];
   rk4_buffers(h, b);
+  if (h->c.control_forcing == 2)
+    AXJ_CUDA(h, launch_harmonic_phase(h->time, h->dt, h->c.harm_omega, 0, h->harm, h->stream));
   for (int st = 1; st <= 4; ++st) {
     const int rc = h->learned ? enqueue_stage_learned(h, b[st - 1], b[st], st, judge && st == 1, judge && st > 1)
                               : enqueue_stage(h, b[st - 1], b[st], st);
@@ -967,6 +974,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->dt = dalloc<double>(h, 1, &rc);
   h->staleT = dalloc<double>(h, 1, &rc);
   h->time = dalloc<double>(h, 1, &rc);
+  h->harm = dalloc<double>(h, 5, &rc);
   h->flags = dalloc<int>(h, 1, &rc);
   h->counter = dalloc<unsigned int>(h, 1, &rc);
   h->dt_blocks = 148 * 4;
@@ -1179,8 +1187,13 @@ int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launch
   if (rc == AXJ_OK) rc = check_model(h);
   for (int64_t s = 0; s < nsteps && rc == AXJ_OK; ++s) {
     const bool judge = judge_due(h);
-    rc = timed(0, [&] { return enqueue_dt(h, 1); });
-    nl[0] += 1;
+    rc = timed(0, [&]() -> int {
+      int r = enqueue_dt(h, 1);
+      if (r == AXJ_OK && h->c.control_forcing == 2)
+        AXJ_CUDA(h, launch_harmonic_phase(h->time, h->dt, h->c.harm_omega, 0, h->harm, h->stream));
+      return r;
+    });
+    nl[0] += 1 + (h->c.control_forcing == 2);
     for (int st = 1; st <= 4 && rc == AXJ_OK; ++st) {
       const bool lrn_plain = h->learned && judge && st > 1;
       const bool lrn = h->learned && !lrn_plain;
@@ -1245,6 +1258,8 @@ int axj_rhs(axj_handle* h, const double* pv, double* rhs) {
   if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called (the target is needed)");
   AXJ_CUDA(h, cudaSetDevice(h->device));
   AXJ_CUDA(h, h2d(h, h->Ua, pv, 5));
+  if (h->c.control_forcing == 2)
+    AXJ_CUDA(h, launch_harmonic_phase(h->time, h->dt, h->c.harm_omega, 1, h->harm, h->stream));
   int rc = enqueue_stage(h, BUA, BUB, 0);
   if (rc != AXJ_OK) return rc;
   AXJ_CUDA(h, d2h(h, rhs, h->Ub, 5));
@@ -1694,6 +1709,614 @@ int axj_learned_stats(axj_handle* h, int64_t* judged, int64_t* fallback, int64_t
   if (fallback) *fallback = (int64_t)c[1];
   if (njudges) *njudges = h->njudges;
   return AXJ_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches: many solver instances advanced together, every kernel of the step launched
+// once for all of them (persistent grid-stride kernels over per-instance tile tables,
+// per-instance arguments and tensor maps in device tables), the step captured in a
+// CUDA graph.
+// ---------------------------------------------------------------------------
+struct axj_batch {
+  int n = 0;
+  int device = 0;
+  std::vector<axj_handle*> h;
+  cudaStream_t stream = nullptr;
+  SideStream side{nullptr, nullptr, nullptr};
+  std::string err;
+  std::vector<void*> mem;
+  bool mixed = false, learned = false, held_only = false, sc = false, any_harm = false;
+  int64_t iteration = 0, judge_every = 50, njudges = 0;
+  // device tables
+  CUtensorMap* maps = nullptr;
+  StageArgs* stage_argv[2][5] = {};
+  SensorArgs* sens_argv[5] = {};
+  FeatArgs* feat_argv = nullptr;
+  InferArgs* infer_argv[2] = {};
+  JudgeArgs* judge_argv = nullptr;
+  DtArgs* dt_argv = nullptr;
+  HarmArgs* harm_argv = nullptr;
+  // host copies of instance 0's arguments (dispatch decisions, model pointer)
+  StageArgs a0_stage[2][5];
+  SensorArgs a0_sens[5];
+  InferArgs a0_infer[2];
+  // host tile lists (i0, j0, instance) and their device copies
+  std::vector<int4> h_st_int, h_st_gen, h_se_int, h_se_gen, h_ft, h_mt;
+  int4 *st_int = nullptr, *st_gen = nullptr, *se_int = nullptr, *se_gen = nullptr, *ft = nullptr, *mt = nullptr;
+  int2* zrows = nullptr;
+  int nzrows = 0, zthreads = 32;
+  size_t zsmem = 0;
+  long long max_pts = 0;
+  int dt_blocks = 1, nsm = 148;
+  axj_batch_tuning tune{};
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // normal step, judge step
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+int bfail(axj_batch* b, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (b) b->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+#define BATCH_CUDA(b, call)                                                                                \
+  do {                                                                                                     \
+    cudaError_t e_ = (call);                                                                               \
+    if (e_ != cudaSuccess) return bfail((b), AXJ_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+int bupload(axj_batch* b, T** dst, const std::vector<T>& v) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
+  BATCH_CUDA(b, cudaMalloc(&p, bytes));
+  b->mem.push_back(p);
+  if (!v.empty()) BATCH_CUDA(b, cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *dst = static_cast<T*>(p);
+  return AXJ_OK;
+}
+
+template <typename T>
+int bupdate(axj_batch* b, T* dst, const std::vector<T>& v) {
+  if (!v.empty()) BATCH_CUDA(b, cudaMemcpy(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return AXJ_OK;
+}
+
+std::vector<int2> download_tiles(const int2* d, int n) {
+  std::vector<int2> v((size_t)std::max(n, 0));
+  if (n > 0) cudaMemcpy(v.data(), d, v.size() * sizeof(int2), cudaMemcpyDeviceToHost);
+  return v;
+}
+
+// Tile list of all instances in the tuning's order: instance after instance, or
+// round-robin over the instances (tile k of every instance in turn).
+std::vector<int4> order_tiles(const std::vector<std::vector<int2>>& per, int order) {
+  std::vector<int4> out;
+  size_t total = 0, mx = 0;
+  for (const auto& v : per) {
+    total += v.size();
+    mx = std::max(mx, v.size());
+  }
+  out.reserve(total);
+  if (order == 0) {
+    for (size_t k = 0; k < per.size(); ++k)
+      for (const int2& t : per[k]) out.push_back(make_int4(t.x, t.y, (int)k, 0));
+  } else {
+    for (size_t q = 0; q < mx; ++q)
+      for (size_t k = 0; k < per.size(); ++k)
+        if (q < per[k].size()) out.push_back(make_int4(per[k][q].x, per[k][q].y, (int)k, 0));
+  }
+  return out;
+}
+
+std::vector<std::vector<int2>> block_tiles(const axj_batch* b, int tz, int tr) {
+  std::vector<std::vector<int2>> per(b->n);
+  for (int k = 0; k < b->n; ++k)
+    for (int j = 0; j < b->h[k]->Nr; j += tr)
+      for (int i = 0; i < b->h[k]->Nz; i += tz) per[k].push_back(make_int2(i, j));
+  return per;
+}
+
+// (Re)build the ordered tile tables of the batch for its tuning.
+int batch_tiles(axj_batch* b, bool first) {
+  std::vector<std::vector<int2>> si(b->n), sg(b->n), ei(b->n), eg(b->n);
+  for (int k = 0; k < b->n; ++k) {
+    axj_handle* h = b->h[k];
+    si[k] = download_tiles(h->tiles_int, h->ntiles_int);
+    sg[k] = download_tiles(h->tiles_gen, h->ntiles_gen);
+    ei[k] = download_tiles(h->stiles_int, h->nstiles_int);
+    eg[k] = download_tiles(h->stiles_gen, h->nstiles_gen);
+  }
+  const int o = (int)b->tune.tile_order;
+  b->h_st_int = order_tiles(si, o);
+  b->h_st_gen = order_tiles(sg, o);
+  b->h_se_int = order_tiles(ei, o);
+  b->h_se_gen = order_tiles(eg, o);
+  b->h_ft = order_tiles(block_tiles(b, FEAT_TILE_Z, FEAT_TILE_R), o);
+  b->h_mt = order_tiles(block_tiles(b, MLP_TILE_Z, MLP_TILE_R), o);
+  int rc = AXJ_OK;
+  if (first) {
+    if (rc == AXJ_OK) rc = bupload(b, &b->st_int, b->h_st_int);
+    if (rc == AXJ_OK) rc = bupload(b, &b->st_gen, b->h_st_gen);
+    if (rc == AXJ_OK) rc = bupload(b, &b->se_int, b->h_se_int);
+    if (rc == AXJ_OK) rc = bupload(b, &b->se_gen, b->h_se_gen);
+    if (rc == AXJ_OK) rc = bupload(b, &b->ft, b->h_ft);
+    if (rc == AXJ_OK) rc = bupload(b, &b->mt, b->h_mt);
+  } else {
+    if (rc == AXJ_OK) rc = bupdate(b, b->st_int, b->h_st_int);
+    if (rc == AXJ_OK) rc = bupdate(b, b->st_gen, b->h_st_gen);
+    if (rc == AXJ_OK) rc = bupdate(b, b->se_int, b->h_se_int);
+    if (rc == AXJ_OK) rc = bupdate(b, b->se_gen, b->h_se_gen);
+    if (rc == AXJ_OK) rc = bupdate(b, b->ft, b->h_ft);
+    if (rc == AXJ_OK) rc = bupdate(b, b->mt, b->h_mt);
+  }
+  return rc;
+}
+
+BatchTiles btiles(const axj_batch* b, const int4* d, const std::vector<int4>& hv, int64_t per_sm) {
+  BatchTiles t;
+  t.tiles = d;
+  t.ntiles = (int)hv.size();
+  const long long g = (long long)std::max<int64_t>(per_sm, 1) * b->nsm;
+  t.grid = (int)std::max<long long>(1, std::min<long long>(g, t.ntiles));
+  return t;
+}
+
+// One batched RK stage (mirrors enqueue_stage / enqueue_stage_learned of a handle).
+int batch_stage(axj_batch* b, int bin, int bout, int stage, bool judge) {
+  (void)bout;
+  const bool lrn_plain = b->learned && judge && stage > 1;
+  const bool lrn = b->learned && !lrn_plain;
+  const BatchTiles sti = btiles(b, b->st_int, b->h_st_int, b->tune.stage_ctas_per_sm);
+  const BatchTiles stg = btiles(b, b->st_gen, b->h_st_gen, 1);
+  const BatchTiles sei = btiles(b, b->se_int, b->h_se_int, b->tune.sensor_ctas_per_sm);
+  const BatchTiles seg = btiles(b, b->se_gen, b->h_se_gen, 1);
+  auto sensor = [&](bool rfilter) -> int {
+    BATCH_CUDA(b, launch_sensor_batch(b->sens_argv[bin], b->a0_sens[bin], sei, seg, b->maps, bin, b->zrows, b->nzrows,
+                                      b->zthreads, b->zsmem, rfilter, b->n, b->max_pts, b->side, b->stream));
+    return AXJ_OK;
+  };
+  if (lrn) {
+    if (b->held_only) {
+      if (judge && stage == 1)
+        if (int rc = sensor(true)) return rc;
+    } else if (stage == 1) {
+      const BatchTiles ft = btiles(b, b->ft, b->h_ft, 4);
+      BATCH_CUDA(b, launch_features_batch(b->feat_argv, ft.tiles, ft.ntiles, ft.grid, b->stream));
+      if (judge) {
+        if (int rc = sensor(true)) return rc;
+        BATCH_CUDA(b, launch_mlp_infer_batch(b->a0_infer[0], b->infer_argv[0], b->mt, (int)b->h_mt.size(), b->stream));
+        BATCH_CUDA(b, launch_judge_batch(b->judge_argv, b->n, b->max_pts, b->stream));
+      } else {
+        BATCH_CUDA(b, launch_mlp_infer_batch(b->a0_infer[1], b->infer_argv[1], b->mt, (int)b->h_mt.size(), b->stream));
+      }
+    }
+  } else if (b->sc) {
+    if (int rc = sensor(false)) return rc;
+  }
+  const int L = lrn ? 1 : 0;
+  BATCH_CUDA(b, launch_stage_batch(b->stage_argv[L][stage], b->a0_stage[L][stage], sti, stg, b->maps, bin, b->side,
+                                   b->stream));
+  return AXJ_OK;
+}
+
+int batch_enqueue_step(axj_batch* b, bool judge) {
+  BATCH_CUDA(b, launch_dt_batch(b->dt_argv, b->n, b->dt_blocks, b->stream));
+  if (b->any_harm) BATCH_CUDA(b, launch_harmonic_phase_batch(b->harm_argv, b->n, b->stream));
+  int bufs[5];
+  rk4_buffers(b->h[0], bufs);
+  for (int st = 1; st <= 4; ++st)
+    if (int rc = batch_stage(b, bufs[st - 1], bufs[st], st, judge)) return rc;
+  return AXJ_OK;
+}
+
+void batch_drop_graphs(axj_batch* b) {
+  for (int k = 0; k < 2; ++k) {
+    if (b->gexec[k]) cudaGraphExecDestroy(b->gexec[k]);
+    if (b->graph[k]) cudaGraphDestroy(b->graph[k]);
+    b->gexec[k] = nullptr;
+    b->graph[k] = nullptr;
+  }
+}
+
+int batch_graph(axj_batch* b, bool judge, cudaGraphExec_t* out) {
+  const int k = judge ? 1 : 0;
+  if (!b->gexec[k]) {
+    BATCH_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_enqueue_step(b, judge);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc != AXJ_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return bfail(b, AXJ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    b->graph[k] = g;
+    BATCH_CUDA(b, cudaGraphInstantiate(&b->gexec[k], g, 0));
+  }
+  *out = b->gexec[k];
+  return AXJ_OK;
+}
+
+bool batch_judge_due(const axj_batch* b) {
+  if (!b->learned) return false;
+  for (const axj_handle* h : b->h)
+    if (!h->judged) return true;
+  return b->judge_every > 0 && b->iteration % b->judge_every == 0;
+}
+
+int batch_launch_step(axj_batch* b) {
+  const bool judge = batch_judge_due(b);
+  cudaGraphExec_t ge = nullptr;
+  if (int rc = batch_graph(b, judge, &ge)) return rc;
+  BATCH_CUDA(b, cudaGraphLaunch(ge, b->stream));
+  if (judge) {
+    for (axj_handle* h : b->h) {
+      h->judged = true;
+      h->njudges += 1;
+    }
+    b->njudges += 1;
+  }
+  b->iteration += 1;
+  for (axj_handle* h : b->h) h->iteration += 1;
+  return AXJ_OK;
+}
+
+// After the batch's stream has run: host times and the error flags of every instance.
+int batch_finish(axj_batch* b) {
+  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  for (int k = 0; k < b->n; ++k) {
+    axj_handle* h = b->h[k];
+    BATCH_CUDA(b, cudaMemcpy(&h->time_host, h->time, sizeof(double), cudaMemcpyDeviceToHost));
+    int f = 0;
+    BATCH_CUDA(b, cudaMemcpy(&f, h->flags, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f & 4) return bfail(b, AXJ_ERR_TIMEOUT, "instance %d: a bounded wait on a TMA transfer gave up", k);
+    if (f & 2) return bfail(b, AXJ_ERR_DT_BLOWUP, "instance %d: Time step blow up", k);
+    if (f & 1) return bfail(b, AXJ_ERR_NONFINITE, "instance %d: non-finite value in the solution or time step", k);
+  }
+  return AXJ_OK;
+}
+
+int batch_build_tables(axj_batch* b) {
+  const int n = b->n;
+  // tensor maps: every instance's maps at the fixed batch indices
+  std::vector<CUtensorMap> maps((size_t)n * NM_BATCH);
+  for (int k = 0; k < n; ++k) {
+    axj_handle* h = b->h[k];
+    CUtensorMap* m = maps.data() + (size_t)k * NM_BATCH;
+    const int nb = h->mixed ? NBUF : BUAF;
+    for (int bf = 0; bf < NBUF; ++bf)
+      for (int cls = 0; cls < 2; ++cls) {
+        const int src = bf < nb ? bf : 0;  // unused FP32 slots of an FP64 batch repeat buffer 0
+        m[bmap_state(bf, cls)] = h->map_state[src][cls];
+        m[bmap_sens(bf, cls)] = h->map_sens[src][cls];
+        m[bmap_sensT(bf, cls)] = h->map_sensT[src][cls];
+      }
+    for (int cls = 0; cls < 2; ++cls) {
+      m[bmap_star(cls, false)] = h->map_star[cls];
+      m[bmap_star(cls, true)] = h->map_starL[cls];
+    }
+    m[14] = h->map_u0_tile;
+    m[15] = h->map_acc_tile;
+    for (int bf = 0; bf < NBUF; ++bf) m[bmap_rho(bf)] = h->map_rho[bf < nb ? bf : 0];
+  }
+  {
+    void* p = nullptr;
+    BATCH_CUDA(b, cudaMalloc(&p, maps.size() * sizeof(CUtensorMap)));
+    b->mem.push_back(p);
+    BATCH_CUDA(b, cudaMemcpy(p, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    b->maps = static_cast<CUtensorMap*>(p);
+  }
+  // per-instance arguments
+  int bufs[5];
+  rk4_buffers(b->h[0], bufs);
+  for (int L = 0; L < 2; ++L)
+    for (int st = 1; st <= 4; ++st) {
+      std::vector<StageArgs> v(n);
+      for (int k = 0; k < n; ++k) {
+        v[k] = stage_args(b->h[k], bufs[st - 1], bufs[st], st);
+        v[k].learned = L;
+      }
+      b->a0_stage[L][st] = v[0];
+      if (int rc = bupload(b, &b->stage_argv[L][st], v)) return rc;
+    }
+  for (int bf = 0; bf < NBUF; ++bf) {
+    std::vector<SensorArgs> v(n);
+    for (int k = 0; k < n; ++k) v[k] = sensor_args(b->h[k], (b->mixed || bf < BUAF) ? bf : BU0);
+    b->a0_sens[bf] = v[0];
+    if (int rc = bupload(b, &b->sens_argv[bf], v)) return rc;
+  }
+  if (b->sc) {
+    std::vector<FeatArgs> fv(n);
+    std::vector<InferArgs> i0(n), i1(n);
+    std::vector<JudgeArgs> jv(n);
+    for (int k = 0; k < n; ++k) {
+      axj_handle* h = b->h[k];
+      fv[k] = feat_args(h, BU0);
+      i0[k] = infer_args(h, 0);
+      i1[k] = infer_args(h, 1);
+      jv[k] = JudgeArgs{grid_of(h), h->pred, h->star + h->plane, h->judge_thr, h->mask, h->held, h->counts};
+    }
+    b->a0_infer[0] = i0[0];
+    b->a0_infer[1] = i1[0];
+    if (int rc = bupload(b, &b->feat_argv, fv)) return rc;
+    if (int rc = bupload(b, &b->infer_argv[0], i0)) return rc;
+    if (int rc = bupload(b, &b->infer_argv[1], i1)) return rc;
+    if (int rc = bupload(b, &b->judge_argv, jv)) return rc;
+  }
+  std::vector<DtArgs> dv(n);
+  std::vector<HarmArgs> hv(n);
+  for (int k = 0; k < n; ++k) {
+    axj_handle* h = b->h[k];
+    dv[k] = dt_args(h, 1);
+    hv[k] = HarmArgs{h->time, h->dt, h->c.harm_omega, h->harm};
+    if (h->c.control_forcing == 2) b->any_harm = true;
+  }
+  if (int rc = bupload(b, &b->dt_argv, dv)) return rc;
+  if (int rc = bupload(b, &b->harm_argv, hv)) return rc;
+  // z-filter rows (instance, j)
+  if (b->sc) {
+    std::vector<int2> rows;
+    int bs = 32;
+    for (int k = 0; k < n; ++k) {
+      for (int j = 0; j < b->h[k]->Nr; ++j) rows.push_back(make_int2(k, j));
+      bs = std::max(bs, zrows_threads(b->h[k]->Nz));
+    }
+    size_t sm = 0;
+    for (int k = 0; k < n; ++k) sm = std::max(sm, zrows_smem(b->h[k]->Nz, b->h[k]->P, bs));
+    b->nzrows = (int)rows.size();
+    b->zthreads = bs;
+    b->zsmem = sm;
+    if (int rc = bupload(b, &b->zrows, rows)) return rc;
+  }
+  // dt: the same number of blocks for every instance (the handles' partial arrays hold 592)
+  b->dt_blocks = (int)std::min<long long>(592, std::max<long long>(1, b->max_pts / (DT_THREADS * 8)));
+  return batch_tiles(b, true);
+}
+
+// Device copies of the instances' solutions, times and stale T (autotuning trials
+// advance the batch and are undone).
+struct BatchSave {
+  std::vector<void*> u0;
+  std::vector<double> time_host, stale;
+  std::vector<int64_t> it;
+};
+
+int batch_save(axj_batch* b, BatchSave& s) {
+  for (axj_handle* h : b->h) {
+    void* p = nullptr;
+    const size_t bytes = sizeof(double) * 5 * (size_t)h->plane;
+    BATCH_CUDA(b, cudaMalloc(&p, bytes));
+    s.u0.push_back(p);
+    BATCH_CUDA(b, cudaMemcpy(p, h->U0, bytes, cudaMemcpyDeviceToDevice));
+    double st = 0.0, t = 0.0;
+    BATCH_CUDA(b, cudaMemcpy(&st, h->staleT, sizeof(double), cudaMemcpyDeviceToHost));
+    BATCH_CUDA(b, cudaMemcpy(&t, h->time, sizeof(double), cudaMemcpyDeviceToHost));
+    s.stale.push_back(st);
+    s.time_host.push_back(t);
+    s.it.push_back(h->iteration);
+  }
+  return AXJ_OK;
+}
+
+int batch_restore(axj_batch* b, BatchSave& s) {
+  for (int k = 0; k < b->n; ++k) {
+    axj_handle* h = b->h[k];
+    const size_t bytes = sizeof(double) * 5 * (size_t)h->plane;
+    BATCH_CUDA(b, cudaMemcpy(h->U0, s.u0[k], bytes, cudaMemcpyDeviceToDevice));
+    BATCH_CUDA(b, cudaMemcpy(h->staleT, &s.stale[k], sizeof(double), cudaMemcpyHostToDevice));
+    BATCH_CUDA(b, cudaMemcpy(h->time, &s.time_host[k], sizeof(double), cudaMemcpyHostToDevice));
+    h->time_host = s.time_host[k];
+    h->iteration = s.it[k];
+    h->judged = false;  // the held coefficients are rebuilt by the next judge step
+    cudaFree(s.u0[k]);
+  }
+  s.u0.clear();
+  b->iteration = b->h[0]->iteration;
+  return AXJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void axj_batch_default_tuning(axj_batch_tuning* t) {
+  if (!t) return;
+  std::memset(t, 0, sizeof(*t));
+  t->tile_order = 0;
+  t->stage_ctas_per_sm = 2;
+  t->sensor_ctas_per_sm = 2;
+}
+
+int axj_batch_create(axj_handle* const* handles, int64_t n, axj_batch** out) {
+  if (!handles || !out || n < 1) return bfail(nullptr, AXJ_ERR_ARG, "bad argument");
+  *out = nullptr;
+  axj_handle* h0 = handles[0];
+  for (int64_t k = 0; k < n; ++k) {
+    const axj_handle* h = handles[k];
+    if (!h) return bfail(nullptr, AXJ_ERR_ARG, "null handle %lld", (long long)k);
+    if (!h->state_set) return bfail(nullptr, AXJ_ERR_ARG, "instance %lld: axj_set_state has not been called", (long long)k);
+    if (h->device != h0->device || h->mixed != h0->mixed || h->learned != h0->learned ||
+        h->held_only != h0->held_only || (h->c.shock_capturing != 0) != (h0->c.shock_capturing != 0))
+      return bfail(nullptr, AXJ_ERR_UNSUPPORTED,
+                   "instance %lld: every instance needs the same device, precision, sensor and shock capturing",
+                   (long long)k);
+    if (h->learned && !h->held_only && !h->mlp_set)
+      return bfail(nullptr, AXJ_ERR_ARG, "instance %lld: learned sensor without a model", (long long)k);
+    if (h->c.shock_capturing && h->Nz > 10240)
+      return bfail(nullptr, AXJ_ERR_UNSUPPORTED, "instance %lld: batched z filter takes Nz <= 10240", (long long)k);
+  }
+  axj_batch* b = new axj_batch();
+  b->n = (int)n;
+  b->device = h0->device;
+  b->h.assign(handles, handles + n);
+  b->mixed = h0->mixed;
+  b->learned = h0->learned;
+  b->held_only = h0->held_only;
+  b->sc = h0->c.shock_capturing != 0;
+  b->judge_every = h0->judge_every;
+  b->iteration = h0->iteration;
+  axj_batch_default_tuning(&b->tune);
+  int rc = AXJ_OK;
+  if (cudaSetDevice(b->device) != cudaSuccess) rc = bfail(b, AXJ_ERR_CUDA, "cudaSetDevice failed");
+  // the batch runs the model of instance 0 for every instance: they must agree
+  if (rc == AXJ_OK && b->learned && !b->held_only) {
+    std::vector<float> w0(MLP_NPARAM), wk(MLP_NPARAM);
+    cudaMemcpy(w0.data(), h0->mlp, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost);
+    for (int64_t k = 1; k < n && rc == AXJ_OK; ++k) {
+      cudaMemcpy(wk.data(), handles[k]->mlp, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost);
+      if (std::memcmp(w0.data(), wk.data(), sizeof(float) * MLP_NPARAM) != 0 ||
+          std::memcmp(&h0->norm, &handles[k]->norm, sizeof(MlpNorm)) != 0)
+        rc = bfail(b, AXJ_ERR_UNSUPPORTED, "instance %lld has a different model than instance 0", (long long)k);
+    }
+  }
+  for (int64_t k = 0; k < n; ++k) {
+    b->max_pts = std::max<long long>(b->max_pts, (long long)handles[k]->Nz * handles[k]->Nr);
+    cudaStreamSynchronize(handles[k]->stream);
+  }
+  cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device);
+  if (rc == AXJ_OK && (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+                       cudaStreamCreateWithFlags(&b->side.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                       cudaEventCreateWithFlags(&b->side.fork, cudaEventDisableTiming) != cudaSuccess ||
+                       cudaEventCreateWithFlags(&b->side.join, cudaEventDisableTiming) != cudaSuccess))
+    rc = bfail(b, AXJ_ERR_CUDA, "stream / event creation failed");
+  if (rc == AXJ_OK) rc = batch_build_tables(b);
+  if (rc != AXJ_OK) {
+    g_create_error = b->err;
+    axj_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return AXJ_OK;
+}
+
+int axj_batch_set_tuning(axj_batch* b, const axj_batch_tuning* t) {
+  if (!b || !t) return bfail(b, AXJ_ERR_ARG, "null argument");
+  if (t->tile_order < 0 || t->tile_order > 1 || t->stage_ctas_per_sm < 1 || t->stage_ctas_per_sm > 8 ||
+      t->sensor_ctas_per_sm < 1 || t->sensor_ctas_per_sm > 8)
+    return bfail(b, AXJ_ERR_ARG, "tuning out of range");
+  BATCH_CUDA(b, cudaSetDevice(b->device));
+  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  const bool reorder = t->tile_order != b->tune.tile_order;
+  b->tune = *t;
+  if (reorder)
+    if (int rc = batch_tiles(b, false)) return rc;
+  batch_drop_graphs(b);
+  return AXJ_OK;
+}
+
+int axj_batch_get_tuning(axj_batch* b, axj_batch_tuning* t) {
+  if (!b || !t) return bfail(b, AXJ_ERR_ARG, "null argument");
+  *t = b->tune;
+  return AXJ_OK;
+}
+
+int axj_batch_run(axj_batch* b, int64_t nsteps) {
+  if (!b || nsteps < 0) return bfail(b, AXJ_ERR_ARG, "bad argument");
+  BATCH_CUDA(b, cudaSetDevice(b->device));
+  for (axj_handle* h : b->h) BATCH_CUDA(b, cudaStreamSynchronize(h->stream));
+  for (int64_t s = 0; s < nsteps; ++s)
+    if (int rc = batch_launch_step(b)) return rc;
+  return batch_finish(b);
+}
+
+int axj_batch_run_timed(axj_batch* b, int64_t nsteps, double* ms) {
+  if (!b || !ms || nsteps < 0) return bfail(b, AXJ_ERR_ARG, "bad argument");
+  BATCH_CUDA(b, cudaSetDevice(b->device));
+  for (axj_handle* h : b->h) BATCH_CUDA(b, cudaStreamSynchronize(h->stream));
+  // both step graphs are captured outside the timed region
+  cudaGraphExec_t ge = nullptr;
+  if (int rc = batch_graph(b, false, &ge)) return rc;
+  if (b->learned)
+    if (int rc = batch_graph(b, true, &ge)) return rc;
+  cudaEvent_t e0, e1;
+  BATCH_CUDA(b, cudaEventCreate(&e0));
+  BATCH_CUDA(b, cudaEventCreate(&e1));
+  BATCH_CUDA(b, cudaEventRecord(e0, b->stream));
+  int rc = AXJ_OK;
+  for (int64_t s = 0; s < nsteps && rc == AXJ_OK; ++s) rc = batch_launch_step(b);
+  BATCH_CUDA(b, cudaEventRecord(e1, b->stream));
+  BATCH_CUDA(b, cudaEventSynchronize(e1));
+  float t = 0.f;
+  BATCH_CUDA(b, cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t;
+  if (rc != AXJ_OK) return rc;
+  return batch_finish(b);
+}
+
+int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* chosen, double* trial_ms,
+                       int64_t* ntrials) {
+  if (!b || steps_per_trial < 1) return bfail(b, AXJ_ERR_ARG, "bad argument");
+  BATCH_CUDA(b, cudaSetDevice(b->device));
+  BatchSave save;
+  if (int rc = batch_save(b, save)) return rc;
+  // candidates: tile order x persistent CTAs per SM of the interior stage and sensor kernels
+  std::vector<axj_batch_tuning> cands;
+  for (int o = 0; o < 2; ++o)
+    for (int sc = 1; sc <= 2; ++sc)
+      for (int se = 1; se <= 2; ++se) {
+        axj_batch_tuning t;
+        axj_batch_default_tuning(&t);
+        t.tile_order = o;
+        t.stage_ctas_per_sm = sc;
+        t.sensor_ctas_per_sm = se;
+        if (!b->sc && se > 1) continue;
+        cands.push_back(t);
+      }
+  double best = 1e300;
+  axj_batch_tuning best_t = b->tune;
+  int k = 0;
+  for (const axj_batch_tuning& t : cands) {
+    int rc = axj_batch_set_tuning(b, &t);
+    double ms = 0.0;
+    if (rc == AXJ_OK) rc = axj_batch_run(b, 1);  // warm-up (captures the graphs)
+    if (rc == AXJ_OK) rc = axj_batch_run_timed(b, steps_per_trial, &ms);
+    if (rc != AXJ_OK) {
+      batch_restore(b, save);
+      return rc;
+    }
+    if (trial_ms) trial_ms[k] = ms;
+    ++k;
+    if (ms < best) {
+      best = ms;
+      best_t = t;
+    }
+    if (int r2 = batch_restore(b, save)) return r2;
+    if (int r3 = batch_save(b, save)) return r3;
+  }
+  for (void* p : save.u0) cudaFree(p);
+  save.u0.clear();
+  if (ntrials) *ntrials = k;
+  if (int rc = axj_batch_set_tuning(b, &best_t)) return rc;
+  if (chosen) *chosen = best_t;
+  return AXJ_OK;
+}
+
+const char* axj_batch_last_error(const axj_batch* b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+void axj_batch_destroy(axj_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graphs(b);
+  for (void* p : b->mem) cudaFree(p);
+  if (b->side.stream) cudaStreamSynchronize(b->side.stream);
+  if (b->side.fork) cudaEventDestroy(b->side.fork);
+  if (b->side.join) cudaEventDestroy(b->side.join);
+  if (b->side.stream) cudaStreamDestroy(b->side.stream);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
 }
 
 }  // extern "C"

@@ -193,16 +193,15 @@ template <> __device__ __forceinline__ float pow0666<float>(float T) { return po
 // mixed path's intermediate stages); R: arithmetic type of the stencils and, in
 // interior tiles, of the pointwise terms. General tiles (closure rows, faces, the axis
 // row) evaluate the pointwise terms, face penalties and sponges in double.
+// One tile (i0, j0) of the fused stage. Returns false if a bounded wait gave up (the
+// flag is set; the caller stops).
 template <int H, bool GEN, typename SIN, typename R, bool LRN>
-__global__ void __launch_bounds__(STAGE_THREADS)
-    stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
-                 const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
-                 const __grid_constant__ CUtensorMap mAcc) {
+__device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, const CUtensorMap* mState,
+                                           const CUtensorMap* mQ, const CUtensorMap* mU0, const CUtensorMap* mAcc,
+                                           unsigned char* smem_raw, uint64_t* bar) {
   using SM = StageSmem<H, SIN, R, LRN>;
   using RP = typename std::conditional<GEN, double, R>::type;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT, NTP = SM::NTP, HT = SM::HT, RQ = SM::RQ;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar[2];
   SIN* sU = reinterpret_cast<SIN*>(smem_raw + SM::oU);            // [5][RR][RZ]
   double* sQ = reinterpret_cast<double*>(smem_raw + SM::oQ);      // [3][RQ][RZ]
   double* sMu = sQ + HT * RZ;                                      // [RR][RZ], row stride RZ
@@ -215,8 +214,6 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
 
   const int tid = threadIdx.x;
-  const int2 t0 = tiles[blockIdx.x];
-  const int i0 = t0.x, j0 = t0.y;
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long P = a.g.P, PL = a.g.plane;
   const bool sc = a.c.shock_capturing != 0;
@@ -235,12 +232,12 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   __syncthreads();
   if (tid == 0) {
     mbar_expect_tx(&bar[0], SM::state_bytes + (sc ? SM::q_bytes : 0u));
-    tma_load_3d(sU, &mState, i0 - HZ, j0 - H, 0, &bar[0]);
-    if (sc) tma_load_3d(sQ, &mQ, i0 - HZ, j0 - H - HT, 0, &bar[0]);
+    tma_load_3d(sU, mState, i0 - HZ, j0 - H, 0, &bar[0]);
+    if (sc) tma_load_3d(sQ, mQ, i0 - HZ, j0 - H - HT, 0, &bar[0]);
     if (needU0 || needA) {
       mbar_expect_tx(&bar[1], (needU0 ? SM::tile_bytes : 0u) + (needA ? SM::tile_bytes : 0u));
-      if (needU0) tma_load_3d(sP0, &mU0, i0, j0, 0, &bar[1]);
-      if (needA) tma_load_3d(sPA, &mAcc, i0, j0, 0, &bar[1]);
+      if (needU0) tma_load_3d(sP0, mU0, i0, j0, 0, &bar[1]);
+      if (needA) tma_load_3d(sPA, mAcc, i0, j0, 0, &bar[1]);
     }
   }
   if (GEN) {
@@ -253,7 +250,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   }
   if (!__syncthreads_and(mbar_wait_bounded(&bar[0], 0))) {
     if (tid == 0) atomicOr(a.flags, 4);
-    return;
+    return false;
   }
   // mu = T**0.666 (AssignValues) on the cross of the region. With shock capturing the
   // coefficient box holds the z-filtered quantities; the r filter PerformTGfilter(q, 2,
@@ -358,17 +355,12 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   if (needU0 || needA) {
     if (!__syncthreads_and(mbar_wait_bounded(&bar[1], 0))) {
       if (tid == 0) atomicOr(a.flags, 4);
-      return;
+      return false;
     }
   }
   const double dtv = a.stage > 0 ? *a.dt : 0.0;
-  // stage time t_n + c_s dt, c = (0, 1/2, 1/2, 1); the device time is t_n + dt in stages 1-4
-  double tstage = 0.0;
-  if (a.c.control_forcing == 2) {
-    const double tend = *a.time;
-    const double cs = a.stage == 1 ? 0.0 : (a.stage == 4 ? 1.0 : 0.5);
-    tstage = a.stage == 0 ? tend : (tend - dtv) + cs * dtv;
-  }
+  // cos(omega t_s) at this stage's time (harmonic forcing)
+  const double cwt = a.c.control_forcing == 2 ? a.harm[a.stage] : 0.0;
   for (int pidx = tid; pidx < TZ * TR; pidx += STAGE_THREADS) {
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
@@ -461,7 +453,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       for (int f = 0; f < 5; ++f) tg[f] = __ldg(a.target + f * PL + go);
     }
     if (a.c.control_forcing == 1) control_forcing(zloc, rloc, a.c, a.forcing, pv, tg, rhs);
-    else if (a.c.control_forcing == 2) harmonic_forcing(zloc, rloc, tstage, a.c, rhs);
+    else if (a.c.control_forcing == 2) harmonic_forcing(zloc, rloc, cwt, a.c, rhs);
     if (GEN && face) {
       const Prim qd = convert<double>(q);
       const Deriv dd = convert<double>(d);
@@ -523,6 +515,43 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       if (bad) atomicOr(a.flags, 1);
       if (i == a.iT && j == a.jT) *a.staleT = pv[4];
     }
+  }
+  return true;
+}
+
+
+
+template <int H, bool GEN, typename SIN, typename R, bool LRN>
+__global__ void __launch_bounds__(STAGE_THREADS)
+    stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
+                 const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
+                 const __grid_constant__ CUtensorMap mAcc) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  const int2 t0 = tiles[blockIdx.x];
+  stage_body<H, GEN, SIN, R, LRN>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, smem_raw, bar);
+}
+
+// Batched form: a persistent grid-stride loop over the tiles (i0, j0, instance) of many
+// solver instances; each instance's arguments and tensor maps come from device tables
+// (the arguments are staged in shared memory per tile).
+template <int H, bool GEN, typename SIN, typename R, bool LRN>
+__global__ void __launch_bounds__(STAGE_THREADS)
+    stage_kernel_batch(const StageArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
+                       const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(16) StageArgs sa;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int4 tt = tiles[t];
+    __syncthreads();  // the previous tile is finished with the arguments and the buffers
+    for (int k = threadIdx.x; k < (int)(sizeof(StageArgs) / 8); k += blockDim.x)
+      reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + tt.z)[k];
+    __syncthreads();
+    const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
+    if (!stage_body<H, GEN, SIN, R, LRN>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, m + kmaps.w, smem_raw,
+                                         bar))
+      return;
   }
 }
 
@@ -604,7 +633,9 @@ __device__ __forceinline__ double warp_min(double v) {
   return v;
 }
 
-__global__ void __launch_bounds__(DT_THREADS) dt_kernel(const DtArgs a) {
+// ComputeTimeStep over one instance with blocks blk = 0..nblk-1 (per-block minima in
+// a.partial, the last block to finish reduces them).
+__device__ __forceinline__ void dt_body(const DtArgs& a, int blk, int nblk) {
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long n = (long long)Nz * Nr;
   const long long P = a.g.P, PL = a.g.plane;
@@ -612,7 +643,7 @@ __global__ void __launch_bounds__(DT_THREADS) dt_kernel(const DtArgs a) {
   const bool phys = a.c.dt_mode == DT_PHYSICAL;
   double m = 1.0e300;
   int bad = 0;
-  for (long long p = (long long)blockIdx.x * DT_THREADS + threadIdx.x; p < n; p += (long long)gridDim.x * DT_THREADS) {
+  for (long long p = (long long)blk * DT_THREADS + threadIdx.x; p < n; p += (long long)nblk * DT_THREADS) {
     const int j = (int)(p / Nz), i = (int)(p - (long long)j * Nz);
     const long long o = (long long)j * P + i;
     double v;
@@ -639,17 +670,17 @@ __global__ void __launch_bounds__(DT_THREADS) dt_kernel(const DtArgs a) {
     m = lane < DT_THREADS / 32 ? sred[lane] : 1.0e300;
     m = warp_min(m);
     if (lane == 0) {
-      a.partial[blockIdx.x] = m;
+      a.partial[blk] = m;
       __threadfence();
       const unsigned int done = atomicAdd(a.counter, 1u);
-      last = (done == gridDim.x - 1);
+      last = (done == (unsigned int)nblk - 1);
     }
   }
   __syncthreads();
   if (last) {
     __threadfence();
     double mm = 1.0e300;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += DT_THREADS) mm = fmin(mm, ((volatile double*)a.partial)[b]);
+    for (int b = threadIdx.x; b < nblk; b += DT_THREADS) mm = fmin(mm, ((volatile double*)a.partial)[b]);
     mm = warp_min(mm);
     if (lane == 0) sred[w] = mm;
     __syncthreads();
@@ -662,6 +693,35 @@ __global__ void __launch_bounds__(DT_THREADS) dt_kernel(const DtArgs a) {
       *a.counter = 0u;
     }
   }
+}
+
+__global__ void __launch_bounds__(DT_THREADS) dt_kernel(const DtArgs a) { dt_body(a, blockIdx.x, gridDim.x); }
+
+// Batched: blockIdx.y = instance.
+__global__ void __launch_bounds__(DT_THREADS) dt_kernel_batch(const DtArgs* __restrict__ argv) {
+  __shared__ __align__(16) DtArgs sa;
+  for (int k = threadIdx.x; k < (int)(sizeof(DtArgs) / 8); k += blockDim.x)
+    reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + blockIdx.y)[k];
+  __syncthreads();
+  dt_body(sa, blockIdx.x, gridDim.x);
+}
+
+__global__ void harmonic_phase_kernel(const double* time, const double* dt, double omega, int rhs_mode, double* out) {
+  const int s = threadIdx.x;
+  if (rhs_mode) {
+    if (s == 0) out[0] = cos(omega * *time);
+    return;
+  }
+  if (s < 1 || s > 4) return;
+  const double tend = *time, d = *dt;
+  const double cs = s == 1 ? 0.0 : (s == 4 ? 1.0 : 0.5);
+  out[s] = cos(omega * ((tend - d) + cs * d));
+}
+
+cudaError_t launch_harmonic_phase(const double* time, const double* dt, double omega, int rhs_mode, double* out,
+                                  cudaStream_t s) {
+  harmonic_phase_kernel<<<1, 32, 0, s>>>(time, dt, omega, rhs_mode, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_dt(const DtArgs& a, int nblocks, cudaStream_t s) {
@@ -730,15 +790,14 @@ __device__ __forceinline__ R sqrt_t(R x) { return sqrt(x); }
 template <>
 __device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
 
+// One sensor tile (i0, j0); false if a bounded wait gave up.
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(STAGE_THREADS)
-    sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mV,
-                       const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
+__device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0, const CUtensorMap* mV,
+                                            const CUtensorMap* mT, const CUtensorMap* mRho, unsigned char* smem_raw,
+                                            uint64_t& bar) {
   using SM = SensSmem<HS, HF, SIN, R>;
   constexpr int HV = SM::HV, HVZ = SM::HVZ, HSZ = SM::HSZ, VZ = SM::VZ, NV = SM::NV;
   constexpr int SZ = SM::SZ, NS = SM::NS, DZ = SM::DZ, DR = SM::DR;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar;
   SIN* sVr = reinterpret_cast<SIN*>(smem_raw + SM::oVr);   // [VR][VZ]
   SIN* sVz = reinterpret_cast<SIN*>(smem_raw + SM::oVz);   // [VR][VZ]
   SIN* sT = reinterpret_cast<SIN*>(smem_raw + SM::oT);     // [SR][SZ]
@@ -751,8 +810,6 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
 
   const int tid = threadIdx.x;
-  const int2 t0 = tiles[blockIdx.x];
-  const int i0 = t0.x, j0 = t0.y;
   const Grid g = a.g;
   const int Nz = g.Nz, Nr = g.Nr;
   auto inside = [&](int i, int j) { return i >= 0 && i < Nz && j >= 0 && j < Nr; };
@@ -767,10 +824,10 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   __syncthreads();
   if (tid == 0) {
     mbar_expect_tx(&bar, SM::tx_bytes);
-    tma_load_3d(sVr, &mV, i0 - HVZ, j0 - HV, 1, &bar);
-    tma_load_3d(sVz, &mV, i0 - HVZ, j0 - HV, 3, &bar);
-    tma_load_3d(sT, &mT, i0 - HSZ, j0 - HS, 4, &bar);
-    tma_load_3d(sRho, &mRho, i0, j0, 0, &bar);
+    tma_load_3d(sVr, mV, i0 - HVZ, j0 - HV, 1, &bar);
+    tma_load_3d(sVz, mV, i0 - HVZ, j0 - HV, 3, &bar);
+    tma_load_3d(sT, mT, i0 - HSZ, j0 - HS, 4, &bar);
+    tma_load_3d(sRho, mRho, i0, j0, 0, &bar);
   }
   if (GEN) {
     for (int idx = tid; idx < NV; idx += STAGE_THREADS) {
@@ -781,7 +838,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   }
   if (!__syncthreads_and(mbar_wait_bounded(&bar, 0))) {
     if (tid == 0) atomicOr(a.flags, 4);
-    return;
+    return false;
   }
 
   // ---- phase 2: S and dilatation on the cross of the S region (reach HS either way);
@@ -885,6 +942,37 @@ __global__ void __launch_bounds__(STAGE_THREADS)
     a.Q[g.plane + o] = double(rho * fsw * fabs((d4z[2][q] * (dz * dz) + d4r[2][q] * (dr * dr))));
     a.Q[2 * g.plane + o] = double(rho / (R(a.c.gam) * sqrt_t<R>(T)) * fabs((d4z[1][q] * dz + d4r[1][q] * dr)));
   }
+  return true;
+}
+
+template <int HS, int HF, bool GEN, typename SIN, typename R>
+__global__ void __launch_bounds__(STAGE_THREADS)
+    sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mV,
+                       const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  const int2 t0 = tiles[blockIdx.x];
+  sensor_body<HS, HF, GEN, SIN, R>(a, t0.x, t0.y, &mV, &mT, &mRho, smem_raw, bar);
+}
+
+// Batched form: persistent loop over (i0, j0, instance) tiles; kmaps = indices of the
+// V, T and rho maps in each instance's block of nmaps maps.
+template <int HS, int HF, bool GEN, typename SIN, typename R>
+__global__ void __launch_bounds__(STAGE_THREADS)
+    sensor_tile_kernel_batch(const SensorArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
+                             const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(16) SensorArgs sa;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int4 tt = tiles[t];
+    __syncthreads();
+    for (int k = threadIdx.x; k < (int)(sizeof(SensorArgs) / 8); k += blockDim.x)
+      reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + tt.z)[k];
+    __syncthreads();
+    const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
+    if (!sensor_body<HS, HF, GEN, SIN, R>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, smem_raw, bar)) return;
+  }
 }
 
 // In-place z filter PerformTGfilter(q, 1, q) (ModShockCapturing.f90:63,69,75) as a
@@ -938,10 +1026,9 @@ __global__ void tgfilter_z_inplace_kernel(const Grid g, const uint32_t* __restri
 // r filter PerformTGfilter(q, 2, star) (:65, :71, :77), scaled by C*Re(*Pr) and the
 // z ramp (:66, :72, :79, :85-88). Blanked points keep 0 (the output arrays start
 // at 0 and are never written there).
-__global__ void sensor_rfilter_kernel(const SensorArgs a) {
+__device__ __forceinline__ void rfilter_body(const SensorArgs& a, long long p) {
   const Grid g = a.g;
   const long long n = (long long)g.Nz * g.Nr;
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const int j = (int)(p / g.Nz), i = (int)(p - (long long)j * g.Nz);
   const long long o = (long long)j * g.P + i;
@@ -974,6 +1061,15 @@ static void launch_sensor_tiles(const SensorArgs& a, const SideStream& side, cud
   if (a.ntiles_int > 0)
     sensor_tile_kernel<SENS_HS_INT, H_INT, false, SIN, R>
         <<<a.ntiles_int, STAGE_THREADS, SI::bytes(false), s>>>(a, a.tiles_int, *a.mv_int, *a.mt_int, *a.mrho);
+}
+
+__global__ void sensor_rfilter_kernel(const SensorArgs a) {
+  rfilter_body(a, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Batched: blockIdx.y = instance.
+__global__ void sensor_rfilter_kernel_batch(const SensorArgs* __restrict__ argv) {
+  rfilter_body(argv[blockIdx.y], (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 cudaError_t launch_sensor(const SensorArgs& a, bool rfilter, const SideStream& side, cudaStream_t s) {
@@ -1037,10 +1133,9 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __host__ __device__ constexpr int zr_pad(int nz) { return (nz + 15) & ~15; }
 __host__ __device__ constexpr int zr_xlen(int nz) { return ZR_PADL + zr_pad(nz) + ZR_PADR; }
 
-__global__ void tgfilter_z_rows_kernel(const Grid g, const unsigned char* __restrict__ zcode,
-                                       const double* __restrict__ q, double* __restrict__ out, int* flags) {
-  extern __shared__ __align__(128) unsigned char zr_smem[];
-  __shared__ __align__(8) uint64_t bar;
+__device__ __forceinline__ void zrows_body(const Grid& g, const unsigned char* __restrict__ zcode,
+                                           const double* __restrict__ q, double* __restrict__ out, int* flags, int j,
+                                           int f, unsigned char* zr_smem, uint64_t& bar) {
   const int Nz = g.Nz, P = (int)g.P;
   const int nchunk = (Nz + ZR_L - 1) / ZR_L;
   double* xs = reinterpret_cast<double*>(zr_smem);       // [ZR_PADL + Nz + pad]
@@ -1048,7 +1143,6 @@ __global__ void tgfilter_z_rows_kernel(const Grid g, const unsigned char* __rest
   unsigned char* gen = rs + ZR_PADL + P + ZR_PADR;       // [nchunk]: window holds a non-centred row
   double* ring_s = reinterpret_cast<double*>(                                // [10][blockDim]
       zr_smem + ((sizeof(double) * (size_t)zr_xlen(Nz) + ZR_PADL + P + ZR_PADR + nchunk + 15) & ~(size_t)15));
-  const int j = blockIdx.x, f = blockIdx.y;
   const double* x = q + (long long)f * g.plane + (long long)j * g.P;
   double* y = out + (long long)f * g.plane + (long long)j * g.P;
   // the row of Q and its z stencil codes arrive by two bulk copies
@@ -1160,12 +1254,34 @@ __global__ void tgfilter_z_rows_kernel(const Grid g, const unsigned char* __rest
   }
 }
 
-static size_t zr_smem_bytes(int Nz, long long P) {
+__global__ void tgfilter_z_rows_kernel(const Grid g, const unsigned char* __restrict__ zcode,
+                                       const double* __restrict__ q, double* __restrict__ out, int* flags) {
+  extern __shared__ __align__(128) unsigned char zr_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  zrows_body(g, zcode, q, out, flags, blockIdx.x, blockIdx.y, zr_smem, bar);
+}
+
+// Batched: blockIdx.x indexes rows (instance, j) of all instances, blockIdx.y the field;
+// the instance's grid and buffers come from its sensor arguments.
+__global__ void tgfilter_z_rows_kernel_batch(const SensorArgs* __restrict__ argv, const int2* __restrict__ rows) {
+  extern __shared__ __align__(128) unsigned char zr_smem[];
+  __shared__ __align__(8) uint64_t bar;
+  const int2 r = rows[blockIdx.x];
+  const SensorArgs& a = argv[r.x];
+  const Grid g = a.g;
+  zrows_body(g, a.zcode, a.Q, a.Qz, a.flags, r.y, blockIdx.y, zr_smem, bar);
+}
+
+static int zr_threads(int Nz) {
   const int nchunk = (Nz + ZR_L - 1) / ZR_L;
-  const int bs = std::min(1024, (nchunk + 31) / 32 * 32);
+  return std::min(1024, (nchunk + 31) / 32 * 32);
+}
+static size_t zr_smem_bytes(int Nz, long long P, int bs) {
+  const int nchunk = (Nz + ZR_L - 1) / ZR_L;
   const size_t head = sizeof(double) * (size_t)zr_xlen(Nz) + (size_t)(ZR_PADL + P + ZR_PADR) + nchunk;
   return ((head + 15) & ~(size_t)15) + sizeof(double) * 10 * (size_t)bs;
 }
+static size_t zr_smem_bytes(int Nz, long long P) { return zr_smem_bytes(Nz, P, zr_threads(Nz)); }
 
 cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const unsigned char* zcode, const double* q,
                                       double* out, int nfield, int* flags, cudaStream_t s) {
@@ -1275,9 +1391,28 @@ static cudaError_t sensor_attr() {
   return cudaFuncSetAttribute(sensor_tile_kernel<HS, HF, GEN, SIN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)SensSmem<HS, HF, SIN, R>::bytes(GEN));
 }
+template <int H, bool GEN, typename SIN, typename R>
+static cudaError_t stage_batch_attr() {
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)StageSmem<H, SIN, R, false>::bytes(GEN));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)StageSmem<H, SIN, R, true>::bytes(GEN));
+}
+template <int HS, int HF, bool GEN, typename SIN, typename R>
+static cudaError_t sensor_batch_attr() {
+  return cudaFuncSetAttribute(sensor_tile_kernel_batch<HS, HF, GEN, SIN, R>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SensSmem<HS, HF, SIN, R>::bytes(GEN));
+}
 template <typename SIN, typename R>
 static cudaError_t pair_attrs() {
-  cudaError_t e = stage_attr<H_GEN, true, SIN, R>();
+  cudaError_t e = stage_batch_attr<H_GEN, true, SIN, R>();
+  if (e == cudaSuccess) e = stage_batch_attr<H_INT, false, SIN, R>();
+  if (e == cudaSuccess) e = sensor_batch_attr<SENS_HS_GEN, H_GEN, true, SIN, R>();
+  if (e == cudaSuccess) e = sensor_batch_attr<SENS_HS_INT, H_INT, false, SIN, R>();
+  if (e != cudaSuccess) return e;
+  e = stage_attr<H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = stage_attr<H_INT, false, SIN, R>();
   if (e == cudaSuccess) e = sensor_attr<SENS_HS_GEN, H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = sensor_attr<SENS_HS_INT, H_INT, false, SIN, R>();
@@ -1291,8 +1426,106 @@ cudaError_t init_kernel_attributes() {
   if (e == cudaSuccess) e = pair_attrs<double, float>();
   if (e == cudaSuccess) e = pair_attrs<float, float>();
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tgfilter_z_rows_kernel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)zr_smem_bytes(ZR_MAXNZ, ZR_MAXNZ + 32, 1024));
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(tgfilter_z_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)zr_smem_bytes(ZR_MAXNZ, ZR_MAXNZ + 32));
+}
+
+// ---------------------------------------------------------------------------
+// Batched launches
+// ---------------------------------------------------------------------------
+size_t zrows_smem(int Nz, long long P, int bs) { return zr_smem_bytes(Nz, P, bs); }
+int zrows_threads(int Nz) { return zr_threads(Nz); }
+
+template <int H, bool GEN, typename SIN, typename R, bool LRN>
+static cudaError_t launch_stage_batch_t(const StageArgs* argv, const BatchTiles& t, const CUtensorMap* mapv, int kin,
+                                        cudaStream_t s) {
+  if (t.ntiles <= 0) return cudaSuccess;
+  const int cls = GEN ? 1 : 0;
+  const int4 k = make_int4(bmap_state(kin, cls), bmap_star(cls, LRN), 14, 15);
+  const size_t sm = StageSmem<H, SIN, R, LRN>::bytes(GEN);
+  stage_kernel_batch<H, GEN, SIN, R, LRN><<<t.grid, STAGE_THREADS, sm, s>>>(argv, t.tiles, t.ntiles, mapv, NM_BATCH, k);
+  return cudaGetLastError();
+}
+
+template <typename SIN, typename R, bool LRN>
+static cudaError_t launch_stage_batch_pair(const StageArgs* argv, const BatchTiles& tint, const BatchTiles& tgen,
+                                           const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s) {
+  cudaError_t e = fork(side, s);
+  if (e != cudaSuccess) return e;
+  e = launch_stage_batch_t<H_GEN, true, SIN, R, LRN>(argv, tgen, mapv, kin, side.stream ? side.stream : s);
+  if (e != cudaSuccess) return e;
+  e = launch_stage_batch_t<H_INT, false, SIN, R, LRN>(argv, tint, mapv, kin, s);
+  if (e != cudaSuccess) return e;
+  return join(side, s);
+}
+
+cudaError_t launch_stage_batch(const StageArgs* argv, const StageArgs& a0, const BatchTiles& tint, const BatchTiles& tgen,
+                               const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s) {
+  if (!a0.mixed) {
+    if (a0.learned) return launch_stage_batch_pair<double, double, true>(argv, tint, tgen, mapv, kin, side, s);
+    return launch_stage_batch_pair<double, double, false>(argv, tint, tgen, mapv, kin, side, s);
+  }
+  if (!a0.in_f32) {
+    if (a0.learned) return launch_stage_batch_pair<double, float, true>(argv, tint, tgen, mapv, kin, side, s);
+    return launch_stage_batch_pair<double, float, false>(argv, tint, tgen, mapv, kin, side, s);
+  }
+  if (a0.learned) return launch_stage_batch_pair<float, float, true>(argv, tint, tgen, mapv, kin, side, s);
+  return launch_stage_batch_pair<float, float, false>(argv, tint, tgen, mapv, kin, side, s);
+}
+
+template <typename SIN, typename R>
+static void launch_sensor_tiles_batch(const SensorArgs* argv, const BatchTiles& tint, const BatchTiles& tgen,
+                                      const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s) {
+  using SG = SensSmem<SENS_HS_GEN, H_GEN, SIN, R>;
+  using SI = SensSmem<SENS_HS_INT, H_INT, SIN, R>;
+  if (tgen.ntiles > 0)
+    sensor_tile_kernel_batch<SENS_HS_GEN, H_GEN, true, SIN, R>
+        <<<tgen.grid, STAGE_THREADS, SG::bytes(true), side.stream ? side.stream : s>>>(
+            argv, tgen.tiles, tgen.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 1), bmap_sensT(kin, 1), bmap_rho(kin), 0));
+  if (tint.ntiles > 0)
+    sensor_tile_kernel_batch<SENS_HS_INT, H_INT, false, SIN, R><<<tint.grid, STAGE_THREADS, SI::bytes(false), s>>>(
+        argv, tint.tiles, tint.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 0), bmap_sensT(kin, 0), bmap_rho(kin), 0));
+}
+
+cudaError_t launch_sensor_batch(const SensorArgs* argv, const SensorArgs& a0, const BatchTiles& tint,
+                                const BatchTiles& tgen, const CUtensorMap* mapv, int kin, const int2* zrows,
+                                int nzrows, int zthreads, size_t zsmem, bool rfilter, int ninst, long long max_pts,
+                                const SideStream& side, cudaStream_t s) {
+  cudaError_t e = fork(side, s);
+  if (e != cudaSuccess) return e;
+  if (!a0.mixed) launch_sensor_tiles_batch<double, double>(argv, tint, tgen, mapv, kin, side, s);
+  else if (!a0.in_f32) launch_sensor_tiles_batch<double, float>(argv, tint, tgen, mapv, kin, side, s);
+  else launch_sensor_tiles_batch<float, float>(argv, tint, tgen, mapv, kin, side, s);
+  e = join(side, s);
+  if (e != cudaSuccess) return e;
+  if (nzrows > 0) tgfilter_z_rows_kernel_batch<<<dim3(nzrows, 3), zthreads, zsmem, s>>>(argv, zrows);
+  if (rfilter) {
+    const int bs = 256;
+    sensor_rfilter_kernel_batch<<<dim3((unsigned)((max_pts + bs - 1) / bs), ninst), bs, 0, s>>>(argv);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dt_batch(const DtArgs* argv, int ninst, int nblocks, cudaStream_t s) {
+  dt_kernel_batch<<<dim3(nblocks, ninst), DT_THREADS, 0, s>>>(argv);
+  return cudaGetLastError();
+}
+
+__global__ void harmonic_phase_kernel_batch(const HarmArgs* argv) {
+  const HarmArgs a = argv[blockIdx.x];
+  const int s = threadIdx.x;
+  if (s < 1 || s > 4) return;
+  const double tend = *a.time, d = *a.dt;
+  const double cs = s == 1 ? 0.0 : (s == 4 ? 1.0 : 0.5);
+  a.out[s] = cos(a.omega * ((tend - d) + cs * d));
+}
+
+cudaError_t launch_harmonic_phase_batch(const HarmArgs* argv, int ninst, cudaStream_t s) {
+  harmonic_phase_kernel_batch<<<ninst, 32, 0, s>>>(argv);
+  return cudaGetLastError();
 }
 
 }  // namespace axj

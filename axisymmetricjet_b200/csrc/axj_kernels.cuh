@@ -52,7 +52,7 @@ struct StageArgs {
   const double* ramp;     // shock-capturing z ramp (1+tanh(5(z-10)))/2
   const double* dt;       // device dt (read by stages 1-4)
   double* staleT;         // stage 4: T(i*, j*) of its input, the next ComputeTimeStep's stale T
-  const double* time;     // t_n + dt during stages 1-4 (advanced by the dt kernel); t_n in stage 0
+  const double* harm;     // cos(omega t_s) of the harmonic forcing: [0] at t_n (stage 0), [s] at stage s
   int* flags;             // bit 0: non-finite value produced
   int stage;              // 0: write rhs only; 1..4: RK4 stage
   int iT, jT;             // stale-T point (0-based)
@@ -133,6 +133,10 @@ void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* 
 // V_r / V_z box vw x vh, temperature box tw x th (rho uses the stage tile box).
 void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th);
 cudaError_t launch_dt(const DtArgs& a, int nblocks, cudaStream_t s);
+// cos(omega t_s) of the harmonic forcing: rhs_mode != 0: out[0] at t = *time; else
+// out[s], s = 1..4, at t_s = (*time - *dt) + c_s * *dt (the device time is t_n + dt).
+cudaError_t launch_harmonic_phase(const double* time, const double* dt, double omega, int rhs_mode, double* out,
+                                  cudaStream_t s);
 // rfilter: also run the r filter into a.star (the stage kernel applies it itself; the
 // unit entry point axj_sensor needs the coefficients as output).
 cudaError_t launch_sensor(const SensorArgs& a, bool rfilter, const SideStream& side, cudaStream_t s);
@@ -148,6 +152,52 @@ cudaError_t launch_tgfilter_z_inplace(const Grid& g, const uint32_t* desc, const
                                       const double* q, double* out, int nfield, int* flags, cudaStream_t s);
 
 constexpr int DT_THREADS = 256;
+
+// ---- batched launches: many solver instances per launch ----
+// Per-instance TMA maps of a batch, NM_BATCH per instance, at these indices:
+//   state box of stage buffer b, tile class cls:  b * 2 + cls         (0..9)
+//   z-filtered coefficient box of class cls:      10 + cls
+//   final-coefficient box of class cls:           12 + cls
+//   pv_old tile box, running-sum tile box:         14, 15
+//   sensor V box of buffer b, class cls:           16 + b * 2 + cls  (16..25)
+//   sensor temperature box of buffer b, class cls: 26 + b * 2 + cls  (26..35)
+//   density tile box of buffer b:                  36 + b            (36..40)
+constexpr int NM_BATCH = 41;
+inline int bmap_state(int b, int cls) { return b * 2 + cls; }
+inline int bmap_star(int cls, bool lrn) { return (lrn ? 12 : 10) + cls; }
+inline int bmap_sens(int b, int cls) { return 16 + b * 2 + cls; }
+inline int bmap_sensT(int b, int cls) { return 26 + b * 2 + cls; }
+inline int bmap_rho(int b) { return 36 + b; }
+
+struct BatchTiles {
+  const int4* tiles;  // (i0, j0, instance, 0)
+  int ntiles;
+  int grid;           // persistent CTAs
+};
+
+// Fused stage over the interior and general tiles of all instances (general on the
+// side stream). argv: per-instance arguments of this stage (all with the same stage,
+// precision flags and learned flag); kin = stage-input buffer id.
+cudaError_t launch_stage_batch(const StageArgs* argv, const StageArgs& a0, const BatchTiles& tint, const BatchTiles& tgen,
+                               const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s);
+// Sensor chain over all instances: sensor tiles, the row-staged z filter of every row
+// (zrows: (instance, j)), and with rfilter the r filter (grid y = instance, max_pts
+// points per instance at most).
+cudaError_t launch_sensor_batch(const SensorArgs* argv, const SensorArgs& a0, const BatchTiles& tint,
+                                const BatchTiles& tgen, const CUtensorMap* mapv, int kin, const int2* zrows,
+                                int nzrows, int zthreads, size_t zsmem, bool rfilter, int ninst, long long max_pts,
+                                const SideStream& side, cudaStream_t s);
+cudaError_t launch_dt_batch(const DtArgs* argv, int ninst, int nblocks, cudaStream_t s);
+struct HarmArgs {
+  const double* time;
+  const double* dt;
+  double omega;
+  double* out;
+};
+cudaError_t launch_harmonic_phase_batch(const HarmArgs* argv, int ninst, cudaStream_t s);
+// z-filter smem for a row of Nz points with pitch P and bs threads.
+size_t zrows_smem(int Nz, long long P, int bs);
+int zrows_threads(int Nz);
 
 // Sets the message axj_last_error(NULL) returns.
 void set_global_error(const char* msg);

@@ -167,10 +167,8 @@ __device__ __forceinline__ float fd1s(const FeatArgs& a, const float* box, int r
 }
 
 template <typename SIN>
-__global__ void __launch_bounds__(256) features_kernel(const FeatArgs a) {
-  __shared__ float sb[3][FB_R * FB_Z];
+__device__ __forceinline__ void features_body(const FeatArgs& a, int i0, int j0, float (*sb)[FB_R * FB_Z]) {
   const Grid g = a.g;
-  const int i0 = blockIdx.x * FT_Z, j0 = blockIdx.y * FT_R;
   const SIN* U = static_cast<const SIN*>(a.U);
   const int fld[3] = {0, 1, 3};  // rho, V_r, V_z
   for (int e = threadIdx.x; e < 3 * FB_R * FB_Z; e += 256) {
@@ -204,6 +202,28 @@ __global__ void __launch_bounds__(256) features_kernel(const FeatArgs a) {
   const float vort = fabsf(dVrdz - dVzdr);
   const float h = sqrtf((float)(__ldg(a.dz + i) * __ldg(a.dr + j)));
   a.feat[o] = make_float4(dil, grad, vort, h);
+}
+
+template <typename SIN>
+__global__ void __launch_bounds__(256) features_kernel(const FeatArgs a) {
+  __shared__ float sb[3][FB_R * FB_Z];
+  features_body<SIN>(a, blockIdx.x * FT_Z, blockIdx.y * FT_R, sb);
+}
+
+// Batched: persistent loop over (i0, j0, instance) tiles of 32 x 8 points.
+__global__ void __launch_bounds__(256) features_kernel_batch(const FeatArgs* __restrict__ argv,
+                                                             const int4* __restrict__ tiles, int ntiles) {
+  __shared__ float sb[3][FB_R * FB_Z];
+  __shared__ __align__(16) FeatArgs sa;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int4 tt = tiles[t];
+    __syncthreads();
+    for (int k = threadIdx.x; k < (int)(sizeof(FeatArgs) / 4); k += blockDim.x)
+      reinterpret_cast<unsigned int*>(&sa)[k] = reinterpret_cast<const unsigned int*>(argv + tt.z)[k];
+    __syncthreads();
+    if (sa.f32) features_body<float>(sa, tt.x, tt.y, sb);
+    else features_body<double>(sa, tt.x, tt.y, sb);
+  }
 }
 
 cudaError_t launch_features(const FeatArgs& a, cudaStream_t s) {
@@ -243,7 +263,13 @@ __device__ __forceinline__ uint32_t kmaj(int row, int k, int rows) {
   return (uint32_t)((k >> 3) * rows * 16 + (row >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-__global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a) {
+// BATCH: tiles (i0, j0, instance) from a table over many instances, each with its own
+// arguments in argv (the model, its normalisation and the error flag are a0's, shared by
+// the batch); otherwise the tiles of a0's grid in raster order.
+template <bool BATCH>
+__global__ void __launch_bounds__(MT_THREADS)
+    mlp_infer_kernel(const InferArgs a0, const InferArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles) {
+  const InferArgs& a = a0;
   extern __shared__ unsigned char m_raw[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
@@ -255,8 +281,6 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
   float* sW3 = sB2 + MLP_HID;  // [2][64]
   float* sB3 = sW3 + MLP_OUT * MLP_HID;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const Grid g = a.g;
-
   // weights in BF16, core-matrix layout
   for (int e = tid; e < MLP_HID * MLP_K1; e += MT_THREADS) {
     const int n = e / MLP_K1, k = e - n * MLP_K1;
@@ -276,9 +300,25 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
   if (warp == 0) tmem_alloc(&tmem_slot, 64);
 
   // channel box of a tile: raw loads (zero outside the grid) into registers ...
+  // tile t: origin and instance
+  auto tile_of = [&](int t, int& ti0, int& tj0, int& inst) {
+    if (BATCH) {
+      const int4 tt = tiles[t];
+      ti0 = tt.x;
+      tj0 = tt.y;
+      inst = tt.z;
+    } else {
+      ti0 = (t % a0.ntiles_z) * MT_Z;
+      tj0 = (t / a0.ntiles_z) * MT_R;
+      inst = 0;
+    }
+  };
   auto load_box = [&](int t, float4* v) {
-    const int tz = t % a.ntiles_z, tr = t / a.ntiles_z;
-    const int i0 = tz * MT_Z - 2, j0 = tr * MT_R - 2;
+    int ti0, tj0, inst;
+    tile_of(t, ti0, tj0, inst);
+    const InferArgs& at = BATCH ? argv[inst] : a0;
+    const Grid g = at.g;
+    const int i0 = ti0 - 2, j0 = tj0 - 2;
 #pragma unroll
     for (int q = 0; q < MBOX_PER; ++q) {
       const int e = tid + q * MT_THREADS;
@@ -286,7 +326,7 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
       if (e < MBOX_N) {
         const int br = e / MBOX_Z, bz = e - br * MBOX_Z;
         const int i = i0 + bz, j = j0 + br;
-        if (i >= 0 && i < g.Nz && j >= 0 && j < g.Nr) v[q] = __ldg(a.feat + (long long)j * g.P + i);
+        if (i >= 0 && i < g.Nz && j >= 0 && j < g.Nr) v[q] = __ldg(at.feat + (long long)j * g.P + i);
       }
     }
   };
@@ -304,7 +344,7 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
     }
   };
   float4 nxt[MBOX_PER];
-  if (blockIdx.x < a.ntiles) {
+  if ((int)blockIdx.x < ntiles) {
     load_box(blockIdx.x, nxt);
     store_box(nxt);
   }
@@ -318,9 +358,11 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
   const int c = tid & 31, rr = tid >> 5;  // this thread's point in the tile
   uint32_t phase = 0;
   bool ok = true;
-  for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
-    const int tz = t % a.ntiles_z, tr = t / a.ntiles_z;
-    const int i0 = tz * MT_Z, j0 = tr * MT_R;
+  for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    int i0, j0, inst;
+    tile_of(t, i0, j0, inst);
+    const InferArgs& at = BATCH ? argv[inst] : a0;
+    const Grid g = at.g;
     // A row `tid` of layer 1: feature k = ch*25 + (dr+2)*5 + (dz+2), zero for k >= 100
     const unsigned short* bx = reinterpret_cast<const unsigned short*>(sBox);
 #pragma unroll
@@ -356,7 +398,7 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
     __syncwarp();
     // the next tile's channel values travel while the MMAs run
     const int tn = t + gridDim.x;
-    if (tn < a.ntiles) load_box(tn, nxt);
+    if (tn < ntiles) load_box(tn, nxt);
     ok = __syncthreads_and(bar_wait(&bar, phase));
     phase ^= 1u;
     if (!ok) break;
@@ -389,7 +431,7 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
     }
     __syncwarp();
     // the box of this tile is no longer read: the next tile's goes in while the MMAs run
-    if (tn < a.ntiles) store_box(nxt);
+    if (tn < ntiles) store_box(nxt);
     ok = __syncthreads_and(bar_wait(&bar, phase));
     phase ^= 1u;
     if (!ok) break;
@@ -409,16 +451,16 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
     const int i = i0 + c, j = j0 + rr;
     if (i < g.Nz && j < g.Nr) {
       const long long o = (long long)j * g.P + i;
-      const double ramp = __ldg(a.ramp + i);
+      const double ramp = __ldg(at.ramp + i);
       const double p0 = (double)(y0 * a.norm.out_scale[0]) * ramp;
       const double p1 = (double)(y1 * a.norm.out_scale[1]) * ramp;
-      if (a.mode == 0) {
-        a.out[o] = p0;
-        a.out[g.plane + o] = p1;
+      if (at.mode == 0) {
+        at.out[o] = p0;
+        at.out[g.plane + o] = p1;
       } else {
-        const unsigned char m = __ldg(a.mask + o);
-        a.out[g.plane + o] = (m & 1) ? __ldg(a.held + o) : p0;
-        a.out[2 * g.plane + o] = (m & 2) ? __ldg(a.held + g.plane + o) : p1;
+        const unsigned char m = __ldg(at.mask + o);
+        at.out[g.plane + o] = (m & 1) ? __ldg(at.held + o) : p0;
+        at.out[2 * g.plane + o] = (m & 2) ? __ldg(at.held + g.plane + o) : p1;
       }
     }
     fence_async_smem();  // the next tile's box (generic writes) before its A operand is built
@@ -437,7 +479,9 @@ __global__ void __launch_bounds__(MT_THREADS) mlp_infer_kernel(const InferArgs a
 }
 
 cudaError_t mlp_init_attributes() {
-  return cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M_SMEM);
+  cudaError_t e = cudaFuncSetAttribute(mlp_infer_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M_SMEM);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(mlp_infer_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M_SMEM);
 }
 
 cudaError_t launch_mlp_infer(const InferArgs& a, cudaStream_t s) {
@@ -447,17 +491,16 @@ cudaError_t launch_mlp_infer(const InferArgs& a, cudaStream_t s) {
   // at most 4 CTAs per SM (shared memory): 4 x 64 of the 512 TMEM columns
   const int grid = a.ntiles < M_CTAS_PER_SM * nsm ? a.ntiles : M_CTAS_PER_SM * nsm;
   if (grid <= 0) return cudaSuccess;
-  mlp_infer_kernel<<<grid, MT_THREADS, M_SMEM, s>>>(a);
+  mlp_infer_kernel<false><<<grid, MT_THREADS, M_SMEM, s>>>(a, nullptr, nullptr, a.ntiles);
   return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
 // Judge
 // ---------------------------------------------------------------------------
-__global__ void judge_kernel(const JudgeArgs a) {
+__device__ __forceinline__ void judge_body(const JudgeArgs& a, long long p) {
   const Grid g = a.g;
   const long long n = (long long)g.Nz * g.Nr;
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long fb = 0, judged = 0;
   if (p < n) {
     const int j = (int)(p / g.Nz), i = (int)(p - (long long)j * g.Nz);
@@ -490,6 +533,36 @@ __global__ void judge_kernel(const JudgeArgs a) {
     atomicAdd(a.counts + 0, judged);
     atomicAdd(a.counts + 1, fb);
   }
+}
+
+__global__ void judge_kernel(const JudgeArgs a) { judge_body(a, (long long)blockIdx.x * blockDim.x + threadIdx.x); }
+
+// Batched: blockIdx.y = instance.
+__global__ void judge_kernel_batch(const JudgeArgs* __restrict__ argv) {
+  judge_body(argv[blockIdx.y], (long long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+cudaError_t launch_judge_batch(const JudgeArgs* argv, int ninst, long long max_pts, cudaStream_t s) {
+  const int bs = 256;
+  judge_kernel_batch<<<dim3((unsigned)((max_pts + bs - 1) / bs), ninst), bs, 0, s>>>(argv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_features_batch(const FeatArgs* argv, const int4* tiles, int ntiles, int grid, cudaStream_t s) {
+  if (ntiles <= 0) return cudaSuccess;
+  features_kernel_batch<<<grid, 256, 0, s>>>(argv, tiles, ntiles);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_infer_batch(const InferArgs& a0, const InferArgs* argv, const int4* tiles, int ntiles,
+                                   cudaStream_t s) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = ntiles < M_CTAS_PER_SM * nsm ? ntiles : M_CTAS_PER_SM * nsm;
+  if (grid <= 0) return cudaSuccess;
+  mlp_infer_kernel<true><<<grid, MT_THREADS, M_SMEM, s>>>(a0, argv, tiles, ntiles);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_judge(const JudgeArgs& a, cudaStream_t s) {

@@ -290,10 +290,11 @@ AXJ_HD void control_forcing(double z, double r, const Consts& c, const double* F
 // Harmonic inflow forcing (control_forcing = 2, an extension; the reference's
 // ControlForcingTerms is the feedback above): rhs(V_z) += A omega G cos(omega t) in the
 // same Gaussian window, a V_z fluctuation of amplitude A G.
-AXJ_HD void harmonic_forcing(double z, double r, double t, const Consts& c, double rhs[5]) {
+// cwt = cos(omega t) of the stage, evaluated once per launch.
+AXJ_HD void harmonic_forcing(double z, double r, double cwt, const Consts& c, double rhs[5]) {
   double dz = z - c.forcing_z0, dr = r - c.forcing_r0;
   double G = exp(-((dz * dz) / (c.forcing_lz * c.forcing_lz)) - (dr * dr) / (c.forcing_lr * c.forcing_lr));
-  rhs[3] = rhs[3] + c.harm_amp * c.harm_omega * G * cos(c.harm_omega * t);
+  rhs[3] = rhs[3] + c.harm_amp * c.harm_omega * G * cwt;
 }
 
 // Per-point dt of ComputeTimeStep (ModInputOutput.f90:395-416).

@@ -118,3 +118,30 @@ def case(name, **kw):
     spec = dict(CASES[name])
     spec.update(kw)
     return make_case(**spec)
+
+
+def batch_instances(n=64, seed=2024, nz_range=(256, 2048), nr_range=(96, 384), mach_range=(0.9, 1.5),
+                    re_range=(1000.0, 5000.0), amp_frac=(0.0, 0.02), st_range=(0.2, 0.6), **pkw):
+    """Cases of uneven independent jets for a batch: Nz and Nr drawn uniformly from
+    their ranges and rounded to multiples of 32, Mach and Re uniform, and an
+    azimuthal-mode-0 harmonic inflow forcing (control_forcing = 2) in the shear layer
+    near the inflow with amplitude uniform in amp_frac * U_j and Strouhal number in
+    st_range. Every case has the small plain case's construction (z on [0, 30D], r to
+    10D, tanh profile, seeded perturbation) with shock capturing on; pkw go to the
+    parameters of every case (e.g. precision, sensor)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        Nz = int(np.clip(32 * np.round(rng.uniform(*nz_range) / 32), 32, None))
+        Nr = int(np.clip(32 * np.round(rng.uniform(*nr_range) / 32), 32, None))
+        Mj = float(rng.uniform(*mach_range))
+        Re = float(rng.uniform(*re_range))
+        Uj = Mj  # T_j = T_inf = 1
+        amp = float(rng.uniform(*amp_frac)) * Uj
+        st = float(rng.uniform(*st_range))
+        c = make_case(Nz, Nr, 30.0, 10.0, Mj, Re, sc=True, seed=seed + k, control_forcing=2, forcing_z0=1.0,
+                      forcing_r0=0.5, forcing_lz=0.5, forcing_lr=0.2, harmonic_amp=amp, harmonic_st=st,
+                      harmonic_uj=Uj, **pkw)
+        c.update(Re=Re, amp=amp, St=st)
+        out.append(c)
+    return out

@@ -287,6 +287,40 @@ int axj_mlp_features(axj_handle* h, const double* pv, float* feat);
 int axj_mlp_predict(axj_handle* h, const double* pv, double* betastar, double* kappastar);
 int axj_learned_stats(axj_handle* h, int64_t* judged_outputs, int64_t* fallbacks, int64_t* njudges);
 
+/* ---- Batches: many instances in one launch per kernel ------------------------------
+ * No counterpart in the reference (one jet per run). A batch advances n handles of
+ * uneven grids and parameters together: each kernel of the step runs once for all of
+ * them, as a persistent grid-stride kernel over a table of (tile, instance) entries
+ * with per-instance arguments and TMA descriptors in device tables, and the whole step
+ * is captured in a CUDA graph. The handles keep their state: axj_get_state etc. work
+ * on them between batch calls. All handles need the same device, precision, sensor
+ * kind and shock-capturing setting (and, learned, the same model), and their state
+ * set. The batch does not own the handles; destroy it before them. */
+typedef struct axj_batch axj_batch;
+typedef struct axj_batch_tuning {
+  int64_t tile_order;          /* 0: instance after instance; 1: round-robin over instances */
+  int64_t stage_ctas_per_sm;   /* persistent CTAs per SM of the interior stage kernel (2) */
+  int64_t sensor_ctas_per_sm;  /* persistent CTAs per SM of the interior sensor kernel (2) */
+  int64_t reserved[5];
+} axj_batch_tuning;
+
+void axj_batch_default_tuning(axj_batch_tuning* t);
+int axj_batch_create(axj_handle* const* handles, int64_t n, axj_batch** out);
+/* nsteps x (ComputeTimeStep + RK4) of every instance, each with its own dt. */
+int axj_batch_run(axj_batch* b, int64_t nsteps);
+/* As axj_batch_run, *ms = device time of the nsteps graph launches (CUDA events). */
+int axj_batch_run_timed(axj_batch* b, int64_t nsteps, double* ms);
+int axj_batch_set_tuning(axj_batch* b, const axj_batch_tuning* t);
+int axj_batch_get_tuning(axj_batch* b, axj_batch_tuning* t);
+/* Autotuner: times steps_per_trial batch steps for every candidate tuning (tile order x
+ * CTAs per SM), keeps the fastest and returns it in *chosen; trial_ms (nullable, room for
+ * 8) receives each trial's time. The trial steps are undone: the instances' solutions,
+ * times and iteration counters are restored (the learned sensor re-judges). */
+int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* chosen, double* trial_ms,
+                       int64_t* ntrials);
+const char* axj_batch_last_error(const axj_batch* b);
+void axj_batch_destroy(axj_batch* b);
+
 /* Last error message of the handle (or of the last failed axj_create if h is NULL). */
 const char* axj_last_error(const axj_handle* h);
 

@@ -645,13 +645,14 @@ static void control_forcing(axo* o) {
 static void harmonic_forcing(axo* o, double t) {
   const axj_params* p = &o->p;
   const double omega = 2.0 * 3.141592653589793 * p->harmonic_st * p->harmonic_uj;
+  const double cwt = cos(omega * t);
 #pragma omp parallel for schedule(static)
   for (I8 j = 1; j <= o->Nr; ++j)
     for (I8 i = 1; i <= o->Nz; ++i) {
       double zl = H(o, zvec, i, j), rl = H(o, rvec, i, j);
       double dz = zl - p->forcing_z0, dr = rl - p->forcing_r0;
       double G = exp(-((dz * dz) / (p->forcing_lz * p->forcing_lz)) - (dr * dr) / (p->forcing_lr * p->forcing_lr));
-      S5(o, rhs, i, j, 4) = S5(o, rhs, i, j, 4) + p->harmonic_amp * omega * G * cos(omega * t);
+      S5(o, rhs, i, j, 4) = S5(o, rhs, i, j, 4) + p->harmonic_amp * omega * G * cwt;
     }
 }
 

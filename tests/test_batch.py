@@ -1,0 +1,107 @@
+"""Batches: many uneven jets advanced by one launch per kernel.
+
+The batched kernels run the same per-tile source as a single instance's kernels, but
+they are separate compilations, so FMA contraction may differ in the last bit: a batch
+must reproduce every instance's own run to 1e-12 relative per field after 7 steps on
+the FP64 path (the per-step parity bar), and to 1e-6 with FP32 stage states and the
+learned sensor (judge steps included). Both tile orders are checked, and the
+autotuner's undo of its trial steps.
+"""
+import numpy as np
+import pytest
+
+import axisymmetricjet_b200 as axj
+from axisymmetricjet_b200 import fixtures
+
+SMALL = dict(nz_range=(128, 256), nr_range=(64, 128))  # stable over the test steps (checked with the oracle)
+
+
+def _solvers(cases, model=None):
+    out = []
+    for c in cases:
+        patches = axj.patches_from_records(c["records"], c["Nz"], c["Nr"])
+        s = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+        if model is not None:
+            s.mlp_set(model)
+        s.set_state(c["pv"], c["target"])
+        out.append(s)
+    return out
+
+
+def test_batch_instances_follow_the_distribution():
+    cases = fixtures.batch_instances(64)
+    assert len(cases) == 64
+    for c in cases:
+        assert c["Nz"] % 32 == 0 and 256 <= c["Nz"] <= 2048
+        assert c["Nr"] % 32 == 0 and 96 <= c["Nr"] <= 384
+        assert 0.9 <= c["Mj"] <= 1.5 and 1000.0 <= c["Re"] <= 5000.0
+        assert 0.0 <= c["amp"] <= 0.02 * c["Mj"] and 0.2 <= c["St"] <= 0.6
+        assert c["params"].control_forcing == 2 and c["params"].shock_capturing == 1
+    again = fixtures.batch_instances(64)
+    assert [c["Nz"] for c in cases] == [c["Nz"] for c in again]
+
+
+def _model(cases):
+    m = axj.mlp_init(3)
+    m["out_scale"] = np.array([1e-3, 1e-3], dtype=np.float32)
+    return m
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["fp64", "mixed_learned"])
+@pytest.mark.parametrize("order", [0, 1])
+def test_batch_equals_individual_runs(mode, order):
+    kw = {} if mode == "fp64" else dict(precision=1, sensor=1, judge_every=3)
+    cases = fixtures.batch_instances(3, seed=5, **SMALL, **kw)
+    model = _model(cases) if mode != "fp64" else None
+    single = _solvers(cases, model)
+    batched = _solvers(cases, model)
+    b = axj.AxjBatch(batched)
+    b.set_tuning(tile_order=order, stage_ctas_per_sm=1 + order)
+    steps = 7
+    b.run(steps)
+    for s in single:
+        s.run(steps)
+    tol = 1e-12 if mode == "fp64" else 1e-6
+    for k, (s, t) in enumerate(zip(single, batched)):
+        a, r = t.get_state(), s.get_state()
+        errs = [np.abs(a[f] - r[f]).max() / max(np.abs(r[f]).max(), 1e-300) for f in range(5)]
+        assert max(errs) <= tol, (k, errs)
+        assert t.get_time()[0] == s.get_time()[0]
+        assert abs(t.get_time()[1] - s.get_time()[1]) <= 1e-12 * abs(s.get_time()[1])
+    b.close()
+    for s in single + batched:
+        s.close()
+
+
+@pytest.mark.gpu
+def test_autotune_undoes_its_trials():
+    cases = fixtures.batch_instances(4, seed=9, **SMALL, precision=1, sensor=1)
+    model = _model(cases)
+    batched = _solvers(cases, model)
+    ref = _solvers(cases, model)
+    b = axj.AxjBatch(batched)
+    chosen, trials = b.autotune(steps_per_trial=2)
+    assert len(trials) == 8 and all(t > 0 for t in trials)
+    assert b.tuning() == chosen
+    b.run(3)
+    for s in ref:
+        s.run(3)
+    for s, t in zip(ref, batched):
+        a, r = t.get_state(), s.get_state()
+        errs = [np.abs(a[f] - r[f]).max() / max(np.abs(r[f]).max(), 1e-300) for f in range(5)]
+        assert max(errs) <= 1e-6, errs
+    b.close()
+    for s in ref + batched:
+        s.close()
+
+
+@pytest.mark.gpu
+def test_batch_rejects_mixed_kinds():
+    c1 = fixtures.batch_instances(1, seed=1, **SMALL)[0]
+    c2 = fixtures.batch_instances(1, seed=2, **SMALL, precision=1)[0]
+    s = _solvers([c1, c2])
+    with pytest.raises(axj.AxjError):
+        axj.AxjBatch(s)
+    for x in s:
+        x.close()
