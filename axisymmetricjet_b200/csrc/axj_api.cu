@@ -53,6 +53,7 @@ struct axj_handle {
   unsigned char* zcode = nullptr;  // z stencil code per point for the z filter (9 = blanked)
   int* faces = nullptr;
   double *dxidz = nullptr, *ddxidxidz = nullptr, *detadr = nullptr, *ddetadetadr = nullptr;
+  double* invr = nullptr;  // 1/r_j (0 on the axis row)
   double *zc = nullptr, *rc = nullptr, *dzv = nullptr, *drv = nullptr, *ramp = nullptr, *forcing = nullptr;
   double *dt = nullptr, *staleT = nullptr, *partial = nullptr, *time = nullptr;
   double* harm = nullptr;  // cos(omega t_s) of the harmonic forcing per stage
@@ -288,6 +289,7 @@ StageArgs stage_args(axj_handle* h, int bin, int bout, int stage) {
   a.ddetadetadr = h->ddetadetadr;
   a.zc = h->zc;
   a.rc = h->rc;
+  a.invr = h->invr;
   a.forcing = h->forcing;
   a.ramp = h->ramp;
   a.dt = h->dt;
@@ -967,6 +969,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->ddetadetadr = dalloc<double>(h, Nr, &rc);
   h->zc = dalloc<double>(h, Nz, &rc);
   h->rc = dalloc<double>(h, Nr, &rc);
+  h->invr = dalloc<double>(h, Nr, &rc);
   h->dzv = dalloc<double>(h, Nz, &rc);
   h->drv = dalloc<double>(h, Nr, &rc);
   h->ramp = dalloc<double>(h, Nz, &rc);
@@ -1003,6 +1006,9 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   up(h->ddetadetadr, ddetadetadr.data(), Nr * sizeof(double));
   up(h->zc, z.data(), Nz * sizeof(double));
   up(h->rc, r.data(), Nr * sizeof(double));
+  std::vector<double> invr(Nr, 0.0);
+  for (int64_t j = 1; j < Nr; ++j) invr[j] = 1.0 / r[j];
+  up(h->invr, invr.data(), Nr * sizeof(double));
   up(h->dzv, dzv.data(), Nz * sizeof(double));
   up(h->drv, drv.data(), Nr * sizeof(double));
   up(h->ramp, ramp.data(), Nz * sizeof(double));

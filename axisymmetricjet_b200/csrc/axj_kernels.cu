@@ -184,10 +184,6 @@ struct StageSmem {
   static constexpr int NPER = (NPT + STAGE_THREADS - 1) / STAGE_THREADS;
 };
 
-template <typename R>
-__device__ __forceinline__ R pow0666(R T);
-template <> __device__ __forceinline__ double pow0666<double>(double T) { return pow(T, 0.666); }
-template <> __device__ __forceinline__ float pow0666<float>(float T) { return powf(T, 0.666f); }
 
 // Fused RK stage. SIN: storage type of the stage input (double, or float for the
 // mixed path's intermediate stages); R: arithmetic type of the stencils and, in
@@ -269,7 +265,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
       const int rr = idx / RZ, rz = idx - rr * RZ;
       const bool cross = (rr >= H && rr < H + TR && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
       if (!cross) continue;
-      const double mu = double(pow0666<R>(R(sU[4 * NPT + idx])));
+      const double mu = double(mu_of_T<R>(R(sU[4 * NPT + idx])));
       vmu[k] = mu;
       if (rr >= H && rr < H + TR && rz >= HZ && rz < HZ + TZ) sMu0[(rr - H) * TZ + (rz - HZ)] = mu;
       if (sc) {
@@ -439,8 +435,11 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
     double rhs[5] = {-0.0, -0.0, -0.0, -0.0, -0.0};
     if (!j1) {
       RP rp[5];
-      rhs_inviscid<RP>(q, d, RP(rloc), RP(a.c.gam), rp);
-      if (a.c.do_viscous) rhs_viscous<RP>(q, d, RP(rloc), RP(a.c.gam), RP(a.c.Re), RP(a.c.Pr), sc, rp);
+      const RhsConst<RP> kc = rhs_const<RP>(a.c.gam, a.c.Re, a.c.Pr);
+      const RP onebyr = RP(__ldg(a.invr + j));
+      const RP inv_rho = RP(1.0) / q.rho;
+      rhs_inviscid<RP>(q, d, onebyr, inv_rho, kc, rp);
+      if (a.c.do_viscous) rhs_viscous<RP>(q, d, onebyr, inv_rho, kc, sc, rp);
 #pragma unroll
       for (int f = 0; f < 5; ++f) rhs[f] = double(rp[f]);
     }
@@ -651,7 +650,7 @@ __device__ __forceinline__ void dt_body(const DtArgs& a, int blk, int nblk) {
       v = 100.0;
     } else {
       const double Vr = __ldg(a.U + 1 * PL + o), Vz = __ldg(a.U + 3 * PL + o), T = __ldg(a.U + 4 * PL + o);
-      const double mu = pow(T, 0.666);
+      const double mu = mu_of_T<double>(T);
       const double beta = (3.0 / 5.0) * mu;
       const double lambda = beta - (2.0 / 3.0) * mu;
       v = dt_point(Vz, Vr, phys ? T : Tst, mu, lambda, mu, __ldg(a.dxidz + i), __ldg(a.detadr + j), a.c);

@@ -48,6 +48,7 @@ struct StageArgs {
   const double* ddetadetadr;
   const double* zc;
   const double* rc;
+  const double* invr;     // 1/r_j (0 on the axis row)
   const double* forcing;  // 25 doubles, row-major F(eqn,k)
   const double* ramp;     // shock-capturing z ramp (1+tanh(5(z-10)))/2
   const double* dt;       // device dt (read by stages 1-4)

@@ -44,16 +44,31 @@ AXJ_HD DerivT<RO> convert(const DerivT<RI>& d) {
                     RO(d.d2Vrdzdr), RO(d.d2Vzdzdr)};
 }
 
+// Per-point reciprocals and per-run constants of the right-hand side: the reference
+// divides by r, rho, gam*rho, Re*rho and Re*Pr*rho at every point (about ten FP64
+// divisions); here 1/r comes from a per-row table, 1/rho is formed once and the
+// constant factors once per run. The products differ from the quotients by rounding.
+template <typename R>
+struct RhsConst {
+  R gam, inv_gam, gam_m1, inv_Re, gam_RePr, gg1_Re;  // gam, 1/gam, gam-1, 1/Re, gam/(Re Pr), gam(gam-1)/Re
+};
+template <typename R>
+AXJ_HD RhsConst<R> rhs_const(double gam, double Re, double Pr) {
+  return RhsConst<R>{R(gam), R(1.0 / gam), R(gam - 1.0), R(1.0 / Re), R(gam / (Re * Pr)), R(gam * (gam - 1.0) / Re)};
+}
+
 // Inviscid part, already negated (ModRHS.f90:92-96 and :103-113).
 template <typename R>
-AXJ_HD void rhs_inviscid(const PrimT<R>& q, const DerivT<R>& d, R r, R gam, R rhs[5]) {
-  const R one = R(1.0), mone = R(-1.0);
+AXJ_HD void rhs_inviscid(const PrimT<R>& q, const DerivT<R>& d, R onebyr, R inv_rho, const RhsConst<R>& k, R rhs[5]) {
+  const R mone = R(-1.0);
   const R rho = q.rho, Vr = q.Vr, Vt = q.Vt, Vz = q.Vz, T = q.T;
-  R r1 = Vr * d.drhodr + Vz * d.drhodz + rho * (d.dVrdr + Vr / r + d.dVzdz);
-  R r2 = Vr * d.dVrdr + Vz * d.dVrdz + one / (gam * rho) * d.dpdr;
-  R r3 = Vr * d.dVtdr + Vr * Vt / r + Vz * d.dVtdz;
-  R r4 = Vr * d.dVzdr + Vz * d.dVzdz + one / (gam * rho) * d.dpdz;
-  R r5 = Vr * d.dTdr + Vz * d.dTdz + (gam - one) * T * (d.dVrdr + Vr / r + d.dVzdz);
+  const R Vr_r = Vr * onebyr;
+  const R igr = k.inv_gam * inv_rho;
+  R r1 = Vr * d.drhodr + Vz * d.drhodz + rho * (d.dVrdr + Vr_r + d.dVzdz);
+  R r2 = Vr * d.dVrdr + Vz * d.dVrdz + igr * d.dpdr;
+  R r3 = Vr * d.dVtdr + Vt * Vr_r + Vz * d.dVtdz;
+  R r4 = Vr * d.dVzdr + Vz * d.dVzdz + igr * d.dpdz;
+  R r5 = Vr * d.dTdr + Vz * d.dTdz + k.gam_m1 * T * (d.dVrdr + Vr_r + d.dVzdz);
   rhs[0] = mone * r1;
   rhs[1] = mone * r2;
   rhs[2] = mone * r3;
@@ -64,40 +79,49 @@ AXJ_HD void rhs_inviscid(const PrimT<R>& q, const DerivT<R>& d, R r, R gam, R rh
 // Viscous S_r, S_theta, S_z, S_T (ModRHS.f90:135-209). With shock capturing the
 // per-point constants come from lambda/mu (:180-188).
 template <typename R>
-AXJ_HD void rhs_viscous(const PrimT<R>& q, const DerivT<R>& d, R r, R gam, R Re, R Pr, bool sc, R rhs[5]) {
+AXJ_HD void rhs_viscous(const PrimT<R>& q, const DerivT<R>& d, R onebyr, R inv_rho, const RhsConst<R>& k, bool sc,
+                        R rhs[5]) {
   const R one = R(1.0);
   R fourby3 = R(29.0 / 15.0), oneby3 = R(14.0 / 15.0), twoby3 = R(1.0 / 15.0);
-  const R onebyr = one / r;
-  const R rho = q.rho, Vr = q.Vr, Vt = q.Vt, mu = q.mu, kappa = q.kappa;
+  const R Vr = q.Vr, Vt = q.Vt, mu = q.mu, kappa = q.kappa;
   if (sc) {
     R tmp = q.lambda / q.mu;
     fourby3 = R(2.0) + tmp;
     oneby3 = one + tmp;
     twoby3 = R(-1.0) * tmp;
   }
-  rhs[1] = rhs[1] + one / (Re * rho) *
+  const R iRr = k.inv_Re * inv_rho;  // 1/(Re rho)
+  rhs[1] = rhs[1] + iRr *
                         (mu * (fourby3 * d.d2Vrdr2 + fourby3 * onebyr * d.dVrdr + oneby3 * d.d2Vzdzdr + d.d2Vrdz2 -
                                fourby3 * Vr * (onebyr * onebyr)) +
                          d.dmudr * (fourby3 * d.dVrdr - twoby3 * Vr * onebyr - twoby3 * d.dVzdz) +
                          d.dmudz * (d.dVrdz + d.dVzdr));
-  rhs[2] = rhs[2] + one / (Re * rho) *
+  rhs[2] = rhs[2] + iRr *
                         (mu * (d.d2Vtdr2 + d.d2Vtdz2 + onebyr * d.dVtdr - Vt * (onebyr * onebyr)) +
                          d.dmudr * (d.dVtdr - Vt * onebyr) + d.dmudz * d.dVtdz);
-  rhs[3] = rhs[3] + one / (Re * rho) *
+  rhs[3] = rhs[3] + iRr *
                         (mu * (d.d2Vzdr2 + fourby3 * d.d2Vzdz2 + oneby3 * d.d2Vrdzdr + onebyr * d.dVzdr +
                                oneby3 * onebyr * d.dVrdz) +
                          d.dmudr * (d.dVzdr + d.dVrdz) +
                          d.dmudz * (fourby3 * d.dVzdz - twoby3 * d.dVrdr - twoby3 * Vr * onebyr));
   rhs[4] = rhs[4] +
-           gam / (Re * Pr * rho) *
+           k.gam_RePr * inv_rho *
                (kappa * (d.d2Tdr2 + onebyr * d.dTdr + d.d2Tdz2) + d.dkappadr * d.dTdr + d.dkappadz * d.dTdz) +
-           gam * (gam - one) / Re * mu / rho *
+           k.gg1_Re * mu * inv_rho *
                (d.dVrdr * (fourby3 * d.dVrdr - twoby3 * Vr * onebyr - twoby3 * d.dVzdz) +
                 (d.dVtdr - Vt * onebyr) * (d.dVtdr - Vr * onebyr) +
                 Vr * onebyr * (fourby3 * Vr * onebyr - twoby3 * d.dVrdr - twoby3 * d.dVzdz) + d.dVtdz * d.dVtdz +
                 d.dVzdz * (fourby3 * d.dVzdz - twoby3 * d.dVrdr - twoby3 * Vr * onebyr) +
                 (d.dVrdz + d.dVzdr) * (d.dVzdr + d.dVrdz));
 }
+
+// mu = T**0.666 (ModAssign.f90:20) as exp2(0.666 log2 T): within a few ulp of pow.
+template <typename R>
+AXJ_HD R mu_of_T(R T);
+template <>
+AXJ_HD double mu_of_T<double>(double T) { return exp2(0.666 * log2(T)); }
+template <>
+AXJ_HD float mu_of_T<float>(float T) { return exp2f(0.666f * log2f(T)); }
 
 // ---------------------------------------------------------------------------
 // Characteristic algebra of ModBC.f90:280-545 for primitive variables.
