@@ -32,12 +32,33 @@ def stale():
 
 
 def build(force=False, verbose=False):
+    """Compile every source to an object in parallel (they share no device symbols),
+    then link the shared library with the static CUDA runtime."""
     if not force and not stale():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    comp = [f for f in NVCC_FLAGS if f not in ("-shared", "-cudart", "static")]
+    jobs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        jobs.append((obj, [nvcc()] + comp + ["-c", "-o", obj, os.path.join(CSRC, src)]))
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True, cwd=CSRC)
+        for _, cmd in jobs:
+            print(" ".join(cmd))
+    with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        procs = list(ex.map(lambda c: subprocess.run(c, cwd=CSRC, capture_output=True, text=True),
+                            [cmd for _, cmd in jobs]))
+    for (obj, cmd), pr in zip(jobs, procs):
+        if pr.returncode != 0:
+            sys.stderr.write(pr.stdout + pr.stderr)
+            raise subprocess.CalledProcessError(pr.returncode, cmd)
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "static", "-o", OUT]
+    link += [obj for obj, _ in jobs]
+    if verbose:
+        print(" ".join(link))
+    subprocess.run(link, check=True, cwd=CSRC)
     return OUT
 
 

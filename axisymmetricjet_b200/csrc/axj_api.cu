@@ -47,6 +47,8 @@ struct axj_handle {
   bool mixed = false;
   // shock-capturing buffers
   double *Q = nullptr, *Qz = nullptr, *star = nullptr;
+  double* coef = nullptr;            // mu_eff, beta, kappa_eff of the stage input (fused z/r filter)
+  unsigned char* rcode = nullptr;    // r stencil code per point (9 = blanked)
   int2 *stiles_int = nullptr, *stiles_gen = nullptr;  // sensor tile classes
   int nstiles_int = 0, nstiles_gen = 0;
   uint32_t* desc = nullptr;
@@ -101,6 +103,10 @@ struct axj_handle {
   CUtensorMap map_sens[5][2];  // sensor V boxes of the stage buffers x {interior, general}
   CUtensorMap map_sensT[5][2]; // sensor temperature boxes
   CUtensorMap map_rho[5];      // density tile boxes
+  // fused z/r filter: Q blocks, z and r code blocks, temperature blocks of the stage
+  // buffers; the coefficient planes it writes, as boxes of the two tile classes
+  CUtensorMap map_zrQ, map_zrZc, map_zrRc, map_zrT[5];
+  CUtensorMap map_coef[2];
 };
 
 namespace {
@@ -342,6 +348,52 @@ int make_map(axj_handle* h, CUtensorMap* m, const void* base, int nplanes, int b
   return AXJ_OK;
 }
 
+// 2-D map over an (Nz, Nr) byte array with pitch P (zero outside).
+int make_map_u8(axj_handle* h, CUtensorMap* m, const void* base, int bw, int bh) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return fail(h, AXJ_ERR_NODEVICE, "cuTensorMapEncodeTiled is not available from the driver");
+  const cuuint64_t dims[2] = {(cuuint64_t)h->Nz, (cuuint64_t)h->Nr};
+  const cuuint64_t strides[1] = {(cuuint64_t)h->P};
+  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+  const cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(h, AXJ_ERR_CUDA, "cuTensorMapEncodeTiled (u8) failed (%d)", (int)r);
+  return AXJ_OK;
+}
+
+// The Q blocks of the fused z/r filter: 3 planes of doubles, box {ZRK_BZ, ZRK_NR, 3},
+// written to shared memory with the 128-byte swizzle.
+int make_map_zrq(axj_handle* h, CUtensorMap* m, const double* base) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return fail(h, AXJ_ERR_NODEVICE, "cuTensorMapEncodeTiled is not available from the driver");
+  const cuuint64_t dims[3] = {(cuuint64_t)h->Nz, (cuuint64_t)h->Nr, 3};
+  const cuuint64_t strides[2] = {(cuuint64_t)h->P * sizeof(double), (cuuint64_t)h->plane * sizeof(double)};
+  const cuuint32_t box[3] = {(cuuint32_t)ZRK_BZ, (cuuint32_t)ZRK_NR, 3};
+  const cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(h, AXJ_ERR_CUDA, "cuTensorMapEncodeTiled (Q blocks) failed (%d)", (int)r);
+  return AXJ_OK;
+}
+
+int build_zr_maps(axj_handle* h) {
+  const int nb = h->mixed ? NBUF : BUAF;
+  int rc = make_map_zrq(h, &h->map_zrQ, h->Q);
+  if (rc == AXJ_OK) rc = make_map_u8(h, &h->map_zrZc, h->zcode, ZRK_BZ, ZRK_NR);
+  if (rc == AXJ_OK) rc = make_map_u8(h, &h->map_zrRc, h->rcode, ZRK_BZ, ZRK_RB);
+  for (int b = 0; b < nb && rc == AXJ_OK; ++b)
+    rc = make_map(h, &h->map_zrT[b], buf_ptr(h, b), 5, ZRK_BZ, ZRK_RB, 1, buf_f32(b));
+  for (int cls = 0; cls < 2 && rc == AXJ_OK; ++cls) {
+    int hw, hh, qh, tw, th, qlh;
+    stage_boxes(cls == 1, h->mixed, &hw, &hh, &qh, &tw, &th, &qlh);
+    rc = make_map(h, &h->map_coef[cls], h->coef, 3, hw, qlh, 3);
+  }
+  return rc;
+}
+
 int build_maps(axj_handle* h) {
   const int nb = h->mixed ? NBUF : BUAF;
   for (int cls = 0; cls < 2; ++cls) {
@@ -377,20 +429,43 @@ int build_maps(axj_handle* h) {
   return make_map(h, &h->map_acc_tile, h->A, 5, tw, th, 5);
 }
 
-StageMaps stage_maps(axj_handle* h, int b, int cls, bool lrn) {
+// cm: CM_FILT (z-filtered quantities, r filter in the stage kernel), CM_LRN (learned
+// coefficient planes) or CM_PRE (mu_eff, beta, kappa_eff from the fused z/r filter).
+StageMaps stage_maps(axj_handle* h, int b, int cls, int cm) {
   StageMaps m;
   m.state = &h->map_state[b][cls];
-  m.star = lrn ? &h->map_starL[cls] : &h->map_star[cls];
+  m.star = cm == CM_LRN ? &h->map_starL[cls] : (cm == CM_PRE ? &h->map_coef[cls] : &h->map_star[cls]);
   m.u0 = &h->map_u0_tile;
   m.acc = &h->map_acc_tile;
   return m;
 }
 
-int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage, bool lrn = false) {
+int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage, int cm) {
   StageArgs a = stage_args(h, bin, bout, stage);
-  a.learned = lrn ? 1 : 0;
-  StageMaps mi = stage_maps(h, bin, 0, lrn), mg = stage_maps(h, bin, 1, lrn);
+  a.learned = cm;
+  StageMaps mi = stage_maps(h, bin, 0, cm), mg = stage_maps(h, bin, 1, cm);
   AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, mi, h->ntiles_gen, h->tiles_gen, mg, h->side, h->stream));
+  return AXJ_OK;
+}
+
+// The sensor chain of a stage input: the sensor tiles (quantities Q), then the fused
+// z filter / r filter / coefficient kernel, which leaves mu_eff, beta, kappa_eff in coef.
+int enqueue_sensor_chain(axj_handle* h, int bin) {
+  SensorArgs s = sensor_args(h, bin);
+  AXJ_CUDA(h, launch_sensor_tiles_only(s, h->side, h->stream));
+  ZrArgs z;
+  z.g = grid_of(h);
+  z.ramp = h->ramp;
+  z.coef = h->coef;
+  z.flags = h->flags;
+  // about three CTAs per SM: segments of a multiple of ZRK_BZ positions, at least 64
+  const int nrb = (h->Nr + ZRK_RB - 1) / ZRK_RB;
+  const int nseg = std::max(1, (3 * 148) / nrb);
+  const int seg = (int)((h->Nz + nseg - 1) / nseg);
+  z.seg = std::max(64, (seg + ZRK_BZ - 1) / ZRK_BZ * ZRK_BZ);
+  z.c = h->c;
+  ZrMaps m{&h->map_zrQ, &h->map_zrZc, &h->map_zrRc, &h->map_zrT[bin]};
+  AXJ_CUDA(h, launch_zr(z, m, h->mixed, buf_f32(bin), h->stream));
   return AXJ_OK;
 }
 
@@ -398,10 +473,11 @@ int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage, bool lrn =
 // stage kernel over both tile classes.
 int enqueue_stage(axj_handle* h, int bin, int bout, int stage) {
   if (h->c.shock_capturing) {
-    SensorArgs s = sensor_args(h, bin);
-    AXJ_CUDA(h, launch_sensor(s, false, h->side, h->stream));
+    int rc = enqueue_sensor_chain(h, bin);
+    if (rc != AXJ_OK) return rc;
+    return launch_stage_kernels(h, bin, bout, stage, CM_PRE);
   }
-  return launch_stage_kernels(h, bin, bout, stage);
+  return launch_stage_kernels(h, bin, bout, stage, CM_FILT);
 }
 
 FeatArgs feat_args(axj_handle* h, int b) {
@@ -448,12 +524,12 @@ int enqueue_stage_learned(axj_handle* h, int bin, int bout, int stage, bool judg
       SensorArgs s = sensor_args(h, bin);
       AXJ_CUDA(h, launch_sensor(s, true, h->side, h->stream));
     }
-    return launch_stage_kernels(h, bin, bout, stage, true);
+    return launch_stage_kernels(h, bin, bout, stage, CM_LRN);
   }
   // the network runs once per step, on the first stage's input; its coefficients
   // serve the step's four stages, as the judge's plain values serve the steps between
   // judges
-  if (stage > 1) return launch_stage_kernels(h, bin, bout, stage, true);
+  if (stage > 1) return launch_stage_kernels(h, bin, bout, stage, CM_LRN);
   AXJ_CUDA(h, launch_features(feat_args(h, bin), h->stream));
   if (judge1) {
     SensorArgs s = sensor_args(h, bin);
@@ -471,7 +547,7 @@ int enqueue_stage_learned(axj_handle* h, int bin, int bout, int stage, bool judg
   } else {
     AXJ_CUDA(h, launch_mlp_infer(infer_args(h, 1), h->stream));
   }
-  return launch_stage_kernels(h, bin, bout, stage, true);
+  return launch_stage_kernels(h, bin, bout, stage, CM_LRN);
 }
 
 // Stage input/output buffers of RK4: U0 -> Ua -> Ub -> Ua -> U0 (FP32 Ua, Ub when mixed).
@@ -869,9 +945,11 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
       desc[(size_t)(j - 1) * h->P + (i - 1)] = make_desc(zr, rw, ibval[x] == 0.0, f);
     }
   if (faces.size() >= (1u << 20)) { delete h; return fail(nullptr, AXJ_ERR_BADPATCH, "too many face points"); }
-  std::vector<unsigned char> zcode(desc.size());
-  for (size_t x = 0; x < desc.size(); ++x)
+  std::vector<unsigned char> zcode(desc.size()), rcode(desc.size());
+  for (size_t x = 0; x < desc.size(); ++x) {
     zcode[x] = (unsigned char)(desc_blank(desc[x]) ? ROW_NONE : (uint32_t)desc_zrow(desc[x]));
+    rcode[x] = (unsigned char)(desc_blank(desc[x]) ? ROW_NONE : (uint32_t)desc_rrow(desc[x]));
+  }
 
   // ---- tile classes
   std::vector<int2> tint, tgen, sti, stg;
@@ -959,6 +1037,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   if (c.shock_capturing) {
     h->Q = dalloc<double>(h, 3 * pl, &rc);
     h->Qz = dalloc<double>(h, 3 * pl, &rc);
+    h->coef = dalloc<double>(h, 3 * pl, &rc);
+    h->rcode = dalloc<unsigned char>(h, pl, &rc);
   }
   h->desc = dalloc<uint32_t>(h, pl, &rc);
   h->zcode = dalloc<unsigned char>(h, pl, &rc);
@@ -999,6 +1079,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   };
   up(h->desc, desc.data(), desc.size() * sizeof(uint32_t));
   up(h->zcode, zcode.data(), zcode.size());
+  if (h->rcode) up(h->rcode, rcode.data(), rcode.size());
   up(h->faces, faces.data(), faces.size() * sizeof(int));
   up(h->dxidz, dxidz.data(), Nz * sizeof(double));
   up(h->ddxidxidz, ddxidxidz.data(), Nz * sizeof(double));
@@ -1026,6 +1107,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     if (e != cudaSuccess) rc = fail(h, AXJ_ERR_NODEVICE, "kernel set-up failed (no sm_100a device?): %s", cudaGetErrorString(e));
   }
   if (rc == AXJ_OK) rc = build_maps(h);
+  if (rc == AXJ_OK && c.shock_capturing) rc = build_zr_maps(h);
   if (rc == AXJ_OK) {
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) rc = fail(h, AXJ_ERR_CUDA, "set-up: %s", cudaGetErrorString(e));
@@ -1231,15 +1313,12 @@ int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launch
         });
         nl[1] += 2 + ((judge && st == 1) ? (h->nstiles_int > 0) + (h->nstiles_gen > 0) + 4 : 0);
       } else if (h->c.shock_capturing) {
-        rc = timed(1, [&]() -> int {
-          SensorArgs sa = sensor_args(h, bufs[st - 1]);
-          AXJ_CUDA(h, launch_sensor(sa, false, h->side, h->stream));
-          return AXJ_OK;
-        });
+        rc = timed(1, [&]() -> int { return enqueue_sensor_chain(h, bufs[st - 1]); });
         nl[1] += (h->nstiles_int > 0) + (h->nstiles_gen > 0) + 1;
       }
       if (rc != AXJ_OK) break;
-      rc = timed(2, [&]() -> int { return launch_stage_kernels(h, bufs[st - 1], bufs[st], st, lrn); });
+      const int cm = lrn ? CM_LRN : (h->c.shock_capturing ? CM_PRE : CM_FILT);
+      rc = timed(2, [&]() -> int { return launch_stage_kernels(h, bufs[st - 1], bufs[st], st, cm); });
       nl[2] += stage_launches;
     }
     if (judge) {

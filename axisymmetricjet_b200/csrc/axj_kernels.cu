@@ -152,9 +152,8 @@ __host__ __device__ constexpr int hz_t(int h, int esize) { return (h + 16 / esiz
 
 // HZ follows the arithmetic type: the mixed path rounds to 4 elements in every stage
 // (valid for its double stage-1 input too), so one coefficient-box map serves all stages.
-// LRN: the coefficient box holds the final mu*, beta*, kappa* planes (learned sensor),
-// so it has the state box's halo and no filter reach.
-template <int H, typename SIN, typename R, bool LRN = false>
+// CM, the content of the coefficient box (CM_FILT, CM_LRN, CM_PRE: axj_kernels.cuh).
+template <int H, typename SIN, typename R, int CM = CM_FILT>
 struct StageSmem {
   static constexpr int HZ = hz_t(H, (int)sizeof(R));
   static constexpr int RZ = TZ + 2 * HZ;
@@ -163,7 +162,7 @@ struct StageSmem {
   static constexpr int NTP = TZ * TR;
   // r reach of the truncated-Gaussian filter rows: 4 for the centred row, 10 for the
   // 11-point boundary rows (ModTGfilter.f90:31-44)
-  static constexpr int HT = LRN ? 0 : ((H == H_INT) ? 4 : 10);
+  static constexpr int HT = CM != CM_FILT ? 0 : ((H == H_INT) ? 4 : 10);
   static constexpr int RQ = RR + 2 * HT;  // rows of the z-filtered coefficient box
   // byte offsets: state box [5][RR][RZ] of the stage-input type; coefficient box
   // [3][RQ][RZ] (doubles) holding the z-filtered quantities on arrival and mu_eff,
@@ -191,11 +190,11 @@ struct StageSmem {
 // row) evaluate the pointwise terms, face penalties and sponges in double.
 // One tile (i0, j0) of the fused stage. Returns false if a bounded wait gave up (the
 // flag is set; the caller stops).
-template <int H, bool GEN, typename SIN, typename R, bool LRN>
+template <int H, bool GEN, typename SIN, typename R, int CM>
 __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, const CUtensorMap* mState,
                                            const CUtensorMap* mQ, const CUtensorMap* mU0, const CUtensorMap* mAcc,
                                            unsigned char* smem_raw, uint64_t* bar) {
-  using SM = StageSmem<H, SIN, R, LRN>;
+  using SM = StageSmem<H, SIN, R, CM>;
   using RP = typename std::conditional<GEN, double, R>::type;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT, NTP = SM::NTP, HT = SM::HT, RQ = SM::RQ;
   SIN* sU = reinterpret_cast<SIN*>(smem_raw + SM::oU);            // [5][RR][RZ]
@@ -248,14 +247,15 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
     if (tid == 0) atomicOr(a.flags, 4);
     return false;
   }
-  // mu = T**0.666 (AssignValues) on the cross of the region. With shock capturing the
+  // mu = T**0.666 (AssignValues) on the cross of the region (CM_PRE: the coefficient box
+  // already holds mu_eff, beta and kappa_eff). With shock capturing the
   // coefficient box holds the z-filtered quantities; the r filter PerformTGfilter(q, 2,
   // star) (ModShockCapturing.f90:65,71,77), the C*Re(*Pr) scaling and the z ramp
   // (:66-92) give mu*, beta*, kappa*, and mu_eff = mu + mu*, kappa_eff = mu + kappa*
   // (UpdateTransportCoeffs :248-251). The results overwrite the box only after every
   // thread has read its filter windows. Zero-filled points outside the block give
   // mu = 0, as the never-written halo does; blanked points keep mu* = 0.
-  {
+  if (CM != CM_PRE) {
     double vmu[SM::NPER], vbe[SM::NPER], vka[SM::NPER];
 #pragma unroll
     for (int k = 0; k < SM::NPER; ++k) {
@@ -277,7 +277,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
           if (!(i >= 0 && i < Nz && j >= 0 && j < Nr)) rw = (int)ROW_NONE;
         }
         double f[3] = {0.0, 0.0, 0.0};
-        if (LRN) {
+        if (CM == CM_LRN) {
           // final coefficients (ramp applied), zero at blanked points as the filter gives
           if (rw < 9) {
 #pragma unroll
@@ -424,9 +424,14 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
     {
       // lambda = beta - 2/3 mu with beta = 0.6 mu (+ betastar), ModAssign.f90:22-23,
       // ModShockCapturing.f90:248-251
-      const double mu0 = sMu0[r * TZ + c];
-      double beta = (3.0 / 5.0) * mu0;
-      if (sc) beta = beta + sBe[sidx];
+      double beta;
+      if (CM == CM_PRE) {
+        beta = sBe[sidx];
+      } else {
+        const double mu0 = sMu0[r * TZ + c];
+        beta = (3.0 / 5.0) * mu0;
+        if (sc) beta = beta + sBe[sidx];
+      }
       q.lambda = RP(beta - (2.0 / 3.0) * double(*pMu));
     }
     const DerivT<RP> d = convert<RP>(dr);
@@ -520,7 +525,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
 
 
 
-template <int H, bool GEN, typename SIN, typename R, bool LRN>
+template <int H, bool GEN, typename SIN, typename R, int CM>
 __global__ void __launch_bounds__(STAGE_THREADS)
     stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
                  const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
@@ -528,13 +533,13 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
   const int2 t0 = tiles[blockIdx.x];
-  stage_body<H, GEN, SIN, R, LRN>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, smem_raw, bar);
+  stage_body<H, GEN, SIN, R, CM>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, smem_raw, bar);
 }
 
 // Batched form: a persistent grid-stride loop over the tiles (i0, j0, instance) of many
 // solver instances; each instance's arguments and tensor maps come from device tables
 // (the arguments are staged in shared memory per tile).
-template <int H, bool GEN, typename SIN, typename R, bool LRN>
+template <int H, bool GEN, typename SIN, typename R, int CM>
 __global__ void __launch_bounds__(STAGE_THREADS)
     stage_kernel_batch(const StageArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
                        const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
@@ -548,7 +553,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + tt.z)[k];
     __syncthreads();
     const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
-    if (!stage_body<H, GEN, SIN, R, LRN>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, m + kmaps.w, smem_raw,
+    if (!stage_body<H, GEN, SIN, R, CM>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, m + kmaps.w, smem_raw,
                                          bar))
       return;
   }
@@ -558,12 +563,16 @@ template <int H, bool GEN, typename SIN, typename R>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* tiles, const StageMaps& m,
                                   cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
-  if (a.learned) {
-    const size_t sm = StageSmem<H, SIN, R, true>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, true><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+  if (a.learned == CM_LRN) {
+    const size_t sm = StageSmem<H, SIN, R, CM_LRN>::bytes(GEN);
+    stage_kernel<H, GEN, SIN, R, CM_LRN><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+  } else if (a.learned == CM_PRE) {
+    const size_t sm = StageSmem<H, SIN, R, CM_PRE>::bytes(GEN);
+    stage_kernel<H, GEN, SIN, R, CM_PRE><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
   } else {
-    const size_t sm = StageSmem<H, SIN, R, false>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, false><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+    const size_t sm = StageSmem<H, SIN, R, CM_FILT>::bytes(GEN);
+    stage_kernel<H, GEN, SIN, R, CM_FILT>
+        <<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
   }
   return cudaGetLastError();
 }
@@ -616,7 +625,8 @@ void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* 
   }
   *halo_h = gen ? StageSmem<H_GEN, double, double>::RR : StageSmem<H_INT, double, double>::RR;
   *q_h = gen ? StageSmem<H_GEN, double, double>::RQ : StageSmem<H_INT, double, double>::RQ;
-  if (qlrn_h) *qlrn_h = gen ? StageSmem<H_GEN, double, double, true>::RQ : StageSmem<H_INT, double, double, true>::RQ;
+  if (qlrn_h)
+    *qlrn_h = gen ? StageSmem<H_GEN, double, double, CM_LRN>::RQ : StageSmem<H_INT, double, double, CM_LRN>::RQ;
   *tile_w = TZ;
   *tile_h = TR;
 }
@@ -1091,34 +1101,26 @@ cudaError_t launch_sensor(const SensorArgs& a, bool rfilter, const SideStream& s
 // Row-staged version of the same recurrence: one CTA per (row, field). The row of
 // unfiltered values and its z row codes are bulk-copied into shared memory with ZR_PADL
 // zeros (row code 4) on the left and ZR_PADR on the right, the never-written halo of
-// the reference; each thread owns a chunk of ZR_L points (odd: lanes read shared
-// memory without bank conflicts) and runs ZR_STEPS = ZR_W + ZR_L steps of the
-// recurrence, storing the last ZR_L. Left of a chunk's window it starts from
-// unfiltered values; for the first chunks that window begins inside the zero pad, so
-// they are exact. Chunks whose window holds only centred rows take an unrolled path
-// with the last 10 filtered values in a statically renamed register ring.
+// the reference. Each chunk of ZR_L points runs ZR_STEPS = ZR_W + ZR_L steps of the
+// recurrence; left of its window it starts from unfiltered values (the recurrence
+// forgets them: see ZR_W). Two kinds of chunk:
+//  * centred chunks (every row code in the window is 4, window inside the row): a
+//    fully unrolled loop with the last 10 filtered values in a statically renamed
+//    register ring and the ZR_L outputs in registers, which go back through shared
+//    memory and leave as coalesced row stores;
+//  * general chunks (closure rows, blanked points, or a window that starts left of the
+//    row, which then starts exactly at i = 0 from the zero halo): a rolled loop with a
+//    shifted register ring; centred points use the same arithmetic as above, the others
+//    the padded 21-tap form of their row (left to right, as DOT_PRODUCT sums). They
+//    store their outputs directly.
+// Chunks are reordered so the general ones share warps (thread t runs chunk order[t]).
 constexpr int ZR_L = 31;
 constexpr int ZR_W = 49;
 constexpr int ZR_STEPS = ZR_L + ZR_W;  // 80 = 8 x 10
 constexpr int ZR_PADL = 64;            // >= ZR_W + 10, a multiple of 16 doubles
-constexpr int ZR_PADR = 48;            // >= ZR_L + 4 - 1: the unrolled path reads up to i+4 past the row
-constexpr int ZR_MAXNZ = 10240;  // the staged row, its output, codes and rings fit in 227 KB
-
-// One output of the recurrence for TG row ROW at point i (xs indexed with the pad).
-// p[k] = filtered value at i-k, xs = unfiltered row.
-template <int ROW>
-__device__ __forceinline__ double zr_apply(const double (&p)[11], const double* __restrict__ xs, int i) {
-  constexpr int W0 = ROW < 4 ? -ROW : (ROW == 4 ? -4 : -2 - ROW);
-  constexpr int N = ROW == 4 ? 9 : 11;
-  double s = 0.0;
-#pragma unroll
-  for (int m = 0; m < N; ++m) {
-    const int o = W0 + m;
-    const double v = (o < 0) ? p[o < 0 ? -o : 0] : xs[i + o];
-    s = (m == 0) ? cTG[ROW][0] * v : s + cTG[ROW][m] * v;
-  }
-  return s;
-}
+constexpr int ZR_PADR = 48;            // >= ZR_L + 10 - 1: windows read up to i+10 past the row
+constexpr int ZR_MAXNZ = 10240;  // the staged row and its codes fit in shared memory
+constexpr int ZR_MAXCHUNK = (ZR_MAXNZ + ZR_L - 1) / ZR_L;
 
 // Bulk (non-tensor) global -> shared copy completing on an mbarrier; both addresses
 // 16-byte aligned, size a multiple of 16.
@@ -1132,16 +1134,30 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __host__ __device__ constexpr int zr_pad(int nz) { return (nz + 15) & ~15; }
 __host__ __device__ constexpr int zr_xlen(int nz) { return ZR_PADL + zr_pad(nz) + ZR_PADR; }
 
+// Shared-memory layout of one row: unfiltered row (doubles, padded) | the 21-tap padded
+// TG rows [10][21] (doubles; row 9 = identity) | row codes (bytes, padded) | chunk order
+// (int16) | chunk flags (bytes).
+__host__ __device__ constexpr size_t zr_off_w(int nz) { return sizeof(double) * (size_t)zr_xlen(nz); }
+__host__ __device__ constexpr size_t zr_off_codes(int nz) { return zr_off_w(nz) + sizeof(double) * 10 * 21; }
+__host__ __device__ constexpr size_t zr_off_order(int nz, long long P) {
+  return (zr_off_codes(nz) + (size_t)(ZR_PADL + P + ZR_PADR) + 1) & ~(size_t)1;
+}
+__host__ __device__ constexpr size_t zr_off_flags(int nz, long long P) {
+  return zr_off_order(nz, P) + sizeof(short) * (size_t)ZR_MAXCHUNK;
+}
+
+// Requires blockDim.x >= the number of chunks, (Nz + ZR_L - 1) / ZR_L, and a multiple of 32.
 __device__ __forceinline__ void zrows_body(const Grid& g, const unsigned char* __restrict__ zcode,
                                            const double* __restrict__ q, double* __restrict__ out, int* flags, int j,
                                            int f, unsigned char* zr_smem, uint64_t& bar) {
   const int Nz = g.Nz, P = (int)g.P;
   const int nchunk = (Nz + ZR_L - 1) / ZR_L;
-  double* xs = reinterpret_cast<double*>(zr_smem);       // [ZR_PADL + Nz + pad]
-  unsigned char* rs = reinterpret_cast<unsigned char*>(xs + zr_xlen(Nz));  // [ZR_PADL + P + ZR_PADR]
-  unsigned char* gen = rs + ZR_PADL + P + ZR_PADR;       // [nchunk]: window holds a non-centred row
-  double* ring_s = reinterpret_cast<double*>(                                // [10][blockDim]
-      zr_smem + ((sizeof(double) * (size_t)zr_xlen(Nz) + ZR_PADL + P + ZR_PADR + nchunk + 15) & ~(size_t)15));
+  double* xs = reinterpret_cast<double*>(zr_smem);                           // [zr_xlen(Nz)]
+  double* wt = reinterpret_cast<double*>(zr_smem + zr_off_w(Nz));           // [10][21]
+  unsigned char* rs = zr_smem + zr_off_codes(Nz);                            // [ZR_PADL + P + ZR_PADR]
+  short* order = reinterpret_cast<short*>(zr_smem + zr_off_order(Nz, P));   // [nchunk]
+  unsigned char* genf = zr_smem + zr_off_flags(Nz, P);                       // [nchunk]
+  __shared__ int warp_gen[32];
   const double* x = q + (long long)f * g.plane + (long long)j * g.P;
   double* y = out + (long long)f * g.plane + (long long)j * g.P;
   // the row of Q and its z stencil codes arrive by two bulk copies
@@ -1157,14 +1173,25 @@ __device__ __forceinline__ void zrows_body(const Grid& g, const unsigned char* _
     bulk_g2s(xs + ZR_PADL, x, xbytes, &bar);
     bulk_g2s(rs + ZR_PADL, zcode + (long long)j * g.P, rbytes, &bar);
   }
-  // pads (disjoint from the bulk destinations)
+  // pads (disjoint from the bulk destinations) and the padded TG rows: row r's taps
+  // sit at offsets tg_w0(r) .. tg_w0(r) + tg_len(r) - 1 of [-10, 10]; row 9 copies x(i)
   for (int k = threadIdx.x; k < ZR_PADL; k += blockDim.x) {
     xs[k] = 0.0;
     rs[k] = 4;
   }
   for (int k = ZR_PADL + 2 * (Nz / 2) + threadIdx.x; k < zr_xlen(Nz); k += blockDim.x) xs[k] = 0.0;
   for (int k = threadIdx.x; k < ZR_PADR; k += blockDim.x) rs[ZR_PADL + P + k] = 4;
-  for (int k = threadIdx.x; k < nchunk; k += blockDim.x) gen[k] = 0;
+  for (int k = threadIdx.x; k < 10 * 21; k += blockDim.x) {
+    const int r = k / 21, o = k - r * 21 - 10;
+    double w = 0.0;
+    if (r < 9) {
+      const int m = o - tg_w0(r);
+      if (m >= 0 && m < tg_len(r)) w = cTG[r][m];
+    } else {
+      w = (o == 0) ? 1.0 : 0.0;
+    }
+    wt[k] = w;
+  }
   if (!__syncthreads_and(mbar_wait_bounded(&bar, 0))) {
     if (threadIdx.x == 0) atomicOr(flags, 4);
     return;
@@ -1174,83 +1201,97 @@ __device__ __forceinline__ void zrows_body(const Grid& g, const unsigned char* _
   // are never stored and only feed later, also unstored, positions)
   for (int k = Nz + threadIdx.x; k < P; k += blockDim.x) rs[ZR_PADL + k] = 4;
   __syncthreads();
-  // mark chunks whose window [c*L - W, c*L + L) contains a non-centred row
-  for (int i = threadIdx.x; i < Nz; i += blockDim.x) {
-    if (rs[ZR_PADL + i] != 4) {
-      const int c0 = max(0, (i - ZR_L + 1 + ZR_L - 1) / ZR_L), c1 = min(nchunk - 1, (i + ZR_W) / ZR_L);
-      for (int c = c0; c <= c1; ++c) gen[c] = 1;
-    }
-  }
-  __syncthreads();
   const double* X = xs + ZR_PADL;  // X[i], i in [-ZR_PADL, Nz + pad)
   const unsigned char* R = rs + ZR_PADL;
+  // classify the chunks, then order them: general chunks first (an exclusive scan over
+  // the block of the general flags)
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  bool g_me = false;
+  if (t < nchunk) {
+    const int is = t * ZR_L - ZR_W;
+    g_me = is < 0;
+    for (int k = max(is, 0); k < min(is + ZR_STEPS, Nz) && !g_me; ++k) g_me = R[k] != 4;
+    genf[t] = g_me ? 1 : 0;
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, g_me);
+  if (lane == 0) warp_gen[wid] = __popc(bal);
+  __syncthreads();
+  int gbefore = 0, ngen = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    gbefore += (w < wid) ? warp_gen[w] : 0;
+    ngen += warp_gen[w];
+  }
+  if (t < nchunk) {
+    const int grank = gbefore + __popc(bal & ((1u << lane) - 1u));
+    order[g_me ? grank : ngen + (t - grank)] = (short)t;
+  }
+  __syncthreads();
+
   const double t0 = cTG[4][0], t1 = cTG[4][1], t2 = cTG[4][2], t3 = cTG[4][3], t4 = cTG[4][4];
   const double t5 = cTG[4][5], t6 = cTG[4][6], t7 = cTG[4][7], t8 = cTG[4][8];
-  for (int c = threadIdx.x; c < nchunk; c += blockDim.x) {
-    const int ib = c * ZR_L, is = ib - ZR_W;
-    if (!gen[c]) {
-      double ring[10];
-#pragma unroll
-      for (int m = 1; m <= 10; ++m) ring[10 - m] = X[is - m];
-#pragma unroll
-      for (int s = 0; s < ZR_STEPS; ++s) {
-        const int i = is + s;
-        const double* xp = X + i;
-        // the feed-forward terms and the older feedback terms first, the newest
-        // filtered value last: one FMA of latency per step on the recurrence (the
-        // reference sums left to right; the two orders differ by rounding only)
+  const int c = (t < nchunk) ? order[t] : 0;
+  const int ib = c * ZR_L, is = ib - ZR_W;
+  double outv[ZR_L];
+  if (t < ngen) {
+    // general chunk: h1..h10 = filtered values at i-1..i-10
+    const int i0c = max(is, 0);
+    const int ie = min(Nz, ib + ZR_L);
+    double h1 = X[i0c - 1], h2 = X[i0c - 2], h3 = X[i0c - 3], h4 = X[i0c - 4], h5 = X[i0c - 5];
+    double h6 = X[i0c - 6], h7 = X[i0c - 7], h8 = X[i0c - 8], h9 = X[i0c - 9], h10 = X[i0c - 10];
+    for (int i = i0c; i < ie; ++i) {
+      const double* xp = X + i;
+      const int row = R[i];
+      double v;
+      if (row == 4) {
         const double ff = t4 * xp[0] + t5 * xp[1] + t6 * xp[2] + t7 * xp[3] + t8 * xp[4];
-        const double fb = t0 * ring[(s + 6) % 10] + t1 * ring[(s + 7) % 10] + t2 * ring[(s + 8) % 10];
-        const double v = (ff + fb) + t3 * ring[(s + 9) % 10];
-        ring[s % 10] = v;
-        if (s >= ZR_W && i < Nz) y[i] = v;
+        const double fb = t0 * h4 + t1 * h3 + t2 * h2;
+        v = (ff + fb) + t3 * h1;
+      } else {
+        const double* w = wt + (row < 9 ? row : 9) * 21;  // w[o + 10], o = -10..10
+        double sacc = w[0] * h10;
+        sacc = sacc + w[1] * h9;
+        sacc = sacc + w[2] * h8;
+        sacc = sacc + w[3] * h7;
+        sacc = sacc + w[4] * h6;
+        sacc = sacc + w[5] * h5;
+        sacc = sacc + w[6] * h4;
+        sacc = sacc + w[7] * h3;
+        sacc = sacc + w[8] * h2;
+        sacc = sacc + w[9] * h1;
+#pragma unroll
+        for (int o = 0; o <= 10; ++o) sacc = sacc + w[10 + o] * xp[o];
+        v = sacc;
       }
-    } else {
-      // general rows: the last 10 filtered values live in a per-thread ring in shared
-      // memory (slot = position mod 10, interleaved across threads). A window that
-      // begins in the left pad starts exactly at i = 0 from the zero halo.
-      const int bd = blockDim.x;
-      double* rg = ring_s + threadIdx.x;
-      const int i0c = max(is, 0);
-      const int ie = min(Nz, ib + ZR_L);
-      for (int k = 1; k <= 10; ++k) rg[((i0c - k + 1000) % 10) * bd] = X[i0c - k];
-      int slot = (i0c + 1000) % 10;
-      for (int i = i0c; i < ie; ++i) {
-        const int row = R[i];
-        double v;
-        if (row == 4) {
-          int s4 = slot - 4, s3 = slot - 3, s2 = slot - 2, s1 = slot - 1;
-          s4 += s4 < 0 ? 10 : 0;
-          s3 += s3 < 0 ? 10 : 0;
-          s2 += s2 < 0 ? 10 : 0;
-          s1 += s1 < 0 ? 10 : 0;
-          v = t0 * rg[s4 * bd] + t1 * rg[s3 * bd] + t2 * rg[s2 * bd] + t3 * rg[s1 * bd] + t4 * X[i] + t5 * X[i + 1] +
-              t6 * X[i + 2] + t7 * X[i + 3] + t8 * X[i + 4];
-        } else if (row < 9) {
-          const int w0 = tg_w0(row), n = tg_len(row);
-          double s = 0.0;
-          for (int m = 0; m < n; ++m) {
-            const int o = w0 + m;
-            double val;
-            if (o < 0) {
-              int sl = slot + o;
-              sl += sl < 0 ? 10 : 0;
-              val = rg[sl * bd];
-            } else {
-              val = X[i + o];
-            }
-            s = (m == 0) ? cTG[row][0] * val : s + cTG[row][m] * val;
-          }
-          v = s;
-        } else {
-          v = X[i];  // blanked / no row: left unchanged in place
-        }
-        rg[slot * bd] = v;
-        slot = (slot == 9) ? 0 : slot + 1;
-        if (i >= ib) y[i] = v;
-      }
+      h10 = h9; h9 = h8; h8 = h7; h7 = h6; h6 = h5; h5 = h4; h4 = h3; h3 = h2; h2 = h1; h1 = v;
+      if (i >= ib) y[i] = v;
+    }
+  } else if (t < nchunk) {
+    double ring[10];
+#pragma unroll
+    for (int m = 1; m <= 10; ++m) ring[10 - m] = X[is - m];
+#pragma unroll
+    for (int s = 0; s < ZR_STEPS; ++s) {
+      const double* xp = X + is + s;
+      // the feed-forward terms and the older feedback terms first, the newest
+      // filtered value last: one FMA of latency per step on the recurrence (the
+      // reference sums left to right; the two orders differ by rounding only)
+      const double ff = t4 * xp[0] + t5 * xp[1] + t6 * xp[2] + t7 * xp[3] + t8 * xp[4];
+      const double fb = t0 * ring[(s + 6) % 10] + t1 * ring[(s + 7) % 10] + t2 * ring[(s + 8) % 10];
+      const double v = (ff + fb) + t3 * ring[(s + 9) % 10];
+      ring[s % 10] = v;
+      if (s >= ZR_W) outv[s - ZR_W] = v;
     }
   }
+  // every thread has finished reading the unfiltered row: the centred chunks' outputs
+  // replace it, and leave with the rest of the row (general chunks stored theirs)
+  __syncthreads();
+  if (t >= ngen && t < nchunk) {
+#pragma unroll
+    for (int k = 0; k < ZR_L; ++k) xs[ZR_PADL + ib + k] = outv[k];  // ib + k < zr_xlen(Nz) - ZR_PADL
+  }
+  __syncthreads();
+  for (int k = t; k < Nz; k += blockDim.x)
+    if (!genf[k / ZR_L]) y[k] = X[k];
 }
 
 __global__ void tgfilter_z_rows_kernel(const Grid g, const unsigned char* __restrict__ zcode,
@@ -1271,14 +1312,275 @@ __global__ void tgfilter_z_rows_kernel_batch(const SensorArgs* __restrict__ argv
   zrows_body(g, a.zcode, a.Q, a.Qz, a.flags, r.y, blockIdx.y, zr_smem, bar);
 }
 
+// ---------------------------------------------------------------------------
+// Fused z filter, r filter and transport coefficients (ModShockCapturing.f90:63-92,
+// :248-251; ModAssign.f90:20-23): from the unfiltered sensor quantities Q to
+// mu_eff = mu + mu*, beta = 0.6 mu + beta* and kappa_eff = mu + kappa* at every point.
+//
+// A CTA owns a segment of z positions (a multiple of ZRK_BZ) and ZRK_RB rows. It runs the
+// in-place z recurrence of PerformTGfilter(q, 1, q) for the three quantities on its rows
+// and ZRK_HR rows either side (the reach of the 11-point TG boundary rows of the r
+// filter): one thread per (quantity, row), marching along z in blocks of ZRK_BZ
+// positions. Segments start ZRK_WARM positions early from a zero history (the
+// recurrence forgets its start: the dominant root of its feedback part is about 0.47, so
+// 0.47**64 < 1e-20); the first segment starts exactly at i = 0 from the reference's zero
+// halo. The z-filtered block goes to shared memory, where the r filter
+// PerformTGfilter(q, 2, star) of the CTA's rows is applied with the point's r row, then
+// the C*Re(*Pr) scaling, the z ramp and mu = T**0.666 of the stage input.
+// Blocks of Q arrive by TMA (128-byte swizzle: a thread reads its row's 16 values as 8
+// conflict-free 16-byte loads) into two slots: block k supplies the up to 10 values
+// right of block k-1 that the filter rows reach, and once both are in registers the
+// slot of block k-1 takes block k+1, which lands while block k-1 is filtered.
+// ---------------------------------------------------------------------------
+constexpr int ZRK_LANES = 3 * ZRK_NR;  // 156 recurrences per CTA
+constexpr int ZRK_WARM = 64;           // warm-up positions (4 blocks)
+constexpr int ZRK_QROW = ZRK_BZ * 8;   // bytes of one row of a Q block (128)
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Byte offset of 16-byte chunk c of row R in a block stored with the 128-byte swizzle
+// (chunk index XOR row mod 8); TMA writes the Q blocks this way, the kernel the Z blocks.
+__device__ __forceinline__ int zrk_chunk(int R, int c) { return R * ZRK_QROW + ((c ^ (R & 7)) << 4); }
+__device__ __forceinline__ int zrk_elem(int R, int p) { return zrk_chunk(R, p >> 1) + ((p & 1) << 3); }
+
+template <typename SIN>
+struct ZrSmem {
+  static constexpr size_t qbytes = (size_t)ZRK_LANES * ZRK_QROW;           // 19968
+  static constexpr size_t qslot = (qbytes + 1023) / 1024 * 1024;           // 20480
+  static constexpr size_t oQ = 0;                                            // [2] Q blocks (swizzled)
+  static constexpr size_t oZ = 2 * qslot;                                    // z-filtered block (swizzled)
+  static constexpr size_t oZc = oZ + qslot;                                  // [2][ZRK_NR][16] z row codes
+  static constexpr size_t zcbytes = (size_t)ZRK_NR * ZRK_BZ;
+  static constexpr size_t oT = oZc + 2 * 1024;                               // [2][ZRK_RB][16] T
+  static constexpr size_t tbytes = (size_t)ZRK_RB * ZRK_BZ * sizeof(SIN);
+  static constexpr size_t oRc = oT + 2 * ((tbytes + 127) / 128 * 128);       // [2][ZRK_RB][16] r row codes
+  static constexpr size_t rcbytes = (size_t)ZRK_RB * ZRK_BZ;
+  static constexpr size_t oW = oRc + 2 * 512;                                // [10][21] padded TG rows
+  static constexpr size_t bytes = oW + 10 * 21 * sizeof(double) + 1024;      // + alignment slack
+  static constexpr uint32_t tx = (uint32_t)(qbytes + zcbytes + tbytes + rcbytes);
+};
+
+template <typename SIN, typename R>
+__global__ void __launch_bounds__(ZRK_THREADS, 3)
+    zr_kernel(const ZrArgs a, const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mZc,
+              const __grid_constant__ CUtensorMap mRc, const __grid_constant__ CUtensorMap mT) {
+  using SM = ZrSmem<SIN>;
+  extern __shared__ __align__(128) unsigned char zrk_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  unsigned char* base = zrk_raw + ((1024u - (smem_u32(zrk_raw) & 1023u)) & 1023u);
+  double* wt = reinterpret_cast<double*>(base + SM::oW);
+  const int tid = threadIdx.x;
+  const int Nz = a.g.Nz, Nr = a.g.Nr;
+  const long long P = a.g.P, PL = a.g.plane;
+  const int zs = blockIdx.x * a.seg, ze = min(Nz, zs + a.seg);
+  const int j0 = blockIdx.y * ZRK_RB;
+  const int bs = max(0, zs - ZRK_WARM) / ZRK_BZ;  // first block filtered (zs is a multiple of ZRK_BZ)
+  const int be = (ze + ZRK_BZ - 1) / ZRK_BZ;       // blocks bs..be-1 are filtered, block be is loaded too
+  // padded TG rows: row r's taps at offsets tg_w0(r) .. tg_w0(r) + tg_len(r) - 1 of
+  // [-10, 10]; row 9 (blanked, or no filter row) keeps the value in place
+  for (int k = tid; k < 10 * 21; k += ZRK_THREADS) {
+    const int r = k / 21, o = k - r * 21 - 10;
+    double w = 0.0;
+    if (r < 9) {
+      const int m = o - tg_w0(r);
+      if (m >= 0 && m < tg_len(r)) w = cTG[r][m];
+    } else {
+      w = (o == 0) ? 1.0 : 0.0;
+    }
+    wt[k] = w;
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  // slot k & 1 receives Q and the z codes of block k, and T and the r codes of block
+  // k - 1 (the block the r filter handles in iteration k)
+  auto issue = [&](int k) {
+    const int sl = k & 1;
+    unsigned char* q = base + SM::oQ + sl * SM::qslot;
+    mbar_expect_tx(&bar[sl], SM::tx);
+    tma_load_3d(q, &mQ, ZRK_BZ * k, j0 - ZRK_HR, 0, &bar[sl]);
+    tma_load_2d(base + SM::oZc + sl * 1024, &mZc, ZRK_BZ * k, j0 - ZRK_HR, &bar[sl]);
+    tma_load_3d(base + SM::oT + sl * ((SM::tbytes + 127) / 128 * 128), &mT, ZRK_BZ * (k - 1), j0, 4, &bar[sl]);
+    tma_load_2d(base + SM::oRc + sl * 512, &mRc, ZRK_BZ * (k - 1), j0, &bar[sl]);
+  };
+  if (tid == 0) issue(bs);
+
+  const bool lane_on = tid < ZRK_LANES;
+  const int fq = lane_on ? tid / ZRK_NR : 0;
+  const int rr = lane_on ? tid - fq * ZRK_NR : 0;
+  const int Rq = fq * ZRK_NR + rr;  // row of this recurrence in the Q / Z blocks
+  const int jr = j0 - ZRK_HR + rr;
+  const bool row_on = lane_on && jr >= 0 && jr < Nr;
+  const double t0 = cTG[4][0], t1 = cTG[4][1], t2 = cTG[4][2], t3 = cTG[4][3], t4 = cTG[4][4];
+  const double t5 = cTG[4][5], t6 = cTG[4][6], t7 = cTG[4][7], t8 = cTG[4][8];
+  double ring[16];  // filtered values, ring[p & 15] at position p
+#pragma unroll
+  for (int k = 0; k < 16; ++k) ring[k] = 0.0;
+  uint32_t par = 0;  // bit s: parity of the next wait on slot s
+  for (int k = bs; k <= be; ++k) {
+    const int sl = k & 1;
+    const bool ok = mbar_wait_bounded(&bar[sl], (par >> sl) & 1u);
+    par ^= 1u << sl;
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) atomicOr(a.flags, 4);
+      return;
+    }
+    const int m = k - 1;  // the block filtered in this iteration
+    unsigned char* zb = base + SM::oZ;
+    const bool work = k > bs && row_on;
+    double xv[26];  // Q at positions 16m .. 16m + 25
+    uint32_t cws[4];
+    if (work) {
+      const unsigned char* qm = base + SM::oQ + (sl ^ 1) * SM::qslot;
+      const unsigned char* qk = base + SM::oQ + sl * SM::qslot;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const double2 v = *reinterpret_cast<const double2*>(qm + zrk_chunk(Rq, c));
+        xv[2 * c] = v.x;
+        xv[2 * c + 1] = v.y;
+      }
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const double2 v = *reinterpret_cast<const double2*>(qk + zrk_chunk(Rq, c));
+        xv[16 + 2 * c] = v.x;
+        xv[16 + 2 * c + 1] = v.y;
+      }
+      const uint4 cw = *reinterpret_cast<const uint4*>(base + SM::oZc + (sl ^ 1) * 1024 + rr * ZRK_BZ);
+      cws[0] = cw.x;
+      cws[1] = cw.y;
+      cws[2] = cw.z;
+      cws[3] = cw.w;
+    }
+    // block k-1's slot is free (its T and r codes were used in iteration k-1): block k+1
+    __syncthreads();
+    if (tid == 0 && k + 1 <= be) {
+      // the slot's previous contents were read through the generic proxy
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(k + 1);
+    }
+    if (k > bs && lane_on) {
+      if (row_on) {
+#pragma unroll
+        for (int s2 = 0; s2 < 16; ++s2) {
+          const int p = ZRK_BZ * m + s2;
+          const int code = (int)((cws[s2 >> 2] >> (8 * (s2 & 3))) & 255u);
+          double v;
+          if (p >= Nz) {
+            v = 0.0;  // past the row: never stored, feeds only later positions past the row
+          } else if (code == 4) {
+            // feed-forward and older feedback terms first, the newest filtered value last:
+            // one FMA of latency per step (the reference sums left to right; the orders
+            // differ by rounding only)
+            const double ff = t4 * xv[s2] + t5 * xv[s2 + 1] + t6 * xv[s2 + 2] + t7 * xv[s2 + 3] + t8 * xv[s2 + 4];
+            const double fb = t0 * ring[(s2 + 12) & 15] + t1 * ring[(s2 + 13) & 15] + t2 * ring[(s2 + 14) & 15];
+            v = (ff + fb) + t3 * ring[(s2 + 15) & 15];
+          } else {
+            // closure rows and blanked points: the padded 21-tap row, left to right
+            const double* w = wt + (code < 9 ? code : 9) * 21;
+            double acc = w[0] * ring[(s2 + 6) & 15];
+#pragma unroll
+            for (int o = -9; o < 0; ++o) acc = acc + w[10 + o] * ring[(s2 + 16 + o) & 15];
+#pragma unroll
+            for (int o = 0; o <= 10; ++o) acc = acc + w[10 + o] * xv[s2 + o];
+            v = acc;
+          }
+          ring[s2] = v;
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          *reinterpret_cast<double2*>(zb + zrk_chunk(Rq, c)) = make_double2(ring[2 * c], ring[2 * c + 1]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) *reinterpret_cast<double2*>(zb + zrk_chunk(Rq, c)) = make_double2(0.0, 0.0);
+      }
+    }
+    __syncthreads();
+    if (k > bs && ZRK_BZ * m + ZRK_BZ > zs) {
+      // r filter, scaling and coefficients of block m on the CTA's rows
+      const SIN* tb = reinterpret_cast<const SIN*>(base + SM::oT + sl * ((SM::tbytes + 127) / 128 * 128));
+      const unsigned char* rcb = base + SM::oRc + sl * 512;
+      // the points of a thread are independent: unrolled so their T**0.666 and filter
+      // chains interleave
+#pragma unroll
+      for (int u = 0; u < (ZRK_RB * ZRK_BZ + ZRK_THREADS - 1) / ZRK_THREADS; ++u) {
+        const int qd = tid + u * ZRK_THREADS;
+        const int row = qd / ZRK_BZ, p = qd - row * ZRK_BZ;
+        const int j = j0 + row, i = ZRK_BZ * m + p;
+        if (qd >= ZRK_RB * ZRK_BZ || j >= Nr || i < zs || i >= ze) continue;
+        const double mu = double(mu_of_T<R>(R(tb[qd])));
+        const int rw = rcb[qd];
+        double fv[3] = {0.0, 0.0, 0.0};
+        if (rw == 4) {
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            const int R0 = f * ZRK_NR + row + ZRK_HR - 4;
+            double sacc = t0 * *reinterpret_cast<const double*>(zb + zrk_elem(R0, p));
+#pragma unroll
+            for (int mm = 1; mm < 9; ++mm)
+              sacc = sacc + cTG[4][mm] * *reinterpret_cast<const double*>(zb + zrk_elem(R0 + mm, p));
+            fv[f] = sacc;
+          }
+        } else if (rw < 9) {
+          const int w0 = tg_w0(rw), n = tg_len(rw);
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            const int R0 = f * ZRK_NR + row + ZRK_HR + w0;
+            double sacc = cTG[rw][0] * *reinterpret_cast<const double*>(zb + zrk_elem(R0, p));
+            for (int mm = 1; mm < n; ++mm)
+              sacc = sacc + cTG[rw][mm] * *reinterpret_cast<const double*>(zb + zrk_elem(R0 + mm, p));
+            fv[f] = sacc;
+          }
+        }
+        const double ramp = __ldg(a.ramp + i);
+        const long long o = (long long)j * P + i;
+        a.coef[o] = mu + a.c.C_mu_Re * fv[0] * ramp;
+        a.coef[PL + o] = (3.0 / 5.0) * mu + a.c.C_beta_Re * fv[1] * ramp;
+        a.coef[2 * PL + o] = mu + a.c.C_kappa_Re_Pr * fv[2] * ramp;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename SIN, typename R>
+static cudaError_t launch_zr_t(const ZrArgs& a, const ZrMaps& m, cudaStream_t s) {
+  const dim3 grid((a.g.Nz + a.seg - 1) / a.seg, (a.g.Nr + ZRK_RB - 1) / ZRK_RB);
+  zr_kernel<SIN, R><<<grid, ZRK_THREADS, ZrSmem<SIN>::bytes, s>>>(a, *m.q, *m.zc, *m.rc, *m.t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zr(const ZrArgs& a, const ZrMaps& m, bool mixed, bool in_f32, cudaStream_t s) {
+  if (!mixed) return launch_zr_t<double, double>(a, m, s);
+  if (!in_f32) return launch_zr_t<double, float>(a, m, s);
+  return launch_zr_t<float, float>(a, m, s);
+}
+
+cudaError_t launch_sensor_tiles_only(const SensorArgs& a, const SideStream& side, cudaStream_t s) {
+  cudaError_t e = fork(side, s);
+  if (e != cudaSuccess) return e;
+  if (!a.mixed) launch_sensor_tiles<double, double>(a, side, s);
+  else if (!a.in_f32) launch_sensor_tiles<double, float>(a, side, s);
+  else launch_sensor_tiles<float, float>(a, side, s);
+  e = join(side, s);
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
 static int zr_threads(int Nz) {
   const int nchunk = (Nz + ZR_L - 1) / ZR_L;
   return std::min(1024, (nchunk + 31) / 32 * 32);
 }
 static size_t zr_smem_bytes(int Nz, long long P, int bs) {
-  const int nchunk = (Nz + ZR_L - 1) / ZR_L;
-  const size_t head = sizeof(double) * (size_t)zr_xlen(Nz) + (size_t)(ZR_PADL + P + ZR_PADR) + nchunk;
-  return ((head + 15) & ~(size_t)15) + sizeof(double) * 10 * (size_t)bs;
+  (void)bs;
+  return (zr_off_flags(Nz, P) + ZR_MAXCHUNK + 15) & ~(size_t)15;
 }
 static size_t zr_smem_bytes(int Nz, long long P) { return zr_smem_bytes(Nz, P, zr_threads(Nz)); }
 
@@ -1379,11 +1681,15 @@ void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th) {
 
 template <int H, bool GEN, typename SIN, typename R>
 static cudaError_t stage_attr() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)StageSmem<H, SIN, R, false>::bytes(GEN));
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_FILT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)StageSmem<H, SIN, R, CM_FILT>::bytes(GEN));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)StageSmem<H, SIN, R, true>::bytes(GEN));
+  e = cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)StageSmem<H, SIN, R, CM_PRE>::bytes(GEN));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)StageSmem<H, SIN, R, CM_LRN>::bytes(GEN));
 }
 template <int HS, int HF, bool GEN, typename SIN, typename R>
 static cudaError_t sensor_attr() {
@@ -1392,12 +1698,12 @@ static cudaError_t sensor_attr() {
 }
 template <int H, bool GEN, typename SIN, typename R>
 static cudaError_t stage_batch_attr() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, false>,
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, CM_FILT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)StageSmem<H, SIN, R, false>::bytes(GEN));
+                                       (int)StageSmem<H, SIN, R, CM_FILT>::bytes(GEN));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)StageSmem<H, SIN, R, true>::bytes(GEN));
+  return cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, CM_LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)StageSmem<H, SIN, R, CM_LRN>::bytes(GEN));
 }
 template <int HS, int HF, bool GEN, typename SIN, typename R>
 static cudaError_t sensor_batch_attr() {
@@ -1428,6 +1734,15 @@ cudaError_t init_kernel_attributes() {
   e = cudaFuncSetAttribute(tgfilter_z_rows_kernel_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)zr_smem_bytes(ZR_MAXNZ, ZR_MAXNZ + 32, 1024));
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(zr_kernel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)ZrSmem<double>::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(zr_kernel<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ZrSmem<double>::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(zr_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ZrSmem<float>::bytes);
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(tgfilter_z_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)zr_smem_bytes(ZR_MAXNZ, ZR_MAXNZ + 32));
 }
@@ -1444,8 +1759,9 @@ static cudaError_t launch_stage_batch_t(const StageArgs* argv, const BatchTiles&
   if (t.ntiles <= 0) return cudaSuccess;
   const int cls = GEN ? 1 : 0;
   const int4 k = make_int4(bmap_state(kin, cls), bmap_star(cls, LRN), 14, 15);
-  const size_t sm = StageSmem<H, SIN, R, LRN>::bytes(GEN);
-  stage_kernel_batch<H, GEN, SIN, R, LRN><<<t.grid, STAGE_THREADS, sm, s>>>(argv, t.tiles, t.ntiles, mapv, NM_BATCH, k);
+  constexpr int CM = LRN ? CM_LRN : CM_FILT;
+  const size_t sm = StageSmem<H, SIN, R, CM>::bytes(GEN);
+  stage_kernel_batch<H, GEN, SIN, R, CM><<<t.grid, STAGE_THREADS, sm, s>>>(argv, t.tiles, t.ntiles, mapv, NM_BATCH, k);
   return cudaGetLastError();
 }
 

@@ -26,6 +26,14 @@ struct Grid {
   long long plane;   // P * Nr
 };
 
+// Content of the stage kernel's coefficient box (StageArgs::learned):
+//   CM_FILT: the z-filtered sensor quantities; the kernel applies the r filter, so the
+//            box reaches the filter's rows beyond the state box;
+//   CM_LRN:  the final mu*, beta*, kappa* planes (learned sensor), on the state box;
+//   CM_PRE:  mu_eff, beta (0.6 mu + beta*) and kappa_eff, formed by the fused z/r filter
+//            kernel, on the state box (the stage kernel evaluates no T**0.666).
+constexpr int CM_FILT = 0, CM_LRN = 1, CM_PRE = 2;
+
 // Arguments of the fused RK-stage kernel.
 struct StageArgs {
   Grid g;
@@ -60,7 +68,7 @@ struct StageArgs {
   int mixed;              // 1: FP32 stencils and interior pointwise terms
   int in_f32;             // 1: the stage input (maps) is FP32
   int out_f32;            // 1: stages 1-3 write Uout_f instead of Uout
-  int learned;            // 1: the coefficient maps hold final mu*, beta*, kappa* (learned sensor)
+  int learned;            // coefficient box content: CM_FILT, CM_LRN or CM_PRE
   Consts c;
 };
 
@@ -141,6 +149,36 @@ cudaError_t launch_harmonic_phase(const double* time, const double* dt, double o
 // rfilter: also run the r filter into a.star (the stage kernel applies it itself; the
 // unit entry point axj_sensor needs the coefficients as output).
 cudaError_t launch_sensor(const SensorArgs& a, bool rfilter, const SideStream& side, cudaStream_t s);
+
+// Sensor tile kernels only (the quantities Q), for the fused z/r filter path.
+cudaError_t launch_sensor_tiles_only(const SensorArgs& a, const SideStream& side, cudaStream_t s);
+
+// Fused z filter + r filter + transport coefficients (zr_kernel): from Q to the planes
+// mu_eff, beta = 0.6 mu + beta*, kappa_eff of the stage input. A CTA of ZRK_THREADS
+// threads owns seg z positions (a multiple of ZRK_BZ) and ZRK_RB rows.
+constexpr int ZRK_BZ = 16;                    // z positions per block (one 128-byte row of doubles)
+constexpr int ZRK_RB = 32;                    // rows per CTA
+constexpr int ZRK_HR = 10;                    // r reach of the TG boundary rows
+constexpr int ZRK_NR = ZRK_RB + 2 * ZRK_HR;   // rows of the z recurrence per CTA
+constexpr int ZRK_THREADS = 160;
+struct ZrArgs {
+  Grid g;
+  const double* ramp;  // (1+tanh(5(z-10)))/2 per i
+  double* coef;        // 3 planes: mu_eff, beta, kappa_eff
+  int* flags;          // bit 2: a bounded wait gave up
+  int seg;             // z positions per CTA (multiple of ZRK_BZ)
+  Consts c;
+};
+// TMA maps: q = Q (3 planes of doubles, box {ZRK_BZ, ZRK_NR, 3}, 128-byte swizzle);
+// zc / rc = z / r row codes (uint8, 9 = blanked; boxes {ZRK_BZ, ZRK_NR} / {ZRK_BZ, ZRK_RB});
+// t = the stage input's planes (box {ZRK_BZ, ZRK_RB, 1}, FP32 when in_f32).
+struct ZrMaps {
+  const CUtensorMap* q;
+  const CUtensorMap* zc;
+  const CUtensorMap* rc;
+  const CUtensorMap* t;
+};
+cudaError_t launch_zr(const ZrArgs& a, const ZrMaps& m, bool mixed, bool in_f32, cudaStream_t s);
 
 // Unit entry points (one operator on one field, host-facing).
 cudaError_t launch_deriv(const Grid& g, const uint32_t* desc, const double* var, const double* first,
