@@ -144,7 +144,7 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
+__host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
 
 // z halo of a box in elements, rounded up so the box's x coordinate starts on a
 // 16-byte boundary (TMA requirement): even for doubles, a multiple of 4 for floats.
@@ -167,16 +167,24 @@ struct StageSmem {
   // byte offsets: state box [5][RR][RZ] of the stage-input type; coefficient box
   // [3][RQ][RZ] (doubles) holding the z-filtered quantities on arrival and mu_eff,
   // beta*, kappa_eff (rows HT..HT+RR) after the r filter (without shock capturing plane
-  // 0 rows HT.. hold mu); plain mu on the tile [TR][TZ]; pv_old tile [5][TR][TZ];
-  // running-sum tile [5][TR][TZ]; dV/dz [2][RR][TZ] (stencil type); descriptors [RR][RZ]
+  // 0 rows HT.. hold mu); plain mu on the tile [TR][TZ]; interior tiles only: pv_old
+  // tile [5][TR][TZ] and running-sum tile [5][TR][TZ] (general tiles read them from
+  // global memory, which keeps two of their CTAs on an SM); dV/dz [2][RR][TZ] (stencil
+  // type); general tiles only: descriptors [RR][RZ]
   static constexpr size_t oU = 0;
   static constexpr size_t oQ = align128(oU + sizeof(SIN) * 5 * NPT);
   static constexpr size_t oMu0 = align128(oQ + sizeof(double) * 3 * RQ * RZ);
   static constexpr size_t oP0 = align128(oMu0 + sizeof(double) * NTP);
   static constexpr size_t oPA = align128(oP0 + sizeof(double) * 5 * NTP);
-  static constexpr size_t oDz = align128(oPA + sizeof(double) * 5 * NTP);
-  static constexpr size_t oDesc = align128(oDz + sizeof(double) * 2 * RR * TZ);
-  static constexpr size_t bytes(bool gen) { return align128(oDesc + (gen ? sizeof(uint32_t) * NPT : 0)); }
+  __host__ __device__ static constexpr size_t oDz(bool gen) {
+    return gen ? oP0 : align128(oPA + sizeof(double) * 5 * NTP);
+  }
+  __host__ __device__ static constexpr size_t oDesc(bool gen) {
+    return align128(oDz(gen) + sizeof(double) * 2 * RR * TZ);
+  }
+  __host__ __device__ static constexpr size_t bytes(bool gen) {
+    return align128(oDesc(gen) + (gen ? sizeof(uint32_t) * NPT : 0));
+  }
   static constexpr uint32_t state_bytes = sizeof(SIN) * 5 * NPT;
   static constexpr uint32_t q_bytes = sizeof(double) * 3 * RQ * RZ;
   static constexpr uint32_t tile_bytes = sizeof(double) * 5 * NTP;
@@ -205,17 +213,17 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   double* sMu0 = reinterpret_cast<double*>(smem_raw + SM::oMu0);  // [TR][TZ]
   double* sP0 = reinterpret_cast<double*>(smem_raw + SM::oP0);    // [5][TR][TZ]
   double* sPA = reinterpret_cast<double*>(smem_raw + SM::oPA);    // [5][TR][TZ]
-  R* sDz = reinterpret_cast<R*>(smem_raw + SM::oDz);              // [2][RR][TZ]
-  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
+  R* sDz = reinterpret_cast<R*>(smem_raw + SM::oDz(GEN));         // [2][RR][TZ]
+  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
 
   const int tid = threadIdx.x;
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long P = a.g.P, PL = a.g.plane;
   const bool sc = a.c.shock_capturing != 0;
   // pv_old is needed as a tile in stages 2 and 3 (stage 1 reads it from the state box),
-  // the running sum A in stages 3 and 4
-  const bool needU0 = a.stage == 2 || a.stage == 3;
-  const bool needA = a.stage == 3 || a.stage == 4;
+  // the running sum A in stages 3 and 4; interior tiles stage them by TMA
+  const bool needU0 = !GEN && (a.stage == 2 || a.stage == 3);
+  const bool needA = !GEN && (a.stage == 3 || a.stage == 4);
 
   // ---- phase 1: one thread issues the TMA loads; the RK operands complete on the
   // second barrier while phases 1-2 run
@@ -487,15 +495,15 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
         un[f] = add_rn(u0, mul_rn(0.5, k));
         a.A[o] = add_rn(u0, mul_rn(c6, k));
       } else if (a.stage == 2) {
-        const double u0 = sP0[f * NTP + tp];
+        const double u0 = GEN ? __ldg(a.U0 + o) : sP0[f * NTP + tp];
         un[f] = add_rn(u0, mul_rn(0.5, k));
         a.B[o] = k;
       } else if (a.stage == 3) {
-        const double u0 = sP0[f * NTP + tp];
+        const double u0 = GEN ? __ldg(a.U0 + o) : sP0[f * NTP + tp];
         un[f] = add_rn(u0, k);
-        a.A[o] = add_rn(sPA[f * NTP + tp], mul_rn(c3, add_rn(__ldg(a.B + o), k)));
+        a.A[o] = add_rn(GEN ? a.A[o] : sPA[f * NTP + tp], mul_rn(c3, add_rn(__ldg(a.B + o), k)));
       } else {
-        un[f] = blank ? pv[f] : add_rn(sPA[f * NTP + tp], mul_rn(c6, k));
+        un[f] = blank ? pv[f] : add_rn(GEN ? a.A[o] : sPA[f * NTP + tp], mul_rn(c6, k));
       }
     }
     if (j1) {
@@ -526,7 +534,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
 
 
 template <int H, bool GEN, typename SIN, typename R, int CM>
-__global__ void __launch_bounds__(STAGE_THREADS)
+__global__ void __launch_bounds__(STAGE_THREADS, 2)
     stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
                  const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
                  const __grid_constant__ CUtensorMap mAcc) {
