@@ -99,7 +99,7 @@ struct axj_handle {
   CUtensorMap map_state[5][2];
   CUtensorMap map_star[2];
   CUtensorMap map_starL[2];    // final mu*, beta*, kappa* planes (learned sensor)
-  CUtensorMap map_u0_tile, map_acc_tile;
+  CUtensorMap map_u0_tile, map_acc_tile, map_b_tile;
   CUtensorMap map_sens[5][2];  // sensor V boxes of the stage buffers x {interior, general}
   CUtensorMap map_sensT[5][2]; // sensor temperature boxes
   CUtensorMap map_rho[5];      // density tile boxes
@@ -426,6 +426,8 @@ int build_maps(axj_handle* h) {
   }
   int rc = make_map(h, &h->map_u0_tile, h->U0, 5, tw, th, 5);
   if (rc != AXJ_OK) return rc;
+  rc = make_map(h, &h->map_b_tile, h->B, 5, tw, th, 5);
+  if (rc != AXJ_OK) return rc;
   return make_map(h, &h->map_acc_tile, h->A, 5, tw, th, 5);
 }
 
@@ -437,6 +439,7 @@ StageMaps stage_maps(axj_handle* h, int b, int cls, int cm) {
   m.star = cm == CM_LRN ? &h->map_starL[cls] : (cm == CM_PRE ? &h->map_coef[cls] : &h->map_star[cls]);
   m.u0 = &h->map_u0_tile;
   m.acc = &h->map_acc_tile;
+  m.bt = &h->map_b_tile;
   return m;
 }
 

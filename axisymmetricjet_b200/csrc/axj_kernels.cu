@@ -144,6 +144,14 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// Prefetch of a tensor box into L2 (no shared memory, no completion to wait for).
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
+
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
 
 // z halo of a box in elements, rounded up so the box's x coordinate starts on a
@@ -201,6 +209,7 @@ struct StageSmem {
 template <int H, bool GEN, typename SIN, typename R, int CM>
 __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, const CUtensorMap* mState,
                                            const CUtensorMap* mQ, const CUtensorMap* mU0, const CUtensorMap* mAcc,
+                                           const CUtensorMap* mB,
                                            unsigned char* smem_raw, uint64_t* bar) {
   using SM = StageSmem<H, SIN, R, CM>;
   using RP = typename std::conditional<GEN, double, R>::type;
@@ -242,6 +251,11 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
       if (needU0) tma_load_3d(sP0, mU0, i0, j0, 0, &bar[1]);
       if (needA) tma_load_3d(sPA, mAcc, i0, j0, 0, &bar[1]);
     }
+    // operands the RK update reads from global memory: into L2 now (k2 in stage 3; pv_old
+    // and the running sum in general tiles, which do not stage them)
+    if (mB && a.stage == 3) tma_prefetch_3d(mB, i0, j0, 0);
+    if (GEN && (a.stage == 2 || a.stage == 3)) tma_prefetch_3d(mU0, i0, j0, 0);
+    if (GEN && (a.stage == 3 || a.stage == 4)) tma_prefetch_3d(mAcc, i0, j0, 0);
   }
   if (GEN) {
     for (int idx = tid; idx < NPT; idx += STAGE_THREADS) {
@@ -537,11 +551,11 @@ template <int H, bool GEN, typename SIN, typename R, int CM>
 __global__ void __launch_bounds__(STAGE_THREADS, 2)
     stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
                  const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
-                 const __grid_constant__ CUtensorMap mAcc) {
+                 const __grid_constant__ CUtensorMap mAcc, const __grid_constant__ CUtensorMap mB) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
   const int2 t0 = tiles[blockIdx.x];
-  stage_body<H, GEN, SIN, R, CM>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, smem_raw, bar);
+  stage_body<H, GEN, SIN, R, CM>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, &mB, smem_raw, bar);
 }
 
 // Batched form: a persistent grid-stride loop over the tiles (i0, j0, instance) of many
@@ -561,7 +575,8 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + tt.z)[k];
     __syncthreads();
     const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
-    if (!stage_body<H, GEN, SIN, R, CM>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, m + kmaps.w, smem_raw,
+    if (!stage_body<H, GEN, SIN, R, CM>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, m + kmaps.w, nullptr,
+                                        smem_raw,
                                          bar))
       return;
   }
@@ -573,14 +588,14 @@ static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* ti
   if (ntiles <= 0) return cudaSuccess;
   if (a.learned == CM_LRN) {
     const size_t sm = StageSmem<H, SIN, R, CM_LRN>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, CM_LRN><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+    stage_kernel<H, GEN, SIN, R, CM_LRN><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
   } else if (a.learned == CM_PRE) {
     const size_t sm = StageSmem<H, SIN, R, CM_PRE>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, CM_PRE><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+    stage_kernel<H, GEN, SIN, R, CM_PRE><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
   } else {
     const size_t sm = StageSmem<H, SIN, R, CM_FILT>::bytes(GEN);
     stage_kernel<H, GEN, SIN, R, CM_FILT>
-        <<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc);
+        <<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
   }
   return cudaGetLastError();
 }

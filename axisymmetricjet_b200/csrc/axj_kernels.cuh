@@ -17,6 +17,7 @@ struct StageMaps {
   const CUtensorMap* star;
   const CUtensorMap* u0;
   const CUtensorMap* acc;
+  const CUtensorMap* bt;  // tile box of k2 (prefetched into L2 for stage 3)
 };
 
 // Device view of one solver instance.
