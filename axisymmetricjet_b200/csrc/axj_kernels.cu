@@ -29,6 +29,9 @@ __constant__ double cTG[9][11];
 __constant__ float cSBP1f[9][6];
 __constant__ float cSBP2f[9][6];
 __constant__ PatchDev cPatch[MAX_PATCHES];
+// SBP2 centred row composed with itself: the 9-point fourth-difference row (offsets -4..4)
+__constant__ double cC9[9];
+__constant__ float cC9f[9];
 
 void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const double tg[9][11],
                    const PatchDev* patches, int npatch, cudaStream_t s) {
@@ -46,6 +49,14 @@ void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const doubl
   cudaMemcpyToSymbolAsync(cSBP1f, f1, sizeof(float) * 54, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(cSBP2f, f2, sizeof(float) * 54, 0, cudaMemcpyHostToDevice, s);
   if (npatch > 0) cudaMemcpyToSymbolAsync(cPatch, patches, sizeof(PatchDev) * npatch, 0, cudaMemcpyHostToDevice, s);
+  static double c9[9];
+  static float c9f[9];
+  for (int k = 0; k < 9; ++k) c9[k] = 0.0;
+  for (int a = 0; a < 5; ++a)
+    for (int b = 0; b < 5; ++b) c9[a + b] += sbp2[4][a] * sbp2[4][b];
+  for (int k = 0; k < 9; ++k) c9f[k] = (float)c9[k];
+  cudaMemcpyToSymbolAsync(cC9, c9, sizeof(double) * 9, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(cC9f, c9f, sizeof(float) * 9, 0, cudaMemcpyHostToDevice, s);
 }
 
 // Round-to-nearest arithmetic that the compiler may not contract into an FMA; used
@@ -93,6 +104,16 @@ __device__ __forceinline__ R dst_p(int row, const S* rho, const S* T, int stride
 #pragma unroll
   for (int m = 1; m < 6; ++m)
     if (m < n) s = s + tabv<R, 1>(rw, m) * (R(rho[(w0 + m) * stride]) * R(T[(w0 + m) * stride]));
+  return s;
+}
+
+// 9-point fourth difference cC9 centred at p (stride in elements), left to right.
+template <typename R, typename S>
+__device__ __forceinline__ R c9dot(const S* p, int stride) {
+  const R* c = std::is_same<R, float>::value ? reinterpret_cast<const R*>(cC9f) : reinterpret_cast<const R*>(cC9);
+  R s = c[0] * R(p[-4 * stride]);
+#pragma unroll
+  for (int m = 1; m < 9; ++m) s = s + c[m] * R(p[(m - 4) * stride]);
   return s;
 }
 
@@ -812,8 +833,14 @@ struct SensSmem {
   static constexpr size_t oD = align128(oS + sizeof(R) * NS);
   static constexpr size_t oRho = align128(oD + sizeof(R) * NS);
   static constexpr size_t oD2 = align128(oRho + sizeof(SIN) * TR * TZ);
-  static constexpr size_t oDesc = align128(oD2 + sizeof(R) * (TR * DZ + DR * TZ + TR * TZ));
-  static constexpr size_t bytes(bool gen) { return align128(oDesc + (gen ? sizeof(uint32_t) * NV : 0)); }
+  // the arms exist only in general tiles (interior tiles use the composite 9-point row)
+  __host__ __device__ static constexpr size_t oFsw(bool gen) {
+    return oD2 + (gen ? sizeof(R) * (TR * DZ + DR * TZ) : 0);
+  }
+  __host__ __device__ static constexpr size_t oDesc(bool gen) { return align128(oFsw(gen) + sizeof(R) * TR * TZ); }
+  __host__ __device__ static constexpr size_t bytes(bool gen) {
+    return align128(oDesc(gen) + (gen ? sizeof(uint32_t) * NV : 0));
+  }
   static constexpr uint32_t tx_bytes = sizeof(SIN) * (2 * NV + NS + TR * TZ);
 };
 
@@ -836,10 +863,10 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   R* sS = reinterpret_cast<R*>(smem_raw + SM::oS);         // [SR][SZ]
   R* sD = reinterpret_cast<R*>(smem_raw + SM::oD);         // [SR][SZ]
   SIN* sRho = reinterpret_cast<SIN*>(smem_raw + SM::oRho); // [TR][TZ]
-  R* sd2z = reinterpret_cast<R*>(smem_raw + SM::oD2);      // [TR][DZ]
-  R* sd2r = sd2z + TR * DZ;                                 // [DR][TZ]
-  R* sFsw = sd2r + DR * TZ;                                 // [TR][TZ]
-  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
+  R* sd2z = reinterpret_cast<R*>(smem_raw + SM::oD2);      // [TR][DZ] (general tiles)
+  R* sd2r = sd2z + TR * DZ;                                 // [DR][TZ] (general tiles)
+  R* sFsw = reinterpret_cast<R*>(smem_raw + SM::oFsw(GEN)); // [TR][TZ]
+  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
 
   const int tid = threadIdx.x;
   const Grid g = a.g;
@@ -912,10 +939,28 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   }
   __syncthreads();
 
-  // ---- phases 3-4 per field: second derivatives on the arms, fourth derivatives at
-  // the tile points (kept in registers: 2 points per thread)
+  // ---- phases 3-4 per field: fourth derivatives at the tile points (kept in registers:
+  // 2 points per thread). Interior tiles: SBP2 of SBP2 with the centred row both times is
+  // the 9-point row cC9 = c * c (c the centred SBP2 row), applied to S, T, the dilatation
+  // directly (one rounding per product instead of two stencil passes: the difference is
+  // rounding only). General tiles: second derivatives on the arms with each arm point's
+  // row, then the tile point's row.
   constexpr int PPT = (TZ * TR) / STAGE_THREADS;
   R d4z[3][PPT], d4r[3][PPT];
+  if constexpr (!GEN) {
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) {
+      const int pidx = tid + q * STAGE_THREADS;
+      const int r = pidx / TZ, c = pidx - r * TZ;
+      const int sidx = (HS + r) * SZ + (HSZ + c);
+      d4z[0][q] = c9dot<R>(sS + sidx, 1);
+      d4r[0][q] = c9dot<R>(sS + sidx, SZ);
+      d4z[1][q] = c9dot<R>(sT + sidx, 1);
+      d4r[1][q] = c9dot<R>(sT + sidx, SZ);
+      d4z[2][q] = c9dot<R>(sD + sidx, 1);
+      d4r[2][q] = c9dot<R>(sD + sidx, SZ);
+    }
+  } else {
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
     for (int idx = tid; idx < TR * DZ + DR * TZ; idx += STAGE_THREADS) {
@@ -956,6 +1001,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
       d4r[f][q] = dst<R, 2, GEN>(rw, sd2r + (HF + r) * TZ + c, TZ);
     }
     __syncthreads();
+  }
   }
 
   // ---- quantities to be filtered (ComputeTobeFilteredQuantities :204-215)
