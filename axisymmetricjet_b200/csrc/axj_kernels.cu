@@ -211,9 +211,13 @@ struct StageSmem {
   __host__ __device__ static constexpr size_t oDesc(bool gen) {
     return align128(oDz(gen) + sizeof(double) * 2 * RR * TZ);
   }
-  __host__ __device__ static constexpr size_t bytes(bool gen) {
+  // 1-D metrics and coordinates of the tile: dxidz, ddxidxidz, z on its columns,
+  // detadr, ddetadetadr, r, 1/r on its rows
+  __host__ __device__ static constexpr size_t oMet(bool gen) {
     return align128(oDesc(gen) + (gen ? sizeof(uint32_t) * NPT : 0));
   }
+  static constexpr int NMET = 3 * TZ + 4 * TR;
+  __host__ __device__ static constexpr size_t bytes(bool gen) { return align128(oMet(gen) + sizeof(double) * NMET); }
   static constexpr uint32_t state_bytes = sizeof(SIN) * 5 * NPT;
   static constexpr uint32_t q_bytes = sizeof(double) * 3 * RQ * RZ;
   static constexpr uint32_t tile_bytes = sizeof(double) * 5 * NTP;
@@ -245,6 +249,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   double* sPA = reinterpret_cast<double*>(smem_raw + SM::oPA);    // [5][TR][TZ]
   R* sDz = reinterpret_cast<R*>(smem_raw + SM::oDz(GEN));         // [2][RR][TZ]
   uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
+  double* sMet = reinterpret_cast<double*>(smem_raw + SM::oMet(GEN));  // [3][TZ] + [4][TR]
 
   const int tid = threadIdx.x;
   const int Nz = a.g.Nz, Nr = a.g.Nr;
@@ -285,6 +290,19 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
       sDesc[idx] = (i >= 0 && i < Nz && j >= 0 && j < Nr) ? __ldg(a.desc + (long long)j * P + i)
                                                             : make_desc(ROW_NONE, ROW_NONE, false, 0);
     }
+  }
+  // the tile's metrics and coordinates (read per point in phases 2-3)
+  if (tid < TZ) {
+    const int i = min(i0 + tid, Nz - 1);
+    sMet[tid] = __ldg(a.dxidz + i);
+    sMet[TZ + tid] = __ldg(a.ddxidxidz + i);
+    sMet[2 * TZ + tid] = __ldg(a.zc + i);
+  } else if (tid < TZ + TR) {
+    const int r = tid - TZ, j = min(j0 + r, Nr - 1);
+    sMet[3 * TZ + r] = __ldg(a.detadr + j);
+    sMet[3 * TZ + TR + r] = __ldg(a.ddetadetadr + j);
+    sMet[3 * TZ + 2 * TR + r] = __ldg(a.rc + j);
+    sMet[3 * TZ + 3 * TR + r] = __ldg(a.invr + j);
   }
   if (!__syncthreads_and(mbar_wait_bounded(&bar[0], 0))) {
     if (tid == 0) atomicOr(a.flags, 4);
@@ -381,7 +399,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
         const uint32_t dsc = sDesc[sidx];
         row = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
       }
-      const R m = R(__ldg(a.dxidz + i));
+      const R m = R(sMet[c]);
       dvr = dst<R, 1, GEN>(row, sU + 1 * NPT + sidx, 1) * m;
       dvz = dst<R, 1, GEN>(row, sU + 3 * NPT + sidx, 1) * m;
     }
@@ -416,9 +434,9 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
       rw = blank ? (int)ROW_NONE : desc_rrow(dsc);
       face = desc_face(dsc);
     }
-    const double xzd = __ldg(a.dxidz + i), erd = __ldg(a.detadr + j);
-    const R xz = R(xzd), xzz = R(__ldg(a.ddxidxidz + i));
-    const R er = R(erd), err = R(__ldg(a.ddetadetadr + j));
+    const double xzd = sMet[c], erd = sMet[3 * TZ + r];
+    const R xz = R(xzd), xzz = R(sMet[TZ + c]);
+    const R er = R(erd), err = R(sMet[3 * TZ + TR + r]);
     const SIN* pR = sU + 0 * NPT + sidx;
     const SIN* pVr = sU + 1 * NPT + sidx;
     const SIN* pVt = sU + 2 * NPT + sidx;
@@ -478,13 +496,13 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
       q.lambda = RP(beta - (2.0 / 3.0) * double(*pMu));
     }
     const DerivT<RP> d = convert<RP>(dr);
-    const double rloc = __ldg(a.rc + j), zloc = __ldg(a.zc + i);
+    const double rloc = sMet[3 * TZ + 2 * TR + r], zloc = sMet[2 * TZ + c];
     const bool j1 = (j == 0);
     double rhs[5] = {-0.0, -0.0, -0.0, -0.0, -0.0};
     if (!j1) {
       RP rp[5];
       const RhsConst<RP> kc = rhs_const<RP>(a.c.gam, a.c.Re, a.c.Pr);
-      const RP onebyr = RP(__ldg(a.invr + j));
+      const RP onebyr = RP(sMet[3 * TZ + 3 * TR + r]);
       const RP inv_rho = RP(1.0) / q.rho;
       rhs_inviscid<RP>(q, d, onebyr, inv_rho, kc, rp);
       if (a.c.do_viscous) rhs_viscous<RP>(q, d, onebyr, inv_rho, kc, sc, rp);
