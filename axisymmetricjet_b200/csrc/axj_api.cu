@@ -254,6 +254,7 @@ SensorArgs sensor_args(axj_handle* h, int b) {
   s.detadr = h->detadr;
   s.zc = h->zc;
   s.rc = h->rc;
+  s.invr = h->invr;
   s.dz = h->dzv;
   s.dr = h->drv;
   s.ramp = h->ramp;

@@ -856,9 +856,13 @@ struct SensSmem {
     return oD2 + (gen ? sizeof(R) * (TR * DZ + DR * TZ) : 0);
   }
   __host__ __device__ static constexpr size_t oDesc(bool gen) { return align128(oFsw(gen) + sizeof(R) * TR * TZ); }
-  __host__ __device__ static constexpr size_t bytes(bool gen) {
+  // metrics of the S region: dxidz on its columns [SZ], detadr and 1/r on its rows
+  // [2][SR]; deltaz, deltar on the tile [TZ] + [TR]
+  __host__ __device__ static constexpr size_t oMet(bool gen) {
     return align128(oDesc(gen) + (gen ? sizeof(uint32_t) * NV : 0));
   }
+  static constexpr int NMET = SZ + 2 * SR + TZ + TR;
+  __host__ __device__ static constexpr size_t bytes(bool gen) { return align128(oMet(gen) + sizeof(double) * NMET); }
   static constexpr uint32_t tx_bytes = sizeof(SIN) * (2 * NV + NS + TR * TZ);
 };
 
@@ -885,6 +889,11 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   R* sd2r = sd2z + TR * DZ;                                 // [DR][TZ] (general tiles)
   R* sFsw = reinterpret_cast<R*>(smem_raw + SM::oFsw(GEN)); // [TR][TZ]
   uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
+  double* sMz = reinterpret_cast<double*>(smem_raw + SM::oMet(GEN));  // dxidz, column i0 - HSZ + k
+  double* sMr = sMz + SZ;                                               // detadr, row j0 - HS + k
+  double* sIr = sMr + SM::SR;                                           // 1/r (0 on the axis row)
+  double* sDzv = sIr + SM::SR;                                          // deltaz on the tile columns
+  double* sDrv = sDzv + TZ;                                             // deltar on the tile rows
 
   const int tid = threadIdx.x;
   const Grid g = a.g;
@@ -913,6 +922,22 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
       sDesc[idx] = inside(i, j) ? __ldg(a.desc + (long long)j * g.P + i) : make_desc(ROW_NONE, ROW_NONE, false, 0);
     }
   }
+  // metrics and coordinates of the region (clamped indices: values outside the grid are
+  // never used)
+  for (int k = tid; k < SM::NMET; k += STAGE_THREADS) {
+    double v;
+    if (k < SZ) {
+      v = __ldg(a.dxidz + min(max(i0 - HSZ + k, 0), Nz - 1));
+    } else if (k < SZ + 2 * SM::SR) {
+      const int q = (k - SZ) % SM::SR, j = min(max(j0 - HS + q, 0), Nr - 1);
+      v = (k - SZ) < SM::SR ? __ldg(a.detadr + j) : __ldg(a.invr + j);
+    } else if (k < SZ + 2 * SM::SR + TZ) {
+      v = __ldg(a.dz + min(i0 + (k - SZ - 2 * SM::SR), Nz - 1));
+    } else {
+      v = __ldg(a.dr + min(j0 + (k - SZ - 2 * SM::SR - TZ), Nr - 1));
+    }
+    sMz[k] = v;
+  }
   if (!__syncthreads_and(mbar_wait_bounded(&bar, 0))) {
     if (tid == 0) atomicOr(a.flags, 4);
     return false;
@@ -931,19 +956,20 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
       const uint32_t dsc = vdesc(vidx);
       const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
       const int rw = desc_blank(dsc) ? (int)ROW_NONE : desc_rrow(dsc);
-      const R xz = R(__ldg(a.dxidz + i)), er = R(__ldg(a.detadr + j));
+      const R xz = R(sMz[sz]), er = R(sMr[sr]);
       const R dVrdz = dst<R, 1, GEN>(zr, sVr + vidx, 1) * xz;
       const R dVzdz = dst<R, 1, GEN>(zr, sVz + vidx, 1) * xz;
       const R dVrdr = dst<R, 1, GEN>(rw, sVr + vidx, VZ) * er;
       const R dVzdr = dst<R, 1, GEN>(rw, sVz + vidx, VZ) * er;
       const R vr = R(sVr[vidx]);
-      const R r = R(__ldg(a.rc + j));
+      // V_r / r as V_r * (1/r) (the reference divides; the two differ by rounding)
+      const R vr_r = vr * R(sIr[sr]);
       if (j == 0) dil = R(2.0) * dVrdr + dVzdz;
-      else dil = dVrdr + vr / r + dVzdz;
+      else dil = dVrdr + vr_r + dVzdz;
       const R S11 = dVrdr - R(1.0 / 3.0) * dil;
       const R S13 = R(0.5) * (dVrdz + dVzdr);
       const R S33 = dVzdz - R(1.0 / 3.0) * dil;
-      const R S22 = (j == 0) ? dVrdr - R(1.0 / 3.0) * dil : vr / r - R(1.0 / 3.0) * dil;
+      const R S22 = (j == 0) ? dVrdr - R(1.0 / 3.0) * dil : vr_r - R(1.0 / 3.0) * dil;
       S = sqrt_t<R>(S11 * S11 + S13 * S13 + S22 * S22 + S13 * S13 + S33 * S33);
       if (zarm && rarm) {
         const R vort = fabs(dVrdz - dVzdr);
@@ -1030,7 +1056,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     const int i = i0 + c, j = j0 + r;
     if (GEN && !inside(i, j)) continue;
     const long long o = (long long)j * g.P + i;
-    const R dz = R(__ldg(a.dz + i)), dr = R(__ldg(a.dr + j));
+    const R dz = R(sDzv[c]), dr = R(sDrv[r]);
     const R rho = R(sRho[r * TZ + c]);
     const R T = R(sT[(HS + r) * SZ + HSZ + c]);
     const R fsw = sFsw[r * TZ + c];

@@ -98,6 +98,7 @@ struct SensorArgs {
   const double* detadr;
   const double* zc;
   const double* rc;
+  const double* invr;    // 1/r_j (0 on the axis row)
   const double* dz;      // deltaz(i) (:171-179)
   const double* dr;      // deltar(j) (:181-189)
   const double* ramp;    // (1+tanh(5(z-10)))/2 (:85)
