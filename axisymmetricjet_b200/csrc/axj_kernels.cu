@@ -1456,17 +1456,21 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-// Byte offset of 16-byte chunk c of row R in a block stored with the 128-byte swizzle
-// (chunk index XOR row mod 8); TMA writes the Q blocks this way, the kernel the Z blocks.
+// Byte offset of 16-byte chunk c of row R in a Q block stored with the 128-byte swizzle
+// (chunk index XOR row mod 8), as TMA writes it.
 __device__ __forceinline__ int zrk_chunk(int R, int c) { return R * ZRK_QROW + ((c ^ (R & 7)) << 4); }
-__device__ __forceinline__ int zrk_elem(int R, int p) { return zrk_chunk(R, p >> 1) + ((p & 1) << 3); }
+// The z-filtered block is stored transposed, [quantity][position][row] with ZRK_ZP rows
+// (odd: the r filter's reads, 16 positions x 2 rows per warp, and the recurrence's writes,
+// consecutive rows per warp, are free of bank conflicts), so the r filter's taps are
+// consecutive doubles at fixed offsets.
+constexpr int ZRK_ZP = ZRK_NR + 1;
 
 template <typename SIN>
 struct ZrSmem {
   static constexpr size_t qbytes = (size_t)ZRK_LANES * ZRK_QROW;           // 19968
   static constexpr size_t qslot = (qbytes + 1023) / 1024 * 1024;           // 20480
   static constexpr size_t oQ = 0;                                            // [2] Q blocks (swizzled)
-  static constexpr size_t oZ = 2 * qslot;                                    // z-filtered block (swizzled)
+  static constexpr size_t oZ = 2 * qslot;                                    // z-filtered block [3][16][ZRK_ZP]
   static constexpr size_t oZc = oZ + qslot;                                  // [2][ZRK_NR][16] z row codes
   static constexpr size_t zcbytes = (size_t)ZRK_NR * ZRK_BZ;
   static constexpr size_t oT = oZc + 2 * 1024;                               // [2][ZRK_RB][16] T
@@ -1583,7 +1587,7 @@ __global__ void __launch_bounds__(ZRK_THREADS, 3)
       if (row_on) {
 #pragma unroll
         for (int s2 = 0; s2 < 16; ++s2) {
-          const int p = ZRK_BZ * m + s2;
+          const int p = ZRK_BZ * m + s2;  // z position of this step
           const int code = (int)((cws[s2 >> 2] >> (8 * (s2 & 3))) & 255u);
           double v;
           if (p >= Nz) {
@@ -1607,12 +1611,13 @@ __global__ void __launch_bounds__(ZRK_THREADS, 3)
           }
           ring[s2] = v;
         }
+        double* zt = reinterpret_cast<double*>(zb) + fq * ZRK_BZ * ZRK_ZP + rr;
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-          *reinterpret_cast<double2*>(zb + zrk_chunk(Rq, c)) = make_double2(ring[2 * c], ring[2 * c + 1]);
+        for (int s2 = 0; s2 < 16; ++s2) zt[s2 * ZRK_ZP] = ring[s2];
       } else {
+        double* zt = reinterpret_cast<double*>(zb) + fq * ZRK_BZ * ZRK_ZP + rr;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) *reinterpret_cast<double2*>(zb + zrk_chunk(Rq, c)) = make_double2(0.0, 0.0);
+        for (int s2 = 0; s2 < 16; ++s2) zt[s2 * ZRK_ZP] = 0.0;
       }
     }
     __syncthreads();
@@ -1631,24 +1636,24 @@ __global__ void __launch_bounds__(ZRK_THREADS, 3)
         const double mu = double(mu_of_T<R>(R(tb[qd])));
         const int rw = rcb[qd];
         double fv[3] = {0.0, 0.0, 0.0};
+        // column of this point in the transposed block: row j0 + row is Z row row + ZRK_HR
+        const double* zc = reinterpret_cast<const double*>(zb) + p * ZRK_ZP + row + ZRK_HR;
         if (rw == 4) {
 #pragma unroll
           for (int f = 0; f < 3; ++f) {
-            const int R0 = f * ZRK_NR + row + ZRK_HR - 4;
-            double sacc = t0 * *reinterpret_cast<const double*>(zb + zrk_elem(R0, p));
+            const double* col = zc + f * ZRK_BZ * ZRK_ZP - 4;
+            double sacc = t0 * col[0];
 #pragma unroll
-            for (int mm = 1; mm < 9; ++mm)
-              sacc = sacc + cTG[4][mm] * *reinterpret_cast<const double*>(zb + zrk_elem(R0 + mm, p));
+            for (int mm = 1; mm < 9; ++mm) sacc = sacc + cTG[4][mm] * col[mm];
             fv[f] = sacc;
           }
         } else if (rw < 9) {
           const int w0 = tg_w0(rw), n = tg_len(rw);
 #pragma unroll
           for (int f = 0; f < 3; ++f) {
-            const int R0 = f * ZRK_NR + row + ZRK_HR + w0;
-            double sacc = cTG[rw][0] * *reinterpret_cast<const double*>(zb + zrk_elem(R0, p));
-            for (int mm = 1; mm < n; ++mm)
-              sacc = sacc + cTG[rw][mm] * *reinterpret_cast<const double*>(zb + zrk_elem(R0 + mm, p));
+            const double* col = zc + f * ZRK_BZ * ZRK_ZP + w0;
+            double sacc = cTG[rw][0] * col[0];
+            for (int mm = 1; mm < n; ++mm) sacc = sacc + cTG[rw][mm] * col[mm];
             fv[f] = sacc;
           }
         }
