@@ -698,6 +698,11 @@ void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* 
 // block, and the last block to finish reduces the partials (no memset needed,
 // the counter is returned to 0).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
 __device__ __forceinline__ double warp_min(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -706,42 +711,58 @@ __device__ __forceinline__ double warp_min(double v) {
 
 // ComputeTimeStep over one instance with blocks blk = 0..nblk-1 (per-block minima in
 // a.partial, the last block to finish reduces them).
+// The minimum of dt = CFL / x over the points is CFL / (maximum of x): division by a
+// positive x is monotonic and correctly rounded, so the two agree exactly; the kernel
+// reduces x and divides once. Likewise max(mu/Re, lambda/Re) = max(mu, lambda)/Re. The
+// stale T's square root is formed once. Blanked points contribute dt = 100
+// (ModInputOutput.f90:398-400).
 __device__ __forceinline__ void dt_body(const DtArgs& a, int blk, int nblk) {
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long n = (long long)Nz * Nr;
-  const long long P = a.g.P, PL = a.g.plane;
-  const double Tst = *a.staleT;
+  const long long PL = a.g.plane;
   const bool phys = a.c.dt_mode == DT_PHYSICAL;
-  double m = 1.0e300;
-  int bad = 0;
+  const double sqrtTst = sqrt(*a.staleT);
+  const double RePr = a.c.Re * a.c.Pr;
+  double xm = 0.0;  // maximum of the denominators (0: no unblanked point yet)
+  int bad = 0, blank = 0;
   for (long long p = (long long)blk * DT_THREADS + threadIdx.x; p < n; p += (long long)nblk * DT_THREADS) {
     const int j = (int)(p / Nz), i = (int)(p - (long long)j * Nz);
-    const long long o = (long long)j * P + i;
-    double v;
+    const long long o = (long long)j * a.g.P + i;
     if (desc_blank(__ldg(a.desc + o))) {
-      v = 100.0;
-    } else {
-      const double Vr = __ldg(a.U + 1 * PL + o), Vz = __ldg(a.U + 3 * PL + o), T = __ldg(a.U + 4 * PL + o);
-      const double mu = mu_of_T<double>(T);
-      const double beta = (3.0 / 5.0) * mu;
-      const double lambda = beta - (2.0 / 3.0) * mu;
-      v = dt_point(Vz, Vr, phys ? T : Tst, mu, lambda, mu, __ldg(a.dxidz + i), __ldg(a.detadr + j), a.c);
+      blank = 1;
+      continue;
     }
-    if (!(v == v)) bad = 1;
-    m = fmin(m, v);
+    const double Vr = __ldg(a.U + 1 * PL + o), Vz = __ldg(a.U + 3 * PL + o), T = __ldg(a.U + 4 * PL + o);
+    const double dxidz = __ldg(a.dxidz + i), detadr = __ldg(a.detadr + j);
+    const double mu = mu_of_T<double>(T);
+    const double beta = (3.0 / 5.0) * mu;
+    const double lambda = beta - (2.0 / 3.0) * mu;
+    // dt_point's denominator, term for term
+    const double inv = fabs(Vz * dxidz + Vr * detadr) + (phys ? sqrt(T) : sqrtTst) * sqrt(dxidz * dxidz + detadr * detadr);
+    double mx = (lambda > mu ? lambda : mu) / a.c.Re;
+    const double k = mu / RePr;
+    if (k > mx) mx = k;
+    const double sabs = fabs(dxidz) + fabs(detadr);
+    const double x = inv + 2.0 * mx * (sabs * sabs);
+    if (!(x == x)) bad = 1;
+    xm = fmax(xm, x);
   }
   __shared__ double sred[DT_THREADS / 32];
   __shared__ bool last;
-  m = warp_min(m);
+  const bool anyblank = __syncthreads_or(blank);
+  xm = warp_max(xm);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) sred[w] = m;
+  if (lane == 0) sred[w] = xm;
   if (bad) atomicOr(a.flags, 1);
   __syncthreads();
   if (w == 0) {
-    m = lane < DT_THREADS / 32 ? sred[lane] : 1.0e300;
-    m = warp_min(m);
+    xm = lane < DT_THREADS / 32 ? sred[lane] : 0.0;
+    xm = warp_max(xm);
     if (lane == 0) {
-      a.partial[blk] = m;
+      // per-block dt (CFL / its largest denominator; 100 if it only met blanked points)
+      double v = a.c.CFL / xm;
+      if (anyblank) v = fmin(v, 100.0);
+      a.partial[blk] = v;
       __threadfence();
       const unsigned int done = atomicAdd(a.counter, 1u);
       last = (done == (unsigned int)nblk - 1);
@@ -1584,7 +1605,20 @@ __global__ void __launch_bounds__(ZRK_THREADS, 3)
       issue(k + 1);
     }
     if (k > bs && lane_on) {
-      if (row_on) {
+      // a block of centred points inside the row (the common case) needs no per-step checks
+      const bool centred = row_on && cws[0] == 0x04040404u && cws[1] == 0x04040404u && cws[2] == 0x04040404u &&
+                           cws[3] == 0x04040404u && ZRK_BZ * m + ZRK_BZ <= Nz;
+      if (centred) {
+#pragma unroll
+        for (int s2 = 0; s2 < 16; ++s2) {
+          const double ff = t4 * xv[s2] + t5 * xv[s2 + 1] + t6 * xv[s2 + 2] + t7 * xv[s2 + 3] + t8 * xv[s2 + 4];
+          const double fb = t0 * ring[(s2 + 12) & 15] + t1 * ring[(s2 + 13) & 15] + t2 * ring[(s2 + 14) & 15];
+          ring[s2] = (ff + fb) + t3 * ring[(s2 + 15) & 15];
+        }
+        double* zt = reinterpret_cast<double*>(zb) + fq * ZRK_BZ * ZRK_ZP + rr;
+#pragma unroll
+        for (int s2 = 0; s2 < 16; ++s2) zt[s2 * ZRK_ZP] = ring[s2];
+      } else if (row_on) {
 #pragma unroll
         for (int s2 = 0; s2 < 16; ++s2) {
           const int p = ZRK_BZ * m + s2;  // z position of this step
