@@ -887,6 +887,10 @@ struct SensSmem {
   static constexpr uint32_t tx_bytes = sizeof(SIN) * (2 * NV + NS + TR * TZ);
 };
 
+// Threads of a sensor tile CTA: general tiles (one CTA per SM, bound by shared memory)
+// take 512 so the SM has 16 warps to hide latency with; interior tiles 256.
+__host__ __device__ constexpr int sens_threads(bool gen) { return gen ? 512 : STAGE_THREADS; }
+
 template <typename R>
 __device__ __forceinline__ R sqrt_t(R x) { return sqrt(x); }
 template <>
@@ -898,6 +902,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
                                             const CUtensorMap* mT, const CUtensorMap* mRho, unsigned char* smem_raw,
                                             uint64_t& bar) {
   using SM = SensSmem<HS, HF, SIN, R>;
+  constexpr int NT = sens_threads(GEN);
   constexpr int HV = SM::HV, HVZ = SM::HVZ, HSZ = SM::HSZ, VZ = SM::VZ, NV = SM::NV;
   constexpr int SZ = SM::SZ, NS = SM::NS, DZ = SM::DZ, DR = SM::DR;
   SIN* sVr = reinterpret_cast<SIN*>(smem_raw + SM::oVr);   // [VR][VZ]
@@ -937,7 +942,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     tma_load_3d(sRho, mRho, i0, j0, 0, &bar);
   }
   if (GEN) {
-    for (int idx = tid; idx < NV; idx += STAGE_THREADS) {
+    for (int idx = tid; idx < NV; idx += NT) {
       const int vr = idx / VZ, vz = idx - vr * VZ;
       const int i = i0 - HVZ + vz, j = j0 - HV + vr;
       sDesc[idx] = inside(i, j) ? __ldg(a.desc + (long long)j * g.P + i) : make_desc(ROW_NONE, ROW_NONE, false, 0);
@@ -945,7 +950,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   }
   // metrics and coordinates of the region (clamped indices: values outside the grid are
   // never used)
-  for (int k = tid; k < SM::NMET; k += STAGE_THREADS) {
+  for (int k = tid; k < SM::NMET; k += NT) {
     double v;
     if (k < SZ) {
       v = __ldg(a.dxidz + min(max(i0 - HSZ + k, 0), Nz - 1));
@@ -966,7 +971,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
 
   // ---- phase 2: S and dilatation on the cross of the S region (reach HS either way);
   // f_sw on the tile
-  for (int idx = tid; idx < NS; idx += STAGE_THREADS) {
+  for (int idx = tid; idx < NS; idx += NT) {
     const int sr = idx / SZ, sz = idx - sr * SZ;
     const bool zarm = sr >= HS && sr < HS + TR && sz >= HSZ - HS && sz < HSZ + TZ + HS;
     const bool rarm = sz >= HSZ && sz < HSZ + TZ;
@@ -1010,12 +1015,12 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   // directly (one rounding per product instead of two stencil passes: the difference is
   // rounding only). General tiles: second derivatives on the arms with each arm point's
   // row, then the tile point's row.
-  constexpr int PPT = (TZ * TR) / STAGE_THREADS;
+  constexpr int PPT = (TZ * TR) / NT;
   R d4z[3][PPT], d4r[3][PPT];
   if constexpr (!GEN) {
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {
-      const int pidx = tid + q * STAGE_THREADS;
+      const int pidx = tid + q * NT;
       const int r = pidx / TZ, c = pidx - r * TZ;
       const int sidx = (HS + r) * SZ + (HSZ + c);
       d4z[0][q] = c9dot<R>(sS + sidx, 1);
@@ -1028,7 +1033,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   } else {
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
-    for (int idx = tid; idx < TR * DZ + DR * TZ; idx += STAGE_THREADS) {
+    for (int idx = tid; idx < TR * DZ + DR * TZ; idx += NT) {
       if (idx < TR * DZ) {
         const int r = idx / DZ, c = idx - r * DZ;  // point (i0 - HF + c, j0 + r)
         const int i = i0 - HF + c, j = j0 + r;
@@ -1057,7 +1062,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {
-      const int pidx = tid + q * STAGE_THREADS;
+      const int pidx = tid + q * NT;
       const int r = pidx / TZ, c = pidx - r * TZ;
       const uint32_t dsc = vdesc((HV + r) * VZ + (HVZ + c));
       const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
@@ -1072,7 +1077,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   // ---- quantities to be filtered (ComputeTobeFilteredQuantities :204-215)
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
-    const int pidx = tid + q * STAGE_THREADS;
+    const int pidx = tid + q * NT;
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
     if (GEN && !inside(i, j)) continue;
@@ -1089,7 +1094,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
 }
 
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(STAGE_THREADS)
+__global__ void __launch_bounds__(sens_threads(GEN))
     sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mV,
                        const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1101,7 +1106,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
 // Batched form: persistent loop over (i0, j0, instance) tiles; kmaps = indices of the
 // V, T and rho maps in each instance's block of nmaps maps.
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(STAGE_THREADS)
+__global__ void __launch_bounds__(sens_threads(GEN))
     sensor_tile_kernel_batch(const SensorArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
                              const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1198,7 +1203,7 @@ static void launch_sensor_tiles(const SensorArgs& a, const SideStream& side, cud
   using SG = SensSmem<SENS_HS_GEN, H_GEN, SIN, R>;
   using SI = SensSmem<SENS_HS_INT, H_INT, SIN, R>;
   if (a.ntiles_gen > 0)
-    sensor_tile_kernel<SENS_HS_GEN, H_GEN, true, SIN, R><<<a.ntiles_gen, STAGE_THREADS, SG::bytes(true),
+    sensor_tile_kernel<SENS_HS_GEN, H_GEN, true, SIN, R><<<a.ntiles_gen, sens_threads(true), SG::bytes(true),
                                                            side.stream ? side.stream : s>>>(a, a.tiles_gen, *a.mv_gen,
                                                                                             *a.mt_gen, *a.mrho);
   if (a.ntiles_int > 0)
@@ -1950,7 +1955,7 @@ static void launch_sensor_tiles_batch(const SensorArgs* argv, const BatchTiles& 
   using SI = SensSmem<SENS_HS_INT, H_INT, SIN, R>;
   if (tgen.ntiles > 0)
     sensor_tile_kernel_batch<SENS_HS_GEN, H_GEN, true, SIN, R>
-        <<<tgen.grid, STAGE_THREADS, SG::bytes(true), side.stream ? side.stream : s>>>(
+        <<<tgen.grid, sens_threads(true), SG::bytes(true), side.stream ? side.stream : s>>>(
             argv, tgen.tiles, tgen.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 1), bmap_sensT(kin, 1), bmap_rho(kin), 0));
   if (tint.ntiles > 0)
     sensor_tile_kernel_batch<SENS_HS_INT, H_INT, false, SIN, R><<<tint.grid, STAGE_THREADS, SI::bytes(false), s>>>(
