@@ -958,9 +958,34 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   // ---- tile classes
   std::vector<int2> tint, tgen, sti, stg;
   auto dsc = [&](int64_t i, int64_t j) { return desc[(size_t)j * h->P + i]; };
-  for (int64_t j0 = 0; j0 < Nr; j0 += TR)
+  // r bands: [0, 8), then bands of TR rows up to 8 rows short of the top, then the rest
+  // in bands of at most TR rows. Interior tiles need a full band; the thin bands along
+  // r = 0 and r = r_max (closure rows, the axis, faces) hold general tiles that own only
+  // their band's rows (the row count is packed into the tile's j0: bits 24-31 hold
+  // TR - rows).
+  std::vector<std::pair<int64_t, int64_t>> bands;
+  {
+    int64_t j = 0;
+    if (Nr > 24) {
+      bands.push_back({0, 8});
+      j = 8;
+    }
+    while (j + TR <= Nr - 8) {
+      bands.push_back({j, TR});
+      j += TR;
+    }
+    while (j < Nr) {
+      const int64_t rows = std::min<int64_t>(TR, Nr - j);
+      bands.push_back({j, rows});
+      j += rows;
+    }
+  }
+  for (const auto& band : bands)
     for (int64_t i0 = 0; i0 < Nz; i0 += TZ) {
-      bool interior = i0 - H_INT >= 0 && i0 + TZ + H_INT <= Nz && j0 - H_INT >= 0 && j0 + TR + H_INT <= Nr;
+      const int64_t j0 = band.first, brows = band.second;
+      const int ytile = (int)j0 | (int)((TR - brows) << 24);
+      bool interior = brows == TR && i0 - H_INT >= 0 && i0 + TZ + H_INT <= Nz && j0 - H_INT >= 0 &&
+                      j0 + TR + H_INT <= Nr;
       for (int64_t j = j0; interior && j < j0 + TR; ++j)
         for (int64_t i = i0; interior && i < i0 + TZ; ++i) {
           uint32_t d = dsc(i, j);
@@ -982,19 +1007,19 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
           uint32_t d = dsc(i, j);
           if (desc_rrow(d) != 4 || desc_blank(d)) interior = false;
         }
-      (interior ? tint : tgen).push_back(make_int2((int)i0, (int)j0));
+      (interior ? tint : tgen).push_back(make_int2((int)i0, interior ? (int)j0 : ytile));
       // sensor classes: S, T and the dilatation are formed on a cross of halo
       // SENS_HS_INT from V_r, V_z stencils of reach H_INT, so every point within
       // SENS_HS_INT of the tile must use centred rows, and the V region must lie inside.
       const int64_t hv = SENS_HS_INT + H_INT, hs = SENS_HS_INT;
-      bool sint = i0 - hz_of((int)hv) >= 0 && i0 + TZ + hz_of((int)hv) <= Nz && j0 - hv >= 0 &&
+      bool sint = brows == TR && i0 - hz_of((int)hv) >= 0 && i0 + TZ + hz_of((int)hv) <= Nz && j0 - hv >= 0 &&
                   j0 + TR + hv <= Nr;
       for (int64_t j = j0 - hs; sint && j < j0 + TR + hs; ++j)
         for (int64_t i = i0 - hs; sint && i < i0 + TZ + hs; ++i) {
           uint32_t d = dsc(i, j);
           if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d)) sint = false;
         }
-      (sint ? sti : stg).push_back(make_int2((int)i0, (int)j0));
+      (sint ? sti : stg).push_back(make_int2((int)i0, sint ? (int)j0 : ytile));
     }
   h->ntiles_int = (int)tint.size();
   h->ntiles_gen = (int)tgen.size();

@@ -255,6 +255,12 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long P = a.g.P, PL = a.g.plane;
   const bool sc = a.c.shock_capturing != 0;
+  // general tiles of a thin r band own only its rows: TR - (bits 24-31 of j0)
+  int nrow = TR;
+  if (GEN) {
+    nrow = TR - (j0 >> 24);
+    j0 &= 0xFFFFFF;
+  }
   // pv_old is needed as a tile in stages 2 and 3 (stage 1 reads it from the state box),
   // the running sum A in stages 3 and 4; interior tiles stage them by TMA
   const bool needU0 = !GEN && (a.stage == 2 || a.stage == 3);
@@ -421,7 +427,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   for (int pidx = tid; pidx < TZ * TR; pidx += STAGE_THREADS) {
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
-    if (GEN && (i >= Nz || j >= Nr)) continue;
+    if (GEN && (i >= Nz || j >= Nr || r >= nrow)) continue;
     const int rr = H + r, rz = HZ + c;
     const int sidx = rr * RZ + rz;
     int zr = 4, rw = 4;
@@ -924,6 +930,12 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   const int tid = threadIdx.x;
   const Grid g = a.g;
   const int Nz = g.Nz, Nr = g.Nr;
+  // general tiles of a thin r band own only its rows: TR - (bits 24-31 of j0)
+  int nrow = TR;
+  if (GEN) {
+    nrow = TR - (j0 >> 24);
+    j0 &= 0xFFFFFF;
+  }
   auto inside = [&](int i, int j) { return i >= 0 && i < Nz && j >= 0 && j < Nr; };
   auto vdesc = [&](int vidx) -> uint32_t { return GEN ? sDesc[vidx] : make_desc(4, 4, false, 0); };
 
@@ -1080,7 +1092,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     const int pidx = tid + q * NT;
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
-    if (GEN && !inside(i, j)) continue;
+    if (GEN && (!inside(i, j) || r >= nrow)) continue;
     const long long o = (long long)j * g.P + i;
     const R dz = R(sDzv[c]), dr = R(sDrv[r]);
     const R rho = R(sRho[r * TZ + c]);
