@@ -235,7 +235,7 @@ template <int H, bool GEN, typename SIN, typename R, int CM>
 __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, const CUtensorMap* mState,
                                            const CUtensorMap* mQ, const CUtensorMap* mU0, const CUtensorMap* mAcc,
                                            const CUtensorMap* mB,
-                                           unsigned char* smem_raw, uint64_t* bar) {
+                                           unsigned char* smem_raw, uint64_t* bar, uint32_t& phase) {
   using SM = StageSmem<H, SIN, R, CM>;
   using RP = typename std::conditional<GEN, double, R>::type;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT, NTP = SM::NTP, HT = SM::HT, RQ = SM::RQ;
@@ -267,14 +267,13 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   const bool needA = !GEN && (a.stage == 3 || a.stage == 4);
 
   // ---- phase 1: one thread issues the TMA loads; the RK operands complete on the
-  // second barrier while phases 1-2 run
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    fence_mbar_init();
-  }
+  // second barrier while phases 1-2 run. The barriers are initialised once per CTA by the
+  // caller; phase bit b is the parity of bar[b]'s next completion. Prior generic-proxy
+  // accesses of the shared buffers (a previous tile of a persistent CTA) are ordered
+  // before the TMA writes by the proxy fence.
   __syncthreads();
   if (tid == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&bar[0], SM::state_bytes + (sc ? SM::q_bytes : 0u));
     tma_load_3d(sU, mState, i0 - HZ, j0 - H, 0, &bar[0]);
     if (sc) tma_load_3d(sQ, mQ, i0 - HZ, j0 - H - HT, 0, &bar[0]);
@@ -310,10 +309,11 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
     sMet[3 * TZ + 2 * TR + r] = __ldg(a.rc + j);
     sMet[3 * TZ + 3 * TR + r] = __ldg(a.invr + j);
   }
-  if (!__syncthreads_and(mbar_wait_bounded(&bar[0], 0))) {
+  if (!__syncthreads_and(mbar_wait_bounded(&bar[0], phase & 1u))) {
     if (tid == 0) atomicOr(a.flags, 4);
     return false;
   }
+  phase ^= 1u;
   // mu = T**0.666 (AssignValues) on the cross of the region (CM_PRE: the coefficient box
   // already holds mu_eff, beta and kappa_eff). With shock capturing the
   // coefficient box holds the z-filtered quantities; the r filter PerformTGfilter(q, 2,
@@ -416,10 +416,11 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
 
   // ---- phase 3: one point per thread per pass
   if (needU0 || needA) {
-    if (!__syncthreads_and(mbar_wait_bounded(&bar[1], 0))) {
+    if (!__syncthreads_and(mbar_wait_bounded(&bar[1], (phase >> 1) & 1u))) {
       if (tid == 0) atomicOr(a.flags, 4);
       return false;
     }
+    phase ^= 2u;
   }
   const double dtv = a.stage > 0 ? *a.dt : 0.0;
   // cos(omega t_s) at this stage's time (harmonic forcing)
@@ -599,8 +600,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
                  const __grid_constant__ CUtensorMap mAcc, const __grid_constant__ CUtensorMap mB) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  uint32_t phase = 0;
   const int2 t0 = tiles[blockIdx.x];
-  stage_body<H, GEN, SIN, R, CM>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, &mB, smem_raw, bar);
+  stage_body<H, GEN, SIN, R, CM>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, &mB, smem_raw, bar, phase);
 }
 
 // Batched form: a persistent grid-stride loop over the tiles (i0, j0, instance) of many
@@ -613,6 +620,13 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ __align__(16) StageArgs sa;
+  // the barriers live across the CTA's tiles: initialised once, phases tracked
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  uint32_t phase = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int4 tt = tiles[t];
     __syncthreads();  // the previous tile is finished with the arguments and the buffers
@@ -621,8 +635,7 @@ __global__ void __launch_bounds__(STAGE_THREADS)
     __syncthreads();
     const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
     if (!stage_body<H, GEN, SIN, R, CM>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, m + kmaps.w, nullptr,
-                                        smem_raw,
-                                         bar))
+                                        smem_raw, bar, phase))
       return;
   }
 }
@@ -906,7 +919,7 @@ __device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
 template <int HS, int HF, bool GEN, typename SIN, typename R>
 __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0, const CUtensorMap* mV,
                                             const CUtensorMap* mT, const CUtensorMap* mRho, unsigned char* smem_raw,
-                                            uint64_t& bar) {
+                                            uint64_t& bar, uint32_t& phase) {
   using SM = SensSmem<HS, HF, SIN, R>;
   constexpr int NT = sens_threads(GEN);
   constexpr int HV = SM::HV, HVZ = SM::HVZ, HSZ = SM::HSZ, VZ = SM::VZ, NV = SM::NV;
@@ -940,13 +953,12 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   auto vdesc = [&](int vidx) -> uint32_t { return GEN ? sDesc[vidx] : make_desc(4, 4, false, 0); };
 
   // ---- phase 1: V_r, V_z on the V region, T on the S region and rho on the tile by
-  // TMA (zero outside the block), descriptors by plain loads meanwhile
-  if (tid == 0) {
-    mbar_init(&bar, 1);
-    fence_mbar_init();
-  }
+  // TMA (zero outside the block), descriptors by plain loads meanwhile. The barrier is
+  // initialised once per CTA by the caller (phase = parity of its next completion); the
+  // proxy fence orders a previous tile's generic accesses before the TMA writes.
   __syncthreads();
   if (tid == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&bar, SM::tx_bytes);
     tma_load_3d(sVr, mV, i0 - HVZ, j0 - HV, 1, &bar);
     tma_load_3d(sVz, mV, i0 - HVZ, j0 - HV, 3, &bar);
@@ -976,10 +988,11 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     }
     sMz[k] = v;
   }
-  if (!__syncthreads_and(mbar_wait_bounded(&bar, 0))) {
+  if (!__syncthreads_and(mbar_wait_bounded(&bar, phase & 1u))) {
     if (tid == 0) atomicOr(a.flags, 4);
     return false;
   }
+  phase ^= 1u;
 
   // ---- phase 2: S and dilatation on the cross of the S region (reach HS either way);
   // f_sw on the tile
@@ -1111,8 +1124,13 @@ __global__ void __launch_bounds__(sens_threads(GEN))
                        const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  uint32_t phase = 0;
   const int2 t0 = tiles[blockIdx.x];
-  sensor_body<HS, HF, GEN, SIN, R>(a, t0.x, t0.y, &mV, &mT, &mRho, smem_raw, bar);
+  sensor_body<HS, HF, GEN, SIN, R>(a, t0.x, t0.y, &mV, &mT, &mRho, smem_raw, bar, phase);
 }
 
 // Batched form: persistent loop over (i0, j0, instance) tiles; kmaps = indices of the
@@ -1124,6 +1142,12 @@ __global__ void __launch_bounds__(sens_threads(GEN))
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ __align__(16) SensorArgs sa;
+  // the barrier lives across the CTA's tiles: initialised once, its phase tracked
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  uint32_t phase = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int4 tt = tiles[t];
     __syncthreads();
@@ -1131,7 +1155,8 @@ __global__ void __launch_bounds__(sens_threads(GEN))
       reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + tt.z)[k];
     __syncthreads();
     const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
-    if (!sensor_body<HS, HF, GEN, SIN, R>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, smem_raw, bar)) return;
+    if (!sensor_body<HS, HF, GEN, SIN, R>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, smem_raw, bar, phase))
+      return;
   }
 }
 
