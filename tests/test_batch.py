@@ -105,3 +105,25 @@ def test_batch_rejects_mixed_kinds():
         axj.AxjBatch(s)
     for x in s:
         x.close()
+
+
+@pytest.mark.gpu
+def test_batch_with_many_tiles_per_cta():
+    """Large instances and one persistent CTA per SM: every CTA loops over many tiles, so
+    its TMA barriers complete many phases (a batch of small test instances gives each CTA
+    about one tile). Three steps must finish and reproduce the individual runs."""
+    cases = fixtures.batch_instances(3, seed=2024, nz_range=(1024, 2048), nr_range=(256, 384))
+    single = _solvers(cases)
+    batched = _solvers(cases)
+    b = axj.AxjBatch(batched)
+    b.set_tuning(tile_order=0, stage_ctas_per_sm=1, sensor_ctas_per_sm=1)
+    b.run(3)
+    for s in single:
+        s.run(3)
+    for k, (s, t) in enumerate(zip(single, batched)):
+        a, r = t.get_state(), s.get_state()
+        errs = [np.abs(a[f] - r[f]).max() / max(np.abs(r[f]).max(), 1e-300) for f in range(5)]
+        assert max(errs) <= 1e-12, (k, errs)
+    b.close()
+    for s in single + batched:
+        s.close()
