@@ -67,7 +67,8 @@ def profile_traffic(case):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms; the summary keeps the
+    samples read between mark_start() and mark_end() (the timed region)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -77,11 +78,18 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self.proc = None
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -90,17 +98,22 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.time(), [x.strip() for x in line.split(",")]))
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
+        time.sleep(0.1)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        rows = [r for t, r in self.rows
+                if self.t0 is None or self.t1 is None or (self.t0 <= t <= self.t1 + 0.06)]
+        if not rows:
+            rows = [r for _, r in self.rows]
+        self.rows = rows
         sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -195,7 +208,8 @@ def workload_config(name, c):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 200 on the GPU; 20 for --impl reference, 1.3 s each on the CPU)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default="jet4400x640")
@@ -205,6 +219,8 @@ def main():
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the timing of the mixed-precision form of the same workload")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.impl == "reference" else 200
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
@@ -241,9 +257,12 @@ def main():
     barrier()
     clocks = ClockSampler(local)
     clocks.start()
+    time.sleep(0.2)  # the sampler is running before the timed region starts
     barrier()
+    clocks.mark_start()
     ms = solver.run_timed(args.steps)
     barrier()
+    clocks.mark_end()
     clk = clocks.stop()
     ms_max = max_over_ranks(ms)
     value = replica_throughput(npts, args.steps, world, ms_max)
