@@ -1041,11 +1041,14 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   // rounding only). General tiles: second derivatives on the arms with each arm point's
   // row, then the tile point's row.
   constexpr int PPT = (TZ * TR) / NT;
+  // point q of a thread: a warp owns PPT consecutive rows of the tile, so a thread's
+  // points are vertically adjacent and share most taps of their r stencils (loaded once)
+  auto ppoint = [](int t, int q) { return (t >> 5) * (TZ * PPT) + q * TZ + (t & 31); };
   R d4z[3][PPT], d4r[3][PPT];
   if constexpr (!GEN) {
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {
-      const int pidx = tid + q * NT;
+      const int pidx = ppoint(tid, q);
       const int r = pidx / TZ, c = pidx - r * TZ;
       const int sidx = (HS + r) * SZ + (HSZ + c);
       d4z[0][q] = c9dot<R>(sS + sidx, 1);
@@ -1087,7 +1090,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < PPT; ++q) {
-      const int pidx = tid + q * NT;
+      const int pidx = ppoint(tid, q);
       const int r = pidx / TZ, c = pidx - r * TZ;
       const uint32_t dsc = vdesc((HV + r) * VZ + (HVZ + c));
       const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
@@ -1102,7 +1105,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   // ---- quantities to be filtered (ComputeTobeFilteredQuantities :204-215)
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
-    const int pidx = tid + q * NT;
+    const int pidx = ppoint(tid, q);
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
     if (GEN && (!inside(i, j) || r >= nrow)) continue;
