@@ -93,7 +93,15 @@ struct axj_handle {
   float4* ds_feat = nullptr;
   float2* ds_targ = nullptr;
   int64_t ds_cap = 0, ds_n = 0;
-  std::vector<double> host_out;  // output-callback staging
+  // output of axj_run (the WriteOutput hook): a device snapshot of the state taken in
+  // stream order, copied to pinned host memory on its own stream while the next steps
+  // run, handed to the callback one output later (or at the end of the run)
+  double* out_snap = nullptr;     // 5 planes (pitch P) + time + flags (device)
+  double* out_host = nullptr;     // 5 * Nz * Nr + time + flags (pinned host)
+  cudaStream_t out_stream = nullptr;
+  cudaEvent_t out_snapped = nullptr, out_copied = nullptr;
+  bool out_pending = false;
+  int64_t out_iter = 0;
   // TMA descriptors: stage-input halo boxes for the stage buffers x {interior, general}
   // tiles, coefficient halo boxes, and tile boxes of pv_old and the running sum A
   CUtensorMap map_state[5][2];
@@ -647,6 +655,13 @@ int launch_step(axj_handle* h) {
   return AXJ_OK;
 }
 
+int flags_status(axj_handle* h, int f) {
+  if (f & 4) return fail(h, AXJ_ERR_TIMEOUT, "a bounded wait on a TMA transfer gave up");
+  if (f & 2) return fail(h, AXJ_ERR_DT_BLOWUP, "Time step blow up (every point blanked, dt == 100)");
+  if (f & 1) return fail(h, AXJ_ERR_NONFINITE, "non-finite value in the solution or time step");
+  return AXJ_OK;
+}
+
 int check_flags(axj_handle* h) {
   int f = 0;
   AXJ_CUDA(h, cudaMemcpyAsync(&f, h->flags, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -768,6 +783,14 @@ void axj_destroy(axj_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->out_stream) {
+    cudaStreamSynchronize(h->out_stream);
+    cudaStreamDestroy(h->out_stream);
+  }
+  if (h->out_snapped) cudaEventDestroy(h->out_snapped);
+  if (h->out_copied) cudaEventDestroy(h->out_copied);
+  if (h->out_snap) cudaFree(h->out_snap);
+  if (h->out_host) cudaFreeHost(h->out_host);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->graph_judge_exec) cudaGraphExecDestroy(h->graph_judge_exec);
@@ -1216,6 +1239,55 @@ int axj_rk4_step(axj_handle* h, double delt) {
   return rc;
 }
 
+namespace {
+// Output of axj_run, first use: snapshot, pinned staging, copy stream and events.
+int out_setup(axj_handle* h) {
+  if (h->out_snap) return AXJ_OK;
+  const size_t n = (size_t)h->Nz * h->Nr * 5;
+  AXJ_CUDA(h, cudaMalloc(&h->out_snap, (5 * (size_t)h->plane + 2) * sizeof(double)));
+  AXJ_CUDA(h, cudaHostAlloc(&h->out_host, (n + 2) * sizeof(double), cudaHostAllocDefault));
+  AXJ_CUDA(h, cudaStreamCreateWithFlags(&h->out_stream, cudaStreamNonBlocking));
+  AXJ_CUDA(h, cudaEventCreateWithFlags(&h->out_snapped, cudaEventDisableTiming));
+  AXJ_CUDA(h, cudaEventCreateWithFlags(&h->out_copied, cudaEventDisableTiming));
+  return AXJ_OK;
+}
+
+// Snapshot of the state, time and flags after the step just enqueued (device copies in
+// stream order), then the copy to pinned host memory on the output stream.
+int out_snapshot(axj_handle* h) {
+  const size_t n = (size_t)h->Nz * h->Nr * 5;
+  double* aux = h->out_snap + 5 * (size_t)h->plane;
+  AXJ_CUDA(h, cudaMemcpyAsync(h->out_snap, h->U0, 5 * (size_t)h->plane * sizeof(double), cudaMemcpyDeviceToDevice,
+                              h->stream));
+  AXJ_CUDA(h, cudaMemcpyAsync(aux, h->time, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  AXJ_CUDA(h, cudaMemcpyAsync(aux + 1, h->flags, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+  AXJ_CUDA(h, cudaEventRecord(h->out_snapped, h->stream));
+  AXJ_CUDA(h, cudaStreamWaitEvent(h->out_stream, h->out_snapped, 0));
+  AXJ_CUDA(h, cudaMemcpy2DAsync(h->out_host, (size_t)h->Nz * sizeof(double), h->out_snap,
+                                (size_t)h->P * sizeof(double), (size_t)h->Nz * sizeof(double), (size_t)h->Nr * 5,
+                                cudaMemcpyDeviceToHost, h->out_stream));
+  AXJ_CUDA(h, cudaMemcpyAsync(h->out_host + n, aux, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->out_stream));
+  AXJ_CUDA(h, cudaEventRecord(h->out_copied, h->out_stream));
+  h->out_pending = true;
+  h->out_iter = h->iteration;
+  return AXJ_OK;
+}
+
+// Hands the pending snapshot to the callback once its copy is complete (or reports the
+// error flags it recorded).
+int out_deliver(axj_handle* h, axj_output_cb cb, void* user) {
+  if (!h->out_pending) return AXJ_OK;
+  h->out_pending = false;
+  AXJ_CUDA(h, cudaEventSynchronize(h->out_copied));
+  const size_t n = (size_t)h->Nz * h->Nr * 5;
+  int f = 0;
+  std::memcpy(&f, h->out_host + n + 1, sizeof(int));
+  if (int rc = flags_status(h, f)) return rc;
+  cb(user, h->out_iter, h->out_host[n], h->out_host);
+  return AXJ_OK;
+}
+}  // namespace
+
 int axj_run(axj_handle* h, int64_t nsteps, int64_t out_every, axj_output_cb cb, void* user, double* last_dt) {
   if (!h) return fail(h, AXJ_ERR_ARG, "null handle");
   if (!h->state_set) return fail(h, AXJ_ERR_ARG, "axj_set_state has not been called");
@@ -1227,18 +1299,22 @@ int axj_run(axj_handle* h, int64_t nsteps, int64_t out_every, axj_output_cb cb, 
     int rc = step_graph(h, false, &ge);  // capture outside the step loop
     if (rc != AXJ_OK) return rc;
   }
+  h->out_pending = false;
   for (int64_t s = 0; s < nsteps; ++s) {
     int rc = launch_step(h);
     if (rc != AXJ_OK) return rc;
     if (out_every > 0 && cb && (h->iteration % out_every == 0)) {
-      int rc = check_flags(h);
+      // the previous output reaches the callback now (its copy ran beside the steps
+      // since); this one is snapshot and copied while the next steps run
+      rc = out_deliver(h, cb, user);
+      if (rc == AXJ_OK) rc = out_setup(h);
+      if (rc == AXJ_OK) rc = out_snapshot(h);
       if (rc != AXJ_OK) return rc;
-      h->host_out.resize((size_t)h->Nz * h->Nr * 5);
-      AXJ_CUDA(h, d2h(h, h->host_out.data(), h->U0, 5));
-      AXJ_CUDA(h, cudaMemcpyAsync(&h->time_host, h->time, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-      AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
-      cb(user, h->iteration, h->time_host, h->host_out.data());
     }
+  }
+  if (cb) {
+    int rc = out_deliver(h, cb, user);
+    if (rc != AXJ_OK) return rc;
   }
   double dlast = 0.0;
   AXJ_CUDA(h, cudaMemcpyAsync(&dlast, h->dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));

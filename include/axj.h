@@ -159,8 +159,13 @@ int axj_rk4_step(axj_handle* h, double delt);
 /* nsteps x (ComputeTimeStep + RK4) with dt kept on the device, no host sync
  * inside; the step sequence is captured once in a CUDA graph and replayed.
  * If out_every > 0 and cb != NULL, cb(user, iteration, time, pv) is called with a
- * host copy of the state every out_every iterations (the noutput hook,
- * ModRungeKutta.f90:161-165). last_dt (nullable) receives the last dt used. */
+ * host copy of the state of every out_every-th iteration (the noutput hook,
+ * ModRungeKutta.f90:161-165). The state is copied on the device in step order and
+ * brought to pinned host memory on a second stream while the following steps run; the
+ * callback for an output runs when the next output is taken or before axj_run returns,
+ * in order, and pv is valid only during the callback. A step that left a non-finite
+ * value or a dt blow-up makes the delivery of its output return the error instead.
+ * last_dt (nullable) receives the last dt used. */
 typedef void (*axj_output_cb)(void* user, int64_t iteration, double time, const double* pv);
 int axj_run(axj_handle* h, int64_t nsteps, int64_t out_every, axj_output_cb cb, void* user,
             double* last_dt);

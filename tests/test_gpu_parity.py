@@ -129,6 +129,47 @@ def test_run_output_callback(oracle_mod):
     assert seen[-1][1] == dev.get_time()[1]
 
 
+def test_run_outputs_equal_the_stepped_states():
+    """The outputs of axj_run (device snapshot, copy on a second stream while the next
+    steps run, callback one output later) are the states of those iterations exactly."""
+    c = CASES["jet_sc"]()
+    patches = axj.patches_from_records(c["records"], c["Nz"], c["Nr"])
+    a = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+    b = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+    a.set_state(c["pv"], c["target"])
+    b.set_state(c["pv"], c["target"])
+    seen = []
+    a.run(9, out_every=3, callback=lambda it, t, pv: seen.append((it, t, pv)))
+    assert [s[0] for s in seen] == [3, 6, 9]
+    for it, t, pv in seen:
+        b.run(3)
+        assert b.get_time() == (it, t)
+        assert np.array_equal(pv, b.get_state())
+    a.close()
+    b.close()
+
+
+def test_restart_round_trip():
+    """Restart (ModSolver.f90:103-106): a run continued from a written state, its
+    iteration and time equals the uninterrupted run. With the physical dt the step
+    depends on nothing else (the stale-T dt of the reference restarts from T = 0, as
+    the reference's module scalar does)."""
+    c = CASES["jet_forcing_physdt"]()
+    patches = axj.patches_from_records(c["records"], c["Nz"], c["Nr"])
+    full = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+    full.set_state(c["pv"], c["target"])
+    saved = []
+    full.run(8, out_every=4, callback=lambda it, t, pv: saved.append((it, t, pv)))
+    it4, t4, pv4 = saved[0]
+    rest = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
+    rest.set_state(pv4, c["target"], iteration=it4, time=t4)
+    rest.run(4)
+    assert rest.get_time() == full.get_time()
+    assert np.array_equal(rest.get_state(), full.get_state())
+    full.close()
+    rest.close()
+
+
 def test_multistep_jet512x128(oracle_mod):
     """configs[0]-sized run: 100 RK4 steps, relative L2 error per field."""
     c = fixtures.case("jet512x128")
