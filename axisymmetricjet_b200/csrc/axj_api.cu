@@ -72,6 +72,9 @@ struct axj_handle {
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_judge_exec = nullptr;  // learned sensor: the judge step
+  // RK4 alone (dt from the host: axj_rk4_step), plain and judge step
+  cudaGraphExec_t graph_rk4_exec[2] = {nullptr, nullptr};
+  cudaGraph_t graph_rk4[2] = {nullptr, nullptr};
   cudaGraph_t graph_judge = nullptr;
   // learned sensor
   double S1[9][6];              // SBP first-derivative rows (feature stencils)
@@ -639,6 +642,37 @@ int step_graph(axj_handle* h, bool judge, cudaGraphExec_t* out) {
   return AXJ_OK;
 }
 
+// The captured graphs hold the model's normalisation by value: a new model (or new
+// statistics) drops them, and the next step captures them again.
+void drop_graphs(axj_handle* h) {
+  cudaStreamSynchronize(h->stream);
+  cudaGraphExec_t* ex[4] = {&h->graph_exec, &h->graph_judge_exec, &h->graph_rk4_exec[0], &h->graph_rk4_exec[1]};
+  cudaGraph_t* gr[4] = {&h->graph, &h->graph_judge, &h->graph_rk4[0], &h->graph_rk4[1]};
+  for (int k = 0; k < 4; ++k) {
+    if (*ex[k]) cudaGraphExecDestroy(*ex[k]);
+    if (*gr[k]) cudaGraphDestroy(*gr[k]);
+    *ex[k] = nullptr;
+    *gr[k] = nullptr;
+  }
+}
+
+// Captured RK4 stages alone (the dt the host passed to axj_rk4_step is on the device).
+int rk4_graph(axj_handle* h, bool judge, cudaGraphExec_t* out) {
+  const int k = judge ? 1 : 0;
+  if (!h->graph_rk4_exec[k]) {
+    AXJ_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_rk4(h, judge);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc != AXJ_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(h, AXJ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    h->graph_rk4[k] = g;
+    AXJ_CUDA(h, cudaGraphInstantiate(&h->graph_rk4_exec[k], g, 0));
+  }
+  *out = h->graph_rk4_exec[k];
+  return AXJ_OK;
+}
+
 // One graph-launched step; advances the iteration counter.
 int launch_step(axj_handle* h) {
   if (int rc = check_model(h)) return rc;
@@ -795,6 +829,10 @@ void axj_destroy(axj_handle* h) {
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->graph_judge_exec) cudaGraphExecDestroy(h->graph_judge_exec);
   if (h->graph_judge) cudaGraphDestroy(h->graph_judge);
+  for (int k = 0; k < 2; ++k) {
+    if (h->graph_rk4_exec[k]) cudaGraphExecDestroy(h->graph_rk4_exec[k]);
+    if (h->graph_rk4[k]) cudaGraphDestroy(h->graph_rk4[k]);
+  }
   for (void* p : h->allocs) cudaFree(p);
   if (h->ds_feat) cudaFree(h->ds_feat);
   if (h->ds_targ) cudaFree(h->ds_targ);
@@ -1225,8 +1263,11 @@ int axj_rk4_step(axj_handle* h, double delt) {
   h->time_end = h->time_host + delt;
   AXJ_CUDA(h, cudaMemcpyAsync(h->time, &h->time_end, sizeof(double), cudaMemcpyHostToDevice, h->stream));
   const bool judge = judge_due(h);
-  int rc = enqueue_rk4(h, judge);
+  // the stages replay a captured graph (one launch instead of some thirty)
+  cudaGraphExec_t ge = nullptr;
+  int rc = rk4_graph(h, judge, &ge);
   if (rc != AXJ_OK) return rc;
+  AXJ_CUDA(h, cudaGraphLaunch(ge, h->stream));
   if (judge) {
     h->judged = true;
     h->njudges += 1;
@@ -1695,6 +1736,7 @@ int axj_mlp_set(axj_handle* h, const axj_mlp* m) {
     if (!std::isfinite(m->out_scale[k])) return fail(h, AXJ_ERR_ARG, "out_scale[%d] is not finite", k);
   AXJ_CUDA(h, cudaSetDevice(h->device));
   std::vector<float> flat;
+  drop_graphs(h);
   mlp_to_flat(m, flat, &h->norm);
   AXJ_CUDA(h, cudaMemcpyAsync(h->mlp, flat.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, h->stream));
   AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1833,6 +1875,7 @@ int axj_mlp_train(axj_handle* h, const axj_train_cfg* cfg, float* loss) {
       const double rms = std::sqrt(a[8 + k] / n);
       h->norm.out_scale[k] = (float)(rms > 1e-30 ? rms : 1.0);
     }
+    drop_graphs(h);
   }
   TrainWs w;
   AXJ_CUDA(h, w.alloc((int)cfg->batch, (int)std::max<int64_t>(cfg->steps, 1)));

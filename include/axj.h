@@ -153,7 +153,9 @@ int axj_get_time(axj_handle* h, int64_t* iteration, double* time);
 /* ComputeTimeStep (ModInputOutput.f90:389-438): global CFL/viscous dt. */
 int axj_compute_dt(axj_handle* h, double* delt);
 
-/* RK4 (ModRungeKutta.f90:5-171) with the given delt; advances iteration and time. */
+/* RK4 (ModRungeKutta.f90:5-171) with the given delt; advances iteration and time. The
+ * four stages replay a CUDA graph captured on the first call (a second one for the
+ * learned sensor's judge steps); a new model (axj_mlp_set, training) drops the graphs. */
 int axj_rk4_step(axj_handle* h, double delt);
 
 /* nsteps x (ComputeTimeStep + RK4) with dt kept on the device, no host sync
