@@ -11,12 +11,17 @@ so cases are generated from their published shapes:
 * small test cases of the same construction, and a nozzle case with a blanked
   lip and no-slip wall patches laid out like the reference's own nozzle bc file
   (bc_4400x640_nozzle.dat, WriteMeshAndSoln/write_soln_file.f90:223-257).
+* the case of the reference's own generator (WriteMeshAndSoln/write_soln_file.f90):
+  its stretched 250 x 50 grid, blanked lip, bc file and initial condition, restated
+  operation for operation (writemesh_case).
 
 Initial condition: V_z = U_j/2 (1 + tanh((0.5D - r)/(2*0.05D))), V_r = V_theta = 0,
 T from Crocco-Busemann (write_soln_file.f90:68-72), rho = 1/T (p = rho T = 1), plus a
 seeded Gaussian perturbation of amplitude 1e-3 U_j on V_r and V_z where |r-0.5D| < 0.2D.
 The target (pv_target) is the unperturbed profile.
 """
+import math
+
 import numpy as np
 
 from ._ffi import AXIS, NSCBC_NONREFLECTING, NSCBC_NOSLIP_WALL, SAT_FARFIELD, SAT_NOSLIP_WALL, default_params
@@ -101,6 +106,117 @@ def nozzle_case(Nz=96, Nr=64, zmax=30.0, rmax=15.0, Mj=0.9, Re=1000.0, iw=20, jb
     ib[jb:jt - 1, :iw - 1] = 0.0  # rows jb+1..jt-1, columns 1..iw-1 (1-based) are inside the lip
     return make_case(Nz, Nr, zmax, rmax, Mj, Re, sc=sc, seed=seed, records=nozzle_records(iw, jb, jt, wall),
                      ibval=ib, **pkw)
+
+
+def _stretched(i, n, delta, pos, cmin, cmax):
+    """compute_coord_val (WriteMeshAndSoln/write_soln_file.f90:102-123): a tanh-stretched
+    coordinate clustered at cmin + pos. xi = float(i)/float(n) is a default-REAL (single
+    precision) division and 1.0 - xi a single-precision difference, as in the Fortran;
+    the rest is double precision."""
+    f32 = np.float32
+    pos1 = pos / (cmax - cmin)
+    xi = f32(i) / f32(n)
+    u1 = math.tanh(delta * float(f32(1.0) - xi)) * (1.0 - pos1)
+    u2 = (2.0 - math.tanh(delta * float(xi))) * pos1
+    fac = 1.0 - ((u1 + u2) - pos1)
+    return cmin + fac * (cmax - cmin)
+
+
+def writemesh_grid(nx=150, ny=50, n_wall_zone=100):
+    """create_AxiJet_CartGrid (write_soln_file.f90:125-217): the z coordinate of the
+    first nx columns up to the first one beyond z = 11 (ipos2), a second stretching from
+    11 to 15 over the wall zone from ipos2 on, the r coordinate, and iblank = 0 inside
+    the nozzle lip (1 < r < 1.05, z < 6). Returns (z, r, iblank[Nr, Nz]) with 1-based
+    quantities of the Fortran turned into 0-based arrays."""
+    Nz = nx + n_wall_zone
+    z = np.zeros(Nz)
+    ipos2 = None
+    for i in range(1, nx + 1):
+        xval = _stretched(i, nx, 3.0, 6.0, 0.0, 15.0)
+        if xval > 11.0:
+            ipos2 = i
+            break
+        z[i - 1] = xval
+    if ipos2 is None:
+        raise ValueError("the first stretching never passes z = 11")
+    for i in range(ipos2, Nz + 1):
+        z[i - 1] = _stretched(i - ipos2, Nz - ipos2, 2.0, 3.0, 11.0, 15.0)
+    r = np.array([_stretched(j, ny, 6.0, 1.0, 0.0, 15.0) for j in range(1, ny + 1)])
+    lip = (r[:, None] > 1.0) & (r[:, None] < 1.05) & (z[None, :] < 6.0)
+    iblank = np.where(lip, 0.0, 1.0)
+    return z, r, iblank
+
+
+def writemesh_records(z, r):
+    """The bc file written by create_AxiJet_CartGrid (write_soln_file.f90:219-255):
+    jbottom = the last row at or below r = 1, jtop = the first row at or above r = 1.05,
+    iright = the first column at or beyond z = 6 (all 1-based), no-slip NSCBC walls
+    around the lip and at the outflow, a non-reflecting top and the axis."""
+    jbottom = int(np.nonzero(r > 1.0)[0][0])          # first 1-based j with r > 1, minus 1
+    jtop = int(np.nonzero(r < 1.05)[0][-1]) + 2       # last 1-based j with r < 1.05, plus 1
+    iright = int(np.nonzero(z < 6.0)[0][-1]) + 2      # last 1-based i with z < 6, plus 1
+    return [
+        (SAT_FARFIELD, 1, 1, 1, 1, jbottom),
+        (NSCBC_NOSLIP_WALL, -2, 1, iright, jbottom, jbottom),
+        (NSCBC_NOSLIP_WALL, 1, iright, iright, jbottom, jtop),
+        (NSCBC_NOSLIP_WALL, 2, 1, iright, jtop, jtop),
+        (SAT_FARFIELD, 1, 1, 1, jtop, -1),
+        (NSCBC_NONREFLECTING, -2, 1, -1, -1, -1),
+        (NSCBC_NOSLIP_WALL, -1, -1, -1, 1, -1),
+        (AXIS, 2, 1, -1, 1, 1),
+    ]
+
+
+def write_bc_file(path, records):
+    """A bc file in the layout create_AxiJet_CartGrid writes (write_soln_file.f90:246-255):
+    per row grid, bc, dir, istart, iend, jstart, jend, kstart, kend as '(9(I0,2X))'."""
+    with open(path, "w") as f:
+        for bc, d, i0, i1, j0, j1 in records:
+            f.write("".join("%d  " % v for v in (1, bc, d, i0, i1, j0, j1, 1, 1)) + "\n")
+
+
+def writemesh_solution(z, r, Mj=0.8, Tj_Tinf=0.6, gam=1.4):
+    """The initial condition of write_soln_file.f90:44-90 as pv[5, Nr, Nz]: a tanh jet
+    of radius 1 (theta = 0.1, a default-REAL literal stored in a double), decaying as
+    (z - 5)**-1.5 beyond z = 6, zero velocity beyond r = 1, density from the
+    Crocco-Busemann relation and T = 1/rho."""
+    theta = float(np.float32(0.1))
+    Uj = Mj * math.pow(Tj_Tinf, 0.5)
+    Nz, Nr = z.shape[0], r.shape[0]
+    # libm tanh and pow per value, as the Fortran calls them
+    u = np.array([0.5 * (1.0 - math.tanh(1.0 / (4.0 * theta) * (rj - 1.0 / rj))) for rj in r])
+    u = 2.0 * u - 1.0
+    uu = np.broadcast_to(u[:, None], (Nr, Nz)).copy()
+    decay = np.array([math.pow(zi - 6.0 + 1.0, 1.5) if zi > 6.0 else 1.0 for zi in z])
+    far = z > 6.0
+    uu[:, far] = uu[:, far] / decay[far][None, :]
+    uu[r > 1.0, :] = 0.0
+    term1 = 0.5 * (gam - 1.0) * uu * (1.0 - uu) * (Mj * Mj)
+    term3 = (1.0 / Tj_Tinf) * (1.0 - uu)
+    rho = (1.0 / ((term1 + uu) + term3)) / Tj_Tinf
+    pv = np.zeros((5, Nr, Nz))
+    pv[0] = rho
+    pv[3] = uu * Uj
+    pv[4] = 1.0 / rho
+    return pv
+
+
+def writemesh_case(sc=False, **pkw):
+    """The case WriteMeshAndSoln generates (write_soln_file.f90:1-265): the 250 x 50
+    stretched grid with the blanked nozzle lip, its bc file and its initial condition,
+    which is also the target (the reference reads the one solution file for both).
+    pkw go to the parameters (reference defaults otherwise)."""
+    z, r, ib = writemesh_grid()
+    Nz, Nr = z.shape[0], r.shape[0]
+    kw = dict(pkw)
+    if sc:
+        kw = dict(shock_capturing=1, **SC_COEFFS, **kw)
+    pv = writemesh_solution(z, r)
+    return dict(Nz=Nz, Nr=Nr, z=z, r=r,
+                zvec=np.ascontiguousarray(np.broadcast_to(z[None, :], (Nr, Nz))),
+                rvec=np.ascontiguousarray(np.broadcast_to(r[:, None], (Nr, Nz))),
+                ibval=np.ascontiguousarray(ib), records=writemesh_records(z, r), params=default_params(**kw),
+                pv=np.ascontiguousarray(pv), target=pv.copy(), Mj=0.8)
 
 
 CASES = {

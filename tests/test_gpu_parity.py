@@ -36,6 +36,9 @@ CASES = {
         "jet96x64", control_forcing=1, forcing_z0=3.0, forcing_r0=0.5, forcing_lz=1.0, forcing_lr=0.3,
         forcing_mat=np.arange(25.0).reshape(5, 5) * 1e-3, dt_mode=1),
     "jet_ragged": lambda: fixtures.make_case(77, 45, 30.0, 15.0, 0.9, 1000.0),
+    # the reference generator's case: stretched z and r, blanked lip, NSCBC wall outflow
+    "writemesh": lambda: fixtures.writemesh_case(),
+    "writemesh_sc": lambda: fixtures.writemesh_case(sc=True, Re=5000.0),
     # harmonic inflow forcing (control_forcing = 2), the batched instances' forcing
     "jet_harmonic": lambda: fixtures.case(
         "jet96x64", control_forcing=2, forcing_z0=1.0, forcing_r0=0.5, forcing_lz=0.5, forcing_lr=0.2,
@@ -54,7 +57,7 @@ def pair(c, oracle_mod):
     return dev, ora
 
 
-@pytest.mark.parametrize("name", ["nozzle_nscbc_wall", "jet_ragged"])
+@pytest.mark.parametrize("name", ["nozzle_nscbc_wall", "jet_ragged", "writemesh"])
 def test_operators(oracle_mod, name):
     c = CASES[name]()
     dev, ora = pair(c, oracle_mod)
@@ -80,7 +83,7 @@ def test_rhs(oracle_mod, name):
     assert max(errs) < REL, errs
 
 
-@pytest.mark.parametrize("name", ["jet_sc", "nozzle_sat_wall_sc"])
+@pytest.mark.parametrize("name", ["jet_sc", "nozzle_sat_wall_sc", "writemesh_sc"])
 def test_sensor(oracle_mod, name):
     c = CASES[name]()
     dev, ora = pair(c, oracle_mod)
@@ -180,3 +183,18 @@ def test_multistep_jet512x128(oracle_mod):
     for k in (0, 1, 3, 4):
         l2 = np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k])
         assert l2 < 1e-11, (k, l2)
+
+
+def test_multistep_writemesh(oracle_mod):
+    """The reference generator's case with shock capturing: 60 RK4 steps (graph-run on
+    the device), relative L2 error per field."""
+    c = CASES["writemesh_sc"]()
+    dev, ora = pair(c, oracle_mod)
+    dev.run(60)
+    ora.run(60)
+    a, b = dev.get_state(), ora.get_state()
+    for k in (0, 1, 3, 4):
+        l2 = np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k])
+        assert l2 < 1e-11, (k, l2)
+    (itd, td), (ito, to) = dev.get_time(), ora.get_time()
+    assert itd == ito == 60 and abs(td - to) <= 1e-12 * to

@@ -33,6 +33,7 @@ CASES = {
     "jet_sc": lambda **kw: fixtures.case("jet96x64sc", **kw),
     "nozzle_sat_wall_sc": lambda **kw: fixtures.nozzle_case(wall=SAT_NOSLIP_WALL, sc=True, Mj=1.5, Re=5000.0, **kw),
     "jet_ragged": lambda **kw: fixtures.make_case(77, 45, 30.0, 15.0, 0.9, 1000.0, **kw),
+    "writemesh_sc": lambda **kw: fixtures.writemesh_case(sc=True, Re=5000.0, **kw),
 }
 
 
