@@ -139,13 +139,14 @@ __device__ __forceinline__ float gelu_grad_f(float x) {
 // ---------------------------------------------------------------------------
 // Feature channels
 // ---------------------------------------------------------------------------
-// Tile of 32 (z) x 8 (r) points per CTA (256 threads). rho, V_r, V_z of the tile and
-// a halo of 5 (the widest SBP boundary row reaches 5 points) are staged in shared
-// memory as FP32 (zero outside the grid, the never-written halo); each thread forms
-// its six first derivatives in FP32 on differences from its own value: every SBP row
-// sums to zero, so sum c_m (f_m - f_0) equals sum c_m f_m, and the differences of
-// nearby values are exact in FP32 (the network reads its inputs in BF16).
-constexpr int FT_Z = 32, FT_R = 8, FT_H = 5;
+// Tile of 32 (z) x 16 (r) points per CTA (256 threads, two points per thread: rows
+// tr and tr + 8). rho, V_r, V_z of the tile and a halo of 5 (the widest SBP boundary row
+// reaches 5 points) are staged in shared memory as FP32 (zero outside the grid, the
+// never-written halo), one box row per warp and pass; each thread forms its six first
+// derivatives in FP32 on differences from its own value: every SBP row sums to zero, so
+// sum c_m (f_m - f_0) equals sum c_m f_m, and the differences of nearby values are exact
+// in FP32 (the network reads its inputs in BF16).
+constexpr int FT_Z = FEAT_TILE_Z, FT_R = FEAT_TILE_R, FT_H = 5;
 constexpr int FB_Z = FT_Z + 2 * FT_H, FB_R = FT_R + 2 * FT_H;
 
 __device__ __forceinline__ float fd1s(const FeatArgs& a, const float* box, int row, int bz, int br, int dirn) {
@@ -166,23 +167,10 @@ __device__ __forceinline__ float fd1s(const FeatArgs& a, const float* box, int r
   return s;
 }
 
-template <typename SIN>
-__device__ __forceinline__ void features_body(const FeatArgs& a, int i0, int j0, float (*sb)[FB_R * FB_Z]) {
+// The four channels of point (i, j) = (i0 + tz, j0 + tr) from the staged box.
+__device__ __forceinline__ void features_point(const FeatArgs& a, float (*sb)[FB_R * FB_Z], int i, int j, int tz,
+                                               int tr) {
   const Grid g = a.g;
-  const SIN* U = static_cast<const SIN*>(a.U);
-  const int fld[3] = {0, 1, 3};  // rho, V_r, V_z
-  for (int e = threadIdx.x; e < 3 * FB_R * FB_Z; e += 256) {
-    const int f = e / (FB_R * FB_Z), q = e - f * (FB_R * FB_Z);
-    const int br = q / FB_Z, bz = q - br * FB_Z;
-    const int i = i0 - FT_H + bz, j = j0 - FT_H + br;
-    float v = 0.0f;
-    if (i >= 0 && i < g.Nz && j >= 0 && j < g.Nr) v = float(U[fld[f] * g.plane + (long long)j * g.P + i]);
-    sb[f][q] = v;
-  }
-  __syncthreads();
-  const int tz = threadIdx.x & 31, tr = threadIdx.x >> 5;
-  const int i = i0 + tz, j = j0 + tr;
-  if (i >= g.Nz || j >= g.Nr) return;
   const long long o = (long long)j * g.P + i;
   const uint32_t dsc = __ldg(a.desc + o);
   const int zr = desc_blank(dsc) ? (int)ROW_NONE : desc_zrow(dsc);
@@ -205,12 +193,46 @@ __device__ __forceinline__ void features_body(const FeatArgs& a, int i0, int j0,
 }
 
 template <typename SIN>
+__device__ __forceinline__ void features_body(const FeatArgs& a, int i0, int j0, float (*sb)[FB_R * FB_Z]) {
+  const Grid g = a.g;
+  const SIN* Urho = static_cast<const SIN*>(a.U);  // planes 0 (rho), 1 (V_r), 3 (V_z)
+  const SIN* Uvr = Urho + g.plane;
+  const SIN* Uvz = Urho + 3 * g.plane;
+  const int tz = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int br = w; br < FB_R; br += 8) {
+    const int j = j0 - FT_H + br;
+    const bool jin = j >= 0 && j < g.Nr;
+    const long long ro = (long long)j * g.P;
+    for (int bz = tz; bz < FB_Z; bz += 32) {
+      const int i = i0 - FT_H + bz;
+      float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+      if (jin && i >= 0 && i < g.Nz) {
+        v0 = float(Urho[ro + i]);
+        v1 = float(Uvr[ro + i]);
+        v2 = float(Uvz[ro + i]);
+      }
+      const int q = br * FB_Z + bz;
+      sb[0][q] = v0;
+      sb[1][q] = v1;
+      sb[2][q] = v2;
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int tr = w; tr < FT_R; tr += 8) {
+    const int i = i0 + tz, j = j0 + tr;
+    if (i >= g.Nz || j >= g.Nr) continue;
+    features_point(a, sb, i, j, tz, tr);
+  }
+}
+
+template <typename SIN>
 __global__ void __launch_bounds__(256) features_kernel(const FeatArgs a) {
   __shared__ float sb[3][FB_R * FB_Z];
   features_body<SIN>(a, blockIdx.x * FT_Z, blockIdx.y * FT_R, sb);
 }
 
-// Batched: persistent loop over (i0, j0, instance) tiles of 32 x 8 points.
+// Batched: persistent loop over (i0, j0, instance) tiles of 32 x 16 points.
 __global__ void __launch_bounds__(256) features_kernel_batch(const FeatArgs* __restrict__ argv,
                                                              const int4* __restrict__ tiles, int ntiles) {
   __shared__ float sb[3][FB_R * FB_Z];

@@ -83,7 +83,7 @@ cudaError_t launch_features_batch(const FeatArgs* argv, const int4* tiles, int n
 cudaError_t launch_mlp_infer_batch(const InferArgs& a0, const InferArgs* argv, const int4* tiles, int ntiles,
                                    cudaStream_t s);
 cudaError_t launch_judge_batch(const JudgeArgs* argv, int ninst, long long max_pts, cudaStream_t s);
-constexpr int FEAT_TILE_Z = 32, FEAT_TILE_R = 8;
+constexpr int FEAT_TILE_Z = 32, FEAT_TILE_R = 16;
 constexpr int MLP_TILE_Z = 32, MLP_TILE_R = 4;
 cudaError_t launch_mlp_infer(const InferArgs& a, cudaStream_t s);
 cudaError_t launch_judge(const JudgeArgs& a, cudaStream_t s);
