@@ -69,6 +69,7 @@ def load_library():
         "axj_last_error": (C.c_char_p, [h]),
         "axj_destroy": (None, [h]),
         "axj_read_bc_file": (C.c_int, [C.c_char_p, C.POINTER(AxjBcRecord), i64, C.POINTER(i64)]),
+        "axj_operator_tables": (C.c_int, [dp, dp, dp]),
         "axj_patches_from_records": (C.c_int, [C.POINTER(AxjBcRecord), i64, i64, i64, C.POINTER(AxjPatch),
                                                C.POINTER(i64)]),
         "axj_version": (C.c_char_p, []),
@@ -110,6 +111,15 @@ def _check(lib, h, rc):
     if rc != AXJ_OK:
         msg = lib.axj_last_error(h)
         raise AxjError(rc, msg.decode() if msg else "")
+
+
+def operator_tables():
+    """(SBP1 [9, 6], SBP2 [9, 6], TGfilt [9, 11]) as the device kernels use them
+    (ModOperator.f90:5-121)."""
+    lib = load_library()
+    s1, s2, tg = np.empty((9, 6)), np.empty((9, 6)), np.empty((9, 11))
+    _check(lib, None, lib.axj_operator_tables(dptr(s1), dptr(s2), dptr(tg)))
+    return s1, s2, tg
 
 
 def read_bc_file(path):

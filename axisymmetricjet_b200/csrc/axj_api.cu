@@ -715,6 +715,16 @@ void set_global_error(const char* msg) { g_create_error = msg; }
 
 extern "C" {
 
+int axj_operator_tables(double* sbp1, double* sbp2, double* tgfilt) {
+  if (!sbp1 || !sbp2 || !tgfilt) return fail(nullptr, AXJ_ERR_ARG, "null argument");
+  double S1[9][6], S2[9][6], G[9][11];
+  build_tables(S1, S2, G);
+  std::memcpy(sbp1, S1, sizeof(S1));
+  std::memcpy(sbp2, S2, sizeof(S2));
+  std::memcpy(tgfilt, G, sizeof(G));
+  return AXJ_OK;
+}
+
 void axj_default_params(axj_params* p) {
   if (!p) return;
   std::memset(p, 0, sizeof(*p));

@@ -345,6 +345,11 @@ int axj_read_bc_file(const char* path, axj_bc_record* records, int64_t max_recor
 int axj_patches_from_records(const axj_bc_record* records, int64_t nrecords, int64_t Nz_grid,
                              int64_t Nr_grid, axj_patch* patches, int64_t* npatch);
 
+/* The operator tables the device kernels use, as SBP_operator forms them
+ * (ModOperator.f90:5-121): SBP1(0:8,0:5) and SBP2(0:8,0:5) into sbp1[54] and sbp2[54],
+ * TGfilt(0:8,0:10) into tgfilt[99], row-major (row = the SBP row). */
+int axj_operator_tables(double* sbp1, double* sbp2, double* tgfilt);
+
 /* Library build information, e.g. "axj 0.1 sm_100a". */
 const char* axj_version(void);
 
