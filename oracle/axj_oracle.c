@@ -7,6 +7,22 @@
  * ProcessorCommunication is a no-op). It is used only by tests/, by the smoke check and
  * by bench.py's CPU baseline, as the checker. The product (libaxj.so) never calls it.
  *
+ * Decomposition replica (axo_set_decomposition): the numerics of the reference run on a
+ * dims_z x dims_r process grid (ModDecomp.f90:5-105), on the same global arrays. Every
+ * operator reads halo cells that ProcessorCommunication refreshed just before it
+ * (ModRHS.f90:20-51, ModShockCapturing.f90:23-76, ModSolver.f90:56-73), so a
+ * decomposed run equals the single block except where a rank's own loops use its local
+ * extent or its own module state:
+ *  - the in-place z filter restarts at every block start from the neighbour's
+ *    unfiltered values (exchanged at ModShockCapturing.f90:58-60, filtered at :63);
+ *  - the stale scalar T is per rank (ModRHS.f90:76,145 set it at the block's last
+ *    point, the rank's face loops override it) and dt is the MIN over ranks
+ *    (ModInputOutput.f90:405-422);
+ *  - the top sponge divides by r at the block's last row (ModBC.f90:571);
+ *  - deltaz / deltar are one-sided at the block's edges (ModShockCapturing.f90:169-186);
+ *  - the block's first row takes the axis form of the dilatation and of S22
+ *    (ModShockCapturing.f90:114-118, :146-150, :188-192).
+ *
  * PARITY STATUS: unpinned against reference outputs. The reference ships no tests or
  * golden vectors and its Fortran cannot be compiled in this image (no gfortran/flang).
  * The restatement is pinned instead by operator known-answer tests (polynomial
@@ -56,13 +72,18 @@ typedef struct axo {
   I8 *is_it_i_patch, *which_i_patch, *is_it_j_patch, *which_j_patch;
   axj_patch* patch;
   I8 no_bcs;
-  double T;       /* the module scalar T (ModuleVariables.f90:53) */
+  /* decomposition replica: blocks along z and r, block of each i and j, block ranges
+     (1-based, inclusive), and each block's module scalar T (ModuleVariables.f90:53) */
+  I8 nbz, nbr;
+  I8 *bz, *br, *zlo, *zhi, *rlo, *rhi;
+  double* Tb;
   double delt, time;
   double t_stage;  /* time of the current RHS evaluation (harmonic forcing) */
   I8 iteration;
 } axo;
 
 #define HIX(o, i, j) ((size_t)((i) + 3) + (size_t)((j) + 3) * (size_t)(o)->LZ)
+#define BLK(o, i, j) ((o)->bz[i] + (o)->nbz * (o)->br[j])
 #define H(o, a, i, j) ((o)->a[HIX(o, i, j)])
 #define IIX(o, i, j) ((size_t)((i)-1) + (size_t)((j)-1) * (size_t)(o)->Nz)
 #define S5(o, a, i, j, e) ((o)->a[IIX(o, i, j) + (size_t)((e)-1) * (size_t)(o)->Nz * (size_t)(o)->Nr])
@@ -232,6 +253,33 @@ static void compute_metric(axo* o, const double* var, int dirn, double* out) {
  * z pass is the in-place recurrence of ModShockCapturing.f90:63 and runs in the
  * reference's loop order (i outer, j inner); rows j are independent of each other. */
 static void tgfilter(axo* o, const double* var, int dirn, double* out) {
+  if (dirn == 1 && var == out && o->nbz > 1) {
+    /* decomposed in-place z filter: a block reads its left neighbour's unfiltered values */
+    const size_t nh = (size_t)o->LZ * (size_t)o->LR;
+    double* pre = (double*)malloc(nh * sizeof(double));
+    memcpy(pre, var, nh * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (I8 j = 1; j <= o->Nr; ++j)
+      for (I8 i = 1; i <= o->Nz; ++i) {
+        if (o->ibval[IIX(o, i, j)] == 0.0) continue;
+        int row; I8 w0;
+        int c = zrow(o, i, j, &row, &w0, 10);
+        const double* tr;
+        int n;
+        if (c == 1) { tr = o->TG[row]; n = 11; }
+        else if (c == 0) { tr = o->TG[4]; n = 9; w0 = i - 4; }
+        else continue;
+        const I8 lo = o->zlo[o->bz[i]];
+        double sum = 0.0;
+        for (int m = 0; m < n; ++m) {
+          const I8 q = w0 + m;
+          sum = sum + tr[m] * (q < lo ? pre : out)[HIX(o, q, j)];
+        }
+        out[HIX(o, i, j)] = sum;
+      }
+    free(pre);
+    return;
+  }
   if (dirn == 1) {
 #pragma omp parallel for schedule(static)
     for (I8 j = 1; j <= o->Nr; ++j)
@@ -297,7 +345,7 @@ static void shock_capturing(axo* o) {
   for (I8 j = 1; j <= Nr; ++j)
     for (I8 i = 1; i <= Nz; ++i) {
       size_t x = HIX(o, i, j);
-      if (j == 1) o->dilvec[x] = 2.0 * o->dVrdr[x] + o->dVzdz[x];
+      if (j == o->rlo[o->br[j]]) o->dilvec[x] = 2.0 * o->dVrdr[x] + o->dVzdz[x];
       else o->dilvec[x] = o->dVrdr[x] + o->Vrvec[x] / o->rvec[x] + o->dVzdz[x];
     }
 #pragma omp parallel for schedule(static)
@@ -311,7 +359,7 @@ static void shock_capturing(axo* o) {
       double S31 = S13, S32 = 0.0;
       double S33 = o->dVzdz[x] - (1.0 / 3.0) * o->dilvec[x];
       double S22;
-      if (j == 1) S22 = o->dVrdr[x] - (1.0 / 3.0) * o->dilvec[x];
+      if (j == o->rlo[o->br[j]]) S22 = o->dVrdr[x] - (1.0 / 3.0) * o->dilvec[x];
       else S22 = o->Vrvec[x] / o->rvec[x] - (1.0 / 3.0) * o->dilvec[x];
       o->MgnStrRate[x] = sqrt(S11 * S11 + S12 * S12 + S13 * S13 + S21 * S21 + S22 * S22 + S23 * S23 +
                               S31 * S31 + S32 * S32 + S33 * S33);
@@ -336,15 +384,17 @@ static void shock_capturing(axo* o) {
   for (I8 j = 1; j <= Nr; ++j)
     for (I8 i = 1; i <= Nz; ++i) {
       size_t x = HIX(o, i, j);
+      /* the rank's own extent: i1..i2, j1..j2 (1..Nz, 1..Nr for one block) */
+      const I8 i1 = o->zlo[o->bz[i]], i2 = o->zhi[o->bz[i]], j1 = o->rlo[o->br[j]], j2 = o->rhi[o->br[j]];
       double deltaz = 0.0, deltar = 0.0;
-      if (i >= 2 && i <= Nz - 1) deltaz = (H(o, zvec, i + 1, j) - H(o, zvec, i - 1, j)) / 2.0;
-      if (i == 1) deltaz = H(o, zvec, 2, j) - H(o, zvec, 1, j);
-      if (i == Nz) deltaz = H(o, zvec, Nz, j) - H(o, zvec, Nz - 1, j);
-      if (j >= 2 && j <= Nr - 1) deltar = (H(o, rvec, i, j + 1) - H(o, rvec, i, j - 1)) / 2.0;
-      if (j == 1) deltar = H(o, rvec, i, 2) - H(o, rvec, i, 1);
-      if (j == Nr) deltar = H(o, rvec, i, Nr) - H(o, rvec, i, Nr - 1);
+      if (i >= i1 + 1 && i <= i2 - 1) deltaz = (H(o, zvec, i + 1, j) - H(o, zvec, i - 1, j)) / 2.0;
+      if (i == i1) deltaz = H(o, zvec, i1 + 1, j) - H(o, zvec, i1, j);
+      if (i == i2) deltaz = H(o, zvec, i2, j) - H(o, zvec, i2 - 1, j);
+      if (j >= j1 + 1 && j <= j2 - 1) deltar = (H(o, rvec, i, j + 1) - H(o, rvec, i, j - 1)) / 2.0;
+      if (j == j1) deltar = H(o, rvec, i, j1 + 1) - H(o, rvec, i, j1);
+      if (j == j2) deltar = H(o, rvec, i, j2) - H(o, rvec, i, j2 - 1);
       double dil;
-      if (j == 1) dil = 2.0 * o->dVrdr[x] + o->dVzdz[x];
+      if (j == j1) dil = 2.0 * o->dVrdr[x] + o->dVzdz[x];
       else dil = o->dVrdr[x] + o->Vrvec[x] / o->rvec[x] + o->dVzdz[x];
       double vort = fabs(o->dVrdz[x] - o->dVzdr[x]);
       double mdil = -1.0 * dil;
@@ -469,7 +519,8 @@ static void tlam_w(double Tm[5][5], double lam[5][5], const double* w, double* o
   matvec(M, w, out);
 }
 
-/* BoundaryConditions (:16-277) + sponge_bcs (:548-617). Sequential: sets o->T. */
+/* BoundaryConditions (:16-277) + sponge_bcs (:548-617). Sequential: sets the module
+   scalar T of the block of every face point it visits. */
 static void boundary_conditions(axo* o) {
   const double gam = o->p.gam;
   const double sigma_1 = -2.0, sigma_2 = -2.0, one_by_h_44 = 48.0 / 49.0;
@@ -494,7 +545,7 @@ static void boundary_conditions(axo* o) {
           if (j == 1) continue;
           if (adir == 1) {
             eigen_matrices(0, rho, Vz, T, gam, &e);
-            o->T = T;
+            o->Tb[BLK(o, i, j)] = T;
             /* compute_SAT_RHS :439-469 */
             for (int q = 0; q < 5; ++q)
               e.lam[q][q] = pt->bc_dir > 0 ? (fabs(e.lam[q][q]) + e.lam[q][q]) / 2.0
@@ -516,7 +567,7 @@ static void boundary_conditions(axo* o) {
             tI[4] = pvl[4];
             for (int q = 0; q < 5; ++q) S5(o, pv_targetI, i, j, q + 1) = tI[q];
             eigen_matrices(rd, rho, rd ? Vr : Vz, T, gam, &e);
-            o->T = T;
+            o->Tb[BLK(o, i, j)] = T;
             for (int q = 0; q < 5; ++q)
               e.lam[q][q] = pt->bc_dir > 0 ? (fabs(e.lam[q][q]) + e.lam[q][q]) / 2.0
                                            : (fabs(e.lam[q][q]) - e.lam[q][q]) / 2.0;
@@ -535,7 +586,7 @@ static void boundary_conditions(axo* o) {
         } else if (pt->bc == AXJ_BC_NSCBC_NONREFLECTING) {
           if (j == 1) continue;
           double Vt = o->Vtvec[x];
-          o->T = T;
+          o->Tb[BLK(o, i, j)] = T;
           double drhodr = o->drhodr[x], dVrdr = o->dVrdr[x], dVtdr = o->dVtdr[x], dVzdr = o->dVzdr[x];
           double dTdr = o->dTdr[x], dpdr = o->dpdr[x];
           double drhodz = o->drhodz[x], dVrdz = o->dVrdz[x], dVtdz = o->dVtdz[x], dVzdz = o->dVzdz[x];
@@ -573,11 +624,11 @@ static void boundary_conditions(axo* o) {
           double dv[5];
           if (adir == 1) {
             eigen_matrices(0, rho, Vz, T, gam, &e);
-            o->T = T;
+            o->Tb[BLK(o, i, j)] = T;
             dv[0] = o->drhodz[x]; dv[1] = o->dVrdz[x]; dv[2] = o->dVtdz[x]; dv[3] = o->dVzdz[x]; dv[4] = o->dTdz[x];
           } else if (adir == 2) {
             eigen_matrices(1, rho, Vr, T, gam, &e);
-            o->T = T;
+            o->Tb[BLK(o, i, j)] = T;
             dv[0] = o->drhodr[x]; dv[1] = o->dVrdr[x]; dv[2] = o->dVtdr[x]; dv[3] = o->dVzdr[x]; dv[4] = o->dTdr[x];
           } else {
             continue;
@@ -605,7 +656,7 @@ static void sponge_bcs(axo* o) {
     for (I8 i = 1; i <= Nz; ++i) {
       if (H(o, rvec, i, j) >= st) {
         for (int e = 1; e <= 5; ++e) {
-          double zeta = (H(o, rvec, i, j) - st) / (H(o, rvec, i, Nr) - st);
+          double zeta = (H(o, rvec, i, j) - st) / (H(o, rvec, i, o->rhi[o->br[j]]) - st);
           S5(o, rhs, i, j, e) =
               S5(o, rhs, i, j, e) - At * pow(zeta, n_sponge) * (S5(o, pv, i, j, e) - S5(o, pv_target, i, j, e));
         }
@@ -657,6 +708,16 @@ static void harmonic_forcing(axo* o, double t) {
 }
 
 /* ComputeRHS (ModRHS.f90:5-258) */
+/* T = Tvec(Nz,Nr) at the end of a rank's RHS loops (ModRHS.f90:76,145), which start at
+   row 2 on the axis rank (nbrs(2) < 0) and at row 1 elsewhere. */
+static void set_T_block_ends(axo* o) {
+  for (I8 b = 0; b < o->nbz * o->nbr; ++b) {
+    const I8 bzz = b % o->nbz, brr = b / o->nbz;
+    const I8 j0 = (o->rlo[brr] == 1) ? 2 : o->rlo[brr];
+    if (o->rhi[brr] >= j0) o->Tb[b] = H(o, Tvec, o->zhi[bzz], o->rhi[brr]);
+  }
+}
+
 static void compute_rhs(axo* o) {
   const I8 Nz = o->Nz, Nr = o->Nr;
   const double gam = o->p.gam, Re = o->p.Re, Pr = o->p.Pr;
@@ -690,7 +751,7 @@ static void compute_rhs(axo* o) {
       S5(o, rhs, i, j, 4) = Vr * dVzdr + Vz * dVzdz + 1.0 / (gam * rho) * dpdz;
       S5(o, rhs, i, j, 5) = Vr * dTdr + Vz * dTdz + (gam - 1.0) * T * (dVrdr + Vr / r + dVzdz);
     }
-  if (Nr >= j0) o->T = H(o, Tvec, Nz, Nr);
+  set_T_block_ends(o);
   {
     const size_t n = (size_t)Nz * (size_t)Nr * 5;
     for (size_t x = 0; x < n; ++x) o->rhs[x] = -1.0 * o->rhs[x];
@@ -759,7 +820,7 @@ static void compute_rhs(axo* o) {
                  dVzdz * (fourby3 * dVzdz - twoby3 * dVrdr - twoby3 * Vr * onebyr) +
                  (dVrdz + dVzdr) * (dVzdr + dVrdz));
       }
-    if (Nr >= j0) o->T = H(o, Tvec, Nz, Nr);
+    set_T_block_ends(o);
   }
   if (o->p.control_forcing == 1) control_forcing(o);
   else if (o->p.control_forcing == 2) harmonic_forcing(o, o->t_stage);
@@ -799,8 +860,11 @@ void axo_destroy(axo* o) {
   for (size_t k = 0; k < sizeof(hf) / sizeof(hf[0]); ++k) free(*hf[k]);
   free(o->is_it_i_patch); free(o->which_i_patch); free(o->is_it_j_patch); free(o->which_j_patch);
   free(o->patch);
+  free(o->bz); free(o->br); free(o->zlo); free(o->zhi); free(o->rlo); free(o->rhi); free(o->Tb);
   free(o);
 }
+
+static int set_blocks(axo* o, I8 dz, I8 dr);
 
 axo* axo_create(const axj_params* p, I8 Nz, I8 Nr, const double* zvec, const double* rvec, const double* ibval,
                 const axj_patch* patches, I8 npatch) {
@@ -857,8 +921,59 @@ axo* axo_create(const axj_params* p, I8 Nz, I8 Nr, const double* zvec, const dou
     }
   compute_metric(o, o->dxidz, 1, o->ddxidxidz);
   compute_metric(o, o->detadr, 2, o->ddetadetadr);
-  o->T = 0.0; /* never assigned before the first ComputeRHS */
+  /* one block: the whole grid; T is never assigned before the first ComputeRHS */
+  if (set_blocks(o, 1, 1) != 0) { axo_destroy(o); return NULL; }
   return o;
+}
+
+/* DistributeGridDims / DistributeGridPoints (ModDecomp.f90:35-105) along one direction:
+   N/d points per block (integer division, as ND/dims is), the last block the rest. */
+static void partition(I8 N, I8 d, I8* lo, I8* hi, I8* of) {
+  const I8 w = N / d;
+  for (I8 b = 0; b < d; ++b) {
+    lo[b] = b * w + 1;
+    hi[b] = (b == d - 1) ? N : (b + 1) * w;
+    for (I8 i = lo[b]; i <= hi[b]; ++i) of[i] = b;
+  }
+}
+
+static int set_blocks(axo* o, I8 dz, I8 dr) {
+  free(o->bz); free(o->br); free(o->zlo); free(o->zhi); free(o->rlo); free(o->rhi); free(o->Tb);
+  o->nbz = dz; o->nbr = dr;
+  o->bz = (I8*)calloc((size_t)o->Nz + 1, sizeof(I8));
+  o->br = (I8*)calloc((size_t)o->Nr + 1, sizeof(I8));
+  o->zlo = (I8*)calloc((size_t)dz, sizeof(I8)); o->zhi = (I8*)calloc((size_t)dz, sizeof(I8));
+  o->rlo = (I8*)calloc((size_t)dr, sizeof(I8)); o->rhi = (I8*)calloc((size_t)dr, sizeof(I8));
+  o->Tb = (double*)calloc((size_t)(dz * dr), sizeof(double));
+  if (!o->bz || !o->br || !o->zlo || !o->zhi || !o->rlo || !o->rhi || !o->Tb) return AXJ_ERR_NOMEM;
+  partition(o->Nz, dz, o->zlo, o->zhi, o->bz);
+  partition(o->Nr, dr, o->rlo, o->rhi, o->br);
+  return 0;
+}
+
+/* The replica of a dims_z x dims_r run (ModDecomp.f90). Every block must hold at least 8
+   points each way, and no 4-wide closure strip may be split along its own direction (the
+   rank's PatchCreation would then renumber its closure rows). Resets every block's T to
+   0, as at the start of a run. */
+int axo_set_decomposition(axo* o, I8 dims_z, I8 dims_r) {
+  if (dims_z < 1 || dims_r < 1 || o->Nz / dims_z < 8 || o->Nr / dims_r < 8) return AXJ_ERR_ARG;
+  int rc = set_blocks(o, dims_z, dims_r);
+  if (rc != 0) return rc;
+  for (I8 pn = 1; pn <= o->no_bcs; ++pn) {
+    const axj_patch* pt = &o->patch[pn - 1];
+    const int adir = (int)(pt->bc_dir < 0 ? -pt->bc_dir : pt->bc_dir);
+    if (adir == 1 && o->bz[pt->i_start < 1 ? 1 : pt->i_start] != o->bz[pt->i_end > o->Nz ? o->Nz : pt->i_end])
+      rc = AXJ_ERR_BADPATCH;
+    if (adir == 2 && o->br[pt->j_start < 1 ? 1 : pt->j_start] != o->br[pt->j_end > o->Nr ? o->Nr : pt->j_end])
+      rc = AXJ_ERR_BADPATCH;
+  }
+  if (rc != 0) set_blocks(o, 1, 1);
+  return rc;
+}
+
+/* The module scalar T of every block (block bz + dims_z * br). */
+void axo_block_T(axo* o, double* out) {
+  for (I8 b = 0; b < o->nbz * o->nbr; ++b) out[b] = o->Tb[b];
 }
 
 int axo_set_state(axo* o, const double* pv, const double* pv_target, I8 iteration, double time) {
@@ -877,7 +992,7 @@ int axo_get_state(axo* o, double* pv) {
 }
 
 void axo_get_time(axo* o, I8* iteration, double* time, double* stale_T) {
-  *iteration = o->iteration; *time = o->time; *stale_T = o->T;
+  *iteration = o->iteration; *time = o->time; *stale_T = o->Tb[0];
 }
 
 /* ComputeTimeStep (ModInputOutput.f90:389-438) */
@@ -889,7 +1004,7 @@ int axo_compute_dt(axo* o, double* delt) {
     for (I8 i = 1; i <= o->Nz; ++i) {
       if (o->ibval[IIX(o, i, j)] == 0.0) { o->deltvec[IIX(o, i, j)] = 100.0; continue; }
       size_t x = HIX(o, i, j);
-      double Ts = phys ? o->Tvec[x] : o->T;
+      double Ts = phys ? o->Tvec[x] : o->Tb[BLK(o, i, j)];
       double dx = o->dxidz[x], dr = o->detadr[x];
       double inv = fabs(o->Vzvec[x] * dx + o->Vrvec[x] * dr) + sqrt(Ts) * sqrt(dx * dx + dr * dr);
       double a = o->muvec[x] / Re, b = o->lambdavec[x] / Re, c = o->kappavec[x] / (Re * Pr);
@@ -947,14 +1062,17 @@ int axo_rhs(axo* o, const double* pv, double* rhs) {
   const size_t n = (size_t)o->Nz * (size_t)o->Nr * 5;
   double* save = (double*)malloc(n * sizeof(double));
   memcpy(save, o->pv, n * sizeof(double));
-  double Tsave = o->T;
+  const size_t nb = (size_t)(o->nbz * o->nbr);
+  double* Tsave = (double*)malloc(nb * sizeof(double));
+  memcpy(Tsave, o->Tb, nb * sizeof(double));
   memcpy(o->pv, pv, n * sizeof(double));
   assign_values(o);
   o->t_stage = o->time;
   compute_rhs(o);
   memcpy(rhs, o->rhs, n * sizeof(double));
   memcpy(o->pv, save, n * sizeof(double));
-  o->T = Tsave;
+  memcpy(o->Tb, Tsave, nb * sizeof(double));
+  free(Tsave);
   assign_values(o);
   free(save);
   return 0;

@@ -49,6 +49,8 @@ def load():
         "axo_sensor": (C.c_int, [v, dp, dp, dp, dp]),
         "axo_tables": (None, [v, dp, dp, dp]),
         "axo_metrics": (None, [v, dp, dp, dp, dp]),
+        "axo_set_decomposition": (C.c_int, [v, i64, i64]),
+        "axo_block_T": (None, [v, dp]),
         "axo_patches_from_records": (C.c_int, [C.POINTER(AxjBcRecord), i64, i64, i64, C.POINTER(AxjPatch),
                                                C.POINTER(i64)]),
     }
@@ -118,6 +120,22 @@ class Oracle:
         it, t, ts = C.c_int64(0), C.c_double(0.0), C.c_double(0.0)
         self.lib.axo_get_time(self.h, C.byref(it), C.byref(t), C.byref(ts))
         return ts.value
+
+    def set_decomposition(self, dims_z, dims_r):
+        """Replica of the reference run on a dims_z x dims_r process grid (ModDecomp.f90):
+        block-local sensor edges and first rows, the in-place z filter restarted at block
+        starts, per-block stale T and top-sponge denominator. Resets the blocks' T to 0."""
+        rc = self.lib.axo_set_decomposition(self.h, int(dims_z), int(dims_r))
+        if rc != 0:
+            raise ValueError(f"oracle: decomposition {dims_z} x {dims_r} rejected (status {rc})")
+        self.dims = (int(dims_z), int(dims_r))
+
+    def block_T(self):
+        """The module scalar T of every block, as [dims_r, dims_z]."""
+        dz, dr = getattr(self, "dims", (1, 1))
+        out = np.empty(dz * dr)
+        self.lib.axo_block_T(self.h, dptr(out))
+        return out.reshape(dr, dz)
 
     def compute_time_step(self):
         d = C.c_double(0.0)
