@@ -26,9 +26,10 @@
  * PARITY STATUS: unpinned against reference outputs. The reference ships no tests or
  * golden vectors and its Fortran cannot be compiled in this image (no gfortran/flang).
  * The restatement is pinned instead by operator known-answer tests (polynomial
- * exactness of SBP1/SBP2, TG row sums), the shipped bc fixture
- * (bc_4400x640_nozzle.dat), free-stream preservation and the manufactured-solution
- * check in tests/.
+ * exactness of SBP1/SBP2, TG row sums), the operator tables and default constants as the
+ * reference's source text states them (tests/golden/reference_constants.json, equal bit
+ * for bit), the shipped bc fixture (bc_4400x640_nozzle.dat) and free-stream
+ * preservation, all in tests/.
  *
  * Restatement rules:
  *  - Same arithmetic and evaluation order as the Fortran source (left-to-right,
