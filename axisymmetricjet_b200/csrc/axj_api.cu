@@ -765,8 +765,10 @@ int axj_read_bc_file(const char* path, axj_bc_record* rec, int64_t max_records, 
     long long v[9];
     int k = std::sscanf(line, "%lld %lld %lld %lld %lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4],
                         &v[5], &v[6], &v[7], &v[8]);
-    if (k <= 0) continue;  // blank line
-    if (k < 7) { rc = fail(nullptr, AXJ_ERR_BADPATCH, "bc file %s: short record %lld", path, (long long)n + 1); break; }
+    if (k <= 0) continue;  // blank line: list-directed input skips it
+    // a record is 9 integers (ModPatch.f90:48); the reference's list-directed READ would
+    // take the missing values from the next line, so a short record is an error here
+    if (k < 9) { rc = fail(nullptr, AXJ_ERR_BADPATCH, "bc file %s: short record %lld", path, (long long)n + 1); break; }
     if (n < max_records && rec) {
       rec[n].bc = v[1];
       rec[n].bc_dir = v[2];

@@ -48,6 +48,22 @@ def test_read_reference_bc_file(oracle_mod):
     assert axj.patches_from_records(rec, 4400, 640) == oracle_mod.patches_from_records(rec, 4400, 640)
 
 
+def test_bc_file_parsing(tmp_path):
+    """Records of 9 integers (ModPatch.f90:30-63); blank lines are skipped as list-directed
+    input skips them; a missing file or a short record is an error."""
+    with pytest.raises(axj.AxjError) as e:
+        axj.read_bc_file(str(tmp_path / "missing.dat"))
+    assert e.value.code == 1
+    p = tmp_path / "bc.dat"
+    p.write_text("\n1 91 1 1 1 1 5 1 1\n\n1 90 2 1 -1 1 1 1 1\n\n")
+    assert axj.read_bc_file(str(p)) == [(91, 1, 1, 1, 1, 5), (90, 2, 1, -1, 1, 1)]
+    for short in ("1 91 1 1 1 1 5 1\n", "1 91 1 1 1 x 5 1 1\n"):
+        p.write_text(short)
+        with pytest.raises(axj.AxjError) as e:
+            axj.read_bc_file(str(p))
+        assert e.value.code == 6
+
+
 def test_bad_bc_record_rejected():
     with pytest.raises(axj.AxjError) as e:
         axj.patches_from_records([(91, 3, 1, 1, 1, -1)], 64, 64)
