@@ -19,7 +19,7 @@ from ._ffi import (AXJ_OK, STATUS, AxjBatchTuning, AxjBcRecord, AxjMlp, AxjParam
                    default_params, default_train_cfg, dptr, patch_array, patches_to_tuples, record_array)
 
 __all__ = ["AxiJetSolver", "AxjBatch", "AxjError", "AxjMlp", "default_params", "default_train_cfg", "load_library",
-           "read_bc_file", "patches_from_records", "library_path", "mlp_init"]
+           "read_bc_file", "patches_from_records", "operator_tables", "library_path", "mlp_init"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
