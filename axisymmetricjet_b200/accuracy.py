@@ -1,8 +1,9 @@
 """Error measures of a solution against a reference solution of the same grid.
 
 Fields are the solver's primitive planes (rho, V_r, V_theta, V_z, T), each (Nr, Nz) with
-z fastest. Pressure is p = rho*T/gamma, the nondimensional equation of state of the
-reference (ModAssign.f90: pvec = rhovec*Tvec/gam in the outputs).
+z fastest. Pressure is the reference's pvec = rho*T (ModAssign.f90:19; the momentum
+equations divide its gradient by gam*rho, ModRHS.f90:92-96). Every measure here is
+relative, so the scale of p does not enter.
 """
 import numpy as np
 
@@ -10,7 +11,8 @@ FIELDS = ("rho", "Vr", "Vt", "Vz", "T")
 
 
 def pressure(pv, gam=1.4):
-    return pv[0] * pv[4] / gam
+    """pvec = rho*T (ModAssign.f90:19); gam is accepted for the callers' signatures."""
+    return pv[0] * pv[4]
 
 
 def rel_l2(a, b):
