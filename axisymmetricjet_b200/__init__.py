@@ -19,7 +19,7 @@ from ._ffi import (AXJ_OK, STATUS, AxjBatchTuning, AxjBcRecord, AxjMlp, AxjParam
                    default_params, default_train_cfg, dptr, patch_array, patches_to_tuples, record_array)
 
 __all__ = ["AxiJetSolver", "AxjBatch", "AxjError", "AxjMlp", "default_params", "default_train_cfg", "load_library",
-           "read_bc_file", "patches_from_records", "operator_tables", "library_path", "mlp_init"]
+           "read_bc_file", "patches_from_records", "operator_tables", "point_maps", "library_path", "mlp_init"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -70,6 +70,8 @@ def load_library():
         "axj_destroy": (None, [h]),
         "axj_read_bc_file": (C.c_int, [C.c_char_p, C.POINTER(AxjBcRecord), i64, C.POINTER(i64)]),
         "axj_operator_tables": (C.c_int, [dp, dp, dp]),
+        "axj_point_maps": (C.c_int, [C.POINTER(AxjPatch), i64, i64, i64, dp, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]),
         "axj_patches_from_records": (C.c_int, [C.POINTER(AxjBcRecord), i64, i64, i64, C.POINTER(AxjPatch),
                                                C.POINTER(i64)]),
         "axj_version": (C.c_char_p, []),
@@ -120,6 +122,22 @@ def operator_tables():
     s1, s2, tg = np.empty((9, 6)), np.empty((9, 6)), np.empty((9, 11))
     _check(lib, None, lib.axj_operator_tables(dptr(s1), dptr(s2), dptr(tg)))
     return s1, s2, tg
+
+
+def point_maps(patches, Nz, Nr, ibval):
+    """The per-point stencil rows and face operations the device descriptors encode
+    (CreateAllPatches, ModPatch.f90:214-242; the BoundaryConditions loop, ModBC.f90:25-274):
+    dict of zrow, rrow, blank, nfaceops (uint8) and faceop_ids (uint64: 1-based patch
+    numbers, one per byte), each (Nr, Nz)."""
+    lib = load_library()
+    ib = np.ascontiguousarray(ibval, dtype=np.float64)
+    pa = patch_array(patches)
+    out = {k: np.zeros((Nr, Nz), dtype=np.uint8) for k in ("zrow", "rrow", "blank", "nfaceops")}
+    out["faceop_ids"] = np.zeros((Nr, Nz), dtype=np.uint64)
+    _check(lib, None, lib.axj_point_maps(pa, len(patches), Nz, Nr, dptr(ib), out["zrow"].ctypes.data,
+                                         out["rrow"].ctypes.data, out["blank"].ctypes.data,
+                                         out["nfaceops"].ctypes.data, out["faceop_ids"].ctypes.data))
+    return out
 
 
 def read_bc_file(path):

@@ -713,6 +713,90 @@ namespace axj {
 void set_global_error(const char* msg) { g_create_error = msg; }
 }  // namespace axj
 
+// The per-point descriptors of one block holding the grid (CreateAllPatches,
+// ModPatch.f90:214-242: the last patch of a direction wins a point) with pitch P, and the
+// face-operation lists in patch order (the BoundaryConditions loop, ModBC.f90:25-274):
+// faces[0] = 0, then per face point its count and 0-based patch indices, referenced from
+// the descriptor. iT, jT (1-based): the last face point the loop visits, else the last
+// point of the RHS loops (ModRHS.f90:76,145), where the stale scalar T is taken.
+static int build_point_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, int64_t P,
+                            const double* ibval, std::vector<uint32_t>& desc, std::vector<int>& faces, int64_t& iT,
+                            int64_t& jT, std::string& msg) {
+  const size_t npt = (size_t)Nz * Nr;
+  std::vector<int> which_i(npt, 0), which_j(npt, 0);  // 1-based patch number, 0 = none
+  for (int64_t k = 0; k < npatch; ++k) {
+    const axj_patch& p = patches[k];
+    for (int64_t i = std::max<int64_t>(p.i_start, 1); i <= std::min<int64_t>(p.i_end, Nz); ++i)
+      for (int64_t j = std::max<int64_t>(p.j_start, 1); j <= std::min<int64_t>(p.j_end, Nr); ++j) {
+        const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
+        if (p.bc_dir == 1 || p.bc_dir == -1) which_i[x] = (int)k + 1;
+        if (p.bc_dir == 2 || p.bc_dir == -2) which_j[x] = (int)k + 1;
+      }
+  }
+  // face-operation lists in patch order (BoundaryConditions loop, ModBC.f90:25-274)
+  std::vector<std::vector<int>> ops(npt);
+  iT = Nz;
+  jT = Nr;
+  for (int64_t k = 0; k < npatch; ++k) {
+    const axj_patch& p = patches[k];
+    if (p.bc == AXJ_BC_AXIS) continue;
+    int64_t is, ie, js, je;
+    if (p.bc_dir == 1) { is = ie = p.i_start; js = p.j_start; je = p.j_end; }
+    else if (p.bc_dir == -1) { is = ie = p.i_end; js = p.j_start; je = p.j_end; }
+    else if (p.bc_dir == 2) { is = p.i_start; ie = p.i_end; js = je = p.j_start; }
+    else { is = p.i_start; ie = p.i_end; js = je = p.j_end; }
+    for (int64_t i = is; i <= ie; ++i)
+      for (int64_t j = js; j <= je; ++j) {
+        if (i < 1 || i > Nz || j < 1 || j > Nr) continue;
+        const bool j1 = (j == 1);
+        const int adir = (int)(p.bc_dir < 0 ? -p.bc_dir : p.bc_dir);
+        bool active = false;
+        if (p.bc == AXJ_BC_SAT_FARFIELD) active = !j1 && adir == 1;
+        else if (p.bc == AXJ_BC_SAT_NOSLIP_WALL || p.bc == AXJ_BC_NSCBC_NOSLIP_WALL) active = true;
+        else if (p.bc == AXJ_BC_NSCBC_NONREFLECTING) active = !j1;
+        if (!active) continue;
+        const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
+        ops[x].push_back((int)k);
+        if ((int)ops[x].size() > MAX_FACE_OPS) {
+          char b[128];
+          std::snprintf(b, sizeof(b), "more than %d face operations at (%lld,%lld)", MAX_FACE_OPS, (long long)i,
+                        (long long)j);
+          msg = b;
+          return AXJ_ERR_BADPATCH;
+        }
+        iT = i;
+        jT = j;
+      }
+  }
+  faces.assign(1, 0);
+  desc.assign((size_t)P * Nr, make_desc(ROW_NONE, ROW_NONE, false, 0));
+  for (int64_t j = 1; j <= Nr; ++j)
+    for (int64_t i = 1; i <= Nz; ++i) {
+      const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
+      int zr = 4, rw = 4;
+      if (which_i[x]) {
+        const axj_patch& p = patches[which_i[x] - 1];
+        zr = p.bc_dir == 1 ? (int)(i - p.i_start) : (int)(8 + i - p.i_end);
+      }
+      if (which_j[x]) {
+        const axj_patch& p = patches[which_j[x] - 1];
+        rw = p.bc_dir == 2 ? (int)(j - p.j_start) : (int)(8 + j - p.j_end);
+      }
+      uint32_t f = 0;
+      if (!ops[x].empty()) {
+        f = (uint32_t)faces.size();
+        faces.push_back((int)ops[x].size());
+        for (int id : ops[x]) faces.push_back(id);
+      }
+      desc[(size_t)(j - 1) * P + (i - 1)] = make_desc(zr, rw, ibval[x] == 0.0, f);
+    }
+  if (faces.size() >= (1u << 20)) {
+    msg = "too many face points";
+    return AXJ_ERR_BADPATCH;
+  }
+  return AXJ_OK;
+}
+
 extern "C" {
 
 int axj_operator_tables(double* sbp1, double* sbp2, double* tgfilt) {
@@ -722,6 +806,37 @@ int axj_operator_tables(double* sbp1, double* sbp2, double* tgfilt) {
   std::memcpy(sbp1, S1, sizeof(S1));
   std::memcpy(sbp2, S2, sizeof(S2));
   std::memcpy(tgfilt, G, sizeof(G));
+  return AXJ_OK;
+}
+
+int axj_point_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, const double* ibval,
+                   uint8_t* zrow, uint8_t* rrow, uint8_t* blank, uint8_t* nfaceops, uint64_t* faceop_ids) {
+  if ((npatch > 0 && !patches) || !ibval || !zrow || !rrow || !blank || !nfaceops || !faceop_ids)
+    return fail(nullptr, AXJ_ERR_ARG, "null argument");
+  if (Nz < 1 || Nr < 1) return fail(nullptr, AXJ_ERR_ARG, "grid %lld x %lld", (long long)Nz, (long long)Nr);
+  if (npatch < 0 || npatch > MAX_PATCHES) return fail(nullptr, AXJ_ERR_BADPATCH, "%lld patches", (long long)npatch);
+  for (int64_t k = 0; k < npatch; ++k) {
+    const int64_t d = patches[k].bc_dir;
+    if (d != 1 && d != -1 && d != 2 && d != -2)
+      return fail(nullptr, AXJ_ERR_BADPATCH, "patch %lld: bc_dir %lld", (long long)k + 1, (long long)d);
+  }
+  std::vector<uint32_t> desc;
+  std::vector<int> faces;
+  int64_t iT = 0, jT = 0;
+  std::string msg;
+  const int rc = build_point_maps(patches, npatch, Nz, Nr, Nz, ibval, desc, faces, iT, jT, msg);
+  if (rc != AXJ_OK) return fail(nullptr, rc, "%s", msg.c_str());
+  for (size_t x = 0; x < (size_t)Nz * Nr; ++x) {
+    const uint32_t d = desc[x];
+    zrow[x] = (uint8_t)desc_zrow(d);
+    rrow[x] = (uint8_t)desc_rrow(d);
+    blank[x] = desc_blank(d) ? 1 : 0;
+    const uint32_t f = desc_face(d);
+    nfaceops[x] = f ? (uint8_t)faces[f] : 0;
+    uint64_t ids = 0;
+    for (int k = 0; f && k < faces[f]; ++k) ids |= (uint64_t)(faces[f + 1 + k] + 1) << (8 * k);
+    faceop_ids[x] = ids;
+  }
   return AXJ_OK;
 }
 
@@ -954,74 +1069,19 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   }
 
   // ---- stencil maps (CreateAllPatches, ModPatch.f90:214-242) -> per-point descriptors
-  const size_t npt = (size_t)Nz * Nr;
-  std::vector<int> which_i(npt, 0), which_j(npt, 0);  // 1-based patch number, 0 = none
-  for (int64_t k = 0; k < npatch; ++k) {
-    const axj_patch& p = patches[k];
-    for (int64_t i = std::max<int64_t>(p.i_start, 1); i <= std::min<int64_t>(p.i_end, Nz); ++i)
-      for (int64_t j = std::max<int64_t>(p.j_start, 1); j <= std::min<int64_t>(p.j_end, Nr); ++j) {
-        const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
-        if (p.bc_dir == 1 || p.bc_dir == -1) which_i[x] = (int)k + 1;
-        if (p.bc_dir == 2 || p.bc_dir == -2) which_j[x] = (int)k + 1;
-      }
-  }
-  // face-operation lists in patch order (BoundaryConditions loop, ModBC.f90:25-274)
-  std::vector<std::vector<int>> ops(npt);
-  int64_t iT = Nz, jT = Nr;  // stale T: last point of the RHS loops (ModRHS.f90:76,145)
-  for (int64_t k = 0; k < npatch; ++k) {
-    const axj_patch& p = patches[k];
-    if (p.bc == AXJ_BC_AXIS) continue;
-    int64_t is, ie, js, je;
-    if (p.bc_dir == 1) { is = ie = p.i_start; js = p.j_start; je = p.j_end; }
-    else if (p.bc_dir == -1) { is = ie = p.i_end; js = p.j_start; je = p.j_end; }
-    else if (p.bc_dir == 2) { is = p.i_start; ie = p.i_end; js = je = p.j_start; }
-    else { is = p.i_start; ie = p.i_end; js = je = p.j_end; }
-    for (int64_t i = is; i <= ie; ++i)
-      for (int64_t j = js; j <= je; ++j) {
-        if (i < 1 || i > Nz || j < 1 || j > Nr) continue;
-        const bool j1 = (j == 1);
-        const int adir = (int)(p.bc_dir < 0 ? -p.bc_dir : p.bc_dir);
-        bool active = false;
-        if (p.bc == AXJ_BC_SAT_FARFIELD) active = !j1 && adir == 1;
-        else if (p.bc == AXJ_BC_SAT_NOSLIP_WALL || p.bc == AXJ_BC_NSCBC_NOSLIP_WALL) active = true;
-        else if (p.bc == AXJ_BC_NSCBC_NONREFLECTING) active = !j1;
-        if (!active) continue;
-        const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
-        ops[x].push_back((int)k);
-        if ((int)ops[x].size() > MAX_FACE_OPS) {
-          delete h;
-          return fail(nullptr, AXJ_ERR_BADPATCH, "more than %d face operations at (%lld,%lld)", MAX_FACE_OPS,
-                      (long long)i, (long long)j);
-        }
-        iT = i;
-        jT = j;
-      }
+  std::vector<uint32_t> desc;
+  std::vector<int> faces;
+  int64_t iT = Nz, jT = Nr;
+  {
+    std::string msg;
+    const int prc = build_point_maps(patches, npatch, Nz, Nr, h->P, ibval, desc, faces, iT, jT, msg);
+    if (prc != AXJ_OK) {
+      delete h;
+      return fail(nullptr, prc, "%s", msg.c_str());
+    }
   }
   h->iT = (int)(iT - 1);
   h->jT = (int)(jT - 1);
-  std::vector<int> faces(1, 0);
-  std::vector<uint32_t> desc((size_t)h->P * Nr, make_desc(ROW_NONE, ROW_NONE, false, 0));
-  for (int64_t j = 1; j <= Nr; ++j)
-    for (int64_t i = 1; i <= Nz; ++i) {
-      const size_t x = (size_t)(i - 1) + (size_t)(j - 1) * Nz;
-      int zr = 4, rw = 4;
-      if (which_i[x]) {
-        const axj_patch& p = patches[which_i[x] - 1];
-        zr = p.bc_dir == 1 ? (int)(i - p.i_start) : (int)(8 + i - p.i_end);
-      }
-      if (which_j[x]) {
-        const axj_patch& p = patches[which_j[x] - 1];
-        rw = p.bc_dir == 2 ? (int)(j - p.j_start) : (int)(8 + j - p.j_end);
-      }
-      uint32_t f = 0;
-      if (!ops[x].empty()) {
-        f = (uint32_t)faces.size();
-        faces.push_back((int)ops[x].size());
-        for (int id : ops[x]) faces.push_back(id);
-      }
-      desc[(size_t)(j - 1) * h->P + (i - 1)] = make_desc(zr, rw, ibval[x] == 0.0, f);
-    }
-  if (faces.size() >= (1u << 20)) { delete h; return fail(nullptr, AXJ_ERR_BADPATCH, "too many face points"); }
   std::vector<unsigned char> zcode(desc.size()), rcode(desc.size());
   for (size_t x = 0; x < desc.size(); ++x) {
     zcode[x] = (unsigned char)(desc_blank(desc[x]) ? ROW_NONE : (uint32_t)desc_zrow(desc[x]));

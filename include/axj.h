@@ -345,6 +345,16 @@ int axj_read_bc_file(const char* path, axj_bc_record* records, int64_t max_recor
 int axj_patches_from_records(const axj_bc_record* records, int64_t nrecords, int64_t Nz_grid,
                              int64_t Nr_grid, axj_patch* patches, int64_t* npatch);
 
+/* The per-point maps of CreateAllPatches (ModPatch.f90:214-242) and of the
+ * BoundaryConditions loop (ModBC.f90:25-274) exactly as axj_create builds the device
+ * descriptors from them, for x = (i-1) + (j-1)*Nz: zrow[x], rrow[x] = the SBP row (0..8,
+ * 4 = centred) of the z and r stencils (the last patch of a direction wins a point);
+ * blank[x] = 1 where ibval == 0; nfaceops[x] = the number of face operations (SAT /
+ * NSCBC patches that act at the point, in patch order) and faceop_ids[x] their 1-based
+ * patch numbers, one per byte from the lowest. */
+int axj_point_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, const double* ibval,
+                   uint8_t* zrow, uint8_t* rrow, uint8_t* blank, uint8_t* nfaceops, uint64_t* faceop_ids);
+
 /* The operator tables the device kernels use, as SBP_operator forms them
  * (ModOperator.f90:5-121): SBP1(0:8,0:5) and SBP2(0:8,0:5) into sbp1[54] and sbp2[54],
  * TGfilt(0:8,0:10) into tgfilt[99], row-major (row = the SBP row). */

@@ -78,6 +78,10 @@ typedef struct axo {
   I8 nbz, nbr;
   I8 *bz, *br, *zlo, *zhi, *rlo, *rhi;
   double* Tb;
+  /* when set: every face operation the bc loop applies is recorded per point (count and
+     1-based patch numbers, one per byte) */
+  uint8_t* rec_n;
+  uint64_t* rec_ids;
   double delt, time;
   double t_stage;  /* time of the current RHS evaluation (harmonic forcing) */
   I8 iteration;
@@ -522,6 +526,14 @@ static void tlam_w(double Tm[5][5], double lam[5][5], const double* w, double* o
 
 /* BoundaryConditions (:16-277) + sponge_bcs (:548-617). Sequential: sets the module
    scalar T of the block of every face point it visits. */
+static inline void rec_op(axo* o, I8 pn, I8 i, I8 j) {
+  if (!o->rec_n) return;
+  const size_t x = IIX(o, i, j);
+  const uint8_t n = o->rec_n[x];
+  if (n < 8) o->rec_ids[x] |= (uint64_t)pn << (8 * n);
+  o->rec_n[x] = (uint8_t)(n + 1);
+}
+
 static void boundary_conditions(axo* o) {
   const double gam = o->p.gam;
   const double sigma_1 = -2.0, sigma_2 = -2.0, one_by_h_44 = 48.0 / 49.0;
@@ -545,6 +557,7 @@ static void boundary_conditions(axo* o) {
         if (pt->bc == AXJ_BC_SAT_FARFIELD) {
           if (j == 1) continue;
           if (adir == 1) {
+            rec_op(o, pn, i, j);
             eigen_matrices(0, rho, Vz, T, gam, &e);
             o->Tb[BLK(o, i, j)] = T;
             /* compute_SAT_RHS :439-469 */
@@ -559,6 +572,7 @@ static void boundary_conditions(axo* o) {
           }
         } else if (pt->bc == AXJ_BC_SAT_NOSLIP_WALL) {
           if (adir == 1 || adir == 2) {
+            rec_op(o, pn, i, j);
             int rd = adir == 2;
             double tI[5];
             tI[0] = pvl[0];
@@ -610,6 +624,7 @@ static void boundary_conditions(axo* o) {
           } else {
             continue;
           }
+          rec_op(o, pn, i, j);
           /* ComputeNSCBCRHS :471-545: the non-reflecting face always uses z-derivatives */
           double dv[5] = {drhodz, dVrdz, dVtdz, dVzdz, dTdz};
           matvec(e.Ti, dv, w);
@@ -634,6 +649,7 @@ static void boundary_conditions(axo* o) {
           } else {
             continue;
           }
+          rec_op(o, pn, i, j);
           matvec(e.Ti, dv, w);
           if (pt->bc_dir < 0) w[3] = -1.0 * w[4];
           else if (pt->bc_dir > 0) w[4] = -1.0 * w[3];
@@ -970,6 +986,44 @@ int axo_set_decomposition(axo* o, I8 dims_z, I8 dims_r) {
   }
   if (rc != 0) set_blocks(o, 1, 1);
   return rc;
+}
+
+/* The stencil rows the oracle's operators select per point (zrow / rrow: the SBP row,
+   4 where no patch applies), the blanking, and the face operations its bc loop applies
+   (recorded from one pass of that loop on the current state; rhs, the SAT wall targets
+   and the stale T are restored). x = (i-1) + (j-1)*Nz. */
+void axo_point_maps(axo* o, uint8_t* zr, uint8_t* rr, uint8_t* blank, uint8_t* nops, uint64_t* ids) {
+  for (I8 j = 1; j <= o->Nr; ++j)
+    for (I8 i = 1; i <= o->Nz; ++i) {
+      int row; I8 w0;
+      const size_t x = IIX(o, i, j);
+      int c = zrow(o, i, j, &row, &w0, 5);
+      zr[x] = (uint8_t)(c == 1 ? row : (c == 0 ? 4 : 9));
+      c = rrow(o, i, j, &row, &w0, 5);
+      rr[x] = (uint8_t)(c == 1 ? row : (c == 0 ? 4 : 9));
+      blank[x] = o->ibval[x] == 0.0;
+    }
+  const size_t n = (size_t)o->Nz * (size_t)o->Nr;
+  const size_t n5 = n * 5, nb = (size_t)(o->nbz * o->nbr);
+  double* save = (double*)malloc(3 * n5 * sizeof(double));
+  double* Tsave = (double*)malloc(nb * sizeof(double));
+  memcpy(save, o->rhs, n5 * sizeof(double));
+  memcpy(save + n5, o->pv_targetI, n5 * sizeof(double));
+  memcpy(save + 2 * n5, o->pv_targetV, n5 * sizeof(double));
+  memcpy(Tsave, o->Tb, nb * sizeof(double));
+  memset(nops, 0, n);
+  memset(ids, 0, n * sizeof(uint64_t));
+  o->rec_n = nops;
+  o->rec_ids = ids;
+  boundary_conditions(o);
+  o->rec_n = NULL;
+  o->rec_ids = NULL;
+  memcpy(o->rhs, save, n5 * sizeof(double));
+  memcpy(o->pv_targetI, save + n5, n5 * sizeof(double));
+  memcpy(o->pv_targetV, save + 2 * n5, n5 * sizeof(double));
+  memcpy(o->Tb, Tsave, nb * sizeof(double));
+  free(save);
+  free(Tsave);
 }
 
 /* The module scalar T of every block (block bz + dims_z * br). */

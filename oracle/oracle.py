@@ -51,6 +51,7 @@ def load():
         "axo_metrics": (None, [v, dp, dp, dp, dp]),
         "axo_set_decomposition": (C.c_int, [v, i64, i64]),
         "axo_block_T": (None, [v, dp]),
+        "axo_point_maps": (None, [v, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "axo_patches_from_records": (C.c_int, [C.POINTER(AxjBcRecord), i64, i64, i64, C.POINTER(AxjPatch),
                                                C.POINTER(i64)]),
     }
@@ -129,6 +130,15 @@ class Oracle:
         if rc != 0:
             raise ValueError(f"oracle: decomposition {dims_z} x {dims_r} rejected (status {rc})")
         self.dims = (int(dims_z), int(dims_r))
+
+    def point_maps(self):
+        """zrow, rrow, blank, nfaceops, faceop_ids per point (see axo_point_maps); needs a
+        state (set_state) for the recorded pass of the bc loop."""
+        out = {k: np.zeros((self.Nr, self.Nz), dtype=np.uint8) for k in ("zrow", "rrow", "blank", "nfaceops")}
+        out["faceop_ids"] = np.zeros((self.Nr, self.Nz), dtype=np.uint64)
+        self.lib.axo_point_maps(self.h, out["zrow"].ctypes.data, out["rrow"].ctypes.data, out["blank"].ctypes.data,
+                                out["nfaceops"].ctypes.data, out["faceop_ids"].ctypes.data)
+        return out
 
     def block_T(self):
         """The module scalar T of every block, as [dims_r, dims_z]."""
