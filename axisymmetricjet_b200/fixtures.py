@@ -109,7 +109,7 @@ def nozzle_case(Nz=96, Nr=64, zmax=30.0, rmax=15.0, Mj=0.9, Re=1000.0, iw=20, jb
 
 
 def _stretched(i, n, delta, pos, cmin, cmax):
-    """compute_coord_val (WriteMeshAndSoln/write_soln_file.f90:102-123): a tanh-stretched
+    """compute_coord_val (WriteMeshAndSoln/write_soln_file.f90:95-115): a tanh-stretched
     coordinate clustered at cmin + pos. xi = float(i)/float(n) is a default-REAL (single
     precision) division and 1.0 - xi a single-precision difference, as in the Fortran;
     the rest is double precision."""
@@ -123,7 +123,7 @@ def _stretched(i, n, delta, pos, cmin, cmax):
 
 
 def writemesh_grid(nx=150, ny=50, n_wall_zone=100):
-    """create_AxiJet_CartGrid (write_soln_file.f90:125-217): the z coordinate of the
+    """create_AxiJet_CartGrid (write_soln_file.f90:117-213): the z coordinate of the
     first nx columns up to the first one beyond z = 11 (ipos2), a second stretching from
     11 to 15 over the wall zone from ipos2 on, the r coordinate, and iblank = 0 inside
     the nozzle lip (1 < r < 1.05, z < 6). Returns (z, r, iblank[Nr, Nz]) with 1-based
@@ -148,7 +148,7 @@ def writemesh_grid(nx=150, ny=50, n_wall_zone=100):
 
 
 def writemesh_records(z, r):
-    """The bc file written by create_AxiJet_CartGrid (write_soln_file.f90:219-255):
+    """The bc file written by create_AxiJet_CartGrid (write_soln_file.f90:219-257):
     jbottom = the last row at or below r = 1, jtop = the first row at or above r = 1.05,
     iright = the first column at or beyond z = 6 (all 1-based), no-slip NSCBC walls
     around the lip and at the outflow, a non-reflecting top and the axis."""
@@ -168,7 +168,7 @@ def writemesh_records(z, r):
 
 
 def write_bc_file(path, records):
-    """A bc file in the layout create_AxiJet_CartGrid writes (write_soln_file.f90:246-255):
+    """A bc file in the layout create_AxiJet_CartGrid writes (write_soln_file.f90:248-257):
     per row grid, bc, dir, istart, iend, jstart, jend, kstart, kend as '(9(I0,2X))'."""
     with open(path, "w") as f:
         for bc, d, i0, i1, j0, j1 in records:
@@ -176,7 +176,7 @@ def write_bc_file(path, records):
 
 
 def writemesh_solution(z, r, Mj=0.8, Tj_Tinf=0.6, gam=1.4):
-    """The initial condition of write_soln_file.f90:44-90 as pv[5, Nr, Nz]: a tanh jet
+    """The initial condition of write_soln_file.f90:36-90 as pv[5, Nr, Nz]: a tanh jet
     of radius 1 (theta = 0.1, a default-REAL literal stored in a double), decaying as
     (z - 5)**-1.5 beyond z = 6, zero velocity beyond r = 1, density from the
     Crocco-Busemann relation and T = 1/rho."""
