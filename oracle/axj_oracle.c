@@ -28,8 +28,10 @@
  * The restatement is pinned instead by operator known-answer tests (polynomial
  * exactness of SBP1/SBP2, TG row sums), the operator tables and default constants as the
  * reference's source text states them (tests/golden/reference_constants.json, equal bit
- * for bit), the shipped bc fixture (bc_4400x640_nozzle.dat) and free-stream
- * preservation, all in tests/.
+ * for bit), the shipped bc fixture (bc_4400x640_nozzle.dat), free-stream
+ * preservation, and a second restatement in plain Python (tests/restatement.py: the
+ * operators, the sensor, the right-hand side with the bc loop and sponges, RK4), equal
+ * to this one bit for bit, all in tests/.
  *
  * Restatement rules:
  *  - Same arithmetic and evaluation order as the Fortran source (left-to-right,

@@ -127,3 +127,295 @@ def sensor(pv, tables, maps, metrics, z, r, params):
         out.append(c * star)
     ramp = np.array([(1.0 + math.tanh(5.0 * (zi - 10.0))) / 2.0 for zi in z])
     return [o * ramp[None, :] for o in out]
+
+
+# ---------------------------------------------------------------------------
+# AssignValues, ComputeRHS with the bc loop and sponges, axis_conditions, RK4
+# ---------------------------------------------------------------------------
+AXIS, SAT_FARFIELD, NSCBC_NONREFLECTING, SAT_NOSLIP_WALL, NSCBC_NOSLIP_WALL = 90, 91, 92, 93, 94
+
+
+def assign_values(pv):
+    """AssignValues (ModAssign.f90:5-29): primitives, p = rho T, mu = kappa = T**0.666,
+    beta = (3/5) mu, lambda = beta - (2/3) mu (libm pow per value)."""
+    rho, Vr, Vt, Vz, T = (pv[k].copy() for k in range(5))
+    mu = np.vectorize(lambda t: math.pow(t, 0.666))(T)
+    beta = (3.0 / 5.0) * mu
+    return dict(rho=rho, Vr=Vr, Vt=Vt, Vz=Vz, T=T, p=rho * T, mu=mu, kappa=mu.copy(), beta=beta,
+                lam=beta - (2.0 / 3.0) * mu)
+
+
+def _eigen(rho, U, T, gam, rdir):
+    """eigen_matrices_in_z_direction (ModBC.f90:280-357, U = V_z) or _in_r_direction
+    (:359-437, U = V_r): the diagonal of lam, T_mat and T_mat_inv, 0-based."""
+    sT = math.sqrt(T)
+    lam = [U, U, U, U - sT, U + sT]
+    t_p = rho / ((gam - 1.0) * T)
+    t_m = -1.0 / ((gam - 1.0) * sT)
+    t_q = 1.0 / ((gam - 1.0) * sT)
+    i1 = -1.0 * (gam - 1.0) * T / (gam * rho)
+    i4 = (gam - 1.0) * T / (2.0 * gam * rho)
+    c_m = -1.0 * (gam - 1.0) * sT / 2.0
+    c_p = (gam - 1.0) * sT / 2.0
+    c5 = (gam - 1.0) / (2.0 * gam)
+    if not rdir:
+        Tm = [[-1.0 * rho / T, 0.0, 0.0, t_p, t_p],
+              [0.0, 0.0, 1.0, 0.0, 0.0],
+              [0.0, 1.0, 0.0, 0.0, 0.0],
+              [0.0, 0.0, 0.0, t_m, t_q],
+              [1.0, 0.0, 0.0, 1.0, 1.0]]
+        Ti = [[i1, 0.0, 0.0, 0.0, 1.0 / gam],
+              [0.0, 0.0, 1.0, 0.0, 0.0],
+              [0.0, 1.0, 0.0, 0.0, 0.0],
+              [i4, 0.0, 0.0, c_m, c5],
+              [i4, 0.0, 0.0, c_p, c5]]
+    else:
+        Tm = [[-1.0 * rho / T, 0.0, 0.0, t_p, t_p],
+              [0.0, 0.0, 0.0, t_m, t_q],
+              [0.0, 0.0, 1.0, 0.0, 0.0],
+              [0.0, 1.0, 0.0, 0.0, 0.0],
+              [1.0, 0.0, 0.0, 1.0, 1.0]]
+        Ti = [[i1, 0.0, 0.0, 0.0, 1.0 / gam],
+              [0.0, 0.0, 0.0, 1.0, 0.0],
+              [0.0, 0.0, 1.0, 0.0, 0.0],
+              [i4, c_m, 0.0, 0.0, c5],
+              [i4, c_p, 0.0, 0.0, c5]]
+    return lam, Tm, Ti
+
+
+def _matvec(A, v):
+    out = []
+    for r_ in range(5):
+        s = 0.0
+        for c in range(5):
+            s = s + A[r_][c] * v[c]
+        out.append(s)
+    return out
+
+
+def _t_lam_w(Tm, lam, w):
+    """MATMUL(MATMUL(T_mat, lam), w) with lam diagonal: the inner product's off-diagonal
+    terms are exact zeros."""
+    TL = [[0.0] * 5 for _ in range(5)]
+    for r_ in range(5):
+        for c in range(5):
+            s = 0.0
+            for k in range(5):
+                s = s + Tm[r_][k] * (lam[k] if k == c else 0.0)
+            TL[r_][c] = s
+    return _matvec(TL, w)
+
+
+def rhs(pv, tgt, tables, maps, metrics, z, r, params, patches):
+    """ComputeRHS (ModRHS.f90:5-258) of a single block on the state pv: the derivatives,
+    the sensor when shock capturing is on, the inviscid and viscous terms, the bc loop
+    (ModBC.f90:13-277) and the sponges (:548-617). Returns rhs[5, Nr, Nz]."""
+    s1, s2, tg = tables
+    dxidz, detadr, ddxidxidz, ddetadetadr = metrics
+    blank = maps["blank"] == 1
+    zr, rr = maps["zrow"], maps["rrow"]
+    gam, Re, Pr = params.gam, params.Re, params.Pr
+    Nr, Nz = pv.shape[1:]
+    q = assign_values(pv)
+    d1z = {k: stencil(s1, q[k], zr, blank, 1, 6, 5) * dxidz for k in ("rho", "Vr", "Vt", "Vz", "T", "p")}
+    d1r = {k: stencil(s1, q[k], rr, blank, 2, 6, 5) * detadr for k in ("rho", "Vr", "Vt", "Vz", "T", "p")}
+    sc = params.shock_capturing == 1
+    if sc:
+        ms, bs, ks = sensor(pv, tables, maps, metrics, z, r, params)
+        q["mu"] = q["mu"] + ms
+        q["beta"] = q["beta"] + bs
+        q["lam"] = q["beta"] - (2.0 / 3.0) * q["mu"]
+        q["kappa"] = q["kappa"] + ks
+    out = np.zeros((5, Nr, Nz))
+    R = np.broadcast_to(r[:, None], (Nr, Nz))
+    rho, Vr, Vt, Vz, T = q["rho"], q["Vr"], q["Vt"], q["Vz"], q["T"]
+    js = slice(1, Nr)  # the axis row is skipped
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out[0, js] = (Vr * d1r["rho"] + Vz * d1z["rho"] + rho * (d1r["Vr"] + Vr / R + d1z["Vz"]))[js]
+        out[1, js] = (Vr * d1r["Vr"] + Vz * d1z["Vr"] + 1.0 / (gam * rho) * d1r["p"])[js]
+        out[2, js] = (Vr * d1r["Vt"] + Vr * Vt / R + Vz * d1z["Vt"])[js]
+        out[3, js] = (Vr * d1r["Vz"] + Vz * d1z["Vz"] + 1.0 / (gam * rho) * d1z["p"])[js]
+        out[4, js] = (Vr * d1r["T"] + Vz * d1z["T"] + (gam - 1.0) * T * (d1r["Vr"] + Vr / R + d1z["Vz"]))[js]
+    out = -1.0 * out
+    if params.do_viscous_terms == 1:
+        def d2(k, dirn):
+            rows, met, met2, first = (zr, dxidz, ddxidxidz, d1z[k]) if dirn == 1 else (rr, detadr, ddetadetadr, d1r[k])
+            return stencil(s2, q[k], rows, blank, dirn, 6, 5) * (met * met) + first * met2
+        d2z = {k: d2(k, 1) for k in ("Vr", "Vt", "Vz", "T")}
+        d2r = {k: d2(k, 2) for k in ("Vr", "Vt", "Vz", "T")}
+        dmudz = stencil(s1, q["mu"], zr, blank, 1, 6, 5) * dxidz
+        dkapdz = stencil(s1, q["kappa"], zr, blank, 1, 6, 5) * dxidz
+        dmudr = stencil(s1, q["mu"], rr, blank, 2, 6, 5) * detadr
+        dkapdr = stencil(s1, q["kappa"], rr, blank, 2, 6, 5) * detadr
+        d2Vrdzdr = stencil(s1, d1z["Vr"], rr, blank, 2, 6, 5) * detadr
+        d2Vzdzdr = stencil(s1, d1z["Vz"], rr, blank, 2, 6, 5) * detadr
+        mu, kap = q["mu"], q["kappa"]
+        if sc:
+            tmp = q["lam"] / mu
+            f43, o13, t23 = 2.0 + tmp, 1.0 + tmp, -1.0 * tmp
+        else:
+            f43, o13, t23 = 29.0 / 15.0, 14.0 / 15.0, 1.0 / 15.0
+        with np.errstate(divide="ignore", invalid="ignore"):
+            obr = 1.0 / R
+        dVrdr, dVzdr, dVtdr, dTdr = d1r["Vr"], d1r["Vz"], d1r["Vt"], d1r["T"]
+        dVrdz, dVzdz, dVtdz, dTdz = d1z["Vr"], d1z["Vz"], d1z["Vt"], d1z["T"]
+        with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+            c = 1.0 / (Re * rho)
+            v2 = c * (mu * (f43 * d2r["Vr"] + f43 * obr * dVrdr + o13 * d2Vzdzdr + d2z["Vr"] - f43 * Vr * (obr * obr))
+                      + dmudr * (f43 * dVrdr - t23 * Vr * obr - t23 * dVzdz) + dmudz * (dVrdz + dVzdr))
+            v3 = c * (mu * (d2r["Vt"] + d2z["Vt"] + obr * dVtdr - Vt * (obr * obr)) + dmudr * (dVtdr - Vt * obr)
+                      + dmudz * dVtdz)
+            v4 = c * (mu * (d2r["Vz"] + f43 * d2z["Vz"] + o13 * d2Vrdzdr + obr * dVzdr + o13 * obr * dVrdz)
+                      + dmudr * (dVzdr + dVrdz) + dmudz * (f43 * dVzdz - t23 * dVrdr - t23 * Vr * obr))
+            x5 = gam / (Re * Pr * rho) * (kap * (d2r["T"] + obr * dTdr + d2z["T"]) + dkapdr * dTdr + dkapdz * dTdz)
+            y5 = gam * (gam - 1.0) / Re * mu / rho * (
+                dVrdr * (f43 * dVrdr - t23 * Vr * obr - t23 * dVzdz) + (dVtdr - Vt * obr) * (dVtdr - Vr * obr)
+                + Vr * obr * (f43 * Vr * obr - t23 * dVrdr - t23 * dVzdz) + dVtdz * dVtdz
+                + dVzdz * (f43 * dVzdz - t23 * dVrdr - t23 * Vr * obr) + (dVrdz + dVzdr) * (dVzdr + dVrdz))
+        out[1, js] = (out[1] + v2)[js]
+        out[2, js] = (out[2] + v3)[js]
+        out[3, js] = (out[3] + v4)[js]
+        out[4, js] = (out[4] + x5 + y5)[js]
+    _bc_loop(out, pv, tgt, q, d1z, d1r, dxidz, detadr, gam, patches)
+    _sponges(out, pv, tgt, z, r, params)
+    return out
+
+
+def _bc_loop(out, pv, tgt, q, d1z, d1r, dxidz, detadr, gam, patches):
+    """BoundaryConditions (ModBC.f90:13-277) for one block: patches in order, the face
+    line of each, SAT (compute_SAT_RHS :439-469) and NSCBC (ComputeNSCBCRHS :471-545)."""
+    sigma_1 = sigma_2 = -2.0
+    one_by_h_44 = 48.0 / 49.0
+    Nr, Nz = pv.shape[1:]
+    for (i_s, i_e, j_s, j_e, bc, d) in patches:
+        if bc == AXIS:
+            continue
+        if d == 1:
+            ii, jj = (i_s, i_s), (j_s, j_e)
+        elif d == -1:
+            ii, jj = (i_e, i_e), (j_s, j_e)
+        elif d == 2:
+            ii, jj = (i_s, i_e), (j_s, j_s)
+        else:
+            ii, jj = (i_s, i_e), (j_e, j_e)
+        adir = abs(d)
+        for i1 in range(ii[0], ii[1] + 1):
+            for j1 in range(jj[0], jj[1] + 1):
+                i, j = i1 - 1, j1 - 1
+                rho, Vr, Vz, T = q["rho"][j, i], q["Vr"][j, i], q["Vz"][j, i], q["T"][j, i]
+                pvl = [pv[e, j, i] for e in range(5)]
+                if bc == SAT_FARFIELD:
+                    if j1 == 1 or adir != 1:
+                        continue
+                    lam, Tm, Ti = _eigen(rho, Vz, T, gam, False)
+                    lam = [(abs(v) + v) / 2.0 if d > 0 else (abs(v) - v) / 2.0 for v in lam]
+                    w = _matvec(Ti, [pvl[e] - tgt[e, j, i] for e in range(5)])
+                    sat = _t_lam_w(Tm, lam, w)
+                    for e in range(5):
+                        out[e, j, i] = out[e, j, i] + sigma_1 * dxidz[j, i] * one_by_h_44 * sat[e]
+                elif bc == SAT_NOSLIP_WALL:
+                    rd = adir == 2
+                    tI = list(pvl)
+                    tI[1 if rd else 3] = 0.0
+                    lam, Tm, Ti = _eigen(rho, Vr if rd else Vz, T, gam, rd)
+                    lam = [(abs(v) + v) / 2.0 if d > 0 else (abs(v) - v) / 2.0 for v in lam]
+                    w = _matvec(Ti, [pvl[e] - tI[e] for e in range(5)])
+                    sat = _t_lam_w(Tm, lam, w)
+                    met = detadr[j, i] if rd else dxidz[j, i]
+                    for e in range(5):
+                        out[e, j, i] = out[e, j, i] + sigma_1 * met * one_by_h_44 * sat[e]
+                    tV = [pvl[0], 0.0, 0.0, 0.0, tgt[4, j, i]]
+                    for e in range(5):
+                        out[e, j, i] = out[e, j, i] + sigma_2 * met * one_by_h_44 * (pvl[e] - tV[e])
+                elif bc == NSCBC_NONREFLECTING:
+                    if j1 == 1:
+                        continue
+                    g = {k: (d1z[k][j, i], d1r[k][j, i]) for k in ("rho", "Vr", "Vt", "Vz", "T", "p")}
+                    if adir == 1:
+                        add = [Vz * g["rho"][0] + rho * g["Vz"][0], Vz * g["Vr"][0], Vz * g["Vt"][0],
+                               Vz * g["Vz"][0] + 1.0 / (gam * rho) * g["p"][0], Vz * g["T"][0] + (gam - 1.0) * T * g["Vz"][0]]
+                        lam, Tm, Ti = _eigen(rho, Vz, T, gam, False)
+                    else:
+                        add = [Vr * g["rho"][1] + rho * g["Vr"][1], Vr * g["Vr"][1] + 1.0 / (gam * rho) * g["p"][1],
+                               Vr * g["Vt"][1], Vr * g["Vz"][1], Vr * g["T"][1] + (gam - 1.0) * T * g["Vr"][1]]
+                        lam, Tm, Ti = _eigen(rho, Vr, T, gam, True)
+                    for e in range(5):
+                        out[e, j, i] = out[e, j, i] + add[e]
+                    # the non-reflecting face takes z-derivatives in both directions (:487-493)
+                    w = _matvec(Ti, [g[k][0] for k in ("rho", "Vr", "Vt", "Vz", "T")])
+                    w = [0.0 if ((d > 0 and lam[e] > 0.0) or (d < 0 and lam[e] < 0.0)) else w[e] for e in range(5)]
+                    ns = _t_lam_w(Tm, lam, w)
+                    for e in range(5):
+                        out[e, j, i] = out[e, j, i] - ns[e]
+                elif bc == NSCBC_NOSLIP_WALL:
+                    rd = adir == 2
+                    lam, Tm, Ti = _eigen(rho, Vr if rd else Vz, T, gam, rd)
+                    dv = [(d1r if rd else d1z)[k][j, i] for k in ("rho", "Vr", "Vt", "Vz", "T")]
+                    w = _matvec(Ti, dv)
+                    if d < 0:
+                        w[3] = -1.0 * w[4]
+                    else:
+                        w[4] = -1.0 * w[3]
+                    ns = _t_lam_w(Tm, lam, w)
+                    if rd:
+                        out[0, j, i] = out[0, j, i] + (Vr * d1r["rho"][j, i] + rho * d1r["Vr"][j, i])
+                    else:
+                        out[0, j, i] = out[0, j, i] + (Vz * d1z["rho"][j, i] + rho * d1z["Vz"][j, i])
+                    for e in range(5):
+                        out[e, j, i] = out[e, j, i] - ns[e]
+                    out[1:, j, i] = 0.0
+
+
+def _sponges(out, pv, tgt, z, r, params):
+    """sponge_bcs (ModBC.f90:548-617): the top sponge on every row, the inflow sponge from
+    row 2 (the axis rank), zeta**n_sponge with the real exponent 2.0 (libm pow)."""
+    st, At, el, Al = params.sponge_start_top, params.sponge_A_top, params.sponge_end_left, params.sponge_A_left
+    Nr, Nz = pv.shape[1:]
+    for i in range(Nz):
+        for j in range(Nr):
+            if r[j] >= st:
+                for e in range(5):
+                    zeta = (r[j] - st) / (r[Nr - 1] - st)
+                    out[e, j, i] = out[e, j, i] - At * math.pow(zeta, 2.0) * (pv[e, j, i] - tgt[e, j, i])
+    for i in range(Nz):
+        for j in range(1, Nr):
+            if z[i] <= el:
+                for e in range(5):
+                    zeta = (el - z[i]) / el
+                    out[e, j, i] = out[e, j, i] - Al * math.pow(zeta, 2.0) * (pv[e, j, i] - tgt[e, j, i])
+
+
+def axis_conditions(pv, prim, s1):
+    """axis_conditions (ModAxis.f90:5-35): row 1 of rho, V_z, T from rows 2..6 of the
+    primitives of the previous AssignValues (the stage input), into pv."""
+    for k, e in (("rho", 0), ("Vz", 3), ("T", 4)):
+        f = prim[k]
+        col = np.zeros(f.shape[1])
+        for i in range(f.shape[1]):
+            d = 0.0
+            for m in range(1, 6):
+                d = d + s1[0][m] * f[m, i]
+            col[i] = -1.0 * d / s1[0][0]
+        pv[e, 0, :] = col
+
+
+def rk4(pv, tgt, delt, tables, maps, metrics, z, r, params, patches):
+    """RK4 (ModRungeKutta.f90:5-171): k_s = delt*rhs, stages pv_old + 0.5 k1, + 0.5 k2,
+    + k3, each followed by axis_conditions on the stage input's primitives; the final
+    update skips blanked points."""
+    pv_old = pv.copy()
+    cur = pv.copy()
+    ks = []
+    for s, a in enumerate((0.5, 0.5, 1.0, None)):
+        prim = assign_values(cur)
+        k = delt * rhs(cur, tgt, tables, maps, metrics, z, r, params, patches)
+        ks.append(k)
+        if a is not None:
+            cur = pv_old + a * k if a != 1.0 else pv_old + k
+            axis_conditions(cur, prim, tables[0])
+    prim = assign_values(cur)
+    new = pv_old + 1.0 / 6.0 * ks[0] + 1.0 / 3.0 * (ks[1] + ks[2]) + 1.0 / 6.0 * ks[3]
+    blank = maps["blank"] == 1
+    new[:, blank] = cur[:, blank]
+    axis_conditions(new, prim, tables[0])
+    return new
