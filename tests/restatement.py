@@ -419,3 +419,27 @@ def rk4(pv, tgt, delt, tables, maps, metrics, z, r, params, patches):
     new[:, blank] = cur[:, blank]
     axis_conditions(new, prim, tables[0])
     return new
+
+
+def compute_time_step(pv, blank, metrics, params, stale_T=None):
+    """ComputeTimeStep (ModInputOutput.f90:389-438) of a single block: the CFL step of
+    every point (100 at blanked points) with the scalar stale_T, or the local T where
+    stale_T is None, and its minimum."""
+    q = assign_values(pv)
+    dxidz, detadr = metrics[0], metrics[1]
+    Re, Pr, CFL = params.Re, params.Pr, params.CFL
+    best = math.inf
+    Nr, Nz = pv.shape[1:]
+    for i in range(Nz):
+        for j in range(Nr):
+            if blank[j, i]:
+                d = 100.0
+            else:
+                x, y = dxidz[j, i], detadr[j, i]
+                Ts = q["T"][j, i] if stale_T is None else stale_T
+                inv = abs(q["Vz"][j, i] * x + q["Vr"][j, i] * y) + math.sqrt(Ts) * math.sqrt(x * x + y * y)
+                s = abs(x) + abs(y)
+                visc = 2.0 * max(q["mu"][j, i] / Re, q["lam"][j, i] / Re, q["kappa"][j, i] / (Re * Pr)) * (s * s)
+                d = CFL / (inv + visc)
+            best = min(best, d)
+    return best

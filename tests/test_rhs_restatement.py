@@ -67,3 +67,17 @@ def test_rk4_step_equals_the_oracle_bit_for_bit(oracle_mod, name):
     o.rk4(dt)
     got = rs.rk4(pv, c["target"], dt, *args)
     assert np.array_equal(got, o.get_state())
+
+
+@pytest.mark.parametrize("dt_mode", [0, 1])
+def test_time_step_equals_the_oracle_bit_for_bit(oracle_mod, dt_mode):
+    """Reference mode: the stale module scalar T (0 before the first right-hand side,
+    then the oracle's tracked value); physical mode: the local T."""
+    c = _nozzle(SAT_NOSLIP_WALL, sc=True, Mj=1.5, Re=5000.0, dt_mode=dt_mode)
+    o, args = _setup(oracle_mod, c)
+    blank = args[1]["blank"] == 1
+    for _ in range(2):
+        stale = None if dt_mode == 1 else o.stale_T()
+        want = o.compute_time_step()
+        assert rs.compute_time_step(o.get_state(), blank, args[2], c["params"], stale) == want
+        o.rk4(want)
