@@ -443,3 +443,32 @@ def compute_time_step(pv, blank, metrics, params, stale_T=None):
                 d = CFL / (inv + visc)
             best = min(best, d)
     return best
+
+
+def compute_metric_1d(s1, x):
+    """ComputeMetric (ModDeriv.f90:241-382) along one coordinate line of a single block
+    (every neighbour is MPI_PROC_NULL): SBP1 closure rows on the 4 points at each end,
+    the centred row between."""
+    n = len(x)
+    out = np.zeros(n)
+    for i in range(n):
+        if i < 4:
+            row, w0, m = i, 0, 6
+        elif i >= n - 4:
+            row, w0, m = 8 - (n - 1) + i, n - 6, 6
+        else:
+            row, w0, m = 4, i - 2, 5
+        out[i] = dot(s1[row], x, w0, m)
+    return out
+
+
+def metrics(s1, z, r):
+    """dxi/dz, deta/dr and their derivatives as ModSolver.f90:56-73 forms them:
+    (dxidz, detadr, ddxidxidz, ddetadetadr) on the (Nr, Nz) grid."""
+    dxidz = 1.0 / compute_metric_1d(s1, z)
+    detadr = 1.0 / compute_metric_1d(s1, r)
+    dd_z = compute_metric_1d(s1, dxidz)
+    dd_r = compute_metric_1d(s1, detadr)
+    Nz, Nr = len(z), len(r)
+    b = lambda v, ax: np.broadcast_to(v[None, :] if ax == 1 else v[:, None], (Nr, Nz)).copy()
+    return b(dxidz, 1), b(detadr, 2), b(dd_z, 1), b(dd_r, 2)

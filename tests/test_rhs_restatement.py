@@ -81,3 +81,26 @@ def test_time_step_equals_the_oracle_bit_for_bit(oracle_mod, dt_mode):
         want = o.compute_time_step()
         assert rs.compute_time_step(o.get_state(), blank, args[2], c["params"], stale) == want
         o.rk4(want)
+
+
+@pytest.mark.parametrize("name", ["jet", "nozzle_nscbc_wall"])
+def test_metrics_equal_the_oracle_bit_for_bit(oracle_mod, name):
+    """ComputeMetric of the coordinates and of the inverted first metrics."""
+    c = CASES[name]()
+    o, _ = _setup(oracle_mod, c)
+    got = rs.metrics(axj.operator_tables()[0], c["z"], c["r"])
+    for g, w in zip(got, o.metrics()):
+        assert np.array_equal(g, w)
+
+
+def test_restated_pipeline_with_restated_metrics(oracle_mod):
+    """The whole second restatement with its own metrics: one RK4 step of the
+    shock-capturing nozzle equals the oracle's."""
+    c = CASES["nozzle_sat_wall_sc"]()
+    c["pv"] = _state(c)
+    o, args = _setup(oracle_mod, c)
+    own = rs.metrics(args[0][0], c["z"], c["r"])
+    dt = o.compute_time_step()
+    o.rk4(dt)
+    got = rs.rk4(c["pv"], c["target"], dt, args[0], args[1], own, *args[3:])
+    assert np.array_equal(got, o.get_state())
