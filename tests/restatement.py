@@ -472,3 +472,46 @@ def metrics(s1, z, r):
     Nz, Nr = len(z), len(r)
     b = lambda v, ax: np.broadcast_to(v[None, :] if ax == 1 else v[:, None], (Nr, Nz)).copy()
     return b(dxidz, 1), b(detadr, 2), b(dd_z, 1), b(dd_r, 2)
+
+
+def create_patches(records, Nz, Nr):
+    """CreateAllPatches + PatchCreation (ModPatch.f90:117-309) for a single block holding
+    the grid: -1 indices resolved to the grid size, each face widened to its 4-wide strip,
+    the strip's first and last points inside the block found in the block's loop order
+    (i outer, j inner), a patch kept when any point of the block lies in its strip.
+    Returns (i_start, i_end, j_start, j_end, bc, bc_dir) tuples."""
+    out = []
+    for bc, d, bis, bie, bjs, bje in records:
+        bis = Nz if bis == -1 else bis
+        bjs = Nr if bjs == -1 else bjs
+        bie = Nz if bie == -1 else bie
+        bje = Nr if bje == -1 else bje
+        if d == 1:
+            ps, pe, qs, qe = bis, bis + 3, bjs, bje
+        elif d == -1:
+            ps, pe, qs, qe = bie - 3, bie, bjs, bje
+        elif d == 2:
+            ps, pe, qs, qe = bis, bie, bjs, bjs + 3
+        else:
+            ps, pe, qs, qe = bis, bie, bje - 3, bje
+        found = 0
+        s_i = s_j = e_i = e_j = 0
+        for i in range(1, Nz + 1):
+            for j in range(1, Nr + 1):
+                if (i - ps) * (i - pe) <= 0 and (j - qs) * (j - qe) <= 0:
+                    if not found:
+                        s_i, s_j, found = i, j, 1
+                    else:
+                        e_i, e_j = i, j
+        if not found:
+            continue
+        if d == 1:
+            p = (s_i, s_i + 3, s_j, e_j)
+        elif d == -1:
+            p = (e_i - 3, e_i, s_j, e_j)
+        elif d == 2:
+            p = (s_i, e_i, s_j, s_j + 3)
+        else:
+            p = (s_i, e_i, e_j - 3, e_j)
+        out.append(p + (bc, d))
+    return out

@@ -104,3 +104,14 @@ def test_restated_pipeline_with_restated_metrics(oracle_mod):
     o.rk4(dt)
     got = rs.rk4(c["pv"], c["target"], dt, args[0], args[1], own, *args[3:])
     assert np.array_equal(got, o.get_state())
+
+
+def test_patch_creation_equals_the_library():
+    """PatchCreation of the library (axj_patches_from_records) against the restatement, on
+    the reference's nozzle bc file and the fixtures' layouts."""
+    import os
+    rec = axj.read_bc_file(os.path.join(os.path.dirname(__file__), "golden", "bc_4400x640_nozzle.dat"))
+    layouts = [(rec, 4400, 640), (rec, 640, 200), (fixtures.JET_RECORDS, 96, 64),
+               (fixtures.nozzle_records(20, 24, 28), 96, 64), (fixtures.writemesh_case()["records"], 250, 50)]
+    for records, Nz, Nr in layouts:
+        assert axj.patches_from_records(records, Nz, Nr) == rs.create_patches(records, Nz, Nr)
