@@ -19,7 +19,7 @@ from ._ffi import (AXJ_OK, STATUS, AxjBatchTuning, AxjBcRecord, AxjMlp, AxjParam
                    default_params, default_train_cfg, dptr, patch_array, patches_to_tuples, record_array)
 
 __all__ = ["AxiJetSolver", "AxjBatch", "AxjError", "AxjMlp", "default_params", "default_train_cfg", "load_library",
-           "read_bc_file", "patches_from_records", "operator_tables", "point_maps", "library_path", "mlp_init"]
+           "read_bc_file", "patches_from_records", "operator_tables", "point_maps", "prep_maps", "library_path", "mlp_init"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -70,6 +70,8 @@ def load_library():
         "axj_destroy": (None, [h]),
         "axj_read_bc_file": (C.c_int, [C.c_char_p, C.POINTER(AxjBcRecord), i64, C.POINTER(i64)]),
         "axj_operator_tables": (C.c_int, [dp, dp, dp]),
+        "axj_prep_maps": (C.c_int, [C.POINTER(AxjPatch), i64, i64, i64, dp, i64, C.c_void_p, C.c_void_p, i64,
+                                    C.POINTER(i64), C.c_void_p, i64, C.c_void_p, C.c_void_p]),
         "axj_point_maps": (C.c_int, [C.POINTER(AxjPatch), i64, i64, i64, dp, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p]),
         "axj_patches_from_records": (C.c_int, [C.POINTER(AxjBcRecord), i64, i64, i64, C.POINTER(AxjPatch),
@@ -138,6 +140,31 @@ def point_maps(patches, Nz, Nr, ibval):
                                          out["rrow"].ctypes.data, out["blank"].ctypes.data,
                                          out["nfaceops"].ctypes.data, out["faceop_ids"].ctypes.data))
     return out
+
+
+def prep_maps(patches, Nz, Nr, ibval, algorithm=0):
+    """The descriptors (Nr rows of pitch P = Nz rounded up to 32), face list, tile lists
+    and stale-T point that axj_create builds: algorithm 0 the host path, 1 the device
+    path's per-row / per-tile functions run on the host, 2 the device path."""
+    lib = load_library()
+    ib = np.ascontiguousarray(ibval, dtype=np.float64)
+    pa = patch_array(patches)
+    P = (Nz + 31) // 32 * 32
+    desc = np.zeros((Nr, P), dtype=np.uint32)
+    nf = C.c_int64(0)
+    counts = np.zeros(4, dtype=np.int64)
+    stale = np.zeros(2, dtype=np.int64)
+    ntile_cap = 2 * ((Nz + 31) // 32) * (Nr // 8 + 2)
+    faces = np.zeros(1 << 20, dtype=np.int32)
+    tiles = np.zeros((ntile_cap, 2), dtype=np.int32)
+    _check(lib, None, lib.axj_prep_maps(pa, len(patches), Nz, Nr, dptr(ib), int(algorithm), desc.ctypes.data,
+                                        faces.ctypes.data, faces.size, C.byref(nf), tiles.ctypes.data, ntile_cap,
+                                        counts.ctypes.data, stale.ctypes.data))
+    lists, n = [], 0
+    for c in counts:
+        lists.append(tiles[n:n + c].copy())
+        n += c
+    return {"desc": desc, "faces": faces[:nf.value].copy(), "tiles": lists, "stale": tuple(int(v) for v in stale)}
 
 
 def read_bc_file(path):

@@ -53,7 +53,8 @@ class AxjParams(C.Structure):
         ("harmonic_amp", C.c_double),
         ("harmonic_st", C.c_double),
         ("harmonic_uj", C.c_double),
-        ("reserved", C.c_int64 * 4),
+        ("patch_prep", C.c_int64),
+        ("reserved", C.c_int64 * 3),
     ]
 
 

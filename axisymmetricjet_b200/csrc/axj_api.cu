@@ -13,6 +13,7 @@
 
 #include "../../include/axj.h"
 #include "axj_common.cuh"
+#include "axj_prep.cuh"
 #include "axj_kernels.cuh"
 #include "axj_mlp.cuh"
 
@@ -797,6 +798,196 @@ static int build_point_maps(const axj_patch* patches, int64_t npatch, int64_t Nz
   return AXJ_OK;
 }
 
+// The tiles of the stage and sensor kernels, in launch order: r bands [0, 8), then bands
+// of TR rows up to 8 rows short of the top, then the rest in bands of at most TR rows;
+// per band the tiles along z. Interior tiles need a full band; the thin bands along r = 0
+// and r = r_max (closure rows, the axis, faces) hold general tiles that own only their
+// band's rows (the row count is packed into the tile's j0: bits 24-31 hold TR - rows).
+// Entries (i0, j0, rows).
+static std::vector<int64_t> tile_candidates(int64_t Nz, int64_t Nr) {
+  std::vector<std::pair<int64_t, int64_t>> bands;
+  int64_t j = 0;
+  if (Nr > 24) {
+    bands.push_back({0, 8});
+    j = 8;
+  }
+  while (j + TR <= Nr - 8) {
+    bands.push_back({j, TR});
+    j += TR;
+  }
+  while (j < Nr) {
+    const int64_t rows = std::min<int64_t>(TR, Nr - j);
+    bands.push_back({j, rows});
+    j += rows;
+  }
+  std::vector<int64_t> c;
+  for (const auto& band : bands)
+    for (int64_t i0 = 0; i0 < Nz; i0 += TZ) {
+      c.push_back(i0);
+      c.push_back(band.first);
+      c.push_back(band.second);
+    }
+  return c;
+}
+
+// The tile lists from the classes of the candidates (bit 0 interior stage tile, bit 1
+// interior sensor tile).
+static void tile_lists(const std::vector<int64_t>& cand, const std::vector<unsigned char>& flags,
+                       std::vector<int2>& tint, std::vector<int2>& tgen, std::vector<int2>& sti,
+                       std::vector<int2>& stg) {
+  tint.clear(); tgen.clear(); sti.clear(); stg.clear();
+  for (size_t t = 0; t < flags.size(); ++t) {
+    const int64_t i0 = cand[3 * t], j0 = cand[3 * t + 1], brows = cand[3 * t + 2];
+    const int ytile = (int)j0 | (int)((TR - brows) << 24);
+    const bool interior = flags[t] & 1, sint = (flags[t] >> 1) & 1;
+    (interior ? tint : tgen).push_back(make_int2((int)i0, interior ? (int)j0 : ytile));
+    (sint ? sti : stg).push_back(make_int2((int)i0, sint ? (int)j0 : ytile));
+  }
+}
+
+// Classes of every candidate tile from the descriptors (pitch P), on the host.
+static std::vector<unsigned char> classify_tiles(const std::vector<uint32_t>& desc, int64_t P, int64_t Nz,
+                                                 int64_t Nr, const std::vector<int64_t>& cand) {
+  std::vector<unsigned char> flags(cand.size() / 3);
+  auto dsc = [&](int64_t i, int64_t j) { return desc[(size_t)j * P + i]; };
+  for (size_t t = 0; t < flags.size(); ++t) {
+    const int64_t i0 = cand[3 * t], j0 = cand[3 * t + 1], brows = cand[3 * t + 2];
+    bool interior = brows == TR && i0 - H_INT >= 0 && i0 + TZ + H_INT <= Nz && j0 - H_INT >= 0 &&
+                    j0 + TR + H_INT <= Nr;
+    for (int64_t j = j0; interior && j < j0 + TR; ++j)
+      for (int64_t i = i0; interior && i < i0 + TZ; ++i) {
+        uint32_t d = dsc(i, j);
+        if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d) || desc_face(d) != 0) interior = false;
+      }
+    // r-halo points on the tile columns: dV/dz there feeds the mixed derivatives, and
+    // the r filter of the coefficients runs there with the centred row
+    for (int64_t j = j0 - H_INT; interior && j < j0 + TR + H_INT; ++j) {
+      if (j >= j0 && j < j0 + TR) continue;
+      for (int64_t i = i0; interior && i < i0 + TZ; ++i) {
+        uint32_t d = dsc(i, j);
+        if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d)) interior = false;
+      }
+    }
+    // z-halo points on the tile rows: the r filter of the coefficients
+    for (int64_t j = j0; interior && j < j0 + TR; ++j)
+      for (int64_t i = i0 - H_INT; interior && i < i0 + TZ + H_INT; ++i) {
+        if (i >= i0 && i < i0 + TZ) continue;
+        uint32_t d = dsc(i, j);
+        if (desc_rrow(d) != 4 || desc_blank(d)) interior = false;
+      }
+    // sensor classes: S, T and the dilatation are formed on a cross of halo
+    // SENS_HS_INT from V_r, V_z stencils of reach H_INT, so every point within
+    // SENS_HS_INT of the tile must use centred rows, and the V region must lie inside.
+    const int64_t hv = SENS_HS_INT + H_INT, hs = SENS_HS_INT;
+    bool sint = brows == TR && i0 - hz_of((int)hv) >= 0 && i0 + TZ + hz_of((int)hv) <= Nz && j0 - hv >= 0 &&
+                j0 + TR + hv <= Nr;
+    for (int64_t j = j0 - hs; sint && j < j0 + TR + hs; ++j)
+      for (int64_t i = i0 - hs; sint && i < i0 + TZ + hs; ++i) {
+        uint32_t d = dsc(i, j);
+        if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d)) sint = false;
+      }
+    flags[t] = (unsigned char)((interior ? 1 : 0) | (sint ? 2 : 0));
+  }
+  return flags;
+}
+
+// The point where the stale scalar T is taken (1-based): the last face point of the bc
+// loop that acts, else the last point of the RHS loops (ModRHS.f90:76,145).
+static void stale_T_point(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, int64_t& iT,
+                          int64_t& jT) {
+  iT = Nz;
+  jT = Nr;
+  for (int64_t k = 0; k < npatch; ++k) {
+    const axj_patch& p = patches[k];
+    if (p.bc == AXJ_BC_AXIS) continue;
+    int64_t is, ie, js, je;
+    if (p.bc_dir == 1) { is = ie = p.i_start; js = p.j_start; je = p.j_end; }
+    else if (p.bc_dir == -1) { is = ie = p.i_end; js = p.j_start; je = p.j_end; }
+    else if (p.bc_dir == 2) { is = p.i_start; ie = p.i_end; js = je = p.j_start; }
+    else { is = p.i_start; ie = p.i_end; js = je = p.j_end; }
+    const int adir = (int)(p.bc_dir < 0 ? -p.bc_dir : p.bc_dir);
+    for (int64_t i = is; i <= ie; ++i)
+      for (int64_t j = js; j <= je; ++j) {
+        if (i < 1 || i > Nz || j < 1 || j > Nr) continue;
+        const bool j1 = (j == 1);
+        bool active = false;
+        if (p.bc == AXJ_BC_SAT_FARFIELD) active = !j1 && adir == 1;
+        else if (p.bc == AXJ_BC_SAT_NOSLIP_WALL || p.bc == AXJ_BC_NSCBC_NOSLIP_WALL) active = true;
+        else if (p.bc == AXJ_BC_NSCBC_NONREFLECTING) active = !j1;
+        if (!active) continue;
+        iT = i;
+        jT = j;
+      }
+  }
+}
+
+// The host algorithm: build_point_maps, the z / r codes and the tile classes.
+static int host_patch_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, int64_t P,
+                           const double* ibval, std::vector<uint32_t>& desc, std::vector<unsigned char>& zcode,
+                           std::vector<unsigned char>& rcode, std::vector<int>& faces, std::vector<int2>& tint,
+                           std::vector<int2>& tgen, std::vector<int2>& sti, std::vector<int2>& stg, int64_t& iT,
+                           int64_t& jT, std::string& msg) {
+  const int rc = build_point_maps(patches, npatch, Nz, Nr, P, ibval, desc, faces, iT, jT, msg);
+  if (rc != AXJ_OK) return rc;
+  zcode.resize(desc.size());
+  rcode.resize(desc.size());
+  for (size_t x = 0; x < desc.size(); ++x) {
+    zcode[x] = (unsigned char)(desc_blank(desc[x]) ? ROW_NONE : (uint32_t)desc_zrow(desc[x]));
+    rcode[x] = (unsigned char)(desc_blank(desc[x]) ? ROW_NONE : (uint32_t)desc_rrow(desc[x]));
+  }
+  const std::vector<int64_t> cand = tile_candidates(Nz, Nr);
+  tile_lists(cand, classify_tiles(desc, P, Nz, Nr, cand), tint, tgen, sti, stg);
+  return AXJ_OK;
+}
+
+// The device algorithm (axj_prep.cuh, one thread per row and per tile), or with
+// emulate the same per-row and per-tile functions run on the host.
+static int device_patch_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, int64_t P,
+                             const double* ibval, std::vector<uint32_t>& desc, std::vector<unsigned char>& zcode,
+                             std::vector<unsigned char>& rcode, std::vector<int>& faces, std::vector<int2>& tint,
+                             std::vector<int2>& tgen, std::vector<int2>& sti, std::vector<int2>& stg, int64_t& iT,
+                             int64_t& jT, std::string& msg, bool emulate = false) {
+  const PrepArgs a{patches, (int)npatch, Nz, Nr, P, ibval};
+  const std::vector<int64_t> cand = tile_candidates(Nz, Nr);
+  const int64_t ncand = (int64_t)cand.size() / 3;
+  desc.assign((size_t)P * Nr, 0);
+  zcode.assign(desc.size(), 0);
+  rcode.assign(desc.size(), 0);
+  std::vector<unsigned char> flags((size_t)ncand);
+  if (emulate) {
+    std::vector<int64_t> off((size_t)Nr);
+    int64_t total = 1;
+    for (int64_t j = 1; j <= Nr; ++j) {
+      const int64_t sz = prep_row_size(a, j);
+      if (sz < 0) {
+        msg = "more than " + std::to_string(MAX_FACE_OPS) + " face operations at a point of row " + std::to_string(j);
+        return AXJ_ERR_BADPATCH;
+      }
+      off[j - 1] = total;
+      total += sz;
+    }
+    if (total >= (1 << 20)) {
+      msg = "too many face points";
+      return AXJ_ERR_BADPATCH;
+    }
+    faces.assign((size_t)total, 0);
+    for (int64_t j = 1; j <= Nr; ++j) prep_row(a, j, off[j - 1], desc.data(), zcode.data(), rcode.data(), faces.data());
+    for (int64_t t = 0; t < ncand; ++t)
+      flags[t] = (unsigned char)prep_tile_flags(desc.data(), P, Nz, Nr, cand[3 * t], cand[3 * t + 1], cand[3 * t + 2]);
+  } else {
+    char b[256] = {0};
+    const int rc = prep_on_device(a, cand.data(), ncand, desc.data(), zcode.data(), rcode.data(), faces, flags.data(),
+                                  b, (int)sizeof(b));
+    if (rc != AXJ_OK) {
+      msg = b;
+      return rc;
+    }
+  }
+  tile_lists(cand, flags, tint, tgen, sti, stg);
+  stale_T_point(patches, npatch, Nz, Nr, iT, jT);
+  return AXJ_OK;
+}
+
 extern "C" {
 
 int axj_operator_tables(double* sbp1, double* sbp2, double* tgfilt) {
@@ -837,6 +1028,54 @@ int axj_point_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t
     for (int k = 0; f && k < faces[f]; ++k) ids |= (uint64_t)(faces[f + 1 + k] + 1) << (8 * k);
     faceop_ids[x] = ids;
   }
+  return AXJ_OK;
+}
+
+int axj_prep_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, const double* ibval,
+                  int64_t algorithm, uint32_t* desc, int32_t* faces, int64_t faces_cap, int64_t* nfaces,
+                  int32_t* tiles, int64_t tiles_cap, int64_t* counts, int64_t* stale) {
+  if ((npatch > 0 && !patches) || !ibval || !desc || !nfaces || !counts || !stale)
+    return fail(nullptr, AXJ_ERR_ARG, "null argument");
+  if (Nz < 1 || Nr < 1) return fail(nullptr, AXJ_ERR_ARG, "grid %lld x %lld", (long long)Nz, (long long)Nr);
+  if (npatch < 0 || npatch > MAX_PATCHES) return fail(nullptr, AXJ_ERR_BADPATCH, "%lld patches", (long long)npatch);
+  for (int64_t k = 0; k < npatch; ++k) {
+    const int64_t d = patches[k].bc_dir;
+    if (d != 1 && d != -1 && d != 2 && d != -2)
+      return fail(nullptr, AXJ_ERR_BADPATCH, "patch %lld: bc_dir %lld", (long long)k + 1, (long long)d);
+  }
+  if (algorithm < 0 || algorithm > 2) return fail(nullptr, AXJ_ERR_ARG, "algorithm %lld", (long long)algorithm);
+  const int64_t P = (Nz + 31) / 32 * 32;
+  std::vector<uint32_t> dv;
+  std::vector<unsigned char> zc, rc_;
+  std::vector<int> fv;
+  std::vector<int2> lists[4];
+  int64_t iT = 0, jT = 0;
+  std::string msg;
+  const int rc = algorithm == 0
+                     ? host_patch_maps(patches, npatch, Nz, Nr, P, ibval, dv, zc, rc_, fv, lists[0], lists[1], lists[2],
+                                       lists[3], iT, jT, msg)
+                     : device_patch_maps(patches, npatch, Nz, Nr, P, ibval, dv, zc, rc_, fv, lists[0], lists[1],
+                                         lists[2], lists[3], iT, jT, msg, algorithm == 1);
+  if (rc != AXJ_OK) return fail(nullptr, rc, "%s", msg.c_str());
+  std::memcpy(desc, dv.data(), dv.size() * sizeof(uint32_t));
+  *nfaces = (int64_t)fv.size();
+  if (faces && (int64_t)fv.size() <= faces_cap) std::memcpy(faces, fv.data(), fv.size() * sizeof(int32_t));
+  int64_t n = 0;
+  for (int c = 0; c < 4; ++c) {
+    counts[c] = (int64_t)lists[c].size();
+    for (const int2& t : lists[c]) {
+      if (tiles && n < tiles_cap) {
+        tiles[2 * n] = t.x;
+        tiles[2 * n + 1] = t.y;
+      }
+      ++n;
+    }
+  }
+  stale[0] = iT;
+  stale[1] = jT;
+  if ((faces && (int64_t)fv.size() > faces_cap) || (tiles && n > tiles_cap))
+    return fail(nullptr, AXJ_ERR_ARG, "output capacity: %lld face entries, %lld tiles", (long long)fv.size(),
+                (long long)n);
   return AXJ_OK;
 }
 
@@ -983,6 +1222,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     return fail(nullptr, AXJ_ERR_UNSUPPORTED, "precision %lld not built", (long long)prm->precision);
   if (prm->sensor != AXJ_SENSOR_PLAIN && prm->sensor != AXJ_SENSOR_LEARNED && prm->sensor != AXJ_SENSOR_HELD)
     return fail(nullptr, AXJ_ERR_ARG, "sensor %lld unknown", (long long)prm->sensor);
+  if (prm->patch_prep != 0 && prm->patch_prep != 1)
+    return fail(nullptr, AXJ_ERR_ARG, "patch_prep %lld unknown", (long long)prm->patch_prep);
   if (prm->sensor != AXJ_SENSOR_PLAIN && !prm->shock_capturing)
     return fail(nullptr, AXJ_ERR_ARG, "the learned sensor needs shock_capturing = 1");
   if (prm->sensor != AXJ_SENSOR_PLAIN && (prm->judge_every < 1 || !(prm->judge_threshold >= 0.0)))
@@ -1068,13 +1309,20 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     if (j == Nr - 1) drv[j] = r[Nr - 1] - r[Nr - 2];
   }
 
-  // ---- stencil maps (CreateAllPatches, ModPatch.f90:214-242) -> per-point descriptors
+  // ---- stencil maps (CreateAllPatches, ModPatch.f90:214-242) -> per-point descriptors,
+  // face-operation lists and tile classes, on the host or on the device
   std::vector<uint32_t> desc;
   std::vector<int> faces;
+  std::vector<unsigned char> zcode, rcode;
+  std::vector<int2> tint, tgen, sti, stg;
   int64_t iT = Nz, jT = Nr;
   {
     std::string msg;
-    const int prc = build_point_maps(patches, npatch, Nz, Nr, h->P, ibval, desc, faces, iT, jT, msg);
+    const int prc = prm->patch_prep == 1
+                        ? device_patch_maps(patches, npatch, Nz, Nr, h->P, ibval, desc, zcode, rcode, faces, tint, tgen,
+                                            sti, stg, iT, jT, msg)
+                        : host_patch_maps(patches, npatch, Nz, Nr, h->P, ibval, desc, zcode, rcode, faces, tint, tgen,
+                                          sti, stg, iT, jT, msg);
     if (prc != AXJ_OK) {
       delete h;
       return fail(nullptr, prc, "%s", msg.c_str());
@@ -1082,78 +1330,6 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   }
   h->iT = (int)(iT - 1);
   h->jT = (int)(jT - 1);
-  std::vector<unsigned char> zcode(desc.size()), rcode(desc.size());
-  for (size_t x = 0; x < desc.size(); ++x) {
-    zcode[x] = (unsigned char)(desc_blank(desc[x]) ? ROW_NONE : (uint32_t)desc_zrow(desc[x]));
-    rcode[x] = (unsigned char)(desc_blank(desc[x]) ? ROW_NONE : (uint32_t)desc_rrow(desc[x]));
-  }
-
-  // ---- tile classes
-  std::vector<int2> tint, tgen, sti, stg;
-  auto dsc = [&](int64_t i, int64_t j) { return desc[(size_t)j * h->P + i]; };
-  // r bands: [0, 8), then bands of TR rows up to 8 rows short of the top, then the rest
-  // in bands of at most TR rows. Interior tiles need a full band; the thin bands along
-  // r = 0 and r = r_max (closure rows, the axis, faces) hold general tiles that own only
-  // their band's rows (the row count is packed into the tile's j0: bits 24-31 hold
-  // TR - rows).
-  std::vector<std::pair<int64_t, int64_t>> bands;
-  {
-    int64_t j = 0;
-    if (Nr > 24) {
-      bands.push_back({0, 8});
-      j = 8;
-    }
-    while (j + TR <= Nr - 8) {
-      bands.push_back({j, TR});
-      j += TR;
-    }
-    while (j < Nr) {
-      const int64_t rows = std::min<int64_t>(TR, Nr - j);
-      bands.push_back({j, rows});
-      j += rows;
-    }
-  }
-  for (const auto& band : bands)
-    for (int64_t i0 = 0; i0 < Nz; i0 += TZ) {
-      const int64_t j0 = band.first, brows = band.second;
-      const int ytile = (int)j0 | (int)((TR - brows) << 24);
-      bool interior = brows == TR && i0 - H_INT >= 0 && i0 + TZ + H_INT <= Nz && j0 - H_INT >= 0 &&
-                      j0 + TR + H_INT <= Nr;
-      for (int64_t j = j0; interior && j < j0 + TR; ++j)
-        for (int64_t i = i0; interior && i < i0 + TZ; ++i) {
-          uint32_t d = dsc(i, j);
-          if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d) || desc_face(d) != 0) interior = false;
-        }
-      // r-halo points on the tile columns: dV/dz there feeds the mixed derivatives, and
-      // the r filter of the coefficients runs there with the centred row
-      for (int64_t j = j0 - H_INT; interior && j < j0 + TR + H_INT; ++j) {
-        if (j >= j0 && j < j0 + TR) continue;
-        for (int64_t i = i0; interior && i < i0 + TZ; ++i) {
-          uint32_t d = dsc(i, j);
-          if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d)) interior = false;
-        }
-      }
-      // z-halo points on the tile rows: the r filter of the coefficients
-      for (int64_t j = j0; interior && j < j0 + TR; ++j)
-        for (int64_t i = i0 - H_INT; interior && i < i0 + TZ + H_INT; ++i) {
-          if (i >= i0 && i < i0 + TZ) continue;
-          uint32_t d = dsc(i, j);
-          if (desc_rrow(d) != 4 || desc_blank(d)) interior = false;
-        }
-      (interior ? tint : tgen).push_back(make_int2((int)i0, interior ? (int)j0 : ytile));
-      // sensor classes: S, T and the dilatation are formed on a cross of halo
-      // SENS_HS_INT from V_r, V_z stencils of reach H_INT, so every point within
-      // SENS_HS_INT of the tile must use centred rows, and the V region must lie inside.
-      const int64_t hv = SENS_HS_INT + H_INT, hs = SENS_HS_INT;
-      bool sint = brows == TR && i0 - hz_of((int)hv) >= 0 && i0 + TZ + hz_of((int)hv) <= Nz && j0 - hv >= 0 &&
-                  j0 + TR + hv <= Nr;
-      for (int64_t j = j0 - hs; sint && j < j0 + TR + hs; ++j)
-        for (int64_t i = i0 - hs; sint && i < i0 + TZ + hs; ++i) {
-          uint32_t d = dsc(i, j);
-          if (desc_zrow(d) != 4 || desc_rrow(d) != 4 || desc_blank(d)) sint = false;
-        }
-      (sint ? sti : stg).push_back(make_int2((int)i0, sint ? (int)j0 : ytile));
-    }
   h->ntiles_int = (int)tint.size();
   h->ntiles_gen = (int)tgen.size();
   h->nstiles_int = (int)sti.size();

@@ -122,7 +122,10 @@ typedef struct axj_params {
   double harmonic_amp;        /* A (velocity units) */
   double harmonic_st;         /* Strouhal number St */
   double harmonic_uj;         /* jet velocity U_j */
-  int64_t reserved[4];
+  /* 0: the stencil maps, face lists and tile classes of axj_create are built on the host;
+   * 1: on the device (one thread per grid row and per tile, the same rules). */
+  int64_t patch_prep;
+  int64_t reserved[3];
 } axj_params;
 
 typedef struct axj_handle axj_handle;
@@ -354,6 +357,17 @@ int axj_patches_from_records(const axj_bc_record* records, int64_t nrecords, int
  * patch numbers, one per byte from the lowest. */
 int axj_point_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, const double* ibval,
                    uint8_t* zrow, uint8_t* rrow, uint8_t* blank, uint8_t* nfaceops, uint64_t* faceop_ids);
+
+/* The stencil maps of one block as axj_create builds them for the device: algorithm 0 is
+ * the host path, 1 the per-row and per-tile functions of the device path run on the host,
+ * 2 the device path itself (needs a device). desc gets Nr rows of pitch P = Nz rounded up
+ * to 32 (P*Nr descriptors); faces the face-operation list (capacity faces_cap, length in
+ * *nfaces); tiles the (i0, j0) pairs of the interior stage, general stage, interior
+ * sensor and general sensor tiles one list after the other (capacity tiles_cap pairs,
+ * lengths in counts[4]); stale[2] the 1-based point where the stale scalar T is taken. */
+int axj_prep_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t Nr, const double* ibval,
+                  int64_t algorithm, uint32_t* desc, int32_t* faces, int64_t faces_cap, int64_t* nfaces,
+                  int32_t* tiles, int64_t tiles_cap, int64_t* counts, int64_t* stale);
 
 /* The operator tables the device kernels use, as SBP_operator forms them
  * (ModOperator.f90:5-121): SBP1(0:8,0:5) and SBP2(0:8,0:5) into sbp1[54] and sbp2[54],
