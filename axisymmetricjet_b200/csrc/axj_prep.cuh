@@ -1,8 +1,8 @@
 // axj_prep.cuh -- the patch preprocessing of one block (CreateAllPatches,
 // ModPatch.f90:214-242; the face lines of the BoundaryConditions loop, ModBC.f90:25-274)
 // as per-item functions: one point, one row, one tile. The device path runs them one
-// thread per row / per tile (axj_prep.cu); the same functions run on the host check it
-// against the host algorithm of axj_create (axj_prep_maps).
+// thread per row / per tile (axj_prep.cu); run on the host (axj_prep_maps, algorithm 1),
+// the same functions are checked against the host algorithm of axj_create.
 #pragma once
 
 #include <cstdint>
