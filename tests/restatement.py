@@ -276,9 +276,26 @@ def rhs(pv, tgt, tables, maps, metrics, z, r, params, patches):
         out[2, js] = (out[2] + v3)[js]
         out[3, js] = (out[3] + v4)[js]
         out[4, js] = (out[4] + x5 + y5)[js]
+    if params.control_forcing == 1:
+        _control_forcing(out, pv, tgt, z, r, params)
     _bc_loop(out, pv, tgt, q, d1z, d1r, dxidz, detadr, gam, patches)
     _sponges(out, pv, tgt, z, r, params)
     return out
+
+
+def _control_forcing(out, pv, tgt, z, r, params):
+    """ControlForcingTerms (ModControlForcing.f90:43-61), with the matrix and the Gaussian
+    window from the parameters instead of Vz_Control_Vr_Feedback.dat."""
+    F = [params.forcing_mat[q] for q in range(25)]
+    Nr, Nz = pv.shape[1:]
+    for i in range(Nz):
+        for j in range(Nr):
+            dz, dr = z[i] - params.forcing_z0, r[j] - params.forcing_r0
+            G = math.exp(-((dz * dz) / (params.forcing_lz * params.forcing_lz))
+                         - (dr * dr) / (params.forcing_lr * params.forcing_lr))
+            for e in range(5):
+                for k in range(5):
+                    out[e, j, i] = out[e, j, i] + params.forcing_alpha * F[5 * e + k] * G * (pv[k, j, i] - tgt[k, j, i])
 
 
 def _bc_loop(out, pv, tgt, q, d1z, d1r, dxidz, detadr, gam, patches):
