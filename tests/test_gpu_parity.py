@@ -194,7 +194,7 @@ def test_restart_round_trip():
 
 
 def test_multistep_jet512x128(oracle_mod):
-    """configs[0]-sized run: 100 RK4 steps, relative L2 error per field."""
+    """The small plain jet (512 x 128): 100 RK4 steps, relative L2 error per field."""
     c = fixtures.case("jet512x128")
     dev, ora = pair(c, oracle_mod)
     dev.run(100)
