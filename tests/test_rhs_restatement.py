@@ -19,6 +19,8 @@ CASES = {
     "jet_sc": lambda: fixtures.make_case(48, 36, 30.0, 15.0, 1.5, 5000.0, sc=True),
     "nozzle_nscbc_wall": lambda: _nozzle(NSCBC_NOSLIP_WALL),
     "nozzle_sat_wall_sc": lambda: _nozzle(SAT_NOSLIP_WALL, sc=True, Mj=1.5, Re=5000.0),
+    # the reference generator's case: stretched grid, blanked lip, wall outflow (250 x 50)
+    "writemesh_sc": lambda: fixtures.writemesh_case(sc=True, Re=5000.0),
     "jet_forcing": lambda: fixtures.make_case(
         48, 36, 30.0, 15.0, 0.9, 1000.0, control_forcing=1, forcing_z0=3.0, forcing_r0=0.5, forcing_lz=1.0,
         forcing_lr=0.3, forcing_mat=np.arange(25.0).reshape(5, 5) * 1e-3),
