@@ -67,6 +67,7 @@ def load_library():
         "axj_tgfilter": (C.c_int, [h, dp, i64, i64, dp]),
         "axj_sensor": (C.c_int, [h, dp, dp, dp, dp]),
         "axj_last_error": (C.c_char_p, [h]),
+        "axj_set_wait_limit": (C.c_int, [h, i64]),
         "axj_destroy": (None, [h]),
         "axj_read_bc_file": (C.c_int, [C.c_char_p, C.POINTER(AxjBcRecord), i64, C.POINTER(i64)]),
         "axj_operator_tables": (C.c_int, [dp, dp, dp]),
@@ -260,6 +261,11 @@ class AxiJetSolver:
 
     def rk4(self, delt):
         self._chk(self.lib.axj_rk4_step(self.h, float(delt)))
+
+    def set_wait_limit(self, tries):
+        """Poll limit of the kernels' bounded TMA waits on this handle's device (< 0: the
+        default; 0: every wait gives up at once and the step reports AXJ_ERR_TIMEOUT)."""
+        self._chk(self.lib.axj_set_wait_limit(self.h, int(tries)))
 
     def run(self, nsteps, out_every=0, callback=None):
         """nsteps x (ComputeTimeStep + RK4) on the device; returns the last dt."""

@@ -1179,6 +1179,16 @@ int axj_patches_from_records(const axj_bc_record* rec, int64_t nrec, int64_t Nzg
 
 const char* axj_last_error(const axj_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
+int axj_set_wait_limit(axj_handle* h, int64_t tries) {
+  if (!h) return fail(h, AXJ_ERR_ARG, "null handle");
+  if (tries > (int64_t)INT32_MAX) return fail(h, AXJ_ERR_ARG, "wait limit %lld too large", (long long)tries);
+  AXJ_CUDA(h, cudaSetDevice(h->device));
+  AXJ_CUDA(h, cudaStreamSynchronize(h->stream));
+  AXJ_CUDA(h, set_wait_tries((int)tries));
+  AXJ_CUDA(h, cudaDeviceSynchronize());
+  return AXJ_OK;
+}
+
 void axj_destroy(axj_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
@@ -1462,6 +1472,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
 int axj_set_state(axj_handle* h, const double* pv, const double* pv_target, int64_t iteration, double time) {
   if (!h || !pv || !pv_target) return fail(h, AXJ_ERR_ARG, "null argument");
   AXJ_CUDA(h, cudaSetDevice(h->device));
+  // a new state starts without the error flags of the previous one
+  AXJ_CUDA(h, cudaMemsetAsync(h->flags, 0, sizeof(int), h->stream));
   AXJ_CUDA(h, h2d(h, h->U0, pv, 5));
   AXJ_CUDA(h, h2d(h, h->target, pv_target, 5));
   AXJ_CUDA(h, cudaMemcpyAsync(h->time, &time, sizeof(double), cudaMemcpyHostToDevice, h->stream));

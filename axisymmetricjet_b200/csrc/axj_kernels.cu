@@ -148,13 +148,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after about a second instead of spinning forever.
+// Tries of a bounded wait before it gives up (about a quarter of a second at the default;
+// axj_set_wait_limit lowers it to exercise the timeout path).
+constexpr int kWaitTriesDefault = 1 << 20;
+__constant__ int c_wait_tries = kWaitTriesDefault;
+// Bounded wait: gives up after c_wait_tries polls instead of spinning forever.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 20); ++it) {
+  const int tries = c_wait_tries;
+  for (int it = 0; it < tries; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if (it > 32) __nanosleep(256);
   }
   return false;
+}
+// The error path after a bounded wait gave up: wait again, bounded by the default limit,
+// for the transfers of that barrier phase still in flight, so that none of them lands in
+// the shared memory of a CTA that has exited.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity) {
+  for (int it = 0; it < kWaitTriesDefault; ++it) {
+    if (mbar_try_wait(bar, parity)) return;
+    if (it > 32) __nanosleep(256);
+  }
 }
 // 3-D tiled TMA load (x = z index, y = r index, z = field plane) into shared memory;
 // out-of-range elements are filled with zeros.
@@ -311,6 +325,8 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   }
   if (!__syncthreads_and(mbar_wait_bounded(&bar[0], phase & 1u))) {
     if (tid == 0) atomicOr(a.flags, 4);
+    mbar_drain(&bar[0], phase & 1u);
+    if (needU0 || needA) mbar_drain(&bar[1], (phase >> 1) & 1u);
     return false;
   }
   phase ^= 1u;
@@ -418,6 +434,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   if (needU0 || needA) {
     if (!__syncthreads_and(mbar_wait_bounded(&bar[1], (phase >> 1) & 1u))) {
       if (tid == 0) atomicOr(a.flags, 4);
+      mbar_drain(&bar[1], (phase >> 1) & 1u);
       return false;
     }
     phase ^= 2u;
@@ -763,7 +780,7 @@ __device__ __forceinline__ void dt_body(const DtArgs& a, int blk, int nblk) {
     if (k > mx) mx = k;
     const double sabs = fabs(dxidz) + fabs(detadr);
     const double x = inv + 2.0 * mx * (sabs * sabs);
-    if (!(x == x)) bad = 1;
+    if (!isfinite(x)) bad = 1;  // NaN, or an infinite input (which would give dt = 0)
     xm = fmax(xm, x);
   }
   __shared__ double sred[DT_THREADS / 32];
@@ -990,6 +1007,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   }
   if (!__syncthreads_and(mbar_wait_bounded(&bar, phase & 1u))) {
     if (tid == 0) atomicOr(a.flags, 4);
+    mbar_drain(&bar, phase & 1u);
     return false;
   }
   phase ^= 1u;
@@ -1373,6 +1391,7 @@ __device__ __forceinline__ void zrows_body(const Grid& g, const unsigned char* _
   }
   if (!__syncthreads_and(mbar_wait_bounded(&bar, 0))) {
     if (threadIdx.x == 0) atomicOr(flags, 4);
+    mbar_drain(&bar, 0);
     return;
   }
   if ((Nz & 1) && threadIdx.x == 0) xs[ZR_PADL + Nz - 1] = __ldg(x + Nz - 1);
@@ -1614,6 +1633,7 @@ __global__ void __launch_bounds__(ZRK_THREADS, 3)
     par ^= 1u << sl;
     if (!__syncthreads_and(ok)) {
       if (tid == 0) atomicOr(a.flags, 4);
+      mbar_drain(&bar[sl], ((par >> sl) & 1u) ^ 1u);
       return;
     }
     const int m = k - 1;  // the block filtered in this iteration
@@ -1919,6 +1939,14 @@ static cudaError_t pair_attrs() {
   if (e == cudaSuccess) e = sensor_attr<SENS_HS_GEN, H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = sensor_attr<SENS_HS_INT, H_INT, false, SIN, R>();
   return e;
+}
+
+// Poll limit of the bounded waits of this file's kernels on the current device (tries < 0:
+// the default; 0: every wait gives up at once). Kernels read it when they run, so captured
+// graphs see a change too.
+cudaError_t set_wait_tries(int tries) {
+  const int v = tries >= 0 ? tries : kWaitTriesDefault;
+  return cudaMemcpyToSymbol(c_wait_tries, &v, sizeof(int));
 }
 
 // Opt-in shared-memory sizes; called once per handle at creation (outside any

@@ -122,6 +122,7 @@ struct SensorArgs {
 };
 
 cudaError_t init_kernel_attributes();
+cudaError_t set_wait_tries(int tries);
 void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const double tg[9][11],
                    const PatchDev* patches, int npatch, cudaStream_t s);
 

@@ -10,6 +10,7 @@
 // loads this library holds it (about 512 KB) until the process exits.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -56,11 +57,14 @@ __global__ void __launch_bounds__(NA_THREADS)
       v = 100.0;
     } else {
       const double Vr = __ldg(U + 1 * plane + o), Vz = __ldg(U + 3 * plane + o), T = __ldg(U + 4 * plane + o);
-      const double mu = pow(T, 0.666);
+      // mu = T**0.666 (AssignValues) by the same definition as the handle-based dt kernel
+      const double mu = axj::mu_of_T<double>(T);
       const double beta = (3.0 / 5.0) * mu;
       const double lambda = beta - (2.0 / 3.0) * mu;
       const bool phys = c.dt_mode == axj::DT_PHYSICAL;
       v = axj::dt_point(Vz, Vr, phys ? T : staleT, mu, lambda, mu, __ldg(dxidz + i), __ldg(detadr + j), c);
+      // an infinite input gives dt = 0, a finite-looking minimum: flag it with the NaNs
+      if (!isfinite(Vr) || !isfinite(Vz) || !isfinite(T)) atomicOr(bad, 1u);
     }
     if (!(v == v)) atomicOr(bad, 1u);
   }
@@ -110,11 +114,17 @@ extern "C" int axj_compute_dt_noalloc(const double* d_pv, int64_t pitch, int64_t
     axj::set_global_error("axj_compute_dt_noalloc: null pointer or bad size");
     return AXJ_ERR_ARG;
   }
-  if (Nz * Nr > NA_MAX_POINTS) {
+  // each factor is bounded before the product is formed (no overflow on any input)
+  if (Nz > NA_MAX_POINTS || Nr > NA_MAX_POINTS / Nz) {
     std::snprintf(msg, sizeof(msg),
-                  "axj_compute_dt_noalloc: %lld points exceed the built-in scratch limit of %lld points",
-                  (long long)(Nz * Nr), NA_MAX_POINTS);
+                  "axj_compute_dt_noalloc: %lld x %lld points exceed the built-in scratch limit of %lld points",
+                  (long long)Nz, (long long)Nr, NA_MAX_POINTS);
     axj::set_global_error(msg);
+    return AXJ_ERR_ARG;
+  }
+  // 5 planes of pitch x Nr doubles must be addressable
+  if (pitch > (INT64_MAX / 8 / 5) / Nr) {
+    axj::set_global_error("axj_compute_dt_noalloc: row pitch too large");
     return AXJ_ERR_ARG;
   }
   int dev = 0;

@@ -222,8 +222,8 @@ int axj_sensor(axj_handle* h, const double* pv, double* mustar, double* betastar
  *   d_ibval  Nz x Nr (pitch `pitch`) blanking values, or NULL for no blanked points
  *   params   CFL, Re, Pr and dt_mode are read; stale_T is the module scalar T used when
  *            dt_mode is AXJ_DT_REFERENCE
- *   d_dt     receives dt on the device (100 if every point is blanked, NaN if any point
- *            gives a non-finite dt); stream is a cudaStream_t (NULL: legacy default stream)
+ *   d_dt     receives dt on the device (100 if every point is blanked; NaN if a point that
+ *            is not blanked holds a non-finite V_r, V_z or T, or gives a NaN dt); stream is a cudaStream_t (NULL: legacy default stream)
  * At most 16,777,216 points (Nz*Nr); larger grids return AXJ_ERR_ARG with a message in
  * axj_last_error(NULL). The call is asynchronous on `stream`. The first call on a device
  * looks up the scratch array's device address with that device current; make that first
@@ -330,6 +330,15 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
                        int64_t* ntrials);
 const char* axj_batch_last_error(const axj_batch* b);
 void axj_batch_destroy(axj_batch* b);
+
+/* Poll limit of the bounded waits (TMA completions) of the stage, sensor and filter
+ * kernels on the handle's device; tries < 0 restores the default (2^20 polls, about a
+ * quarter of a second), 0 makes every such wait give up at once. No counterpart in the
+ * reference: it exists so that a test can make the waits give up and see the kernels
+ * report AXJ_ERR_TIMEOUT and return, each after its transfers in flight have landed, with
+ * the context still usable. It applies to every handle on the device; axj_set_state
+ * clears a handle's error flags. */
+int axj_set_wait_limit(axj_handle* h, int64_t tries);
 
 /* Last error message of the handle (or of the last failed axj_create if h is NULL). */
 const char* axj_last_error(const axj_handle* h);

@@ -15,20 +15,22 @@ from axisymmetricjet_b200._ffi import AxjBcRecord, AxjParams, AxjPatch, dptr, pa
     record_array
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = None
+_LIBS = {}
+# "plain": the oracle proper (no FMA contraction); "fma": the same source with FMA
+# contraction, only used to calibrate how far two correct FP64 builds drift apart.
+_VARIANTS = {"plain": "liboracle_axj.so", "fma": "liboracle_axj_fma.so"}
 
 
-def build():
-    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+def build(variant="plain"):
+    subprocess.run(["make", "-s", "-C", _HERE, _VARIANTS[variant]], check=True)
 
 
-def load():
-    global _LIB
-    if _LIB is not None:
-        return _LIB
-    path = os.path.join(_HERE, "liboracle_axj.so")
+def load(variant="plain"):
+    if variant in _LIBS:
+        return _LIBS[variant]
+    path = os.path.join(_HERE, _VARIANTS[variant])
     if not os.path.exists(path):
-        build()
+        build(variant)
     lib = C.CDLL(path)
     dp = C.POINTER(C.c_double)
     i64 = C.c_int64
@@ -59,7 +61,7 @@ def load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    _LIB = lib
+    _LIBS[variant] = lib
     return lib
 
 
@@ -75,8 +77,8 @@ def patches_from_records(records, Nz, Nr):
 class Oracle:
     """Same method names and array conventions as axisymmetricjet_b200.AxiJetSolver."""
 
-    def __init__(self, params, zvec, rvec, ibval, patches):
-        self.lib = load()
+    def __init__(self, params, zvec, rvec, ibval, patches, variant="plain"):
+        self.lib = load(variant)
         zvec = np.ascontiguousarray(zvec, dtype=np.float64)
         rvec = np.ascontiguousarray(rvec, dtype=np.float64)
         ibval = np.ascontiguousarray(ibval, dtype=np.float64)

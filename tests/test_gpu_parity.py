@@ -8,6 +8,8 @@ start at zero, so their right-hand sides are differences of terms of the V_z equ
 size, and the oracle built with and without FMA contraction differs by 6.6e-12 of the
 V_r right-hand side's own maximum on the generator's case, 1.1e-14 on the shared scale).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -218,3 +220,48 @@ def test_multistep_writemesh(oracle_mod):
         assert l2 < 1e-11, (k, l2)
     (itd, td), (ito, to) = dev.get_time(), ora.get_time()
     assert itd == ito == 60 and abs(td - to) <= 1e-12 * to
+
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def reference_nozzle_4400x640():
+    """The reference's own bc file (bc_4400x640_nozzle.dat: SAT inflow below and above the
+    lip, NSCBC no-slip walls around the lip up to i = 597 between rows 150 and 169, a
+    non-reflecting top and outflow, the axis) on the production grid and flow, with the
+    points inside the lip blanked (rows 151..168, columns 1..596, 1-based) as the
+    reference's generator blanks its lip (WriteMeshAndSoln/write_soln_file.f90:204-213)."""
+    rec = axj.read_bc_file(os.path.join(GOLDEN, "bc_4400x640_nozzle.dat"))
+    c = fixtures.case("jet4400x640", records=rec)
+    ib = np.ones((c["Nr"], c["Nz"]))
+    ib[150:168, :596] = 0.0
+    c["ibval"] = ib
+    return c
+
+
+PRODUCTION = {
+    # the benchmarked configuration: 4400 x 640, Mach 1.5, Re 5000, shock capturing, reference dt
+    "jet4400x640": lambda: fixtures.case("jet4400x640"),
+    "reference_nozzle_4400x640": reference_nozzle_4400x640,
+}
+
+
+@pytest.mark.parametrize("name", list(PRODUCTION))
+def test_rk4_steps_production_size(oracle_mod, name):
+    """Three RK4 steps at the production size against the oracle, <= 1e-12 per field per
+    step, with every path computing its own dt (the stale-T reference dt)."""
+    c = PRODUCTION[name]()
+    dev, ora = pair(c, oracle_mod)
+    if name.startswith("reference_nozzle"):
+        blank = np.asarray(c["ibval"]) == 0
+        assert blank.sum() == 18 * 596
+    for step in range(3):
+        dd = dev.compute_time_step()
+        do = ora.compute_time_step()
+        assert abs(dd - do) <= 1e-14 * abs(do), (step, dd, do)
+        dev.rk4(do)
+        ora.rk4(do)
+        errs = field_relerr(dev.get_state(), ora.get_state())
+        assert max(errs) < REL, (step, errs)
+    dev.close()
+    ora.close()
