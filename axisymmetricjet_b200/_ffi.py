@@ -54,7 +54,8 @@ class AxjParams(C.Structure):
         ("harmonic_st", C.c_double),
         ("harmonic_uj", C.c_double),
         ("patch_prep", C.c_int64),
-        ("reserved", C.c_int64 * 3),
+        ("stage_form", C.c_int64),
+        ("reserved", C.c_int64 * 2),
     ]
 
 

@@ -62,6 +62,7 @@ struct axj_handle {
   double* harm = nullptr;  // cos(omega t_s) of the harmonic forcing per stage
   int* flags = nullptr;
   unsigned int* counter = nullptr;
+  unsigned int* sched = nullptr;  // tile counter of the persistent interior stage kernel (null: one tile per CTA)
   int2 *tiles_int = nullptr, *tiles_gen = nullptr;
   int ntiles_int = 0, ntiles_gen = 0;
   int dt_blocks = 0;
@@ -459,6 +460,7 @@ StageMaps stage_maps(axj_handle* h, int b, int cls, int cm) {
 int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage, int cm) {
   StageArgs a = stage_args(h, bin, bout, stage);
   a.learned = cm;
+  a.sched = h->sched;
   StageMaps mi = stage_maps(h, bin, 0, cm), mg = stage_maps(h, bin, 1, cm);
   AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, mi, h->ntiles_gen, h->tiles_gen, mg, h->side, h->stream));
   return AXJ_OK;
@@ -1234,6 +1236,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     return fail(nullptr, AXJ_ERR_ARG, "sensor %lld unknown", (long long)prm->sensor);
   if (prm->patch_prep != 0 && prm->patch_prep != 1)
     return fail(nullptr, AXJ_ERR_ARG, "patch_prep %lld unknown", (long long)prm->patch_prep);
+  if (prm->stage_form != 0 && prm->stage_form != 1)
+    return fail(nullptr, AXJ_ERR_ARG, "stage_form %lld unknown", (long long)prm->stage_form);
   if (prm->sensor != AXJ_SENSOR_PLAIN && !prm->shock_capturing)
     return fail(nullptr, AXJ_ERR_ARG, "the learned sensor needs shock_capturing = 1");
   if (prm->sensor != AXJ_SENSOR_PLAIN && (prm->judge_every < 1 || !(prm->judge_threshold >= 0.0)))
@@ -1407,6 +1411,11 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->time = dalloc<double>(h, 1, &rc);
   h->harm = dalloc<double>(h, 5, &rc);
   h->flags = dalloc<int>(h, 1, &rc);
+  // the persistent interior stage kernel copies the tiles' 1-D metrics with bulk copies,
+  // which need 16-byte aligned rows: every interior tile starts on an even row
+  bool even_rows = true;
+  for (const int2& t : tint) even_rows = even_rows && (t.y % 2 == 0) && (t.x % 2 == 0);
+  if (prm->stage_form == 0 && even_rows && !tint.empty()) h->sched = dalloc<unsigned int>(h, 2, &rc);
   h->counter = dalloc<unsigned int>(h, 1, &rc);
   h->dt_blocks = 148 * 4;
   h->partial = dalloc<double>(h, h->dt_blocks, &rc);

@@ -179,6 +179,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// Bulk (non-tensor) global -> shared copy completing on an mbarrier; both addresses
+// 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
 // Prefetch of a tensor box into L2 (no shared memory, no completion to wait for).
 __device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int x, int y, int z) {
   asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
@@ -243,93 +252,49 @@ struct StageSmem {
 // mixed path's intermediate stages); R: arithmetic type of the stencils and, in
 // interior tiles, of the pointwise terms. General tiles (closure rows, faces, the axis
 // row) evaluate the pointwise terms, face penalties and sponges in double.
-// One tile (i0, j0) of the fused stage. Returns false if a bounded wait gave up (the
-// flag is set; the caller stops).
-template <int H, bool GEN, typename SIN, typename R, int CM>
-__device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, const CUtensorMap* mState,
-                                           const CUtensorMap* mQ, const CUtensorMap* mU0, const CUtensorMap* mAcc,
-                                           const CUtensorMap* mB,
-                                           unsigned char* smem_raw, uint64_t* bar, uint32_t& phase) {
+// Shared-memory buffers of one stage tile (layout StageSmem: state box, coefficient box,
+// plain mu, pv_old and running-sum tiles, dV/dz, descriptors, metrics).
+template <typename SIN, typename R>
+struct StagePtrs {
+  SIN* sU;
+  double* sQ;
+  double* sMu0;
+  double* sP0;
+  double* sPA;
+  R* sDz;
+  const uint32_t* sDesc;
+  const double* sMet;
+};
+
+// Phases 2-3 of one stage tile (i0, j0; nrow rows of it are owned) whose boxes have
+// arrived in shared memory, with NT threads: mu and the coefficients on the cross, dV/dz on
+// the tile columns, then the points. The RK operand tiles of interior tiles complete on
+// barRK (parity rk_parity). Returns false if that bounded wait gave up (the flag is set and
+// the transfers in flight have landed).
+template <int H, bool GEN, typename SIN, typename R, int CM, int NT>
+__device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0, int nrow,
+                                              const StagePtrs<SIN, R>& sp, uint64_t* barRK, uint32_t rk_parity) {
   using SM = StageSmem<H, SIN, R, CM>;
   using RP = typename std::conditional<GEN, double, R>::type;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT, NTP = SM::NTP, HT = SM::HT, RQ = SM::RQ;
-  SIN* sU = reinterpret_cast<SIN*>(smem_raw + SM::oU);            // [5][RR][RZ]
-  double* sQ = reinterpret_cast<double*>(smem_raw + SM::oQ);      // [3][RQ][RZ]
+  constexpr int NPER = (NPT + NT - 1) / NT;
+  const SIN* sU = sp.sU;
+  double* sQ = sp.sQ;
   double* sMu = sQ + HT * RZ;                                      // [RR][RZ], row stride RZ
   double* sBe = sQ + RQ * RZ + HT * RZ;
   double* sKa = a.c.shock_capturing ? sQ + 2 * RQ * RZ + HT * RZ : sMu;
-  double* sMu0 = reinterpret_cast<double*>(smem_raw + SM::oMu0);  // [TR][TZ]
-  double* sP0 = reinterpret_cast<double*>(smem_raw + SM::oP0);    // [5][TR][TZ]
-  double* sPA = reinterpret_cast<double*>(smem_raw + SM::oPA);    // [5][TR][TZ]
-  R* sDz = reinterpret_cast<R*>(smem_raw + SM::oDz(GEN));         // [2][RR][TZ]
-  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
-  double* sMet = reinterpret_cast<double*>(smem_raw + SM::oMet(GEN));  // [3][TZ] + [4][TR]
-
+  double* sMu0 = sp.sMu0;
+  const double* sP0 = sp.sP0;
+  const double* sPA = sp.sPA;
+  R* sDz = sp.sDz;
+  const uint32_t* sDesc = sp.sDesc;
+  const double* sMet = sp.sMet;
   const int tid = threadIdx.x;
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long P = a.g.P, PL = a.g.plane;
   const bool sc = a.c.shock_capturing != 0;
-  // general tiles of a thin r band own only its rows: TR - (bits 24-31 of j0)
-  int nrow = TR;
-  if (GEN) {
-    nrow = TR - (j0 >> 24);
-    j0 &= 0xFFFFFF;
-  }
-  // pv_old is needed as a tile in stages 2 and 3 (stage 1 reads it from the state box),
-  // the running sum A in stages 3 and 4; interior tiles stage them by TMA
   const bool needU0 = !GEN && (a.stage == 2 || a.stage == 3);
   const bool needA = !GEN && (a.stage == 3 || a.stage == 4);
-
-  // ---- phase 1: one thread issues the TMA loads; the RK operands complete on the
-  // second barrier while phases 1-2 run. The barriers are initialised once per CTA by the
-  // caller; phase bit b is the parity of bar[b]'s next completion. Prior generic-proxy
-  // accesses of the shared buffers (a previous tile of a persistent CTA) are ordered
-  // before the TMA writes by the proxy fence.
-  __syncthreads();
-  if (tid == 0) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&bar[0], SM::state_bytes + (sc ? SM::q_bytes : 0u));
-    tma_load_3d(sU, mState, i0 - HZ, j0 - H, 0, &bar[0]);
-    if (sc) tma_load_3d(sQ, mQ, i0 - HZ, j0 - H - HT, 0, &bar[0]);
-    if (needU0 || needA) {
-      mbar_expect_tx(&bar[1], (needU0 ? SM::tile_bytes : 0u) + (needA ? SM::tile_bytes : 0u));
-      if (needU0) tma_load_3d(sP0, mU0, i0, j0, 0, &bar[1]);
-      if (needA) tma_load_3d(sPA, mAcc, i0, j0, 0, &bar[1]);
-    }
-    // operands the RK update reads from global memory: into L2 now (k2 in stage 3; pv_old
-    // and the running sum in general tiles, which do not stage them)
-    if (mB && a.stage == 3) tma_prefetch_3d(mB, i0, j0, 0);
-    if (GEN && (a.stage == 2 || a.stage == 3)) tma_prefetch_3d(mU0, i0, j0, 0);
-    if (GEN && (a.stage == 3 || a.stage == 4)) tma_prefetch_3d(mAcc, i0, j0, 0);
-  }
-  if (GEN) {
-    for (int idx = tid; idx < NPT; idx += STAGE_THREADS) {
-      const int rr = idx / RZ, rz = idx - rr * RZ;
-      const int i = i0 - HZ + rz, j = j0 - H + rr;
-      sDesc[idx] = (i >= 0 && i < Nz && j >= 0 && j < Nr) ? __ldg(a.desc + (long long)j * P + i)
-                                                            : make_desc(ROW_NONE, ROW_NONE, false, 0);
-    }
-  }
-  // the tile's metrics and coordinates (read per point in phases 2-3)
-  if (tid < TZ) {
-    const int i = min(i0 + tid, Nz - 1);
-    sMet[tid] = __ldg(a.dxidz + i);
-    sMet[TZ + tid] = __ldg(a.ddxidxidz + i);
-    sMet[2 * TZ + tid] = __ldg(a.zc + i);
-  } else if (tid < TZ + TR) {
-    const int r = tid - TZ, j = min(j0 + r, Nr - 1);
-    sMet[3 * TZ + r] = __ldg(a.detadr + j);
-    sMet[3 * TZ + TR + r] = __ldg(a.ddetadetadr + j);
-    sMet[3 * TZ + 2 * TR + r] = __ldg(a.rc + j);
-    sMet[3 * TZ + 3 * TR + r] = __ldg(a.invr + j);
-  }
-  if (!__syncthreads_and(mbar_wait_bounded(&bar[0], phase & 1u))) {
-    if (tid == 0) atomicOr(a.flags, 4);
-    mbar_drain(&bar[0], phase & 1u);
-    if (needU0 || needA) mbar_drain(&bar[1], (phase >> 1) & 1u);
-    return false;
-  }
-  phase ^= 1u;
   // mu = T**0.666 (AssignValues) on the cross of the region (CM_PRE: the coefficient box
   // already holds mu_eff, beta and kappa_eff). With shock capturing the
   // coefficient box holds the z-filtered quantities; the r filter PerformTGfilter(q, 2,
@@ -339,10 +304,10 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   // thread has read its filter windows. Zero-filled points outside the block give
   // mu = 0, as the never-written halo does; blanked points keep mu* = 0.
   if (CM != CM_PRE) {
-    double vmu[SM::NPER], vbe[SM::NPER], vka[SM::NPER];
+    double vmu[NPER], vbe[NPER], vka[NPER];
 #pragma unroll
-    for (int k = 0; k < SM::NPER; ++k) {
-      const int idx = tid + k * STAGE_THREADS;
+    for (int k = 0; k < NPER; ++k) {
+      const int idx = tid + k * NT;
       vmu[k] = vbe[k] = vka[k] = 0.0;
       if (idx >= NPT) continue;
       const int rr = idx / RZ, rz = idx - rr * RZ;
@@ -392,8 +357,8 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < SM::NPER; ++k) {
-      const int idx = tid + k * STAGE_THREADS;
+    for (int k = 0; k < NPER; ++k) {
+      const int idx = tid + k * NT;
       if (idx >= NPT) continue;
       const int rr = idx / RZ, rz = idx - rr * RZ;
       const bool cross = (rr >= H && rr < H + TR && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
@@ -409,7 +374,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
 
   // ---- phase 2: dVr/dz and dVz/dz on the tile columns, all region rows (needed by
   // the mixed derivatives d/dr(dV/dz), ModRHS.f90:132-133)
-  for (int idx = tid; idx < RR * TZ; idx += STAGE_THREADS) {
+  for (int idx = tid; idx < RR * TZ; idx += NT) {
     const int rr = idx / TZ, c = idx - rr * TZ;
     const int i = i0 + c, j = j0 - H + rr;
     R dvr = R(0), dvz = R(0);
@@ -432,17 +397,16 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
 
   // ---- phase 3: one point per thread per pass
   if (needU0 || needA) {
-    if (!__syncthreads_and(mbar_wait_bounded(&bar[1], (phase >> 1) & 1u))) {
+    if (!__syncthreads_and(mbar_wait_bounded(barRK, rk_parity))) {
       if (tid == 0) atomicOr(a.flags, 4);
-      mbar_drain(&bar[1], (phase >> 1) & 1u);
+      mbar_drain(barRK, rk_parity);
       return false;
     }
-    phase ^= 2u;
   }
   const double dtv = a.stage > 0 ? *a.dt : 0.0;
   // cos(omega t_s) at this stage's time (harmonic forcing)
   const double cwt = a.c.control_forcing == 2 ? a.harm[a.stage] : 0.0;
-  for (int pidx = tid; pidx < TZ * TR; pidx += STAGE_THREADS) {
+  for (int pidx = tid; pidx < TZ * TR; pidx += NT) {
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
     if (GEN && (i >= Nz || j >= Nr || r >= nrow)) continue;
@@ -608,6 +572,95 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   return true;
 }
 
+// One tile (i0, j0) of the fused stage. Returns false if a bounded wait gave up (the
+// flag is set; the caller stops).
+template <int H, bool GEN, typename SIN, typename R, int CM>
+__device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, const CUtensorMap* mState,
+                                           const CUtensorMap* mQ, const CUtensorMap* mU0, const CUtensorMap* mAcc,
+                                           const CUtensorMap* mB,
+                                           unsigned char* smem_raw, uint64_t* bar, uint32_t& phase) {
+  using SM = StageSmem<H, SIN, R, CM>;
+  constexpr int HZ = SM::HZ, RZ = SM::RZ, NPT = SM::NPT, HT = SM::HT;
+  SIN* sU = reinterpret_cast<SIN*>(smem_raw + SM::oU);            // [5][RR][RZ]
+  double* sQ = reinterpret_cast<double*>(smem_raw + SM::oQ);      // [3][RQ][RZ]
+  double* sMu0 = reinterpret_cast<double*>(smem_raw + SM::oMu0);  // [TR][TZ]
+  double* sP0 = reinterpret_cast<double*>(smem_raw + SM::oP0);    // [5][TR][TZ]
+  double* sPA = reinterpret_cast<double*>(smem_raw + SM::oPA);    // [5][TR][TZ]
+  R* sDz = reinterpret_cast<R*>(smem_raw + SM::oDz(GEN));         // [2][RR][TZ]
+  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
+  double* sMet = reinterpret_cast<double*>(smem_raw + SM::oMet(GEN));  // [3][TZ] + [4][TR]
+
+  const int tid = threadIdx.x;
+  const int Nz = a.g.Nz, Nr = a.g.Nr;
+  const long long P = a.g.P;
+  const bool sc = a.c.shock_capturing != 0;
+  // general tiles of a thin r band own only its rows: TR - (bits 24-31 of j0)
+  int nrow = TR;
+  if (GEN) {
+    nrow = TR - (j0 >> 24);
+    j0 &= 0xFFFFFF;
+  }
+  // pv_old is needed as a tile in stages 2 and 3 (stage 1 reads it from the state box),
+  // the running sum A in stages 3 and 4; interior tiles stage them by TMA
+  const bool needU0 = !GEN && (a.stage == 2 || a.stage == 3);
+  const bool needA = !GEN && (a.stage == 3 || a.stage == 4);
+
+  // ---- phase 1: one thread issues the TMA loads; the RK operands complete on the
+  // second barrier while phases 1-2 run. The barriers are initialised once per CTA by the
+  // caller; phase bit b is the parity of bar[b]'s next completion. Prior generic-proxy
+  // accesses of the shared buffers (a previous tile of a persistent CTA) are ordered
+  // before the TMA writes by the proxy fence.
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[0], SM::state_bytes + (sc ? SM::q_bytes : 0u));
+    tma_load_3d(sU, mState, i0 - HZ, j0 - H, 0, &bar[0]);
+    if (sc) tma_load_3d(sQ, mQ, i0 - HZ, j0 - H - HT, 0, &bar[0]);
+    if (needU0 || needA) {
+      mbar_expect_tx(&bar[1], (needU0 ? SM::tile_bytes : 0u) + (needA ? SM::tile_bytes : 0u));
+      if (needU0) tma_load_3d(sP0, mU0, i0, j0, 0, &bar[1]);
+      if (needA) tma_load_3d(sPA, mAcc, i0, j0, 0, &bar[1]);
+    }
+    // operands the RK update reads from global memory: into L2 now (k2 in stage 3; pv_old
+    // and the running sum in general tiles, which do not stage them)
+    if (mB && a.stage == 3) tma_prefetch_3d(mB, i0, j0, 0);
+    if (GEN && (a.stage == 2 || a.stage == 3)) tma_prefetch_3d(mU0, i0, j0, 0);
+    if (GEN && (a.stage == 3 || a.stage == 4)) tma_prefetch_3d(mAcc, i0, j0, 0);
+  }
+  if (GEN) {
+    for (int idx = tid; idx < NPT; idx += STAGE_THREADS) {
+      const int rr = idx / RZ, rz = idx - rr * RZ;
+      const int i = i0 - HZ + rz, j = j0 - H + rr;
+      sDesc[idx] = (i >= 0 && i < Nz && j >= 0 && j < Nr) ? __ldg(a.desc + (long long)j * P + i)
+                                                            : make_desc(ROW_NONE, ROW_NONE, false, 0);
+    }
+  }
+  // the tile's metrics and coordinates (read per point in phases 2-3)
+  if (tid < TZ) {
+    const int i = min(i0 + tid, Nz - 1);
+    sMet[tid] = __ldg(a.dxidz + i);
+    sMet[TZ + tid] = __ldg(a.ddxidxidz + i);
+    sMet[2 * TZ + tid] = __ldg(a.zc + i);
+  } else if (tid < TZ + TR) {
+    const int r = tid - TZ, j = min(j0 + r, Nr - 1);
+    sMet[3 * TZ + r] = __ldg(a.detadr + j);
+    sMet[3 * TZ + TR + r] = __ldg(a.ddetadetadr + j);
+    sMet[3 * TZ + 2 * TR + r] = __ldg(a.rc + j);
+    sMet[3 * TZ + 3 * TR + r] = __ldg(a.invr + j);
+  }
+  if (!__syncthreads_and(mbar_wait_bounded(&bar[0], phase & 1u))) {
+    if (tid == 0) atomicOr(a.flags, 4);
+    mbar_drain(&bar[0], phase & 1u);
+    if (needU0 || needA) mbar_drain(&bar[1], (phase >> 1) & 1u);
+    return false;
+  }
+  phase ^= 1u;
+  const StagePtrs<SIN, R> sp{sU, sQ, sMu0, sP0, sPA, sDz, sDesc, sMet};
+  const bool ok = stage_compute<H, GEN, SIN, R, CM, STAGE_THREADS>(a, i0, j0, nrow, sp, &bar[1], (phase >> 1) & 1u);
+  if (ok && (needU0 || needA)) phase ^= 2u;
+  return ok;
+}
+
 
 
 template <int H, bool GEN, typename SIN, typename R, int CM>
@@ -625,6 +678,137 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
   uint32_t phase = 0;
   const int2 t0 = tiles[blockIdx.x];
   stage_body<H, GEN, SIN, R, CM>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, &mB, smem_raw, bar, phase);
+}
+
+// Persistent form of the interior tiles: one CTA of PST_THREADS threads per SM takes tiles
+// from a device counter and double-buffers them: while the points of tile k are computed,
+// the TMA boxes of tile k+1 (state, coefficients, pv_old and running-sum tiles) and its 1-D
+// metrics (bulk copies) land in the other buffer, so the loads overlap the arithmetic. One
+// point per thread; the per-point code is the non-persistent kernel's (stage_compute).
+template <typename SIN, typename R, int CM>
+struct PstSmem {
+  using SM = StageSmem<H_INT, SIN, R, CM>;
+  // one buffer: state box [5][RR][RZ], coefficient box [3][RQ][RZ], pv_old and running-sum
+  // tiles [5][TR][TZ], metrics [3][TZ] + [4][TR]
+  static constexpr size_t oU = 0;
+  static constexpr size_t oQ = align128(sizeof(SIN) * 5 * SM::NPT);
+  static constexpr size_t oP0 = align128(oQ + sizeof(double) * 3 * SM::RQ * SM::RZ);
+  static constexpr size_t oPA = align128(oP0 + sizeof(double) * 5 * SM::NTP);
+  static constexpr size_t oMet = align128(oPA + sizeof(double) * 5 * SM::NTP);
+  static constexpr size_t slot = align128(oMet + sizeof(double) * SM::NMET);
+  // shared by the two buffers: plain mu on the tile, dV/dz [2][RR][TZ]
+  static constexpr size_t oMu0 = 2 * slot;
+  static constexpr size_t oDz = align128(oMu0 + sizeof(double) * SM::NTP);
+  static constexpr size_t bytes = align128(oDz + sizeof(R) * 2 * SM::RR * TZ);
+  static constexpr uint32_t met_bytes = sizeof(double) * SM::NMET;
+};
+static_assert(PstSmem<double, double, CM_FILT>::bytes <= 227 * 1024, "persistent stage buffers exceed shared memory");
+static_assert(PstSmem<double, double, CM_PRE>::bytes <= 227 * 1024, "persistent stage buffers exceed shared memory");
+
+template <typename SIN, typename R, int CM>
+__global__ void __launch_bounds__(PST_THREADS, 1)
+    stage_kernel_pst(const StageArgs a, const int2* __restrict__ tiles, int ntiles,
+                     const __grid_constant__ CUtensorMap mState, const __grid_constant__ CUtensorMap mQ,
+                     const __grid_constant__ CUtensorMap mU0, const __grid_constant__ CUtensorMap mAcc,
+                     const __grid_constant__ CUtensorMap mB) {
+  using SM = StageSmem<H_INT, SIN, R, CM>;
+  using PS = PstSmem<SIN, R, CM>;
+  constexpr int H = H_INT, HZ = SM::HZ, HT = SM::HT;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar[4];  // per buffer b: bar[2b] boxes + metrics, bar[2b+1] RK tiles
+  __shared__ int tile_of[2];                // tile index held by each buffer (>= ntiles: none)
+  const int tid = threadIdx.x;
+  const bool sc = a.c.shock_capturing != 0;
+  const bool needU0 = a.stage == 2 || a.stage == 3;
+  const bool needA = a.stage == 3 || a.stage == 4;
+  const bool needRK = needU0 || needA;
+  auto slot = [&](int b) { return smem_raw + (size_t)b * PS::slot; };
+  // thread 0: the loads of tile t into buffer b
+  auto issue = [&](int t, int b) {
+    const int2 tt = tiles[t];
+    const int i0 = tt.x, j0 = tt.y;
+    unsigned char* base = slot(b);
+    double* met = reinterpret_cast<double*>(base + PS::oMet);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bar[2 * b], SM::state_bytes + (sc ? SM::q_bytes : 0u) + PS::met_bytes);
+    tma_load_3d(base + PS::oU, &mState, i0 - HZ, j0 - H, 0, &bar[2 * b]);
+    if (sc) tma_load_3d(base + PS::oQ, &mQ, i0 - HZ, j0 - H - HT, 0, &bar[2 * b]);
+    // interior tiles lie inside the grid (i0 + TZ <= Nz, j0 + TR <= Nr, i0 and j0 even)
+    bulk_g2s(met, a.dxidz + i0, TZ * 8, &bar[2 * b]);
+    bulk_g2s(met + TZ, a.ddxidxidz + i0, TZ * 8, &bar[2 * b]);
+    bulk_g2s(met + 2 * TZ, a.zc + i0, TZ * 8, &bar[2 * b]);
+    bulk_g2s(met + 3 * TZ, a.detadr + j0, TR * 8, &bar[2 * b]);
+    bulk_g2s(met + 3 * TZ + TR, a.ddetadetadr + j0, TR * 8, &bar[2 * b]);
+    bulk_g2s(met + 3 * TZ + 2 * TR, a.rc + j0, TR * 8, &bar[2 * b]);
+    bulk_g2s(met + 3 * TZ + 3 * TR, a.invr + j0, TR * 8, &bar[2 * b]);
+    if (needRK) {
+      mbar_expect_tx(&bar[2 * b + 1], (needU0 ? SM::tile_bytes : 0u) + (needA ? SM::tile_bytes : 0u));
+      if (needU0) tma_load_3d(base + PS::oP0, &mU0, i0, j0, 0, &bar[2 * b + 1]);
+      if (needA) tma_load_3d(base + PS::oPA, &mAcc, i0, j0, 0, &bar[2 * b + 1]);
+    }
+    if (a.stage == 3) tma_prefetch_3d(&mB, i0, j0, 0);  // k2, read from global memory
+  };
+  if (tid == 0) {
+    for (int k = 0; k < 4; ++k) mbar_init(&bar[k], 1);
+    fence_mbar_init();
+    const int t = (int)atomicAdd(a.sched, 1u);
+    tile_of[0] = t;
+    if (t < ntiles) issue(t, 0);
+  }
+  __syncthreads();
+  uint32_t par = 0;  // bit 2b: parity of bar[2b]'s next completion; bit 2b+1: of bar[2b+1]
+  for (int k = 0;; ++k) {
+    bool ok = true;
+    const int b = k & 1;
+    const int t = tile_of[b];
+    if (t >= ntiles) break;
+    // the other buffer was released by the barrier that ended the previous tile
+    if (tid == 0) {
+      const int tn = (int)atomicAdd(a.sched, 1u);
+      tile_of[b ^ 1] = tn;
+      if (tn < ntiles) issue(tn, b ^ 1);
+    }
+    const int2 tt = tiles[t];
+    unsigned char* base = slot(b);
+    const uint32_t parS = (par >> (2 * b)) & 1u, parR = (par >> (2 * b + 1)) & 1u;
+    const bool got = __syncthreads_and(mbar_wait_bounded(&bar[2 * b], parS));
+    if (!got) {
+      // a bounded wait gave up: this tile's transfers land before the CTA stops
+      if (tid == 0) atomicOr(a.flags, 4);
+      mbar_drain(&bar[2 * b], parS);
+      if (needRK) mbar_drain(&bar[2 * b + 1], parR);
+    } else {
+      par ^= 1u << (2 * b);
+      const StagePtrs<SIN, R> sp{reinterpret_cast<SIN*>(base + PS::oU), reinterpret_cast<double*>(base + PS::oQ),
+                                 reinterpret_cast<double*>(smem_raw + PS::oMu0),
+                                 reinterpret_cast<double*>(base + PS::oP0), reinterpret_cast<double*>(base + PS::oPA),
+                                 reinterpret_cast<R*>(smem_raw + PS::oDz), nullptr,
+                                 reinterpret_cast<const double*>(base + PS::oMet)};
+      // on a give-up stage_compute has let the RK tiles land itself
+      ok = stage_compute<H_INT, false, SIN, R, CM, PST_THREADS>(a, tt.x, tt.y, TR, sp, &bar[2 * b + 1], parR);
+      if (ok && needRK) par ^= 1u << (2 * b + 1);
+    }
+    if (!got || !ok) {
+      // the next tile's transfers, issued above, land too; then no more tiles are taken
+      const int bn = b ^ 1;
+      if (tile_of[bn] < ntiles) {
+        mbar_drain(&bar[2 * bn], (par >> (2 * bn)) & 1u);
+        if (needRK) mbar_drain(&bar[2 * bn + 1], (par >> (2 * bn + 1)) & 1u);
+      }
+      break;
+    }
+    __syncthreads();  // buffer b is free; tile_of[b ^ 1] is visible
+  }
+  // the last CTA to finish returns the tile counter to 0 for the next launch
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    if (atomicAdd(a.sched + 1, 1u) == gridDim.x - 1) {
+      a.sched[0] = 0u;
+      a.sched[1] = 0u;
+      __threadfence();
+    }
+  }
 }
 
 // Batched form: a persistent grid-stride loop over the tiles (i0, j0, instance) of many
@@ -657,10 +841,36 @@ __global__ void __launch_bounds__(STAGE_THREADS)
   }
 }
 
+// Streaming multiprocessors of the current device (cached per ordinal).
+static int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cached[dev] = n > 0 ? n : 148;
+  }
+  return cached[dev];
+}
+
+template <typename SIN, typename R, int CM>
+static void launch_pst(const StageArgs& a, int ntiles, const int2* tiles, const StageMaps& m, cudaStream_t s) {
+  const int grid = std::min(ntiles, sm_count());
+  stage_kernel_pst<SIN, R, CM><<<grid, PST_THREADS, PstSmem<SIN, R, CM>::bytes, s>>>(
+      a, tiles, ntiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
+}
+
 template <int H, bool GEN, typename SIN, typename R>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* tiles, const StageMaps& m,
                                   cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
+  if (!GEN && a.sched) {
+    if (a.learned == CM_LRN) launch_pst<SIN, R, CM_LRN>(a, ntiles, tiles, m, s);
+    else if (a.learned == CM_PRE) launch_pst<SIN, R, CM_PRE>(a, ntiles, tiles, m, s);
+    else launch_pst<SIN, R, CM_FILT>(a, ntiles, tiles, m, s);
+    return cudaGetLastError();
+  }
   if (a.learned == CM_LRN) {
     const size_t sm = StageSmem<H, SIN, R, CM_LRN>::bytes(GEN);
     stage_kernel<H, GEN, SIN, R, CM_LRN><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
@@ -1319,14 +1529,6 @@ constexpr int ZR_PADR = 48;            // >= ZR_L + 10 - 1: windows read up to i
 constexpr int ZR_MAXNZ = 10240;  // the staged row and its codes fit in shared memory
 constexpr int ZR_MAXCHUNK = (ZR_MAXNZ + ZR_L - 1) / ZR_L;
 
-// Bulk (non-tensor) global -> shared copy completing on an mbarrier; both addresses
-// 16-byte aligned, size a multiple of 16.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
 
 __host__ __device__ constexpr int zr_pad(int nz) { return (nz + 15) & ~15; }
 __host__ __device__ constexpr int zr_xlen(int nz) { return ZR_PADL + zr_pad(nz) + ZR_PADR; }
@@ -1908,6 +2110,17 @@ static cudaError_t stage_attr() {
   return cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)StageSmem<H, SIN, R, CM_LRN>::bytes(GEN));
 }
+template <typename SIN, typename R>
+static cudaError_t pst_attr() {
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel_pst<SIN, R, CM_FILT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)PstSmem<SIN, R, CM_FILT>::bytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(stage_kernel_pst<SIN, R, CM_PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)PstSmem<SIN, R, CM_PRE>::bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel_pst<SIN, R, CM_LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)PstSmem<SIN, R, CM_LRN>::bytes);
+}
 template <int HS, int HF, bool GEN, typename SIN, typename R>
 static cudaError_t sensor_attr() {
   return cudaFuncSetAttribute(sensor_tile_kernel<HS, HF, GEN, SIN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1936,6 +2149,7 @@ static cudaError_t pair_attrs() {
   if (e != cudaSuccess) return e;
   e = stage_attr<H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = stage_attr<H_INT, false, SIN, R>();
+  if (e == cudaSuccess) e = pst_attr<SIN, R>();
   if (e == cudaSuccess) e = sensor_attr<SENS_HS_GEN, H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = sensor_attr<SENS_HS_INT, H_INT, false, SIN, R>();
   return e;

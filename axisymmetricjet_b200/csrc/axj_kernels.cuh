@@ -64,6 +64,9 @@ struct StageArgs {
   double* staleT;         // stage 4: T(i*, j*) of its input, the next ComputeTimeStep's stale T
   const double* harm;     // cos(omega t_s) of the harmonic forcing: [0] at t_n (stage 0), [s] at stage s
   int* flags;             // bit 0: non-finite value produced
+  // persistent interior tiles (stage_kernel_pst): [0] next tile, [1] CTAs finished, both 0
+  // between launches; null: the interior tiles run one per CTA (stage_kernel)
+  unsigned int* sched;
   int stage;              // 0: write rhs only; 1..4: RK4 stage
   int iT, jT;             // stale-T point (0-based)
   int mixed;              // 1: FP32 stencils and interior pointwise terms

@@ -127,8 +127,29 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def cpu_step_sample(case, threads, steps=1):
-    """Oracle (CPU restatement) on the full workload grid: seconds per RK4 step."""
+def host_cpu():
+    """(logical CPUs, physical cores, CPU model) of this host."""
+    logical = os.cpu_count() or 1
+    physical = None
+    try:
+        import psutil
+        physical = psutil.cpu_count(logical=False)
+    except Exception:
+        pass
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return logical, physical, model
+
+
+def cpu_step_sample(case, threads, steps=15, warmup=2):
+    """Oracle (CPU restatement) on the full workload grid: seconds per RK4 step over
+    `steps` steps after `warmup` untimed ones (the first step also touches every page)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     os.environ["OMP_NUM_THREADS"] = str(threads)
     import oracle
@@ -137,6 +158,8 @@ def cpu_step_sample(case, threads, steps=1):
     ora = oracle.Oracle(c["params"], c["zvec"], c["rvec"], c["ibval"],
                         oracle.patches_from_records(c["records"], c["Nz"], c["Nr"]))
     ora.set_state(c["pv"], c["target"])
+    for _ in range(warmup):
+        ora.rk4(ora.compute_time_step())
     t0 = time.perf_counter()
     for _ in range(steps):
         d = ora.compute_time_step()
@@ -148,7 +171,7 @@ def run_reference(args):
     rank = env_int("RANK", 0)
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
+    threads, physical, model = host_cpu()
     os.environ["OMP_NUM_THREADS"] = str(threads)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -171,7 +194,8 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args.case, c),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "physical_cores": physical,
+                         "cpu_model": model, "kind": "port",
                          "sample": sample + "; CPU restatement of the reference (oracle/axj_oracle.c, -O2 "
                                             "-ffp-contract=off, OpenMP), not the Fortran binary: no Fortran "
                                             "compiler in this image"},
@@ -218,6 +242,9 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the timing of the mixed-precision form of the same workload")
+    ap.add_argument("--batch-steps", type=int, default=500,
+                    help="steps of the batched 64-jet variant (0: skip it)")
+    ap.add_argument("--batch-instances", type=int, default=64)
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if args.impl == "reference" else 200
@@ -284,25 +311,35 @@ def main():
         from axisymmetricjet_b200.train_sensor import MODEL_FILE, load_model
         variants = {"mixed": time_variant(args, c, patches, npts, world, barrier, max_over_ranks, precision=1)}
         if os.path.exists(MODEL_FILE):
+            # the timed steps hold the plain sensor's judge steps in proportion: a whole number
+            # of judge periods (the judge runs on every judge_every-th iteration)
+            je = int(c["params"].judge_every) or 50
             variants["mixed_learned"] = time_variant(args, c, patches, npts, world, barrier, max_over_ranks,
-                                                     model=load_model(), precision=1, sensor=1)
+                                                     model=load_model(), steps=je * -(-args.steps // je),
+                                                     precision=1, sensor=1)
         for v in variants.values():
             v["speedup_vs_fp64"] = v["value"] / value
+        if args.batch_steps > 0:
+            variants["batched"] = time_batched(args, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        sec, n = cpu_step_sample(args.case, threads, steps=1)
-        cpu = {"value": n / sec, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"1 full RK4 step (ComputeTimeStep + RK4) of {args.case} by the oracle's C restatement "
-                         f"of the reference (OpenMP, {threads} threads): {sec:.2f} s"}
+        threads, physical, model = host_cpu()
+        cw, cs = 2, 15
+        sec, n = cpu_step_sample(args.case, threads, steps=cs, warmup=cw)
+        cpu = {"value": n / sec, "unit": UNIT, "cores": threads, "physical_cores": physical, "cpu_model": model,
+               "kind": "port",
+               "sample": f"{cs} full RK4 steps (ComputeTimeStep + RK4) of {args.case} after {cw} warm-up steps, "
+                         f"by the oracle's C restatement of the reference (OpenMP, {threads} threads on "
+                         f"{physical} physical cores): {sec:.2f} s per step"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload_config(args.case, c), parallelism=f"replicas x{world}"),
+            "config": workload_config(args.case, c),
+            "parallelism": f"replicas x{world} (one jet per GPU, no data-path collective)",
             "roofline": {"bound": "hbm", "kernel": "stage_kernel (fused RK stage, both tile classes)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
@@ -321,10 +358,29 @@ def main():
     return 0
 
 
-def time_variant(args, c, patches, npts, world, barrier, max_over_ranks, model=None, **pkw):
+def time_batched(args, rank):
+    """The batched form of uneven jets: 64 instances (Nz in [256, 2048], Nr in [96, 384],
+    Mach in [0.9, 1.5], Re in [1000, 5000], harmonic inflow forcing) in one persistent launch
+    per kernel, mixed precision + learned sensor, autotuned, graph-captured steps; against the
+    same instances one after another on the plain FP64 path, with each instance's relative
+    L2 error of rho and p against its FP64 run after the same number of steps. Every rank
+    runs its own batch (replicas); the figures are rank 0's."""
+    from axisymmetricjet_b200 import batch_eval
+    rep = batch_eval.evaluate(n=args.batch_instances, steps=args.batch_steps, seed=2024 + rank,
+                              log=lambda m: None)
+    out = {"instances": rep["instances"], "points": rep["points"], "steps": rep["steps"],
+           "timed_steps": rep["steps"] - 3, "tuning": rep["tuning"],
+           "value": rep["batched"]["value"], "unit": UNIT, "ms_per_step": rep["batched"]["ms_per_step"],
+           "sequential_fp64_value": rep["sequential_fp64"]["value"], "speedup_vs_sequential_fp64": rep.get("speedup"),
+           "rel_l2_vs_fp64": rep.get("rel_l2_vs_fp64"), "judge": rep.get("judge")}
+    return out
+
+
+def time_variant(args, c, patches, npts, world, barrier, max_over_ranks, model=None, steps=None, **pkw):
     """The same workload and timing (graph-captured steps, CUDA events, max over ranks)
     with changed solver parameters, e.g. precision = AXJ_MIXED; `model` is installed for
     the learned sensor (its judge steps are part of the timed steps)."""
+    steps = steps or args.steps
     import axisymmetricjet_b200 as axj
     from axisymmetricjet_b200._ffi import AxjParams
     prm = AxjParams.from_buffer_copy(c["params"])
@@ -336,11 +392,15 @@ def time_variant(args, c, patches, npts, world, barrier, max_over_ranks, model=N
     s.set_state(c["pv"], c["target"])
     s.run(args.warmup)
     barrier()
-    ms = max_over_ranks(s.run_timed(args.steps))
+    ms = max_over_ranks(s.run_timed(steps))
     barrier()
+    out = {"params": dict(pkw), "value": replica_throughput(npts, steps, world, ms), "unit": UNIT,
+           "ms_per_step": ms / steps, "steps": steps}
+    if model is not None:
+        st = s.learned_stats()
+        out["judge"] = dict(st, timed_steps=steps, judge_every=int(prm.judge_every))
     s.close()
-    return {"params": dict(pkw), "value": replica_throughput(npts, args.steps, world, ms), "unit": UNIT,
-            "ms_per_step": ms / args.steps}
+    return out
 
 
 def run_e2e(args, c, patches, npts, world, barrier, max_over_ranks):

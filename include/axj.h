@@ -125,7 +125,11 @@ typedef struct axj_params {
   /* 0: the stencil maps, face lists and tile classes of axj_create are built on the host;
    * 1: on the device (one thread per grid row and per tile, the same rules). */
   int64_t patch_prep;
-  int64_t reserved[3];
+  /* 0: the interior tiles of the fused stage run in a persistent kernel (one CTA per SM,
+   * the next tile's boxes loaded while the current tile is computed); 1: one tile per CTA.
+   * Both give the same results bit for bit. */
+  int64_t stage_form;
+  int64_t reserved[2];
 } axj_params;
 
 typedef struct axj_handle axj_handle;

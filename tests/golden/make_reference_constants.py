@@ -1,10 +1,10 @@
 """Writes reference_constants.json: the operator tables and default constants as the
 reference's own source states them, evaluated with Fortran's literal kinds.
 
-    python tests/golden/make_reference_constants.py [REFERENCE_DIR]
+    python tests/golden/make_reference_constants.py REFERENCE_DIR
 
 Reads ModOperator.f90 (SBP_operator, :5-121) and ModuleVariables.f90 from the
-reference checkout (default /root/reference) and evaluates every literal as the
+reference checkout given as the argument and evaluates every literal as the
 compiler does: a literal with a D exponent is double precision, any other real
 literal is a default (single-precision) real, a quotient of two single-precision
 literals is a single-precision division, and a quotient with a double operand is a
@@ -136,4 +136,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_reference_constants.py REFERENCE_DIR (the nataraj2/AxisymmetricJet checkout)")
+    main(sys.argv[1])
