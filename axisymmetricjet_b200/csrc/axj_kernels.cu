@@ -83,12 +83,27 @@ __device__ __forceinline__ R dotc(int row, const S* __restrict__ v, int stride) 
   return s;
 }
 
+// DOT_PRODUCT of the centred SBP1 row (1/12, -2/3, 0, 2/3, -1/12; ModOperator.f90) with the
+// window around p, left to right. Its middle weight is exactly zero, so that term adds
+// nothing to the running sum and is left out (the same result, one product fewer).
+template <typename R, typename S>
+__device__ __forceinline__ R dot_c1(const S* p, int stride) {
+  R s = tabv<R, 1>(4, 0) * R(p[-2 * stride]);
+  s = s + tabv<R, 1>(4, 1) * R(p[-stride]);
+  s = s + tabv<R, 1>(4, 3) * R(p[stride]);
+  s = s + tabv<R, 1>(4, 4) * R(p[2 * stride]);
+  return s;
+}
+
 // Derivative stencil of table TAB with row code `row` (0..8; 9 = none) at p (pointer
 // to the point's own value), stride 1 along z or the row length along r. Interior
 // tiles (GEN = false) always use the centred row.
 template <typename R, int TAB, bool GEN, typename S>
 __device__ __forceinline__ R dst(int row, const S* p, int stride) {
-  if (!GEN || row == 4) return dotc<R, TAB, 5>(4, p - 2 * stride, stride);
+  if (!GEN || row == 4) {
+    if (TAB == 1) return dot_c1<R>(p, stride);
+    return dotc<R, TAB, 5>(4, p - 2 * stride, stride);
+  }
   if (row >= 9) return R(0);
   return dotc<R, TAB, 6>(row, p + sbp_w0(row) * stride, stride);
 }
@@ -102,8 +117,11 @@ __device__ __forceinline__ R dst_p(int row, const S* rho, const S* T, int stride
   else { w0 = sbp_w0(row); n = 6; rw = row; }
   R s = tabv<R, 1>(rw, 0) * (R(rho[w0 * stride]) * R(T[w0 * stride]));
 #pragma unroll
-  for (int m = 1; m < 6; ++m)
-    if (m < n) s = s + tabv<R, 1>(rw, m) * (R(rho[(w0 + m) * stride]) * R(T[(w0 + m) * stride]));
+  for (int m = 1; m < 6; ++m) {
+    if (m >= n) continue;
+    if (rw == 4 && m == 2) continue;  // the centred row's exactly zero middle weight
+    s = s + tabv<R, 1>(rw, m) * (R(rho[(w0 + m) * stride]) * R(T[(w0 + m) * stride]));
+  }
   return s;
 }
 
