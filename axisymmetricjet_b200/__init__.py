@@ -436,7 +436,7 @@ class AxjBatch:
     def autotune(self, steps_per_trial=5):
         """Time every candidate tuning, keep the fastest; returns (chosen, trial times in ms)."""
         t = AxjBatchTuning()
-        ms = (C.c_double * 8)()
+        ms = (C.c_double * 32)()
         n = C.c_int64(0)
         self._chk(self.lib.axj_batch_autotune(self.b, int(steps_per_trial), C.byref(t), ms, C.byref(n)))
         return t.to_dict(), list(ms)[:n.value]

@@ -54,7 +54,7 @@ class AxjParams(C.Structure):
         ("harmonic_st", C.c_double),
         ("harmonic_uj", C.c_double),
         ("patch_prep", C.c_int64),
-        ("stage_form", C.c_int64),
+        ("stage_rows", C.c_int64),
         ("reserved", C.c_int64 * 2),
     ]
 
@@ -127,11 +127,11 @@ def default_train_cfg(**overrides):
 
 class AxjBatchTuning(C.Structure):
     _fields_ = [("tile_order", C.c_int64), ("stage_ctas_per_sm", C.c_int64), ("sensor_ctas_per_sm", C.c_int64),
-                ("reserved", C.c_int64 * 5)]
+                ("stage_rows", C.c_int64), ("reserved", C.c_int64 * 4)]
 
     def to_dict(self):
         return {"tile_order": self.tile_order, "stage_ctas_per_sm": self.stage_ctas_per_sm,
-                "sensor_ctas_per_sm": self.sensor_ctas_per_sm}
+                "sensor_ctas_per_sm": self.sensor_ctas_per_sm, "stage_rows": self.stage_rows}
 
 
 def default_params(**overrides):

@@ -62,7 +62,6 @@ struct axj_handle {
   double* harm = nullptr;  // cos(omega t_s) of the harmonic forcing per stage
   int* flags = nullptr;
   unsigned int* counter = nullptr;
-  unsigned int* sched = nullptr;  // tile counter of the persistent interior stage kernel (null: one tile per CTA)
   int2 *tiles_int = nullptr, *tiles_gen = nullptr;
   int ntiles_int = 0, ntiles_gen = 0;
   int dt_blocks = 0;
@@ -120,6 +119,10 @@ struct axj_handle {
   // buffers; the coefficient planes it writes, as boxes of the two tile classes
   CUtensorMap map_zrQ, map_zrZc, map_zrRc, map_zrT[5];
   CUtensorMap map_coef[2];
+  // interior tiles as two CTAs of TR / 2 rows (int_rows == TR / 2, or a batch tuned so):
+  // their boxes
+  int int_rows = TR;
+  CUtensorMap map_stateH[5], map_starH, map_starLH, map_coefH, map_u0H, map_accH, map_bH;
 };
 
 namespace {
@@ -405,6 +408,11 @@ int build_zr_maps(axj_handle* h) {
     stage_boxes(cls == 1, h->mixed, &hw, &hh, &qh, &tw, &th, &qlh);
     rc = make_map(h, &h->map_coef[cls], h->coef, 3, hw, qlh, 3);
   }
+  if (rc == AXJ_OK) {
+    int hw, hh, qh, tw, th, qlh;
+    stage_boxes(false, h->mixed, &hw, &hh, &qh, &tw, &th, &qlh, TR / 2);
+    rc = make_map(h, &h->map_coefH, h->coef, 3, hw, qlh, 3);
+  }
   return rc;
 }
 
@@ -442,13 +450,33 @@ int build_maps(axj_handle* h) {
   if (rc != AXJ_OK) return rc;
   rc = make_map(h, &h->map_b_tile, h->B, 5, tw, th, 5);
   if (rc != AXJ_OK) return rc;
-  return make_map(h, &h->map_acc_tile, h->A, 5, tw, th, 5);
+  rc = make_map(h, &h->map_acc_tile, h->A, 5, tw, th, 5);
+  if (rc != AXJ_OK) return rc;
+  // the half tiles of the interior class (a handle's int_rows, or a batch's tuning)
+  int qlh;
+  stage_boxes(false, h->mixed, &hw, &hh, &qh, &tw, &th, &qlh, TR / 2);
+  for (int b = 0; b < nb && rc == AXJ_OK; ++b)
+    rc = make_map(h, &h->map_stateH[b], buf_ptr(h, b), 5, hw, hh, 5, buf_f32(b));
+  if (rc == AXJ_OK) rc = make_map(h, &h->map_starH, h->Qz ? h->Qz : h->star, 3, hw, qh, 3);
+  if (rc == AXJ_OK) rc = make_map(h, &h->map_starLH, h->star, 3, hw, qlh, 3);
+  if (rc == AXJ_OK) rc = make_map(h, &h->map_u0H, h->U0, 5, tw, th, 5);
+  if (rc == AXJ_OK) rc = make_map(h, &h->map_bH, h->B, 5, tw, th, 5);
+  if (rc == AXJ_OK) rc = make_map(h, &h->map_accH, h->A, 5, tw, th, 5);
+  return rc;
 }
 
 // cm: CM_FILT (z-filtered quantities, r filter in the stage kernel), CM_LRN (learned
 // coefficient planes) or CM_PRE (mu_eff, beta, kappa_eff from the fused z/r filter).
 StageMaps stage_maps(axj_handle* h, int b, int cls, int cm) {
   StageMaps m;
+  if (cls == 0 && h->int_rows != TR) {
+    m.state = &h->map_stateH[b];
+    m.star = cm == CM_LRN ? &h->map_starLH : (cm == CM_PRE ? &h->map_coefH : &h->map_starH);
+    m.u0 = &h->map_u0H;
+    m.acc = &h->map_accH;
+    m.bt = &h->map_bH;
+    return m;
+  }
   m.state = &h->map_state[b][cls];
   m.star = cm == CM_LRN ? &h->map_starL[cls] : (cm == CM_PRE ? &h->map_coef[cls] : &h->map_star[cls]);
   m.u0 = &h->map_u0_tile;
@@ -460,9 +488,9 @@ StageMaps stage_maps(axj_handle* h, int b, int cls, int cm) {
 int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage, int cm) {
   StageArgs a = stage_args(h, bin, bout, stage);
   a.learned = cm;
-  a.sched = h->sched;
   StageMaps mi = stage_maps(h, bin, 0, cm), mg = stage_maps(h, bin, 1, cm);
-  AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, mi, h->ntiles_gen, h->tiles_gen, mg, h->side, h->stream));
+  AXJ_CUDA(h, launch_stage(a, h->ntiles_int, h->tiles_int, mi, h->ntiles_gen, h->tiles_gen, mg, h->side, h->stream,
+                           h->int_rows));
   return AXJ_OK;
 }
 
@@ -1236,8 +1264,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     return fail(nullptr, AXJ_ERR_ARG, "sensor %lld unknown", (long long)prm->sensor);
   if (prm->patch_prep != 0 && prm->patch_prep != 1)
     return fail(nullptr, AXJ_ERR_ARG, "patch_prep %lld unknown", (long long)prm->patch_prep);
-  if (prm->stage_form != 0 && prm->stage_form != 1)
-    return fail(nullptr, AXJ_ERR_ARG, "stage_form %lld unknown", (long long)prm->stage_form);
+  if (prm->stage_rows != 0 && prm->stage_rows != TR && prm->stage_rows != TR / 2)
+    return fail(nullptr, AXJ_ERR_ARG, "stage_rows %lld is not 0, %d or %d", (long long)prm->stage_rows, TR, TR / 2);
   if (prm->sensor != AXJ_SENSOR_PLAIN && !prm->shock_capturing)
     return fail(nullptr, AXJ_ERR_ARG, "the learned sensor needs shock_capturing = 1");
   if (prm->sensor != AXJ_SENSOR_PLAIN && (prm->judge_every < 1 || !(prm->judge_threshold >= 0.0)))
@@ -1365,6 +1393,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->Ua = dalloc<double>(h, 5 * pl, &rc);
   h->Ub = dalloc<double>(h, 5 * pl, &rc);
   h->mixed = prm->precision == AXJ_MIXED;
+  h->int_rows = prm->stage_rows == 0 ? AXJ_DEFAULT_STAGE_ROWS : (int)prm->stage_rows;
   h->learned = prm->sensor != AXJ_SENSOR_PLAIN;
   h->held_only = prm->sensor == AXJ_SENSOR_HELD;
   h->judge_every = prm->judge_every;
@@ -1411,11 +1440,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->time = dalloc<double>(h, 1, &rc);
   h->harm = dalloc<double>(h, 5, &rc);
   h->flags = dalloc<int>(h, 1, &rc);
-  // the persistent interior stage kernel copies the tiles' 1-D metrics with bulk copies,
-  // which need 16-byte aligned rows: every interior tile starts on an even row
-  bool even_rows = true;
-  for (const int2& t : tint) even_rows = even_rows && (t.y % 2 == 0) && (t.x % 2 == 0);
-  if (prm->stage_form == 0 && even_rows && !tint.empty()) h->sched = dalloc<unsigned int>(h, 2, &rc);
+
   h->counter = dalloc<unsigned int>(h, 1, &rc);
   h->dt_blocks = 148 * 4;
   h->partial = dalloc<double>(h, h->dt_blocks, &rc);
@@ -2245,8 +2270,9 @@ struct axj_batch {
   SensorArgs a0_sens[5];
   InferArgs a0_infer[2];
   // host tile lists (i0, j0, instance) and their device copies
-  std::vector<int4> h_st_int, h_st_gen, h_se_int, h_se_gen, h_ft, h_mt;
+  std::vector<int4> h_st_int, h_st_gen, h_se_int, h_se_gen, h_ft, h_mt, h_st_half;
   int4 *st_int = nullptr, *st_gen = nullptr, *se_int = nullptr, *se_gen = nullptr, *ft = nullptr, *mt = nullptr;
+  int4* st_half = nullptr;  // the interior stage tiles as half tiles of TR / 2 rows
   int2* zrows = nullptr;
   int nzrows = 0, zthreads = 32;
   size_t zsmem = 0;
@@ -2340,6 +2366,13 @@ int batch_tiles(axj_batch* b, bool first) {
   }
   const int o = (int)b->tune.tile_order;
   b->h_st_int = order_tiles(si, o);
+  std::vector<std::vector<int2>> sh(b->n);
+  for (int k = 0; k < b->n; ++k)
+    for (const int2& t : si[k]) {
+      sh[k].push_back(t);
+      sh[k].push_back(make_int2(t.x, t.y + TR / 2));
+    }
+  b->h_st_half = order_tiles(sh, o);
   b->h_st_gen = order_tiles(sg, o);
   b->h_se_int = order_tiles(ei, o);
   b->h_se_gen = order_tiles(eg, o);
@@ -2348,6 +2381,7 @@ int batch_tiles(axj_batch* b, bool first) {
   int rc = AXJ_OK;
   if (first) {
     if (rc == AXJ_OK) rc = bupload(b, &b->st_int, b->h_st_int);
+    if (rc == AXJ_OK) rc = bupload(b, &b->st_half, b->h_st_half);
     if (rc == AXJ_OK) rc = bupload(b, &b->st_gen, b->h_st_gen);
     if (rc == AXJ_OK) rc = bupload(b, &b->se_int, b->h_se_int);
     if (rc == AXJ_OK) rc = bupload(b, &b->se_gen, b->h_se_gen);
@@ -2355,6 +2389,7 @@ int batch_tiles(axj_batch* b, bool first) {
     if (rc == AXJ_OK) rc = bupload(b, &b->mt, b->h_mt);
   } else {
     if (rc == AXJ_OK) rc = bupdate(b, b->st_int, b->h_st_int);
+    if (rc == AXJ_OK) rc = bupdate(b, b->st_half, b->h_st_half);
     if (rc == AXJ_OK) rc = bupdate(b, b->st_gen, b->h_st_gen);
     if (rc == AXJ_OK) rc = bupdate(b, b->se_int, b->h_se_int);
     if (rc == AXJ_OK) rc = bupdate(b, b->se_gen, b->h_se_gen);
@@ -2378,7 +2413,9 @@ int batch_stage(axj_batch* b, int bin, int bout, int stage, bool judge) {
   (void)bout;
   const bool lrn_plain = b->learned && judge && stage > 1;
   const bool lrn = b->learned && !lrn_plain;
-  const BatchTiles sti = btiles(b, b->st_int, b->h_st_int, b->tune.stage_ctas_per_sm);
+  const int rows = (int)b->tune.stage_rows;
+  const BatchTiles sti = rows == TR / 2 ? btiles(b, b->st_half, b->h_st_half, b->tune.stage_ctas_per_sm)
+                                        : btiles(b, b->st_int, b->h_st_int, b->tune.stage_ctas_per_sm);
   const BatchTiles stg = btiles(b, b->st_gen, b->h_st_gen, 1);
   const BatchTiles sei = btiles(b, b->se_int, b->h_se_int, b->tune.sensor_ctas_per_sm);
   const BatchTiles seg = btiles(b, b->se_gen, b->h_se_gen, 1);
@@ -2407,7 +2444,7 @@ int batch_stage(axj_batch* b, int bin, int bout, int stage, bool judge) {
   }
   const int L = lrn ? 1 : 0;
   BATCH_CUDA(b, launch_stage_batch(b->stage_argv[L][stage], b->a0_stage[L][stage], sti, stg, b->maps, bin, b->side,
-                                   b->stream));
+                                   b->stream, rows));
   return AXJ_OK;
 }
 
@@ -2509,6 +2546,11 @@ int batch_build_tables(axj_batch* b) {
     }
     m[14] = h->map_u0_tile;
     m[15] = h->map_acc_tile;
+    for (int bf = 0; bf < NBUF; ++bf) m[bmap_stateH(bf)] = h->map_stateH[bf < nb ? bf : 0];
+    m[bmap_starH(false)] = h->map_starH;
+    m[bmap_starH(true)] = h->map_starLH;
+    m[bmap_u0H] = h->map_u0H;
+    m[bmap_accH] = h->map_accH;
     for (int bf = 0; bf < NBUF; ++bf) m[bmap_rho(bf)] = h->map_rho[bf < nb ? bf : 0];
   }
   {
@@ -2637,6 +2679,7 @@ void axj_batch_default_tuning(axj_batch_tuning* t) {
   t->tile_order = 0;
   t->stage_ctas_per_sm = 2;
   t->sensor_ctas_per_sm = 2;
+  t->stage_rows = TR;
 }
 
 int axj_batch_create(axj_handle* const* handles, int64_t n, axj_batch** out) {
@@ -2704,7 +2747,7 @@ int axj_batch_create(axj_handle* const* handles, int64_t n, axj_batch** out) {
 int axj_batch_set_tuning(axj_batch* b, const axj_batch_tuning* t) {
   if (!b || !t) return bfail(b, AXJ_ERR_ARG, "null argument");
   if (t->tile_order < 0 || t->tile_order > 1 || t->stage_ctas_per_sm < 1 || t->stage_ctas_per_sm > 8 ||
-      t->sensor_ctas_per_sm < 1 || t->sensor_ctas_per_sm > 8)
+      t->sensor_ctas_per_sm < 1 || t->sensor_ctas_per_sm > 8 || (t->stage_rows != TR && t->stage_rows != TR / 2))
     return bfail(b, AXJ_ERR_ARG, "tuning out of range");
   BATCH_CUDA(b, cudaSetDevice(b->device));
   BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
@@ -2763,19 +2806,23 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
   BATCH_CUDA(b, cudaSetDevice(b->device));
   BatchSave save;
   if (int rc = batch_save(b, save)) return rc;
-  // candidates: tile order x persistent CTAs per SM of the interior stage and sensor kernels
+  // candidates: tile order x interior stage tile shape (32 x 16, or 32 x 8 half tiles)
+  // with its persistent CTAs per SM (1 or 2 of 256 threads; 2 or 4 of 128) x persistent
+  // CTAs per SM of the interior sensor kernel
   std::vector<axj_batch_tuning> cands;
   for (int o = 0; o < 2; ++o)
-    for (int sc = 1; sc <= 2; ++sc)
-      for (int se = 1; se <= 2; ++se) {
-        axj_batch_tuning t;
-        axj_batch_default_tuning(&t);
-        t.tile_order = o;
-        t.stage_ctas_per_sm = sc;
-        t.sensor_ctas_per_sm = se;
-        if (!b->sc && se > 1) continue;
-        cands.push_back(t);
-      }
+    for (int rows : {TR, TR / 2})
+      for (int sc = 1; sc <= 2; ++sc)
+        for (int se = 1; se <= 2; ++se) {
+          axj_batch_tuning t;
+          axj_batch_default_tuning(&t);
+          t.tile_order = o;
+          t.stage_rows = rows;
+          t.stage_ctas_per_sm = rows == TR ? sc : 2 * sc;
+          t.sensor_ctas_per_sm = se;
+          if (!b->sc && se > 1) continue;
+          cands.push_back(t);
+        }
   double best = 1e300;
   axj_batch_tuning best_t = b->tune;
   int k = 0;

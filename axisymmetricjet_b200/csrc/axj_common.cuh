@@ -20,8 +20,6 @@ namespace axj {
 constexpr int TZ = 32;
 constexpr int TR = 16;
 constexpr int STAGE_THREADS = 256;
-// Threads of the persistent interior stage kernel: one point of a tile each.
-constexpr int PST_THREADS = TZ * TR;
 
 // Halo of the two tile classes. Interior tiles only use the interior SBP rows
 // (reach 2); general tiles (domain edges, patch strips, blanked points, face

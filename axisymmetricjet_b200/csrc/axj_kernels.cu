@@ -223,13 +223,15 @@ __host__ __device__ constexpr int hz_t(int h, int esize) { return (h + 16 / esiz
 // HZ follows the arithmetic type: the mixed path rounds to 4 elements in every stage
 // (valid for its double stage-1 input too), so one coefficient-box map serves all stages.
 // CM, the content of the coefficient box (CM_FILT, CM_LRN, CM_PRE: axj_kernels.cuh).
-template <int H, typename SIN, typename R, int CM = CM_FILT>
+// TRT: rows of the tile (TR; interior tiles can also run as two halves of TR / 2 rows,
+// which need about half the shared memory and so let four CTAs share an SM).
+template <int H, typename SIN, typename R, int CM = CM_FILT, int TRT = TR>
 struct StageSmem {
   static constexpr int HZ = hz_t(H, (int)sizeof(R));
   static constexpr int RZ = TZ + 2 * HZ;
-  static constexpr int RR = TR + 2 * H;
+  static constexpr int RR = TRT + 2 * H;
   static constexpr int NPT = RZ * RR;
-  static constexpr int NTP = TZ * TR;
+  static constexpr int NTP = TZ * TRT;
   // r reach of the truncated-Gaussian filter rows: 4 for the centred row, 10 for the
   // 11-point boundary rows (ModTGfilter.f90:31-44)
   static constexpr int HT = CM != CM_FILT ? 0 : ((H == H_INT) ? 4 : 10);
@@ -244,7 +246,8 @@ struct StageSmem {
   static constexpr size_t oU = 0;
   static constexpr size_t oQ = align128(oU + sizeof(SIN) * 5 * NPT);
   static constexpr size_t oMu0 = align128(oQ + sizeof(double) * 3 * RQ * RZ);
-  static constexpr size_t oP0 = align128(oMu0 + sizeof(double) * NTP);
+  // (CM_PRE reads beta from the coefficient box and needs no plain mu)
+  static constexpr size_t oP0 = align128(oMu0 + (CM == CM_PRE ? 0 : sizeof(double) * NTP));
   static constexpr size_t oPA = align128(oP0 + sizeof(double) * 5 * NTP);
   __host__ __device__ static constexpr size_t oDz(bool gen) {
     return gen ? oP0 : align128(oPA + sizeof(double) * 5 * NTP);
@@ -257,7 +260,7 @@ struct StageSmem {
   __host__ __device__ static constexpr size_t oMet(bool gen) {
     return align128(oDesc(gen) + (gen ? sizeof(uint32_t) * NPT : 0));
   }
-  static constexpr int NMET = 3 * TZ + 4 * TR;
+  static constexpr int NMET = 3 * TZ + 4 * TRT;
   __host__ __device__ static constexpr size_t bytes(bool gen) { return align128(oMet(gen) + sizeof(double) * NMET); }
   static constexpr uint32_t state_bytes = sizeof(SIN) * 5 * NPT;
   static constexpr uint32_t q_bytes = sizeof(double) * 3 * RQ * RZ;
@@ -289,10 +292,10 @@ struct StagePtrs {
 // the tile columns, then the points. The RK operand tiles of interior tiles complete on
 // barRK (parity rk_parity). Returns false if that bounded wait gave up (the flag is set and
 // the transfers in flight have landed).
-template <int H, bool GEN, typename SIN, typename R, int CM, int NT>
+template <int H, bool GEN, typename SIN, typename R, int CM, int NT, int TRT>
 __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0, int nrow,
                                               const StagePtrs<SIN, R>& sp, uint64_t* barRK, uint32_t rk_parity) {
-  using SM = StageSmem<H, SIN, R, CM>;
+  using SM = StageSmem<H, SIN, R, CM, TRT>;
   using RP = typename std::conditional<GEN, double, R>::type;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, RR = SM::RR, NPT = SM::NPT, NTP = SM::NTP, HT = SM::HT, RQ = SM::RQ;
   constexpr int NPER = (NPT + NT - 1) / NT;
@@ -329,11 +332,11 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
       vmu[k] = vbe[k] = vka[k] = 0.0;
       if (idx >= NPT) continue;
       const int rr = idx / RZ, rz = idx - rr * RZ;
-      const bool cross = (rr >= H && rr < H + TR && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
+      const bool cross = (rr >= H && rr < H + TRT && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
       if (!cross) continue;
       const double mu = double(mu_of_T<R>(R(sU[4 * NPT + idx])));
       vmu[k] = mu;
-      if (rr >= H && rr < H + TR && rz >= HZ && rz < HZ + TZ) sMu0[(rr - H) * TZ + (rz - HZ)] = mu;
+      if (rr >= H && rr < H + TRT && rz >= HZ && rz < HZ + TZ) sMu0[(rr - H) * TZ + (rz - HZ)] = mu;
       if (sc) {
         int rw = 4;
         if (GEN) {
@@ -379,7 +382,7 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
       const int idx = tid + k * NT;
       if (idx >= NPT) continue;
       const int rr = idx / RZ, rz = idx - rr * RZ;
-      const bool cross = (rr >= H && rr < H + TR && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
+      const bool cross = (rr >= H && rr < H + TRT && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
       if (!cross) continue;
       sMu[idx] = vmu[k];
       if (sc) {
@@ -424,7 +427,7 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
   const double dtv = a.stage > 0 ? *a.dt : 0.0;
   // cos(omega t_s) at this stage's time (harmonic forcing)
   const double cwt = a.c.control_forcing == 2 ? a.harm[a.stage] : 0.0;
-  for (int pidx = tid; pidx < TZ * TR; pidx += NT) {
+  for (int pidx = tid; pidx < TZ * TRT; pidx += NT) {
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
     if (GEN && (i >= Nz || j >= Nr || r >= nrow)) continue;
@@ -442,7 +445,7 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
     }
     const double xzd = sMet[c], erd = sMet[3 * TZ + r];
     const R xz = R(xzd), xzz = R(sMet[TZ + c]);
-    const R er = R(erd), err = R(sMet[3 * TZ + TR + r]);
+    const R er = R(erd), err = R(sMet[3 * TZ + TRT + r]);
     const SIN* pR = sU + 0 * NPT + sidx;
     const SIN* pVr = sU + 1 * NPT + sidx;
     const SIN* pVt = sU + 2 * NPT + sidx;
@@ -502,13 +505,13 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
       q.lambda = RP(beta - (2.0 / 3.0) * double(*pMu));
     }
     const DerivT<RP> d = convert<RP>(dr);
-    const double rloc = sMet[3 * TZ + 2 * TR + r], zloc = sMet[2 * TZ + c];
+    const double rloc = sMet[3 * TZ + 2 * TRT + r], zloc = sMet[2 * TZ + c];
     const bool j1 = (j == 0);
     double rhs[5] = {-0.0, -0.0, -0.0, -0.0, -0.0};
     if (!j1) {
       RP rp[5];
       const RhsConst<RP> kc = rhs_const<RP>(a.c.gam, a.c.Re, a.c.Pr);
-      const RP onebyr = RP(sMet[3 * TZ + 3 * TR + r]);
+      const RP onebyr = RP(sMet[3 * TZ + 3 * TRT + r]);
       const RP inv_rho = RP(1.0) / q.rho;
       rhs_inviscid<RP>(q, d, onebyr, inv_rho, kc, rp);
       if (a.c.do_viscous) rhs_viscous<RP>(q, d, onebyr, inv_rho, kc, sc, rp);
@@ -590,14 +593,14 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
   return true;
 }
 
-// One tile (i0, j0) of the fused stage. Returns false if a bounded wait gave up (the
-// flag is set; the caller stops).
-template <int H, bool GEN, typename SIN, typename R, int CM>
+// One tile (i0, j0) of the fused stage with NT threads and TRT rows. Returns false if a
+// bounded wait gave up (the flag is set; the caller stops).
+template <int H, bool GEN, typename SIN, typename R, int CM, int NT = STAGE_THREADS, int TRT = TR>
 __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, const CUtensorMap* mState,
                                            const CUtensorMap* mQ, const CUtensorMap* mU0, const CUtensorMap* mAcc,
                                            const CUtensorMap* mB,
                                            unsigned char* smem_raw, uint64_t* bar, uint32_t& phase) {
-  using SM = StageSmem<H, SIN, R, CM>;
+  using SM = StageSmem<H, SIN, R, CM, TRT>;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, NPT = SM::NPT, HT = SM::HT;
   SIN* sU = reinterpret_cast<SIN*>(smem_raw + SM::oU);            // [5][RR][RZ]
   double* sQ = reinterpret_cast<double*>(smem_raw + SM::oQ);      // [3][RQ][RZ]
@@ -612,10 +615,10 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long P = a.g.P;
   const bool sc = a.c.shock_capturing != 0;
-  // general tiles of a thin r band own only its rows: TR - (bits 24-31 of j0)
-  int nrow = TR;
+  // general tiles of a thin r band own only its rows: TRT - (bits 24-31 of j0)
+  int nrow = TRT;
   if (GEN) {
-    nrow = TR - (j0 >> 24);
+    nrow = TRT - (j0 >> 24);
     j0 &= 0xFFFFFF;
   }
   // pv_old is needed as a tile in stages 2 and 3 (stage 1 reads it from the state box),
@@ -646,7 +649,7 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
     if (GEN && (a.stage == 3 || a.stage == 4)) tma_prefetch_3d(mAcc, i0, j0, 0);
   }
   if (GEN) {
-    for (int idx = tid; idx < NPT; idx += STAGE_THREADS) {
+    for (int idx = tid; idx < NPT; idx += NT) {
       const int rr = idx / RZ, rz = idx - rr * RZ;
       const int i = i0 - HZ + rz, j = j0 - H + rr;
       sDesc[idx] = (i >= 0 && i < Nz && j >= 0 && j < Nr) ? __ldg(a.desc + (long long)j * P + i)
@@ -659,12 +662,12 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
     sMet[tid] = __ldg(a.dxidz + i);
     sMet[TZ + tid] = __ldg(a.ddxidxidz + i);
     sMet[2 * TZ + tid] = __ldg(a.zc + i);
-  } else if (tid < TZ + TR) {
+  } else if (tid < TZ + TRT) {
     const int r = tid - TZ, j = min(j0 + r, Nr - 1);
     sMet[3 * TZ + r] = __ldg(a.detadr + j);
-    sMet[3 * TZ + TR + r] = __ldg(a.ddetadetadr + j);
-    sMet[3 * TZ + 2 * TR + r] = __ldg(a.rc + j);
-    sMet[3 * TZ + 3 * TR + r] = __ldg(a.invr + j);
+    sMet[3 * TZ + TRT + r] = __ldg(a.ddetadetadr + j);
+    sMet[3 * TZ + 2 * TRT + r] = __ldg(a.rc + j);
+    sMet[3 * TZ + 3 * TRT + r] = __ldg(a.invr + j);
   }
   if (!__syncthreads_and(mbar_wait_bounded(&bar[0], phase & 1u))) {
     if (tid == 0) atomicOr(a.flags, 4);
@@ -674,18 +677,27 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   }
   phase ^= 1u;
   const StagePtrs<SIN, R> sp{sU, sQ, sMu0, sP0, sPA, sDz, sDesc, sMet};
-  const bool ok = stage_compute<H, GEN, SIN, R, CM, STAGE_THREADS>(a, i0, j0, nrow, sp, &bar[1], (phase >> 1) & 1u);
+  const bool ok = stage_compute<H, GEN, SIN, R, CM, NT, TRT>(a, i0, j0, nrow, sp, &bar[1], (phase >> 1) & 1u);
   if (ok && (needU0 || needA)) phase ^= 2u;
   return ok;
 }
 
 
 
-template <int H, bool GEN, typename SIN, typename R, int CM>
-__global__ void __launch_bounds__(STAGE_THREADS, 2)
+// Threads of a stage CTA: 256 for tiles of TR rows (two CTAs per SM), 128 for the half
+// tiles of TR / 2 rows (four CTAs per SM: while one waits for its boxes, three compute).
+__host__ __device__ constexpr int stage_threads(int trt) { return trt == TR ? STAGE_THREADS : STAGE_THREADS / 2; }
+__host__ __device__ constexpr int stage_ctas(int trt) { return trt == TR ? 2 : 4; }
+
+// One tile per CTA; with TRT < TR (interior tiles only) CTA k takes rows (k % NH) * TRT ..
+// of tile k / NH, NH = TR / TRT.
+template <int H, bool GEN, typename SIN, typename R, int CM, int TRT = TR>
+__global__ void __launch_bounds__(stage_threads(TRT), stage_ctas(TRT))
     stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
                  const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
                  const __grid_constant__ CUtensorMap mAcc, const __grid_constant__ CUtensorMap mB) {
+  static_assert(TRT == TR || !GEN, "general tiles run whole");
+  constexpr int NH = TR / TRT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
   if (threadIdx.x == 0) {
@@ -694,146 +706,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, 2)
     fence_mbar_init();
   }
   uint32_t phase = 0;
-  const int2 t0 = tiles[blockIdx.x];
-  stage_body<H, GEN, SIN, R, CM>(a, t0.x, t0.y, &mState, &mQ, &mU0, &mAcc, &mB, smem_raw, bar, phase);
-}
-
-// Persistent form of the interior tiles: one CTA of PST_THREADS threads per SM takes tiles
-// from a device counter and double-buffers them: while the points of tile k are computed,
-// the TMA boxes of tile k+1 (state, coefficients, pv_old and running-sum tiles) and its 1-D
-// metrics (bulk copies) land in the other buffer, so the loads overlap the arithmetic. One
-// point per thread; the per-point code is the non-persistent kernel's (stage_compute).
-template <typename SIN, typename R, int CM>
-struct PstSmem {
-  using SM = StageSmem<H_INT, SIN, R, CM>;
-  // one buffer: state box [5][RR][RZ], coefficient box [3][RQ][RZ], pv_old and running-sum
-  // tiles [5][TR][TZ], metrics [3][TZ] + [4][TR]
-  static constexpr size_t oU = 0;
-  static constexpr size_t oQ = align128(sizeof(SIN) * 5 * SM::NPT);
-  static constexpr size_t oP0 = align128(oQ + sizeof(double) * 3 * SM::RQ * SM::RZ);
-  static constexpr size_t oPA = align128(oP0 + sizeof(double) * 5 * SM::NTP);
-  static constexpr size_t oMet = align128(oPA + sizeof(double) * 5 * SM::NTP);
-  static constexpr size_t slot = align128(oMet + sizeof(double) * SM::NMET);
-  // shared by the two buffers: plain mu on the tile, dV/dz [2][RR][TZ]
-  static constexpr size_t oMu0 = 2 * slot;
-  static constexpr size_t oDz = align128(oMu0 + sizeof(double) * SM::NTP);
-  static constexpr size_t bytes = align128(oDz + sizeof(R) * 2 * SM::RR * TZ);
-  static constexpr uint32_t met_bytes = sizeof(double) * SM::NMET;
-};
-static_assert(PstSmem<double, double, CM_FILT>::bytes <= 227 * 1024, "persistent stage buffers exceed shared memory");
-static_assert(PstSmem<double, double, CM_PRE>::bytes <= 227 * 1024, "persistent stage buffers exceed shared memory");
-
-template <typename SIN, typename R, int CM>
-__global__ void __launch_bounds__(PST_THREADS, 1)
-    stage_kernel_pst(const StageArgs a, const int2* __restrict__ tiles, int ntiles,
-                     const __grid_constant__ CUtensorMap mState, const __grid_constant__ CUtensorMap mQ,
-                     const __grid_constant__ CUtensorMap mU0, const __grid_constant__ CUtensorMap mAcc,
-                     const __grid_constant__ CUtensorMap mB) {
-  using SM = StageSmem<H_INT, SIN, R, CM>;
-  using PS = PstSmem<SIN, R, CM>;
-  constexpr int H = H_INT, HZ = SM::HZ, HT = SM::HT;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar[4];  // per buffer b: bar[2b] boxes + metrics, bar[2b+1] RK tiles
-  __shared__ int tile_of[2];                // tile index held by each buffer (>= ntiles: none)
-  const int tid = threadIdx.x;
-  const bool sc = a.c.shock_capturing != 0;
-  const bool needU0 = a.stage == 2 || a.stage == 3;
-  const bool needA = a.stage == 3 || a.stage == 4;
-  const bool needRK = needU0 || needA;
-  auto slot = [&](int b) { return smem_raw + (size_t)b * PS::slot; };
-  // thread 0: the loads of tile t into buffer b
-  auto issue = [&](int t, int b) {
-    const int2 tt = tiles[t];
-    const int i0 = tt.x, j0 = tt.y;
-    unsigned char* base = slot(b);
-    double* met = reinterpret_cast<double*>(base + PS::oMet);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&bar[2 * b], SM::state_bytes + (sc ? SM::q_bytes : 0u) + PS::met_bytes);
-    tma_load_3d(base + PS::oU, &mState, i0 - HZ, j0 - H, 0, &bar[2 * b]);
-    if (sc) tma_load_3d(base + PS::oQ, &mQ, i0 - HZ, j0 - H - HT, 0, &bar[2 * b]);
-    // interior tiles lie inside the grid (i0 + TZ <= Nz, j0 + TR <= Nr, i0 and j0 even)
-    bulk_g2s(met, a.dxidz + i0, TZ * 8, &bar[2 * b]);
-    bulk_g2s(met + TZ, a.ddxidxidz + i0, TZ * 8, &bar[2 * b]);
-    bulk_g2s(met + 2 * TZ, a.zc + i0, TZ * 8, &bar[2 * b]);
-    bulk_g2s(met + 3 * TZ, a.detadr + j0, TR * 8, &bar[2 * b]);
-    bulk_g2s(met + 3 * TZ + TR, a.ddetadetadr + j0, TR * 8, &bar[2 * b]);
-    bulk_g2s(met + 3 * TZ + 2 * TR, a.rc + j0, TR * 8, &bar[2 * b]);
-    bulk_g2s(met + 3 * TZ + 3 * TR, a.invr + j0, TR * 8, &bar[2 * b]);
-    if (needRK) {
-      mbar_expect_tx(&bar[2 * b + 1], (needU0 ? SM::tile_bytes : 0u) + (needA ? SM::tile_bytes : 0u));
-      if (needU0) tma_load_3d(base + PS::oP0, &mU0, i0, j0, 0, &bar[2 * b + 1]);
-      if (needA) tma_load_3d(base + PS::oPA, &mAcc, i0, j0, 0, &bar[2 * b + 1]);
-    }
-    if (a.stage == 3) tma_prefetch_3d(&mB, i0, j0, 0);  // k2, read from global memory
-  };
-  if (tid == 0) {
-    for (int k = 0; k < 4; ++k) mbar_init(&bar[k], 1);
-    fence_mbar_init();
-    const int t = (int)atomicAdd(a.sched, 1u);
-    tile_of[0] = t;
-    if (t < ntiles) issue(t, 0);
-  }
-  __syncthreads();
-  uint32_t par = 0;  // bit 2b: parity of bar[2b]'s next completion; bit 2b+1: of bar[2b+1]
-  for (int k = 0;; ++k) {
-    bool ok = true;
-    const int b = k & 1;
-    const int t = tile_of[b];
-    if (t >= ntiles) break;
-    // the other buffer was released by the barrier that ended the previous tile
-    if (tid == 0) {
-      const int tn = (int)atomicAdd(a.sched, 1u);
-      tile_of[b ^ 1] = tn;
-      if (tn < ntiles) issue(tn, b ^ 1);
-    }
-    const int2 tt = tiles[t];
-    unsigned char* base = slot(b);
-    const uint32_t parS = (par >> (2 * b)) & 1u, parR = (par >> (2 * b + 1)) & 1u;
-    const bool got = __syncthreads_and(mbar_wait_bounded(&bar[2 * b], parS));
-    if (!got) {
-      // a bounded wait gave up: this tile's transfers land before the CTA stops
-      if (tid == 0) atomicOr(a.flags, 4);
-      mbar_drain(&bar[2 * b], parS);
-      if (needRK) mbar_drain(&bar[2 * b + 1], parR);
-    } else {
-      par ^= 1u << (2 * b);
-      const StagePtrs<SIN, R> sp{reinterpret_cast<SIN*>(base + PS::oU), reinterpret_cast<double*>(base + PS::oQ),
-                                 reinterpret_cast<double*>(smem_raw + PS::oMu0),
-                                 reinterpret_cast<double*>(base + PS::oP0), reinterpret_cast<double*>(base + PS::oPA),
-                                 reinterpret_cast<R*>(smem_raw + PS::oDz), nullptr,
-                                 reinterpret_cast<const double*>(base + PS::oMet)};
-      // on a give-up stage_compute has let the RK tiles land itself
-      ok = stage_compute<H_INT, false, SIN, R, CM, PST_THREADS>(a, tt.x, tt.y, TR, sp, &bar[2 * b + 1], parR);
-      if (ok && needRK) par ^= 1u << (2 * b + 1);
-    }
-    if (!got || !ok) {
-      // the next tile's transfers, issued above, land too; then no more tiles are taken
-      const int bn = b ^ 1;
-      if (tile_of[bn] < ntiles) {
-        mbar_drain(&bar[2 * bn], (par >> (2 * bn)) & 1u);
-        if (needRK) mbar_drain(&bar[2 * bn + 1], (par >> (2 * bn + 1)) & 1u);
-      }
-      break;
-    }
-    __syncthreads();  // buffer b is free; tile_of[b ^ 1] is visible
-  }
-  // the last CTA to finish returns the tile counter to 0 for the next launch
-  __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    if (atomicAdd(a.sched + 1, 1u) == gridDim.x - 1) {
-      a.sched[0] = 0u;
-      a.sched[1] = 0u;
-      __threadfence();
-    }
-  }
+  const int2 t0 = tiles[blockIdx.x / NH];
+  const int j0 = NH > 1 ? t0.y + (int)(blockIdx.x % NH) * TRT : t0.y;
+  stage_body<H, GEN, SIN, R, CM, stage_threads(TRT), TRT>(a, t0.x, j0, &mState, &mQ, &mU0, &mAcc, &mB, smem_raw,
+                                                          bar, phase);
 }
 
 // Batched form: a persistent grid-stride loop over the tiles (i0, j0, instance) of many
 // solver instances; each instance's arguments and tensor maps come from device tables
-// (the arguments are staged in shared memory per tile).
-template <int H, bool GEN, typename SIN, typename R, int CM>
-__global__ void __launch_bounds__(STAGE_THREADS)
+// (the arguments are staged in shared memory per tile). With TRT < TR the table holds the
+// half tiles of the interior class (their own origins) and the maps their boxes.
+template <int H, bool GEN, typename SIN, typename R, int CM, int TRT = TR>
+__global__ void __launch_bounds__(stage_threads(TRT), TRT == TR ? 1 : stage_ctas(TRT))
     stage_kernel_batch(const StageArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
                        const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -853,52 +737,28 @@ __global__ void __launch_bounds__(STAGE_THREADS)
       reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + tt.z)[k];
     __syncthreads();
     const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
-    if (!stage_body<H, GEN, SIN, R, CM>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, m + kmaps.w, nullptr,
-                                        smem_raw, bar, phase))
+    if (!stage_body<H, GEN, SIN, R, CM, stage_threads(TRT), TRT>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y,
+                                                                 m + kmaps.z, m + kmaps.w, nullptr, smem_raw, bar,
+                                                                 phase))
       return;
   }
 }
 
-// Streaming multiprocessors of the current device (cached per ordinal).
-static int sm_count() {
-  static int cached[64] = {0};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (!cached[dev]) {
-    int n = 0;
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    cached[dev] = n > 0 ? n : 148;
-  }
-  return cached[dev];
-}
-
-template <typename SIN, typename R, int CM>
-static void launch_pst(const StageArgs& a, int ntiles, const int2* tiles, const StageMaps& m, cudaStream_t s) {
-  const int grid = std::min(ntiles, sm_count());
-  stage_kernel_pst<SIN, R, CM><<<grid, PST_THREADS, PstSmem<SIN, R, CM>::bytes, s>>>(
-      a, tiles, ntiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
-}
-
-template <int H, bool GEN, typename SIN, typename R>
+template <int H, bool GEN, typename SIN, typename R, int TRT = TR>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* tiles, const StageMaps& m,
                                   cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
-  if (!GEN && a.sched) {
-    if (a.learned == CM_LRN) launch_pst<SIN, R, CM_LRN>(a, ntiles, tiles, m, s);
-    else if (a.learned == CM_PRE) launch_pst<SIN, R, CM_PRE>(a, ntiles, tiles, m, s);
-    else launch_pst<SIN, R, CM_FILT>(a, ntiles, tiles, m, s);
-    return cudaGetLastError();
-  }
+  const int grid = ntiles * (TR / TRT), nt = stage_threads(TRT);
   if (a.learned == CM_LRN) {
-    const size_t sm = StageSmem<H, SIN, R, CM_LRN>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, CM_LRN><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
+    const size_t sm = StageSmem<H, SIN, R, CM_LRN, TRT>::bytes(GEN);
+    stage_kernel<H, GEN, SIN, R, CM_LRN, TRT><<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
   } else if (a.learned == CM_PRE) {
-    const size_t sm = StageSmem<H, SIN, R, CM_PRE>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, CM_PRE><<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
+    const size_t sm = StageSmem<H, SIN, R, CM_PRE, TRT>::bytes(GEN);
+    stage_kernel<H, GEN, SIN, R, CM_PRE, TRT><<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
   } else {
-    const size_t sm = StageSmem<H, SIN, R, CM_FILT>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, CM_FILT>
-        <<<ntiles, STAGE_THREADS, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
+    const size_t sm = StageSmem<H, SIN, R, CM_FILT, TRT>::bytes(GEN);
+    stage_kernel<H, GEN, SIN, R, CM_FILT, TRT>
+        <<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
   }
   return cudaGetLastError();
 }
@@ -921,12 +781,13 @@ static cudaError_t join(const SideStream& side, cudaStream_t s) {
 template <typename SIN, typename R>
 static cudaError_t launch_stage_pair(const StageArgs& a, int ntiles_int, const int2* tiles_int, const StageMaps& mint,
                                      int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen,
-                                     const SideStream& side, cudaStream_t s) {
+                                     const SideStream& side, cudaStream_t s, int int_rows) {
   cudaError_t e = fork(side, s);
   if (e != cudaSuccess) return e;
   e = launch_stage_t<H_GEN, true, SIN, R>(a, ntiles_gen, tiles_gen, mgen, side.stream ? side.stream : s);
   if (e != cudaSuccess) return e;
-  e = launch_stage_t<H_INT, false, SIN, R>(a, ntiles_int, tiles_int, mint, s);
+  e = int_rows == TR / 2 ? launch_stage_t<H_INT, false, SIN, R, TR / 2>(a, ntiles_int, tiles_int, mint, s)
+                        : launch_stage_t<H_INT, false, SIN, R>(a, ntiles_int, tiles_int, mint, s);
   if (e != cudaSuccess) return e;
   return join(side, s);
 }
@@ -935,15 +796,29 @@ static cudaError_t launch_stage_pair(const StageArgs& a, int ntiles_int, const i
 // (double), later inputs are FP32 stage states; stencils in FP32.
 cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, const StageMaps& mint,
                          int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen, const SideStream& side,
-                         cudaStream_t s) {
+                         cudaStream_t s, int int_rows) {
   if (!a.mixed)
-    return launch_stage_pair<double, double>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s);
+    return launch_stage_pair<double, double>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s,
+                                             int_rows);
   if (!a.in_f32)
-    return launch_stage_pair<double, float>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s);
-  return launch_stage_pair<float, float>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s);
+    return launch_stage_pair<double, float>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s,
+                                            int_rows);
+  return launch_stage_pair<float, float>(a, ntiles_int, tiles_int, mint, ntiles_gen, tiles_gen, mgen, side, s,
+                                         int_rows);
 }
 
-void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h, int* qlrn_h) {
+void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h, int* qlrn_h,
+                 int rows) {
+  if (!gen && rows == TR / 2) {
+    using S = StageSmem<H_INT, double, double, CM_FILT, TR / 2>;
+    *halo_w = mixed ? StageSmem<H_INT, float, float, CM_FILT, TR / 2>::RZ : S::RZ;
+    *halo_h = S::RR;
+    *q_h = S::RQ;
+    if (qlrn_h) *qlrn_h = StageSmem<H_INT, double, double, CM_LRN, TR / 2>::RQ;
+    *tile_w = TZ;
+    *tile_h = TR / 2;
+    return;
+  }
   if (mixed) {
     *halo_w = gen ? StageSmem<H_GEN, float, float>::RZ : StageSmem<H_INT, float, float>::RZ;
   } else {
@@ -2116,42 +1991,32 @@ void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th) {
   }
 }
 
-template <int H, bool GEN, typename SIN, typename R>
+template <int H, bool GEN, typename SIN, typename R, int TRT = TR>
 static cudaError_t stage_attr() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_FILT>,
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_FILT, TRT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)StageSmem<H, SIN, R, CM_FILT>::bytes(GEN));
+                                       (int)StageSmem<H, SIN, R, CM_FILT, TRT>::bytes(GEN));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)StageSmem<H, SIN, R, CM_PRE>::bytes(GEN));
+  e = cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_PRE, TRT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)StageSmem<H, SIN, R, CM_PRE, TRT>::bytes(GEN));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)StageSmem<H, SIN, R, CM_LRN>::bytes(GEN));
-}
-template <typename SIN, typename R>
-static cudaError_t pst_attr() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel_pst<SIN, R, CM_FILT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)PstSmem<SIN, R, CM_FILT>::bytes);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(stage_kernel_pst<SIN, R, CM_PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)PstSmem<SIN, R, CM_PRE>::bytes);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel_pst<SIN, R, CM_LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)PstSmem<SIN, R, CM_LRN>::bytes);
+  return cudaFuncSetAttribute(stage_kernel<H, GEN, SIN, R, CM_LRN, TRT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)StageSmem<H, SIN, R, CM_LRN, TRT>::bytes(GEN));
 }
 template <int HS, int HF, bool GEN, typename SIN, typename R>
 static cudaError_t sensor_attr() {
   return cudaFuncSetAttribute(sensor_tile_kernel<HS, HF, GEN, SIN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)SensSmem<HS, HF, SIN, R>::bytes(GEN));
 }
-template <int H, bool GEN, typename SIN, typename R>
+template <int H, bool GEN, typename SIN, typename R, int TRT = TR>
 static cudaError_t stage_batch_attr() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, CM_FILT>,
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, CM_FILT, TRT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)StageSmem<H, SIN, R, CM_FILT>::bytes(GEN));
+                                       (int)StageSmem<H, SIN, R, CM_FILT, TRT>::bytes(GEN));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, CM_LRN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)StageSmem<H, SIN, R, CM_LRN>::bytes(GEN));
+  return cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, CM_LRN, TRT>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)StageSmem<H, SIN, R, CM_LRN, TRT>::bytes(GEN));
 }
 template <int HS, int HF, bool GEN, typename SIN, typename R>
 static cudaError_t sensor_batch_attr() {
@@ -2162,12 +2027,13 @@ template <typename SIN, typename R>
 static cudaError_t pair_attrs() {
   cudaError_t e = stage_batch_attr<H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = stage_batch_attr<H_INT, false, SIN, R>();
+  if (e == cudaSuccess) e = stage_batch_attr<H_INT, false, SIN, R, TR / 2>();
   if (e == cudaSuccess) e = sensor_batch_attr<SENS_HS_GEN, H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = sensor_batch_attr<SENS_HS_INT, H_INT, false, SIN, R>();
   if (e != cudaSuccess) return e;
   e = stage_attr<H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = stage_attr<H_INT, false, SIN, R>();
-  if (e == cudaSuccess) e = pst_attr<SIN, R>();
+  if (e == cudaSuccess) e = stage_attr<H_INT, false, SIN, R, TR / 2>();
   if (e == cudaSuccess) e = sensor_attr<SENS_HS_GEN, H_GEN, true, SIN, R>();
   if (e == cudaSuccess) e = sensor_attr<SENS_HS_INT, H_INT, false, SIN, R>();
   return e;
@@ -2210,42 +2076,46 @@ cudaError_t init_kernel_attributes() {
 size_t zrows_smem(int Nz, long long P, int bs) { return zr_smem_bytes(Nz, P, bs); }
 int zrows_threads(int Nz) { return zr_threads(Nz); }
 
-template <int H, bool GEN, typename SIN, typename R, bool LRN>
+template <int H, bool GEN, typename SIN, typename R, bool LRN, int TRT = TR>
 static cudaError_t launch_stage_batch_t(const StageArgs* argv, const BatchTiles& t, const CUtensorMap* mapv, int kin,
                                         cudaStream_t s) {
   if (t.ntiles <= 0) return cudaSuccess;
   const int cls = GEN ? 1 : 0;
-  const int4 k = make_int4(bmap_state(kin, cls), bmap_star(cls, LRN), 14, 15);
+  const int4 k = TRT == TR ? make_int4(bmap_state(kin, cls), bmap_star(cls, LRN), 14, 15)
+                           : make_int4(bmap_stateH(kin), bmap_starH(LRN), bmap_u0H, bmap_accH);
   constexpr int CM = LRN ? CM_LRN : CM_FILT;
-  const size_t sm = StageSmem<H, SIN, R, CM>::bytes(GEN);
-  stage_kernel_batch<H, GEN, SIN, R, CM><<<t.grid, STAGE_THREADS, sm, s>>>(argv, t.tiles, t.ntiles, mapv, NM_BATCH, k);
+  const size_t sm = StageSmem<H, SIN, R, CM, TRT>::bytes(GEN);
+  stage_kernel_batch<H, GEN, SIN, R, CM, TRT>
+      <<<t.grid, stage_threads(TRT), sm, s>>>(argv, t.tiles, t.ntiles, mapv, NM_BATCH, k);
   return cudaGetLastError();
 }
 
 template <typename SIN, typename R, bool LRN>
 static cudaError_t launch_stage_batch_pair(const StageArgs* argv, const BatchTiles& tint, const BatchTiles& tgen,
-                                           const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s) {
+                                           const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s,
+                                           int int_rows) {
   cudaError_t e = fork(side, s);
   if (e != cudaSuccess) return e;
   e = launch_stage_batch_t<H_GEN, true, SIN, R, LRN>(argv, tgen, mapv, kin, side.stream ? side.stream : s);
   if (e != cudaSuccess) return e;
-  e = launch_stage_batch_t<H_INT, false, SIN, R, LRN>(argv, tint, mapv, kin, s);
+  e = int_rows == TR / 2 ? launch_stage_batch_t<H_INT, false, SIN, R, LRN, TR / 2>(argv, tint, mapv, kin, s)
+                         : launch_stage_batch_t<H_INT, false, SIN, R, LRN>(argv, tint, mapv, kin, s);
   if (e != cudaSuccess) return e;
   return join(side, s);
 }
 
 cudaError_t launch_stage_batch(const StageArgs* argv, const StageArgs& a0, const BatchTiles& tint, const BatchTiles& tgen,
-                               const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s) {
+                               const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s, int int_rows) {
   if (!a0.mixed) {
-    if (a0.learned) return launch_stage_batch_pair<double, double, true>(argv, tint, tgen, mapv, kin, side, s);
-    return launch_stage_batch_pair<double, double, false>(argv, tint, tgen, mapv, kin, side, s);
+    if (a0.learned) return launch_stage_batch_pair<double, double, true>(argv, tint, tgen, mapv, kin, side, s, int_rows);
+    return launch_stage_batch_pair<double, double, false>(argv, tint, tgen, mapv, kin, side, s, int_rows);
   }
   if (!a0.in_f32) {
-    if (a0.learned) return launch_stage_batch_pair<double, float, true>(argv, tint, tgen, mapv, kin, side, s);
-    return launch_stage_batch_pair<double, float, false>(argv, tint, tgen, mapv, kin, side, s);
+    if (a0.learned) return launch_stage_batch_pair<double, float, true>(argv, tint, tgen, mapv, kin, side, s, int_rows);
+    return launch_stage_batch_pair<double, float, false>(argv, tint, tgen, mapv, kin, side, s, int_rows);
   }
-  if (a0.learned) return launch_stage_batch_pair<float, float, true>(argv, tint, tgen, mapv, kin, side, s);
-  return launch_stage_batch_pair<float, float, false>(argv, tint, tgen, mapv, kin, side, s);
+  if (a0.learned) return launch_stage_batch_pair<float, float, true>(argv, tint, tgen, mapv, kin, side, s, int_rows);
+  return launch_stage_batch_pair<float, float, false>(argv, tint, tgen, mapv, kin, side, s, int_rows);
 }
 
 template <typename SIN, typename R>

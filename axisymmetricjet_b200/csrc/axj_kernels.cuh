@@ -64,9 +64,6 @@ struct StageArgs {
   double* staleT;         // stage 4: T(i*, j*) of its input, the next ComputeTimeStep's stale T
   const double* harm;     // cos(omega t_s) of the harmonic forcing: [0] at t_n (stage 0), [s] at stage s
   int* flags;             // bit 0: non-finite value produced
-  // persistent interior tiles (stage_kernel_pst): [0] next tile, [1] CTAs finished, both 0
-  // between launches; null: the interior tiles run one per CTA (stage_kernel)
-  unsigned int* sched;
   int stage;              // 0: write rhs only; 1..4: RK4 stage
   int iT, jT;             // stale-T point (0-based)
   int mixed;              // 1: FP32 stencils and interior pointwise terms
@@ -135,15 +132,19 @@ struct SideStream {
   cudaEvent_t fork, join;
 };
 
+// int_rows: rows of the interior tiles' CTAs, TR (one CTA per tile) or TR / 2 (two CTAs per
+// tile; mint then holds the half-tile boxes).
 cudaError_t launch_stage(const StageArgs& a, int ntiles_int, const int2* tiles_int, const StageMaps& mint,
                          int ntiles_gen, const int2* tiles_gen, const StageMaps& mgen, const SideStream& side,
-                         cudaStream_t s);
+                         cudaStream_t s, int int_rows);
 
 // Box sizes (elements) the stage kernel expects in its tensor maps: state halo box
 // halo_w x halo_h, z-filtered coefficient box halo_w x q_h, tile box tile_w x tile_h.
 // The mixed path uses one set of box sizes for its FP64 and FP32 stage inputs.
 // qlrn_h (nullable): box height of the final-coefficient planes of the learned sensor.
-void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h, int* qlrn_h);
+// rows: TR, or TR / 2 for the half tiles of the interior class (gen = false).
+void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* tile_w, int* tile_h, int* qlrn_h,
+                 int rows = TR);
 // Boxes (elements, one plane deep) the sensor tile kernel expects for the stage input:
 // V_r / V_z box vw x vh, temperature box tw x th (rho uses the stage tile box).
 void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th);
@@ -207,12 +208,17 @@ constexpr int DT_THREADS = 256;
 //   sensor V box of buffer b, class cls:           16 + b * 2 + cls  (16..25)
 //   sensor temperature box of buffer b, class cls: 26 + b * 2 + cls  (26..35)
 //   density tile box of buffer b:                  36 + b            (36..40)
-constexpr int NM_BATCH = 41;
+//   interior half tiles (TR / 2 rows): state box of buffer b 41 + b (41..45), z-filtered
+//   coefficient box 46, final-coefficient box 47, pv_old and running-sum tile boxes 48, 49
+constexpr int NM_BATCH = 50;
 inline int bmap_state(int b, int cls) { return b * 2 + cls; }
 inline int bmap_star(int cls, bool lrn) { return (lrn ? 12 : 10) + cls; }
 inline int bmap_sens(int b, int cls) { return 16 + b * 2 + cls; }
 inline int bmap_sensT(int b, int cls) { return 26 + b * 2 + cls; }
 inline int bmap_rho(int b) { return 36 + b; }
+inline int bmap_stateH(int b) { return 41 + b; }
+inline int bmap_starH(bool lrn) { return lrn ? 47 : 46; }
+constexpr int bmap_u0H = 48, bmap_accH = 49;
 
 struct BatchTiles {
   const int4* tiles;  // (i0, j0, instance, 0)
@@ -223,8 +229,9 @@ struct BatchTiles {
 // Fused stage over the interior and general tiles of all instances (general on the
 // side stream). argv: per-instance arguments of this stage (all with the same stage,
 // precision flags and learned flag); kin = stage-input buffer id.
+// int_rows: TR, or TR / 2 with tint holding the interior half tiles.
 cudaError_t launch_stage_batch(const StageArgs* argv, const StageArgs& a0, const BatchTiles& tint, const BatchTiles& tgen,
-                               const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s);
+                               const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s, int int_rows);
 // Sensor chain over all instances: sensor tiles, the row-staged z filter of every row
 // (zrows: (instance, j)), and with rfilter the r filter (grid y = instance, max_pts
 // points per instance at most).

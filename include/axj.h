@@ -89,6 +89,8 @@ enum axj_sensor_kind {
                              sensor's coefficients of the last judge step are held between judges */
 };
 
+#define AXJ_DEFAULT_STAGE_ROWS 8
+
 /* Run parameters: the reference's compile-time module variables
  * (ModuleVariables.f90:4-188) as a POD struct. Fill with axj_default_params. */
 typedef struct axj_params {
@@ -125,10 +127,11 @@ typedef struct axj_params {
   /* 0: the stencil maps, face lists and tile classes of axj_create are built on the host;
    * 1: on the device (one thread per grid row and per tile, the same rules). */
   int64_t patch_prep;
-  /* 0: the interior tiles of the fused stage run in a persistent kernel (one CTA per SM,
-   * the next tile's boxes loaded while the current tile is computed); 1: one tile per CTA.
-   * Both give the same results bit for bit. */
-  int64_t stage_form;
+  /* Rows of the fused stage kernel's CTAs on interior tiles (32 x 16 points each): 16 (one
+   * CTA per tile, two CTAs per SM) or 8 (two CTAs per tile with half the shared memory, four
+   * per SM); 0 is the library's default, AXJ_DEFAULT_STAGE_ROWS. The results agree to
+   * rounding (separate compilations of the same per-point code). */
+  int64_t stage_rows;
   int64_t reserved[2];
 } axj_params;
 
@@ -315,7 +318,8 @@ typedef struct axj_batch_tuning {
   int64_t tile_order;          /* 0: instance after instance; 1: round-robin over instances */
   int64_t stage_ctas_per_sm;   /* persistent CTAs per SM of the interior stage kernel (2) */
   int64_t sensor_ctas_per_sm;  /* persistent CTAs per SM of the interior sensor kernel (2) */
-  int64_t reserved[5];
+  int64_t stage_rows;          /* rows of the interior stage tiles' CTAs: 16 (32 x 16 tiles, default) or 8 */
+  int64_t reserved[4];
 } axj_batch_tuning;
 
 void axj_batch_default_tuning(axj_batch_tuning* t);
@@ -327,8 +331,9 @@ int axj_batch_run_timed(axj_batch* b, int64_t nsteps, double* ms);
 int axj_batch_set_tuning(axj_batch* b, const axj_batch_tuning* t);
 int axj_batch_get_tuning(axj_batch* b, axj_batch_tuning* t);
 /* Autotuner: times steps_per_trial batch steps for every candidate tuning (tile order x
- * CTAs per SM), keeps the fastest and returns it in *chosen; trial_ms (nullable, room for
- * 8) receives each trial's time. The trial steps are undone: the instances' solutions,
+ * interior stage tile shape 32 x 16 or 32 x 8 with its CTAs per SM x sensor CTAs per SM),
+ * keeps the fastest and returns it in *chosen; trial_ms (nullable, room for 16) receives
+ * each trial's time. The trial steps are undone: the instances' solutions,
  * times and iteration counters are restored (the learned sensor re-judges). */
 int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* chosen, double* trial_ms,
                        int64_t* ntrials);

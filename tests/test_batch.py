@@ -49,15 +49,15 @@ def _model(cases):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode", ["fp64", "mixed_learned"])
-@pytest.mark.parametrize("order", [0, 1])
-def test_batch_equals_individual_runs(mode, order):
+@pytest.mark.parametrize("order,rows", [(0, 16), (1, 16), (0, 8), (1, 8)])
+def test_batch_equals_individual_runs(mode, order, rows):
     kw = {} if mode == "fp64" else dict(precision=1, sensor=1, judge_every=3)
     cases = fixtures.batch_instances(3, seed=5, **SMALL, **kw)
     model = _model(cases) if mode != "fp64" else None
     single = _solvers(cases, model)
     batched = _solvers(cases, model)
     b = axj.AxjBatch(batched)
-    b.set_tuning(tile_order=order, stage_ctas_per_sm=1 + order)
+    b.set_tuning(tile_order=order, stage_ctas_per_sm=(1 + order) * (16 // rows), stage_rows=rows)
     steps = 7
     b.run(steps)
     for s in single:
@@ -82,7 +82,7 @@ def test_autotune_undoes_its_trials():
     ref = _solvers(cases, model)
     b = axj.AxjBatch(batched)
     chosen, trials = b.autotune(steps_per_trial=2)
-    assert len(trials) == 8 and all(t > 0 for t in trials)
+    assert len(trials) == 16 and all(t > 0 for t in trials)
     assert b.tuning() == chosen
     b.run(3)
     for s in ref:

@@ -267,19 +267,19 @@ def test_rk4_steps_production_size(oracle_mod, name):
     ora.close()
 
 
-@pytest.mark.parametrize("name", ["jet_sc", "jet", "nozzle_sat_wall_sc"])
+@pytest.mark.parametrize("name", ["jet_sc", "jet", "nozzle_sat_wall_sc", "writemesh_sc"])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_persistent_stage_kernel_equals_one_tile_per_cta(name, precision):
-    """The interior tiles in the persistent, double-buffered kernel (stage_form 0) and one
-    tile per CTA (stage_form 1) run the same per-point code (separate compilations, so FMA
-    contraction may differ in the last bit): equal to 1e-13 of each field's scale after 4
-    steps; a tile in the wrong buffer or a missed tile is an O(1) difference."""
+def test_half_tile_stage_kernel_equals_whole_tiles(name, precision):
+    """Interior tiles as two CTAs of 8 rows (stage_rows 8) and as one CTA of 16 rows
+    (stage_rows 16) run the same per-point code (separate compilations, so FMA contraction
+    may differ in the last bit): equal to 1e-13 of each field's scale after 4 steps; a half
+    tile in the wrong place or a missed half is an O(1) difference."""
     c = CASES[name]()
     c["params"].precision = precision
     patches = axj.patches_from_records(c["records"], c["Nz"], c["Nr"])
     out = []
-    for form in (0, 1):
-        c["params"].stage_form = form
+    for rows in (8, 16):
+        c["params"].stage_rows = rows
         s = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
         s.set_state(c["pv"], c["target"])
         s.run(4)
@@ -289,12 +289,12 @@ def test_persistent_stage_kernel_equals_one_tile_per_cta(name, precision):
     assert max(errs) < 1e-13, errs
 
 
-def test_persistent_stage_kernel_production_size():
+def test_half_tile_stage_kernel_production_size():
     c = fixtures.case("jet4400x640")
     patches = axj.patches_from_records(c["records"], c["Nz"], c["Nr"])
     out = []
-    for form in (0, 1):
-        c["params"].stage_form = form
+    for rows in (8, 16):
+        c["params"].stage_rows = rows
         s = axj.AxiJetSolver(c["params"], c["zvec"], c["rvec"], c["ibval"], patches)
         s.set_state(c["pv"], c["target"])
         s.run(3)
