@@ -55,7 +55,8 @@ class AxjParams(C.Structure):
         ("harmonic_uj", C.c_double),
         ("patch_prep", C.c_int64),
         ("stage_rows", C.c_int64),
-        ("reserved", C.c_int64 * 2),
+        ("judge_stages", C.c_int64),
+        ("reserved", C.c_int64 * 1),
     ]
 
 

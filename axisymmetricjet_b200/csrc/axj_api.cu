@@ -83,6 +83,7 @@ struct axj_handle {
   bool held_only = false;       // AXJ_SENSOR_HELD: no network between judge steps
   bool judged = false;          // a judge step has run since the state or the model changed
   int64_t judge_every = 50;
+  bool judge_all = true;        // a judge step runs the plain sensor on all four stages
   double judge_thr = 0.1;
   float* mlp = nullptr;         // flat FP32 parameters (MLP_NPARAM)
   MlpNorm norm{};
@@ -123,6 +124,7 @@ struct axj_handle {
   // their boxes
   int int_rows = TR;
   CUtensorMap map_stateH[5], map_starH, map_starLH, map_coefH, map_u0H, map_accH, map_bH;
+  CUtensorMap map_tgt, map_tgtH;  // pv_target tile boxes (L2 prefetch of the sponge tiles)
 };
 
 namespace {
@@ -451,6 +453,7 @@ int build_maps(axj_handle* h) {
   rc = make_map(h, &h->map_b_tile, h->B, 5, tw, th, 5);
   if (rc != AXJ_OK) return rc;
   rc = make_map(h, &h->map_acc_tile, h->A, 5, tw, th, 5);
+  if (rc == AXJ_OK) rc = make_map(h, &h->map_tgt, h->target, 5, tw, th, 5);
   if (rc != AXJ_OK) return rc;
   // the half tiles of the interior class (a handle's int_rows, or a batch's tuning)
   int qlh;
@@ -462,6 +465,7 @@ int build_maps(axj_handle* h) {
   if (rc == AXJ_OK) rc = make_map(h, &h->map_u0H, h->U0, 5, tw, th, 5);
   if (rc == AXJ_OK) rc = make_map(h, &h->map_bH, h->B, 5, tw, th, 5);
   if (rc == AXJ_OK) rc = make_map(h, &h->map_accH, h->A, 5, tw, th, 5);
+  if (rc == AXJ_OK) rc = make_map(h, &h->map_tgtH, h->target, 5, tw, th, 5);
   return rc;
 }
 
@@ -475,6 +479,7 @@ StageMaps stage_maps(axj_handle* h, int b, int cls, int cm) {
     m.u0 = &h->map_u0H;
     m.acc = &h->map_accH;
     m.bt = &h->map_bH;
+    m.tg = &h->map_tgtH;
     return m;
   }
   m.state = &h->map_state[b][cls];
@@ -482,6 +487,7 @@ StageMaps stage_maps(axj_handle* h, int b, int cls, int cm) {
   m.u0 = &h->map_u0_tile;
   m.acc = &h->map_acc_tile;
   m.bt = &h->map_b_tile;
+  m.tg = &h->map_tgt;
   return m;
 }
 
@@ -635,7 +641,7 @@ int enqueue_rk4(axj_handle* h, bool judge = false) {
   if (h->c.control_forcing == 2)
     AXJ_CUDA(h, launch_harmonic_phase(h->time, h->dt, h->c.harm_omega, 0, h->harm, h->stream));
   for (int st = 1; st <= 4; ++st) {
-    const int rc = h->learned ? enqueue_stage_learned(h, b[st - 1], b[st], st, judge && st == 1, judge && st > 1)
+    const int rc = h->learned ? enqueue_stage_learned(h, b[st - 1], b[st], st, judge && st == 1, judge && st > 1 && h->judge_all)
                               : enqueue_stage(h, b[st - 1], b[st], st);
     if (rc != AXJ_OK) return rc;
   }
@@ -1270,6 +1276,8 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
     return fail(nullptr, AXJ_ERR_ARG, "the learned sensor needs shock_capturing = 1");
   if (prm->sensor != AXJ_SENSOR_PLAIN && (prm->judge_every < 1 || !(prm->judge_threshold >= 0.0)))
     return fail(nullptr, AXJ_ERR_ARG, "judge_every must be >= 1 and judge_threshold >= 0");
+  if (prm->judge_stages != 0 && prm->judge_stages != 1 && prm->judge_stages != 4)
+    return fail(nullptr, AXJ_ERR_ARG, "judge_stages %lld is not 0, 1 or 4", (long long)prm->judge_stages);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(nullptr, AXJ_ERR_NODEVICE, "no CUDA device available");
@@ -1315,6 +1323,10 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   c.forcing_alpha = prm->forcing_alpha; c.forcing_z0 = prm->forcing_z0; c.forcing_r0 = prm->forcing_r0;
   c.forcing_lz = prm->forcing_lz; c.forcing_lr = prm->forcing_lr;
   c.r_top = rvec[(Nr - 1) * Nz];
+  c.inv_gam = 1.0 / prm->gam;
+  c.inv_Re = 1.0 / prm->Re;
+  c.gam_RePr = prm->gam / (prm->Re * prm->Pr);
+  c.gg1_Re = prm->gam * (prm->gam - 1.0) / prm->Re;
   c.do_viscous = prm->do_viscous_terms == 1;
   c.shock_capturing = prm->shock_capturing == 1;
   c.control_forcing = (prm->control_forcing == 1 || prm->control_forcing == 2) ? (int)prm->control_forcing : 0;
@@ -1397,6 +1409,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->learned = prm->sensor != AXJ_SENSOR_PLAIN;
   h->held_only = prm->sensor == AXJ_SENSOR_HELD;
   h->judge_every = prm->judge_every;
+  h->judge_all = prm->judge_stages != 1;
   h->judge_thr = prm->judge_threshold;
   if (c.shock_capturing) {
     // learned-sensor buffers (also used by the feature/prediction entry points)
@@ -1723,7 +1736,7 @@ int axj_profile_steps(axj_handle* h, int64_t nsteps, double* ms, int64_t* launch
     });
     nl[0] += 1 + (h->c.control_forcing == 2);
     for (int st = 1; st <= 4 && rc == AXJ_OK; ++st) {
-      const bool lrn_plain = h->learned && judge && st > 1;
+      const bool lrn_plain = h->learned && judge && st > 1 && h->judge_all;
       const bool lrn = h->learned && !lrn_plain;
       if (lrn && h->held_only) {
         if (judge && st == 1) {
@@ -2254,7 +2267,7 @@ struct axj_batch {
   SideStream side{nullptr, nullptr, nullptr};
   std::string err;
   std::vector<void*> mem;
-  bool mixed = false, learned = false, held_only = false, sc = false, any_harm = false;
+  bool mixed = false, learned = false, held_only = false, sc = false, any_harm = false, judge_all = true;
   int64_t iteration = 0, judge_every = 50, njudges = 0;
   // device tables
   CUtensorMap* maps = nullptr;
@@ -2411,7 +2424,7 @@ BatchTiles btiles(const axj_batch* b, const int4* d, const std::vector<int4>& hv
 // One batched RK stage (mirrors enqueue_stage / enqueue_stage_learned of a handle).
 int batch_stage(axj_batch* b, int bin, int bout, int stage, bool judge) {
   (void)bout;
-  const bool lrn_plain = b->learned && judge && stage > 1;
+  const bool lrn_plain = b->learned && judge && stage > 1 && b->judge_all;
   const bool lrn = b->learned && !lrn_plain;
   const int rows = (int)b->tune.stage_rows;
   const BatchTiles sti = rows == TR / 2 ? btiles(b, b->st_half, b->h_st_half, b->tune.stage_ctas_per_sm)
@@ -2691,9 +2704,11 @@ int axj_batch_create(axj_handle* const* handles, int64_t n, axj_batch** out) {
     if (!h) return bfail(nullptr, AXJ_ERR_ARG, "null handle %lld", (long long)k);
     if (!h->state_set) return bfail(nullptr, AXJ_ERR_ARG, "instance %lld: axj_set_state has not been called", (long long)k);
     if (h->device != h0->device || h->mixed != h0->mixed || h->learned != h0->learned ||
-        h->held_only != h0->held_only || (h->c.shock_capturing != 0) != (h0->c.shock_capturing != 0))
+        h->held_only != h0->held_only || (h->c.shock_capturing != 0) != (h0->c.shock_capturing != 0) ||
+        h->judge_all != h0->judge_all)
       return bfail(nullptr, AXJ_ERR_UNSUPPORTED,
-                   "instance %lld: every instance needs the same device, precision, sensor and shock capturing",
+                   "instance %lld: every instance needs the same device, precision, sensor, judge stages and shock "
+                   "capturing",
                    (long long)k);
     if (h->learned && !h->held_only && !h->mlp_set)
       return bfail(nullptr, AXJ_ERR_ARG, "instance %lld: learned sensor without a model", (long long)k);
@@ -2709,6 +2724,7 @@ int axj_batch_create(axj_handle* const* handles, int64_t n, axj_batch** out) {
   b->held_only = h0->held_only;
   b->sc = h0->c.shock_capturing != 0;
   b->judge_every = h0->judge_every;
+  b->judge_all = h0->judge_all;
   b->iteration = h0->iteration;
   axj_batch_default_tuning(&b->tune);
   int rc = AXJ_OK;

@@ -81,6 +81,9 @@ struct Consts {
   double forcing_alpha, forcing_z0, forcing_r0, forcing_lz, forcing_lr;
   double r_top;   // r(i, Nr): sponge normalisation (ModBC.f90:571)
   double harm_amp, harm_omega;  // harmonic forcing (control_forcing == 2): A, 2 pi St U_j
+  // per-run factors of the right-hand side, formed once on the host: 1/gam, 1/Re,
+  // gam/(Re Pr), gam (gam - 1)/Re
+  double inv_gam, inv_Re, gam_RePr, gg1_Re;
   int do_viscous;
   int shock_capturing;
   int control_forcing;  // 0 off, 1 feedback (ControlForcingTerms), 2 harmonic source

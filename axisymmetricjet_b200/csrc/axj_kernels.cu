@@ -510,7 +510,7 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
     double rhs[5] = {-0.0, -0.0, -0.0, -0.0, -0.0};
     if (!j1) {
       RP rp[5];
-      const RhsConst<RP> kc = rhs_const<RP>(a.c.gam, a.c.Re, a.c.Pr);
+      const RhsConst<RP> kc = rhs_const<RP>(a.c);
       const RP onebyr = RP(sMet[3 * TZ + 3 * TRT + r]);
       const RP inv_rho = RP(1.0) / q.rho;
       rhs_inviscid<RP>(q, d, onebyr, inv_rho, kc, rp);
@@ -598,7 +598,7 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
 template <int H, bool GEN, typename SIN, typename R, int CM, int NT = STAGE_THREADS, int TRT = TR>
 __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, const CUtensorMap* mState,
                                            const CUtensorMap* mQ, const CUtensorMap* mU0, const CUtensorMap* mAcc,
-                                           const CUtensorMap* mB,
+                                           const CUtensorMap* mB, const CUtensorMap* mTg,
                                            unsigned char* smem_raw, uint64_t* bar, uint32_t& phase) {
   using SM = StageSmem<H, SIN, R, CM, TRT>;
   constexpr int HZ = SM::HZ, RZ = SM::RZ, NPT = SM::NPT, HT = SM::HT;
@@ -645,6 +645,13 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
     // operands the RK update reads from global memory: into L2 now (k2 in stage 3; pv_old
     // and the running sum in general tiles, which do not stage them)
     if (mB && a.stage == 3) tma_prefetch_3d(mB, i0, j0, 0);
+    // pv_target, which the sponges (and the face operations, the feedback forcing) read per
+    // point from global memory: into L2 for the tiles that reach a sponge
+    if (mTg) {
+      const bool tgt = GEN || a.c.control_forcing == 1 || __ldg(a.zc + i0) <= a.c.sponge_end_left ||
+                       __ldg(a.rc + min(j0 + TRT - 1, Nr - 1)) >= a.c.sponge_start_top;
+      if (tgt) tma_prefetch_3d(mTg, i0, j0, 0);
+    }
     if (GEN && (a.stage == 2 || a.stage == 3)) tma_prefetch_3d(mU0, i0, j0, 0);
     if (GEN && (a.stage == 3 || a.stage == 4)) tma_prefetch_3d(mAcc, i0, j0, 0);
   }
@@ -695,7 +702,8 @@ template <int H, bool GEN, typename SIN, typename R, int CM, int TRT = TR>
 __global__ void __launch_bounds__(stage_threads(TRT), stage_ctas(TRT))
     stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
                  const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
-                 const __grid_constant__ CUtensorMap mAcc, const __grid_constant__ CUtensorMap mB) {
+                 const __grid_constant__ CUtensorMap mAcc, const __grid_constant__ CUtensorMap mB,
+                 const __grid_constant__ CUtensorMap mTg) {
   static_assert(TRT == TR || !GEN, "general tiles run whole");
   constexpr int NH = TR / TRT;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -708,8 +716,8 @@ __global__ void __launch_bounds__(stage_threads(TRT), stage_ctas(TRT))
   uint32_t phase = 0;
   const int2 t0 = tiles[blockIdx.x / NH];
   const int j0 = NH > 1 ? t0.y + (int)(blockIdx.x % NH) * TRT : t0.y;
-  stage_body<H, GEN, SIN, R, CM, stage_threads(TRT), TRT>(a, t0.x, j0, &mState, &mQ, &mU0, &mAcc, &mB, smem_raw,
-                                                          bar, phase);
+  stage_body<H, GEN, SIN, R, CM, stage_threads(TRT), TRT>(a, t0.x, j0, &mState, &mQ, &mU0, &mAcc, &mB, &mTg,
+                                                          smem_raw, bar, phase);
 }
 
 // Batched form: a persistent grid-stride loop over the tiles (i0, j0, instance) of many
@@ -738,8 +746,8 @@ __global__ void __launch_bounds__(stage_threads(TRT), TRT == TR ? 1 : stage_ctas
     __syncthreads();
     const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
     if (!stage_body<H, GEN, SIN, R, CM, stage_threads(TRT), TRT>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y,
-                                                                 m + kmaps.z, m + kmaps.w, nullptr, smem_raw, bar,
-                                                                 phase))
+                                                                 m + kmaps.z, m + kmaps.w, nullptr, nullptr, smem_raw,
+                                                                 bar, phase))
       return;
   }
 }
@@ -751,14 +759,16 @@ static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, const int2* ti
   const int grid = ntiles * (TR / TRT), nt = stage_threads(TRT);
   if (a.learned == CM_LRN) {
     const size_t sm = StageSmem<H, SIN, R, CM_LRN, TRT>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, CM_LRN, TRT><<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
+    stage_kernel<H, GEN, SIN, R, CM_LRN, TRT>
+        <<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt, *m.tg);
   } else if (a.learned == CM_PRE) {
     const size_t sm = StageSmem<H, SIN, R, CM_PRE, TRT>::bytes(GEN);
-    stage_kernel<H, GEN, SIN, R, CM_PRE, TRT><<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
+    stage_kernel<H, GEN, SIN, R, CM_PRE, TRT>
+        <<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt, *m.tg);
   } else {
     const size_t sm = StageSmem<H, SIN, R, CM_FILT, TRT>::bytes(GEN);
     stage_kernel<H, GEN, SIN, R, CM_FILT, TRT>
-        <<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt);
+        <<<grid, nt, sm, s>>>(a, tiles, *m.state, *m.star, *m.u0, *m.acc, *m.bt, *m.tg);
   }
   return cudaGetLastError();
 }
@@ -1032,6 +1042,47 @@ __host__ __device__ constexpr int sens_threads(bool gen) { return gen ? 512 : ST
 
 template <typename R>
 __device__ __forceinline__ R sqrt_t(R x) { return sqrt(x); }
+
+// Two neighbouring values of a shared-memory row in one 16-byte (double) or 8-byte
+// (float) load; p must be aligned to the pair.
+template <typename T>
+struct Pair2;
+template <>
+struct Pair2<double> { using t = double2; };
+template <>
+struct Pair2<float> { using t = float2; };
+template <typename T>
+__device__ __forceinline__ void ld_pair(const T* p, T& a, T& b) {
+  const typename Pair2<T>::t v = *reinterpret_cast<const typename Pair2<T>::t*>(p);
+  a = v.x;
+  b = v.y;
+}
+template <typename T>
+__device__ __forceinline__ void st_pair(T* p, T a, T b) {
+  typename Pair2<T>::t v;
+  v.x = a;
+  v.y = b;
+  *reinterpret_cast<typename Pair2<T>::t*>(p) = v;
+}
+// The centred SBP1 row on values at offsets -2, -1, 1, 2 (the zero middle weight left
+// out), in dot_c1's order.
+template <typename R>
+__device__ __forceinline__ R c1_of(R xm2, R xm1, R xp1, R xp2) {
+  R s = tabv<R, 1>(4, 0) * xm2;
+  s = s + tabv<R, 1>(4, 1) * xm1;
+  s = s + tabv<R, 1>(4, 3) * xp1;
+  s = s + tabv<R, 1>(4, 4) * xp2;
+  return s;
+}
+// The 9-point fourth difference cC9 on x[0..8], left to right (c9dot's order).
+template <typename R>
+__device__ __forceinline__ R c9_of(const R* x) {
+  const R* c = std::is_same<R, float>::value ? reinterpret_cast<const R*>(cC9f) : reinterpret_cast<const R*>(cC9);
+  R s = c[0] * x[0];
+#pragma unroll
+  for (int m = 1; m < 9; ++m) s = s + c[m] * x[m];
+  return s;
+}
 template <>
 __device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
 
@@ -1116,7 +1167,92 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   phase ^= 1u;
 
   // ---- phase 2: S and dilatation on the cross of the S region (reach HS either way);
-  // f_sw on the tile
+  // f_sw on the tile. Interior tiles: horizontal pairs of points (S columns sz, sz + 1 with
+  // sz even) whose stencil windows come in pair loads; the arithmetic per point is the
+  // general loop's.
+  if constexpr (!GEN) {
+    static_assert(SZ % 2 == 0 && VZ % 2 == 0 && HSZ % 2 == 0 && HVZ % 2 == 0 && HS % 2 == 0 && TZ % 2 == 0,
+                  "pair loads need even offsets");
+    for (int pp = tid; pp < NS / 2; pp += NT) {
+      const int sr = pp / (SZ / 2), sz = 2 * (pp - sr * (SZ / 2));
+      const bool zarm = sr >= HS && sr < HS + TR && sz >= HSZ - HS && sz < HSZ + TZ + HS;
+      const bool rarm = sz >= HSZ && sz < HSZ + TZ;
+      R S[2] = {R(0), R(0)}, dil[2] = {R(0), R(0)};
+      if (zarm || rarm) {
+        const int j = j0 - HS + sr;
+        const int vidx = (sr + HV - HS) * VZ + (sz + HVZ - HSZ);
+        const R k0 = tabv<R, 1>(4, 0), k1 = tabv<R, 1>(4, 1), k3 = tabv<R, 1>(4, 3), k4 = tabv<R, 1>(4, 4);
+        // the centred SBP1 row at both points, accumulated pair load by pair load in dot_c1's
+        // order (offsets -2, -1, +1, +2 of each point's own column or row)
+        auto zpair = [&](const SIN* row, R& p0, R& p1, R& c0, R& c1v) {
+          SIN u, v;
+          ld_pair(row - 2, u, v);  // columns -2, -1
+          p0 = k0 * R(u);
+          p0 = p0 + k1 * R(v);
+          p1 = k0 * R(v);
+          ld_pair(row, u, v);      // columns 0, +1 (the points themselves)
+          c0 = R(u);
+          c1v = R(v);
+          p0 = p0 + k3 * R(v);
+          p1 = p1 + k1 * R(u);
+          ld_pair(row + 2, u, v);  // columns +2, +3
+          p0 = p0 + k4 * R(u);
+          p1 = p1 + k3 * R(u);
+          p1 = p1 + k4 * R(v);
+        };
+        auto rpair = [&](const SIN* col, R& p0, R& p1) {
+          SIN u, v;
+          ld_pair(col - 2 * VZ, u, v);
+          p0 = k0 * R(u);
+          p1 = k0 * R(v);
+          ld_pair(col - VZ, u, v);
+          p0 = p0 + k1 * R(u);
+          p1 = p1 + k1 * R(v);
+          ld_pair(col + VZ, u, v);
+          p0 = p0 + k3 * R(u);
+          p1 = p1 + k3 * R(v);
+          ld_pair(col + 2 * VZ, u, v);
+          p0 = p0 + k4 * R(u);
+          p1 = p1 + k4 * R(v);
+        };
+        R zr0, zr1, zz0, zz1, rr0, rr1, rz0, rz1, vc0, vc1, wc0, wc1;
+        zpair(sVr + vidx, zr0, zr1, vc0, vc1);
+        zpair(sVz + vidx, zz0, zz1, wc0, wc1);
+        rpair(sVr + vidx, rr0, rr1);
+        rpair(sVz + vidx, rz0, rz1);
+        const R gz[2][2] = {{zr0, zr1}, {zz0, zz1}}, gr[2][2] = {{rr0, rr1}, {rz0, rz1}};
+        const R vrc[2] = {vc0, vc1};
+        const R er = R(sMr[sr]), ir = R(sIr[sr]);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const R xz = R(sMz[sz + h]);
+          const R dVrdz = gz[0][h] * xz;
+          const R dVzdz = gz[1][h] * xz;
+          const R dVrdr = gr[0][h] * er;
+          const R dVzdr = gr[1][h] * er;
+          // V_r / r as V_r * (1/r) (the reference divides; the two differ by rounding)
+          const R vr_r = vrc[h] * ir;
+          R d;
+          if (j == 0) d = R(2.0) * dVrdr + dVzdz;
+          else d = dVrdr + vr_r + dVzdz;
+          const R S11 = dVrdr - R(1.0 / 3.0) * d;
+          const R S13 = R(0.5) * (dVrdz + dVzdr);
+          const R S33 = dVzdz - R(1.0 / 3.0) * d;
+          const R S22 = (j == 0) ? dVrdr - R(1.0 / 3.0) * d : vr_r - R(1.0 / 3.0) * d;
+          S[h] = sqrt_t<R>(S11 * S11 + S13 * S13 + S22 * S22 + S13 * S13 + S33 * S33);
+          dil[h] = d;
+          if (zarm && rarm) {
+            const R vort = fabs(dVrdz - dVzdr);
+            const R Hm = (R(-1.0) * d < R(0)) ? R(0) : R(1);
+            const R eps = R((double)1e-15f);  // single-precision literal of the reference (:202)
+            sFsw[(sr - HS) * TZ + (sz + h - HSZ)] = Hm * (d * d) / (d * d + vort * vort + eps);
+          }
+        }
+      }
+      st_pair(sS + sr * SZ + sz, S[0], S[1]);
+      st_pair(sD + sr * SZ + sz, dil[0], dil[1]);
+    }
+  } else
   for (int idx = tid; idx < NS; idx += NT) {
     const int sr = idx / SZ, sz = idx - sr * SZ;
     const bool zarm = sr >= HS && sr < HS + TR && sz >= HSZ - HS && sz < HSZ + TZ + HS;
@@ -1167,18 +1303,94 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   auto ppoint = [](int t, int q) { return (t >> 5) * (TZ * PPT) + q * TZ + (t & 31); };
   R d4z[3][PPT], d4r[3][PPT];
   if constexpr (!GEN) {
+    // horizontal pairs (columns c, c + 1, c even), every window in pair loads, then the
+    // quantities of both points (cC9 on each point's 9 values, in c9dot's order)
+    static_assert(NT * 2 == TZ * TR, "one pair of points per thread");
+    const int r = tid / (TZ / 2), c = 2 * (tid - r * (TZ / 2));
+    const int sidx = (HS + r) * SZ + (HSZ + c);
+    R qz[3][2], qr[3][2], Tc[2];
+    const R* c9 = std::is_same<R, float>::value ? reinterpret_cast<const R*>(cC9f) : reinterpret_cast<const R*>(cC9);
+    // cC9 at both points, accumulated pair load by pair load in c9dot's order: along z the
+    // pair loads cover columns c - 4 .. c + 5 (point 0 takes columns -4..4, point 1 -3..5),
+    // along r each row's pair serves both points
+    auto four = [&](const auto* base, int f) {
+      using E = std::remove_cv_t<std::remove_reference_t<decltype(base[0])>>;
+      R z0 = R(0), z1 = R(0), r0 = R(0), r1 = R(0);
 #pragma unroll
-    for (int q = 0; q < PPT; ++q) {
-      const int pidx = ppoint(tid, q);
-      const int r = pidx / TZ, c = pidx - r * TZ;
-      const int sidx = (HS + r) * SZ + (HSZ + c);
-      d4z[0][q] = c9dot<R>(sS + sidx, 1);
-      d4r[0][q] = c9dot<R>(sS + sidx, SZ);
-      d4z[1][q] = c9dot<R>(sT + sidx, 1);
-      d4r[1][q] = c9dot<R>(sT + sidx, SZ);
-      d4z[2][q] = c9dot<R>(sD + sidx, 1);
-      d4r[2][q] = c9dot<R>(sD + sidx, SZ);
+      for (int q = 0; q < 5; ++q) {
+        R u, v;
+        {
+          E uu, vv;
+          ld_pair(base + sidx - 4 + 2 * q, uu, vv);
+          u = R(uu);
+          v = R(vv);
+        }
+        const int m = 2 * q;  // u is column m - 4, v column m - 3
+        if (q == 0) {
+          z0 = c9[0] * u;
+          z0 = z0 + c9[1] * v;
+          z1 = c9[0] * v;
+        } else if (q < 4) {
+          z0 = z0 + c9[m] * u;
+          z0 = z0 + c9[m + 1] * v;
+          z1 = z1 + c9[m - 1] * u;
+          z1 = z1 + c9[m] * v;
+        } else {
+          z0 = z0 + c9[8] * u;
+          z1 = z1 + c9[7] * u;
+          z1 = z1 + c9[8] * v;
+        }
+        if (f == 1 && q == 2) {
+          Tc[0] = u;
+          Tc[1] = v;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 9; ++m) {
+        E uu, vv;
+        ld_pair(base + sidx + (m - 4) * SZ, uu, vv);
+        if (m == 0) {
+          r0 = c9[0] * R(uu);
+          r1 = c9[0] * R(vv);
+        } else {
+          r0 = r0 + c9[m] * R(uu);
+          r1 = r1 + c9[m] * R(vv);
+        }
+      }
+      qz[f][0] = z0;
+      qz[f][1] = z1;
+      qr[f][0] = r0;
+      qr[f][1] = r1;
+    };
+    four(sS, 0);
+    four(sT, 1);
+    four(sD, 2);
+    // ---- quantities to be filtered (ComputeTobeFilteredQuantities :204-215)
+    const long long o = (long long)(j0 + r) * g.P + (i0 + c);
+    R dzp[2], rho[2], fsw[2];
+    {
+      double a0, a1;
+      ld_pair(sDzv + c, a0, a1);
+      dzp[0] = R(a0);
+      dzp[1] = R(a1);
+      SIN r0, r1;
+      ld_pair(sRho + r * TZ + c, r0, r1);
+      rho[0] = R(r0);
+      rho[1] = R(r1);
+      ld_pair(sFsw + r * TZ + c, fsw[0], fsw[1]);
     }
+    const R dr = R(sDrv[r]);
+    double out[3][2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const R dz = dzp[h];
+      out[0][h] = double(rho[h] * fabs((qz[0][h] * (dz * dz) + qr[0][h] * (dr * dr))));
+      out[1][h] = double(rho[h] * fsw[h] * fabs((qz[2][h] * (dz * dz) + qr[2][h] * (dr * dr))));
+      out[2][h] = double(rho[h] / (R(a.c.gam) * sqrt_t<R>(Tc[h])) * fabs((qz[1][h] * dz + qr[1][h] * dr)));
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) st_pair(a.Q + q * g.plane + o, out[q][0], out[q][1]);
+    return true;
   } else {
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
@@ -1243,7 +1455,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
 }
 
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(sens_threads(GEN))
+__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 4)
     sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mV,
                        const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
   extern __shared__ __align__(128) unsigned char smem_raw[];

@@ -18,6 +18,7 @@ struct StageMaps {
   const CUtensorMap* u0;
   const CUtensorMap* acc;
   const CUtensorMap* bt;  // tile box of k2 (prefetched into L2 for stage 3)
+  const CUtensorMap* tg;  // tile box of pv_target (prefetched into L2 where sponges or faces read it)
 };
 
 // Device view of one solver instance.

@@ -56,6 +56,12 @@ template <typename R>
 AXJ_HD RhsConst<R> rhs_const(double gam, double Re, double Pr) {
   return RhsConst<R>{R(gam), R(1.0 / gam), R(gam - 1.0), R(1.0 / Re), R(gam / (Re * Pr)), R(gam * (gam - 1.0) / Re)};
 }
+// The same factors from the values the host formed once per run (Consts), so that no
+// division is left in the per-point code.
+template <typename R>
+AXJ_HD RhsConst<R> rhs_const(const Consts& c) {
+  return RhsConst<R>{R(c.gam), R(c.inv_gam), R(c.gam - 1.0), R(c.inv_Re), R(c.gam_RePr), R(c.gg1_Re)};
+}
 
 // Inviscid part, already negated (ModRHS.f90:92-96 and :103-113).
 template <typename R>

@@ -132,7 +132,11 @@ typedef struct axj_params {
    * per SM); 0 is the library's default, AXJ_DEFAULT_STAGE_ROWS. The results agree to
    * rounding (separate compilations of the same per-point code). */
   int64_t stage_rows;
-  int64_t reserved[2];
+  /* Learned and held sensors: the RK stages of a judge step that run the plain sensor. 0 or
+   * 4: all four (the judge step is a plain step); 1: the first stage only, whose plain
+   * coefficients then serve the step's four stages, as the network's do between judges. */
+  int64_t judge_stages;
+  int64_t reserved[1];
 } axj_params;
 
 typedef struct axj_handle axj_handle;

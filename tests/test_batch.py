@@ -47,13 +47,21 @@ def _model(cases):
     return m
 
 
+MODES = {
+    "fp64": {},
+    "mixed_learned": dict(precision=1, sensor=1, judge_every=3),
+    # the plain sensor on the first stage of every second step only (judge_stages = 1)
+    "mixed_held_stage1": dict(precision=1, sensor=2, judge_every=2, judge_stages=1),
+}
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["fp64", "mixed_learned"])
+@pytest.mark.parametrize("mode", list(MODES))
 @pytest.mark.parametrize("order,rows", [(0, 16), (1, 16), (0, 8), (1, 8)])
 def test_batch_equals_individual_runs(mode, order, rows):
-    kw = {} if mode == "fp64" else dict(precision=1, sensor=1, judge_every=3)
+    kw = MODES[mode]
     cases = fixtures.batch_instances(3, seed=5, **SMALL, **kw)
-    model = _model(cases) if mode != "fp64" else None
+    model = _model(cases) if mode == "mixed_learned" else None
     single = _solvers(cases, model)
     batched = _solvers(cases, model)
     b = axj.AxjBatch(batched)
