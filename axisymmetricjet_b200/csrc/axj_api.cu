@@ -502,20 +502,26 @@ int launch_stage_kernels(axj_handle* h, int bin, int bout, int stage, int cm) {
 
 // The sensor chain of a stage input: the sensor tiles (quantities Q), then the fused
 // z filter / r filter / coefficient kernel, which leaves mu_eff, beta, kappa_eff in coef.
-int enqueue_sensor_chain(axj_handle* h, int bin) {
-  SensorArgs s = sensor_args(h, bin);
-  AXJ_CUDA(h, launch_sensor_tiles_only(s, h->side, h->stream));
+ZrArgs zr_args(axj_handle* h, int seg) {
   ZrArgs z;
+  std::memset(&z, 0, sizeof(z));
   z.g = grid_of(h);
   z.ramp = h->ramp;
   z.coef = h->coef;
   z.flags = h->flags;
+  z.seg = seg;
+  z.c = h->c;
+  return z;
+}
+
+int enqueue_sensor_chain(axj_handle* h, int bin) {
+  SensorArgs s = sensor_args(h, bin);
+  AXJ_CUDA(h, launch_sensor_tiles_only(s, h->side, h->stream));
   // about three CTAs per SM: segments of a multiple of ZRK_BZ positions, at least 64
   const int nrb = (h->Nr + ZRK_RB - 1) / ZRK_RB;
   const int nseg = std::max(1, (3 * 148) / nrb);
   const int seg = (int)((h->Nz + nseg - 1) / nseg);
-  z.seg = std::max(64, (seg + ZRK_BZ - 1) / ZRK_BZ * ZRK_BZ);
-  z.c = h->c;
+  ZrArgs z = zr_args(h, std::max(64, (seg + ZRK_BZ - 1) / ZRK_BZ * ZRK_BZ));
   ZrMaps m{&h->map_zrQ, &h->map_zrZc, &h->map_zrRc, &h->map_zrT[bin]};
   AXJ_CUDA(h, launch_zr(z, m, h->mixed, buf_f32(bin), h->stream));
   return AXJ_OK;
@@ -2271,7 +2277,7 @@ struct axj_batch {
   int64_t iteration = 0, judge_every = 50, njudges = 0;
   // device tables
   CUtensorMap* maps = nullptr;
-  StageArgs* stage_argv[2][5] = {};
+  StageArgs* stage_argv[3][5] = {};  // coefficient box CM_FILT, CM_LRN, CM_PRE
   SensorArgs* sens_argv[5] = {};
   FeatArgs* feat_argv = nullptr;
   InferArgs* infer_argv[2] = {};
@@ -2279,7 +2285,12 @@ struct axj_batch {
   DtArgs* dt_argv = nullptr;
   HarmArgs* harm_argv = nullptr;
   // host copies of instance 0's arguments (dispatch decisions, model pointer)
-  StageArgs a0_stage[2][5];
+  StageArgs a0_stage[3][5];
+  // the fused z/r filter of the plain sensor: per-instance arguments, (segment, row block,
+  // instance) work items
+  ZrArgs* zr_argv = nullptr;
+  int4* zr_items = nullptr;
+  int nzr_items = 0;
   SensorArgs a0_sens[5];
   InferArgs a0_infer[2];
   // host tile lists (i0, j0, instance) and their device copies
@@ -2453,9 +2464,13 @@ int batch_stage(axj_batch* b, int bin, int bout, int stage, bool judge) {
       }
     }
   } else if (b->sc) {
-    if (int rc = sensor(false)) return rc;
+    // the plain sensor: sensor tiles, then the fused z/r filter into the coefficient planes
+    BATCH_CUDA(b, launch_sensor_batch(b->sens_argv[bin], b->a0_sens[bin], sei, seg, b->maps, bin, nullptr, 0,
+                                      b->zthreads, b->zsmem, false, b->n, b->max_pts, b->side, b->stream));
+    BATCH_CUDA(b, launch_zr_batch(b->zr_argv, b->zr_items, b->nzr_items, b->maps, bin, b->mixed, buf_f32(bin),
+                                  b->stream));
   }
-  const int L = lrn ? 1 : 0;
+  const int L = lrn ? CM_LRN : (b->sc ? CM_PRE : CM_FILT);
   BATCH_CUDA(b, launch_stage_batch(b->stage_argv[L][stage], b->a0_stage[L][stage], sti, stg, b->maps, bin, b->side,
                                    b->stream, rows));
   return AXJ_OK;
@@ -2564,6 +2579,15 @@ int batch_build_tables(axj_batch* b) {
     m[bmap_starH(true)] = h->map_starLH;
     m[bmap_u0H] = h->map_u0H;
     m[bmap_accH] = h->map_accH;
+    if (h->c.shock_capturing) {
+      m[bmap_zrQ] = h->map_zrQ;
+      m[bmap_zrZc] = h->map_zrZc;
+      m[bmap_zrRc] = h->map_zrRc;
+      for (int bf = 0; bf < NBUF; ++bf) m[bmap_zrT(bf)] = h->map_zrT[bf < nb ? bf : 0];
+      m[bmap_coef(0)] = h->map_coef[0];
+      m[bmap_coef(1)] = h->map_coef[1];
+      m[bmap_coef(2)] = h->map_coefH;
+    }
     for (int bf = 0; bf < NBUF; ++bf) m[bmap_rho(bf)] = h->map_rho[bf < nb ? bf : 0];
   }
   {
@@ -2576,12 +2600,12 @@ int batch_build_tables(axj_batch* b) {
   // per-instance arguments
   int bufs[5];
   rk4_buffers(b->h[0], bufs);
-  for (int L = 0; L < 2; ++L)
+  for (int L = 0; L < 3; ++L)
     for (int st = 1; st <= 4; ++st) {
       std::vector<StageArgs> v(n);
       for (int k = 0; k < n; ++k) {
         v[k] = stage_args(b->h[k], bufs[st - 1], bufs[st], st);
-        v[k].learned = L;
+        v[k].learned = L;  // CM_FILT, CM_LRN, CM_PRE
       }
       b->a0_stage[L][st] = v[0];
       if (int rc = bupload(b, &b->stage_argv[L][st], v)) return rc;
@@ -2634,6 +2658,24 @@ int batch_build_tables(axj_batch* b) {
     b->zthreads = bs;
     b->zsmem = sm;
     if (int rc = bupload(b, &b->zrows, rows)) return rc;
+    // the fused z/r filter over all instances: one segment length for the batch, about
+    // three CTAs per SM in all (segments of a multiple of ZRK_BZ, at least 64 positions)
+    long long work = 0;
+    for (int k = 0; k < n; ++k) work += (long long)b->h[k]->Nz * ((b->h[k]->Nr + ZRK_RB - 1) / ZRK_RB);
+    long long seg = std::max<long long>(64, (work + 3 * b->nsm - 1) / (3 * b->nsm));
+    seg = (seg + ZRK_BZ - 1) / ZRK_BZ * ZRK_BZ;
+    std::vector<ZrArgs> zv(n);
+    std::vector<int4> items;
+    for (int k = 0; k < n; ++k) {
+      axj_handle* h = b->h[k];
+      zv[k] = zr_args(h, (int)seg);
+      const int nx = (int)((h->Nz + seg - 1) / seg), ny = (h->Nr + ZRK_RB - 1) / ZRK_RB;
+      for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) items.push_back(make_int4(x, y, k, 0));
+    }
+    b->nzr_items = (int)items.size();
+    if (int rc = bupload(b, &b->zr_argv, zv)) return rc;
+    if (int rc = bupload(b, &b->zr_items, items)) return rc;
   }
   // dt: the same number of blocks for every instance (the handles' partial arrays hold 592)
   b->dt_blocks = (int)std::min<long long>(592, std::max<long long>(1, b->max_pts / (DT_THREADS * 8)));

@@ -1874,20 +1874,19 @@ struct ZrSmem {
   static constexpr uint32_t tx = (uint32_t)(qbytes + zcbytes + tbytes + rcbytes);
 };
 
+// The fused z/r filter for the CTA (bx, by): z positions bx * a.seg .., rows by * ZRK_RB ..
 template <typename SIN, typename R>
-__global__ void __launch_bounds__(ZRK_THREADS, 3)
-    zr_kernel(const ZrArgs a, const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mZc,
-              const __grid_constant__ CUtensorMap mRc, const __grid_constant__ CUtensorMap mT) {
+__device__ __forceinline__ void zr_body(const ZrArgs& a, const CUtensorMap* pQ, const CUtensorMap* pZc,
+                                        const CUtensorMap* pRc, const CUtensorMap* pT, int bx, int by,
+                                        unsigned char* zrk_raw, uint64_t* bar) {
   using SM = ZrSmem<SIN>;
-  extern __shared__ __align__(128) unsigned char zrk_raw[];
-  __shared__ __align__(8) uint64_t bar[2];
   unsigned char* base = zrk_raw + ((1024u - (smem_u32(zrk_raw) & 1023u)) & 1023u);
   double* wt = reinterpret_cast<double*>(base + SM::oW);
   const int tid = threadIdx.x;
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long P = a.g.P, PL = a.g.plane;
-  const int zs = blockIdx.x * a.seg, ze = min(Nz, zs + a.seg);
-  const int j0 = blockIdx.y * ZRK_RB;
+  const int zs = bx * a.seg, ze = min(Nz, zs + a.seg);
+  const int j0 = by * ZRK_RB;
   const int bs = max(0, zs - ZRK_WARM) / ZRK_BZ;  // first block filtered (zs is a multiple of ZRK_BZ)
   const int be = (ze + ZRK_BZ - 1) / ZRK_BZ;       // blocks bs..be-1 are filtered, block be is loaded too
   // padded TG rows: row r's taps at offsets tg_w0(r) .. tg_w0(r) + tg_len(r) - 1 of
@@ -1915,10 +1914,10 @@ __global__ void __launch_bounds__(ZRK_THREADS, 3)
     const int sl = k & 1;
     unsigned char* q = base + SM::oQ + sl * SM::qslot;
     mbar_expect_tx(&bar[sl], SM::tx);
-    tma_load_3d(q, &mQ, ZRK_BZ * k, j0 - ZRK_HR, 0, &bar[sl]);
-    tma_load_2d(base + SM::oZc + sl * 1024, &mZc, ZRK_BZ * k, j0 - ZRK_HR, &bar[sl]);
-    tma_load_3d(base + SM::oT + sl * ((SM::tbytes + 127) / 128 * 128), &mT, ZRK_BZ * (k - 1), j0, 4, &bar[sl]);
-    tma_load_2d(base + SM::oRc + sl * 512, &mRc, ZRK_BZ * (k - 1), j0, &bar[sl]);
+    tma_load_3d(q, pQ, ZRK_BZ * k, j0 - ZRK_HR, 0, &bar[sl]);
+    tma_load_2d(base + SM::oZc + sl * 1024, pZc, ZRK_BZ * k, j0 - ZRK_HR, &bar[sl]);
+    tma_load_3d(base + SM::oT + sl * ((SM::tbytes + 127) / 128 * 128), pT, ZRK_BZ * (k - 1), j0, 4, &bar[sl]);
+    tma_load_2d(base + SM::oRc + sl * 512, pRc, ZRK_BZ * (k - 1), j0, &bar[sl]);
   };
   if (tid == 0) issue(bs);
 
@@ -2075,10 +2074,54 @@ __global__ void __launch_bounds__(ZRK_THREADS, 3)
 }
 
 template <typename SIN, typename R>
+__global__ void __launch_bounds__(ZRK_THREADS, 3)
+    zr_kernel(const ZrArgs a, const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mZc,
+              const __grid_constant__ CUtensorMap mRc, const __grid_constant__ CUtensorMap mT) {
+  extern __shared__ __align__(128) unsigned char zrk_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  zr_body<SIN, R>(a, &mQ, &mZc, &mRc, &mT, blockIdx.x, blockIdx.y, zrk_raw, bar);
+}
+
+// Batched: one CTA per entry (segment, row block, instance) of a table over all instances;
+// each instance's arguments (staged in shared memory) and maps come from device tables.
+template <typename SIN, typename R>
+__global__ void __launch_bounds__(ZRK_THREADS, 3)
+    zr_kernel_batch(const ZrArgs* __restrict__ argv, const int4* __restrict__ items, const CUtensorMap* __restrict__ mapv,
+                    int nmaps, int4 kmaps) {
+  extern __shared__ __align__(128) unsigned char zrk_raw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(16) ZrArgs sa;
+  const int4 it = items[blockIdx.x];
+  for (int k = threadIdx.x; k < (int)(sizeof(ZrArgs) / 8); k += blockDim.x)
+    reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + it.z)[k];
+  __syncthreads();
+  const CUtensorMap* m = mapv + (size_t)it.z * nmaps;
+  zr_body<SIN, R>(sa, m + kmaps.x, m + kmaps.y, m + kmaps.z, m + kmaps.w, it.x, it.y, zrk_raw, bar);
+}
+
+template <typename SIN, typename R>
 static cudaError_t launch_zr_t(const ZrArgs& a, const ZrMaps& m, cudaStream_t s) {
   const dim3 grid((a.g.Nz + a.seg - 1) / a.seg, (a.g.Nr + ZRK_RB - 1) / ZRK_RB);
   zr_kernel<SIN, R><<<grid, ZRK_THREADS, ZrSmem<SIN>::bytes, s>>>(a, *m.q, *m.zc, *m.rc, *m.t);
   return cudaGetLastError();
+}
+
+static_assert(sizeof(ZrArgs) % 8 == 0, "ZrArgs is staged in 8-byte words");
+
+template <typename SIN, typename R>
+static cudaError_t launch_zr_batch_t(const ZrArgs* argv, const int4* items, int nitems, const CUtensorMap* mapv,
+                                     int kin, cudaStream_t s) {
+  const int4 k = make_int4(bmap_zrQ, bmap_zrZc, bmap_zrRc, bmap_zrT(kin));
+  zr_kernel_batch<SIN, R><<<nitems, ZRK_THREADS, ZrSmem<SIN>::bytes, s>>>(argv, items, mapv, NM_BATCH, k);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zr_batch(const ZrArgs* argv, const int4* items, int nitems, const CUtensorMap* mapv, int kin,
+                            bool mixed, bool in_f32, cudaStream_t s) {
+  if (nitems <= 0) return cudaSuccess;
+  if (!mixed) return launch_zr_batch_t<double, double>(argv, items, nitems, mapv, kin, s);
+  if (!in_f32) return launch_zr_batch_t<double, float>(argv, items, nitems, mapv, kin, s);
+  return launch_zr_batch_t<float, float>(argv, items, nitems, mapv, kin, s);
 }
 
 cudaError_t launch_zr(const ZrArgs& a, const ZrMaps& m, bool mixed, bool in_f32, cudaStream_t s) {
@@ -2226,6 +2269,9 @@ static cudaError_t stage_batch_attr() {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)StageSmem<H, SIN, R, CM_FILT, TRT>::bytes(GEN));
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, CM_PRE, TRT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)StageSmem<H, SIN, R, CM_PRE, TRT>::bytes(GEN));
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(stage_kernel_batch<H, GEN, SIN, R, CM_LRN, TRT>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)StageSmem<H, SIN, R, CM_LRN, TRT>::bytes(GEN));
@@ -2272,6 +2318,15 @@ cudaError_t init_kernel_attributes() {
   e = cudaFuncSetAttribute(zr_kernel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)ZrSmem<double>::bytes);
   if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(zr_kernel_batch<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ZrSmem<double>::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(zr_kernel_batch<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ZrSmem<double>::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(zr_kernel_batch<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ZrSmem<float>::bytes);
+  if (e == cudaSuccess)
     e = cudaFuncSetAttribute(zr_kernel<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)ZrSmem<double>::bytes);
   if (e == cudaSuccess)
@@ -2288,46 +2343,53 @@ cudaError_t init_kernel_attributes() {
 size_t zrows_smem(int Nz, long long P, int bs) { return zr_smem_bytes(Nz, P, bs); }
 int zrows_threads(int Nz) { return zr_threads(Nz); }
 
-template <int H, bool GEN, typename SIN, typename R, bool LRN, int TRT = TR>
+template <int H, bool GEN, typename SIN, typename R, int CM, int TRT = TR>
 static cudaError_t launch_stage_batch_t(const StageArgs* argv, const BatchTiles& t, const CUtensorMap* mapv, int kin,
                                         cudaStream_t s) {
   if (t.ntiles <= 0) return cudaSuccess;
   const int cls = GEN ? 1 : 0;
-  const int4 k = TRT == TR ? make_int4(bmap_state(kin, cls), bmap_star(cls, LRN), 14, 15)
-                           : make_int4(bmap_stateH(kin), bmap_starH(LRN), bmap_u0H, bmap_accH);
-  constexpr int CM = LRN ? CM_LRN : CM_FILT;
+  int4 k;
+  if (TRT == TR) {
+    const int star = CM == CM_PRE ? bmap_coef(cls) : bmap_star(cls, CM == CM_LRN);
+    k = make_int4(bmap_state(kin, cls), star, 14, 15);
+  } else {
+    const int star = CM == CM_PRE ? bmap_coef(2) : bmap_starH(CM == CM_LRN);
+    k = make_int4(bmap_stateH(kin), star, bmap_u0H, bmap_accH);
+  }
   const size_t sm = StageSmem<H, SIN, R, CM, TRT>::bytes(GEN);
   stage_kernel_batch<H, GEN, SIN, R, CM, TRT>
       <<<t.grid, stage_threads(TRT), sm, s>>>(argv, t.tiles, t.ntiles, mapv, NM_BATCH, k);
   return cudaGetLastError();
 }
 
-template <typename SIN, typename R, bool LRN>
+template <typename SIN, typename R, int CM>
 static cudaError_t launch_stage_batch_pair(const StageArgs* argv, const BatchTiles& tint, const BatchTiles& tgen,
                                            const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s,
                                            int int_rows) {
   cudaError_t e = fork(side, s);
   if (e != cudaSuccess) return e;
-  e = launch_stage_batch_t<H_GEN, true, SIN, R, LRN>(argv, tgen, mapv, kin, side.stream ? side.stream : s);
+  e = launch_stage_batch_t<H_GEN, true, SIN, R, CM>(argv, tgen, mapv, kin, side.stream ? side.stream : s);
   if (e != cudaSuccess) return e;
-  e = int_rows == TR / 2 ? launch_stage_batch_t<H_INT, false, SIN, R, LRN, TR / 2>(argv, tint, mapv, kin, s)
-                         : launch_stage_batch_t<H_INT, false, SIN, R, LRN>(argv, tint, mapv, kin, s);
+  e = int_rows == TR / 2 ? launch_stage_batch_t<H_INT, false, SIN, R, CM, TR / 2>(argv, tint, mapv, kin, s)
+                         : launch_stage_batch_t<H_INT, false, SIN, R, CM>(argv, tint, mapv, kin, s);
   if (e != cudaSuccess) return e;
   return join(side, s);
 }
 
+template <typename SIN, typename R>
+static cudaError_t launch_stage_batch_cm(const StageArgs* argv, int cm, const BatchTiles& tint, const BatchTiles& tgen,
+                                         const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s,
+                                         int int_rows) {
+  if (cm == CM_LRN) return launch_stage_batch_pair<SIN, R, CM_LRN>(argv, tint, tgen, mapv, kin, side, s, int_rows);
+  if (cm == CM_PRE) return launch_stage_batch_pair<SIN, R, CM_PRE>(argv, tint, tgen, mapv, kin, side, s, int_rows);
+  return launch_stage_batch_pair<SIN, R, CM_FILT>(argv, tint, tgen, mapv, kin, side, s, int_rows);
+}
+
 cudaError_t launch_stage_batch(const StageArgs* argv, const StageArgs& a0, const BatchTiles& tint, const BatchTiles& tgen,
                                const CUtensorMap* mapv, int kin, const SideStream& side, cudaStream_t s, int int_rows) {
-  if (!a0.mixed) {
-    if (a0.learned) return launch_stage_batch_pair<double, double, true>(argv, tint, tgen, mapv, kin, side, s, int_rows);
-    return launch_stage_batch_pair<double, double, false>(argv, tint, tgen, mapv, kin, side, s, int_rows);
-  }
-  if (!a0.in_f32) {
-    if (a0.learned) return launch_stage_batch_pair<double, float, true>(argv, tint, tgen, mapv, kin, side, s, int_rows);
-    return launch_stage_batch_pair<double, float, false>(argv, tint, tgen, mapv, kin, side, s, int_rows);
-  }
-  if (a0.learned) return launch_stage_batch_pair<float, float, true>(argv, tint, tgen, mapv, kin, side, s, int_rows);
-  return launch_stage_batch_pair<float, float, false>(argv, tint, tgen, mapv, kin, side, s, int_rows);
+  if (!a0.mixed) return launch_stage_batch_cm<double, double>(argv, a0.learned, tint, tgen, mapv, kin, side, s, int_rows);
+  if (!a0.in_f32) return launch_stage_batch_cm<double, float>(argv, a0.learned, tint, tgen, mapv, kin, side, s, int_rows);
+  return launch_stage_batch_cm<float, float>(argv, a0.learned, tint, tgen, mapv, kin, side, s, int_rows);
 }
 
 template <typename SIN, typename R>

@@ -187,6 +187,10 @@ struct ZrMaps {
   const CUtensorMap* t;
 };
 cudaError_t launch_zr(const ZrArgs& a, const ZrMaps& m, bool mixed, bool in_f32, cudaStream_t s);
+// Batched fused z/r filter: items (segment, row block, instance, 0), per-instance arguments
+// and the maps of the batch table (kin = stage-input buffer id).
+cudaError_t launch_zr_batch(const ZrArgs* argv, const int4* items, int nitems, const CUtensorMap* mapv, int kin,
+                            bool mixed, bool in_f32, cudaStream_t s);
 
 // Unit entry points (one operator on one field, host-facing).
 cudaError_t launch_deriv(const Grid& g, const uint32_t* desc, const double* var, const double* first,
@@ -211,7 +215,10 @@ constexpr int DT_THREADS = 256;
 //   density tile box of buffer b:                  36 + b            (36..40)
 //   interior half tiles (TR / 2 rows): state box of buffer b 41 + b (41..45), z-filtered
 //   coefficient box 46, final-coefficient box 47, pv_old and running-sum tile boxes 48, 49
-constexpr int NM_BATCH = 50;
+//   fused z/r filter: Q blocks 50, z and r code blocks 51, 52, temperature blocks of
+//   buffer b 53 + b (53..57); its coefficient planes as boxes of the interior, general and
+//   half tiles 58, 59, 60
+constexpr int NM_BATCH = 61;
 inline int bmap_state(int b, int cls) { return b * 2 + cls; }
 inline int bmap_star(int cls, bool lrn) { return (lrn ? 12 : 10) + cls; }
 inline int bmap_sens(int b, int cls) { return 16 + b * 2 + cls; }
@@ -220,6 +227,9 @@ inline int bmap_rho(int b) { return 36 + b; }
 inline int bmap_stateH(int b) { return 41 + b; }
 inline int bmap_starH(bool lrn) { return lrn ? 47 : 46; }
 constexpr int bmap_u0H = 48, bmap_accH = 49;
+constexpr int bmap_zrQ = 50, bmap_zrZc = 51, bmap_zrRc = 52;
+inline int bmap_zrT(int b) { return 53 + b; }
+inline int bmap_coef(int cls) { return 58 + cls; }  // cls 0 interior, 1 general, 2 half tiles
 
 struct BatchTiles {
   const int4* tiles;  // (i0, j0, instance, 0)

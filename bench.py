@@ -361,18 +361,27 @@ def main():
 def time_batched(args, rank):
     """The batched form of uneven jets: 64 instances (Nz in [256, 2048], Nr in [96, 384],
     Mach in [0.9, 1.5], Re in [1000, 5000], harmonic inflow forcing) in one persistent launch
-    per kernel, mixed precision + learned sensor, autotuned, graph-captured steps; against the
-    same instances one after another on the plain FP64 path, with each instance's relative
-    L2 error of rho and p against its FP64 run after the same number of steps. Every rank
-    runs its own batch (replicas); the figures are rank 0's."""
+    per kernel, mixed precision, autotuned (tile order, stage tile shape, CTAs per SM),
+    graph-captured steps; against the same instances one after another on the plain FP64
+    path, with each instance's relative L2 error of rho and p against its FP64 run after the
+    same number of steps. Forms: the learned sensor judged every 50 steps (the plain sensor
+    on all four stages of a judge step), the learned and the held sensor judged on the first
+    stage of every second step, and the plain sensor on every stage. Every rank runs its own
+    batch (replicas); the figures are rank 0's."""
     from axisymmetricjet_b200 import batch_eval
-    rep = batch_eval.evaluate(n=args.batch_instances, steps=args.batch_steps, seed=2024 + rank,
+    forms = [dict(name="learned_judge50", precision=1, sensor=1, judge_every=50, judge_stages=4),
+             dict(name="learned_judge2_stage1", precision=1, sensor=1, judge_every=2, judge_stages=1),
+             dict(name="held_judge2_stage1", precision=1, sensor=2, judge_every=2, judge_stages=1),
+             dict(name="plain", precision=1, sensor=0, judge_every=50, judge_stages=4)]
+    names = [f.pop("name") for f in forms]
+    rep = batch_eval.evaluate(n=args.batch_instances, steps=args.batch_steps, seed=2024 + rank, forms=forms,
                               log=lambda m: None)
     out = {"instances": rep["instances"], "points": rep["points"], "steps": rep["steps"],
-           "timed_steps": rep["steps"] - 3, "tuning": rep["tuning"],
-           "value": rep["batched"]["value"], "unit": UNIT, "ms_per_step": rep["batched"]["ms_per_step"],
-           "sequential_fp64_value": rep["sequential_fp64"]["value"], "speedup_vs_sequential_fp64": rep.get("speedup"),
-           "rel_l2_vs_fp64": rep.get("rel_l2_vs_fp64"), "judge": rep.get("judge")}
+           "timed_steps": rep["steps"] - 3, "unit": UNIT,
+           "sequential_fp64_value": rep["sequential_fp64"]["value"], "forms": {}}
+    for name, r in zip(names, rep["forms"]):
+        out["forms"][name] = {k: r.get(k) for k in ("precision", "sensor", "judge_every", "judge_stages", "tuning",
+                                                     "value", "ms_per_step", "speedup", "rel_l2_vs_fp64", "judge")}
     return out
 
 

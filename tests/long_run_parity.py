@@ -13,13 +13,16 @@ Two modes:
               (ComputeTimeStep, ModInputOutput.f90:389-438) and runs RK4
               (ModRungeKutta.f90:5-171). Writes the per-field relative L2 per checkpoint
               and, with --calibration, the tolerance: TOL_FACTOR x the calibrated spread
-              at the same step, or the 1e-12 per-step parity bound if that is larger
+              at the same step, or the FP64 unit roundoff (2.2e-16) if that is larger
               (the first steps, where the spread is below it). Exits 1 if a field is out
               of tolerance.
+  verdict     applies the same tolerance to a recorded check (--check) and rewrites it.
 
     python tests/long_run_parity.py calibrate --steps 1000 --out tests/golden/long_run_calibration.json
     python tests/long_run_parity.py check --steps 1000 --calibration tests/golden/long_run_calibration.json \\
         --out long_run_check.json
+    python tests/long_run_parity.py verdict --check long_run_check.json \\
+        --calibration tests/golden/long_run_calibration.json --out long_run_check.json
 
 Fields: rho, V_r, V_z, T (the north_star's four), relative L2 = ||a - b|| / ||b|| over the
 grid; V_r is taken relative to the norm of V_z (V_r's own norm is the perturbation's).
@@ -40,7 +43,9 @@ for p in (ROOT, os.path.join(ROOT, "oracle")):
 
 FIELDS = {"rho": 0, "V_r": 1, "V_z": 3, "T": 4}
 TOL_FACTOR = 10.0
-FLOOR = 1e-12  # the per-step parity bound, as a floor for the first steps
+# a relative L2 below the FP64 unit roundoff is below what a norm of the field resolves:
+# the floor for the first steps, where the spread is smaller still
+FLOOR = 2.2e-16
 
 
 def rel_l2(a, b):
@@ -81,7 +86,8 @@ def make_pair(kind, case_name):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", choices=["calibrate", "check"])
+    ap.add_argument("mode", choices=["calibrate", "check", "verdict"])
+    ap.add_argument("--check", default=None)
     ap.add_argument("--case", default="jet4400x640")
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--every", type=int, default=100)
@@ -89,29 +95,32 @@ def main(argv=None):
     ap.add_argument("--out", required=True)
     args = ap.parse_args(argv)
 
-    c, ora, other = make_pair(args.mode, args.case)
-    pts = checkpoints(args.steps, args.every)
-    rows = []
-    max_dt_rel = 0.0
-    t0 = time.time()
-    done = 0
-    for p in pts:
-        for _ in range(p - done):
-            d_o = ora.compute_time_step()
-            d_b = other.compute_time_step()
-            max_dt_rel = max(max_dt_rel, abs(d_b - d_o) / abs(d_o))
-            ora.rk4(d_o)
-            other.rk4(d_b)
-        done = p
-        err = rel_l2(other.get_state(), ora.get_state())
-        rows.append(dict(step=p, time=ora.get_time()[1], l2=err, max_dt_rel=max_dt_rel))
-        print(json.dumps(rows[-1]), f"{time.time() - t0:.0f}s", flush=True)
-
-    out = dict(mode=args.mode, case=args.case, Nz=c["Nz"], Nr=c["Nr"], steps=args.steps,
-               compared=("oracle vs oracle built with FMA contraction" if args.mode == "calibrate"
-                         else "device FP64 path vs oracle"), checkpoints=rows, seconds=time.time() - t0)
+    if args.mode == "verdict":
+        out = json.load(open(args.check))
+        rows = out["checkpoints"]
+    else:
+        c, ora, other = make_pair(args.mode, args.case)
+        pts = checkpoints(args.steps, args.every)
+        rows = []
+        max_dt_rel = 0.0
+        t0 = time.time()
+        done = 0
+        for p in pts:
+            for _ in range(p - done):
+                d_o = ora.compute_time_step()
+                d_b = other.compute_time_step()
+                max_dt_rel = max(max_dt_rel, abs(d_b - d_o) / abs(d_o))
+                ora.rk4(d_o)
+                other.rk4(d_b)
+            done = p
+            err = rel_l2(other.get_state(), ora.get_state())
+            rows.append(dict(step=p, time=ora.get_time()[1], l2=err, max_dt_rel=max_dt_rel))
+            print(json.dumps(rows[-1]), f"{time.time() - t0:.0f}s", flush=True)
+        out = dict(mode=args.mode, case=args.case, Nz=c["Nz"], Nr=c["Nr"], steps=args.steps,
+                   compared=("oracle vs oracle built with FMA contraction" if args.mode == "calibrate"
+                             else "device FP64 path vs oracle"), checkpoints=rows, seconds=time.time() - t0)
     rc = 0
-    if args.mode == "check" and args.calibration:
+    if args.mode in ("check", "verdict") and args.calibration:
         cal = json.load(open(args.calibration))
         spread = {r["step"]: r["l2"] for r in cal["checkpoints"]}
         verdict = []
@@ -120,7 +129,8 @@ def main(argv=None):
                 continue
             tol = {k: max(TOL_FACTOR * spread[r["step"]][k], FLOOR) for k in FIELDS}
             ok = all(r["l2"][k] <= tol[k] for k in FIELDS)
-            verdict.append(dict(step=r["step"], tol=tol, ok=ok))
+            verdict.append(dict(step=r["step"], tol=tol, ok=ok,
+                                margin=min(tol[k] / max(r["l2"][k], 1e-300) for k in FIELDS)))
             rc |= 0 if ok else 1
         out["tolerance_rule"] = (f"per field: max({TOL_FACTOR:g} x the calibrated spread at the step, "
                                  f"{FLOOR:g})")
