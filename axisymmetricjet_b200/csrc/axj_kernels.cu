@@ -1435,13 +1435,15 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   }
   }
 
-  // ---- quantities to be filtered (ComputeTobeFilteredQuantities :204-215)
+  // ---- quantities to be filtered (ComputeTobeFilteredQuantities :204-215); the interior
+  // tiles returned above
+  if constexpr (GEN) {
 #pragma unroll
   for (int q = 0; q < PPT; ++q) {
     const int pidx = ppoint(tid, q);
     const int r = pidx / TZ, c = pidx - r * TZ;
     const int i = i0 + c, j = j0 + r;
-    if (GEN && (!inside(i, j) || r >= nrow)) continue;
+    if (!inside(i, j) || r >= nrow) continue;
     const long long o = (long long)j * g.P + i;
     const R dz = R(sDzv[c]), dr = R(sDrv[r]);
     const R rho = R(sRho[r * TZ + c]);
@@ -1450,6 +1452,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     a.Q[o] = double(rho * fabs((d4z[0][q] * (dz * dz) + d4r[0][q] * (dr * dr))));
     a.Q[g.plane + o] = double(rho * fsw * fabs((d4z[2][q] * (dz * dz) + d4r[2][q] * (dr * dr))));
     a.Q[2 * g.plane + o] = double(rho / (R(a.c.gam) * sqrt_t<R>(T)) * fabs((d4z[1][q] * dz + d4r[1][q] * dr)));
+  }
   }
   return true;
 }

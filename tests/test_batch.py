@@ -138,13 +138,15 @@ def test_batch_with_many_tiles_per_cta():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("sensor", [1, 2])
+@pytest.mark.parametrize("sensor", [0, 1, 2])
 def test_batch_accuracy_gate_500_steps(sensor):
-    """The batched mixed-precision form with the learned sensor (1, the committed model) or
-    the held schedule without the network (2), judged by the plain sensor on the first stage
-    of every second step: 8 uneven instances, 500 steps, rho and p within 1e-5 relative L2 of
-    each instance's own plain FP64 run (the gate the batched form is held to). The speed-up
-    over the same instances run one after another on the plain FP64 path is printed."""
+    """The batched mixed-precision form with the plain sensor on every stage (0), the learned
+    sensor (1, the committed model) or the held schedule without the network (2), the last
+    two judged by the plain sensor on the first stage of every second step: 8 uneven
+    instances, 500 steps, rho and p within 1e-5 relative L2 of each instance's own plain FP64
+    run (the gate the batched form is held to). The speed-up over the same instances run one
+    after another on the plain FP64 path is printed. (On the 64-instance batch the two judged
+    forms exceed the gate in the instances whose shocks move; the plain form stays far below.)"""
     from axisymmetricjet_b200 import batch_eval
     rep = batch_eval.evaluate(n=8, steps=500, seed=2024, forms=[dict(precision=1, sensor=sensor, judge_every=2,
                                                                      judge_stages=1)], log=lambda m: None)
