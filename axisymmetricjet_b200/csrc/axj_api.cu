@@ -2876,7 +2876,8 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
           axj_batch_default_tuning(&t);
           t.tile_order = o;
           t.stage_rows = rows;
-          t.stage_ctas_per_sm = rows == TR ? sc : 2 * sc;
+          // half tiles: two or four CTAs per SM (FP64), three or six (FP32 stencils)
+          t.stage_ctas_per_sm = rows == TR ? sc : (b->mixed ? 3 : 2) * sc;
           t.sensor_ctas_per_sm = se;
           if (!b->sc && se > 1) continue;
           cands.push_back(t);

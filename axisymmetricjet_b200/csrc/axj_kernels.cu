@@ -223,8 +223,15 @@ __host__ __device__ constexpr int hz_t(int h, int esize) { return (h + 16 / esiz
 // HZ follows the arithmetic type: the mixed path rounds to 4 elements in every stage
 // (valid for its double stage-1 input too), so one coefficient-box map serves all stages.
 // CM, the content of the coefficient box (CM_FILT, CM_LRN, CM_PRE: axj_kernels.cuh).
+// Half tiles with FP32 stencils (the mixed path) read pv_old and the running sum from
+// global memory (L2-prefetched at the tile start) instead of staging them: that leaves them
+// about 25 KB of shared memory, and at 80 registers six CTAs share an SM. The FP64 half
+// tiles stage them and run four CTAs per SM (at 80 registers their per-point code spills).
+template <typename R, int TRT>
+__host__ __device__ constexpr bool rk_global() { return TRT < TR && sizeof(R) == 4; }
+
 // TRT: rows of the tile (TR; interior tiles can also run as two halves of TR / 2 rows,
-// which need about half the shared memory and so let four CTAs share an SM).
+// which need about half the shared memory and so let four to six CTAs share an SM).
 template <int H, typename SIN, typename R, int CM = CM_FILT, int TRT = TR>
 struct StageSmem {
   static constexpr int HZ = hz_t(H, (int)sizeof(R));
@@ -250,7 +257,7 @@ struct StageSmem {
   static constexpr size_t oP0 = align128(oMu0 + (CM == CM_PRE ? 0 : sizeof(double) * NTP));
   static constexpr size_t oPA = align128(oP0 + sizeof(double) * 5 * NTP);
   __host__ __device__ static constexpr size_t oDz(bool gen) {
-    return gen ? oP0 : align128(oPA + sizeof(double) * 5 * NTP);
+    return (gen || rk_global<R, TRT>()) ? oP0 : align128(oPA + sizeof(double) * 5 * NTP);
   }
   __host__ __device__ static constexpr size_t oDesc(bool gen) {
     return align128(oDz(gen) + sizeof(double) * 2 * RR * TZ);
@@ -314,8 +321,10 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long P = a.g.P, PL = a.g.plane;
   const bool sc = a.c.shock_capturing != 0;
-  const bool needU0 = !GEN && (a.stage == 2 || a.stage == 3);
-  const bool needA = !GEN && (a.stage == 3 || a.stage == 4);
+  // RK operands from global memory (general tiles, FP32 half tiles) or staged by TMA
+  constexpr bool RKG = GEN || rk_global<R, TRT>();
+  const bool needU0 = !RKG && (a.stage == 2 || a.stage == 3);
+  const bool needA = !RKG && (a.stage == 3 || a.stage == 4);
   // mu = T**0.666 (AssignValues) on the cross of the region (CM_PRE: the coefficient box
   // already holds mu_eff, beta and kappa_eff). With shock capturing the
   // coefficient box holds the z-filtered quantities; the r filter PerformTGfilter(q, 2,
@@ -557,15 +566,15 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
         un[f] = add_rn(u0, mul_rn(0.5, k));
         a.A[o] = add_rn(u0, mul_rn(c6, k));
       } else if (a.stage == 2) {
-        const double u0 = GEN ? __ldg(a.U0 + o) : sP0[f * NTP + tp];
+        const double u0 = RKG ? __ldg(a.U0 + o) : sP0[f * NTP + tp];
         un[f] = add_rn(u0, mul_rn(0.5, k));
         a.B[o] = k;
       } else if (a.stage == 3) {
-        const double u0 = GEN ? __ldg(a.U0 + o) : sP0[f * NTP + tp];
+        const double u0 = RKG ? __ldg(a.U0 + o) : sP0[f * NTP + tp];
         un[f] = add_rn(u0, k);
-        a.A[o] = add_rn(GEN ? a.A[o] : sPA[f * NTP + tp], mul_rn(c3, add_rn(__ldg(a.B + o), k)));
+        a.A[o] = add_rn(RKG ? a.A[o] : sPA[f * NTP + tp], mul_rn(c3, add_rn(__ldg(a.B + o), k)));
       } else {
-        un[f] = blank ? pv[f] : add_rn(GEN ? a.A[o] : sPA[f * NTP + tp], mul_rn(c6, k));
+        un[f] = blank ? pv[f] : add_rn(RKG ? a.A[o] : sPA[f * NTP + tp], mul_rn(c6, k));
       }
     }
     if (j1) {
@@ -623,8 +632,10 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
   }
   // pv_old is needed as a tile in stages 2 and 3 (stage 1 reads it from the state box),
   // the running sum A in stages 3 and 4; interior tiles stage them by TMA
-  const bool needU0 = !GEN && (a.stage == 2 || a.stage == 3);
-  const bool needA = !GEN && (a.stage == 3 || a.stage == 4);
+  // RK operands from global memory (general tiles, FP32 half tiles) or staged by TMA
+  constexpr bool RKG = GEN || rk_global<R, TRT>();
+  const bool needU0 = !RKG && (a.stage == 2 || a.stage == 3);
+  const bool needA = !RKG && (a.stage == 3 || a.stage == 4);
 
   // ---- phase 1: one thread issues the TMA loads; the RK operands complete on the
   // second barrier while phases 1-2 run. The barriers are initialised once per CTA by the
@@ -652,8 +663,8 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
                        __ldg(a.rc + min(j0 + TRT - 1, Nr - 1)) >= a.c.sponge_start_top;
       if (tgt) tma_prefetch_3d(mTg, i0, j0, 0);
     }
-    if (GEN && (a.stage == 2 || a.stage == 3)) tma_prefetch_3d(mU0, i0, j0, 0);
-    if (GEN && (a.stage == 3 || a.stage == 4)) tma_prefetch_3d(mAcc, i0, j0, 0);
+    if (RKG && (a.stage == 2 || a.stage == 3)) tma_prefetch_3d(mU0, i0, j0, 0);
+    if (RKG && (a.stage == 3 || a.stage == 4)) tma_prefetch_3d(mAcc, i0, j0, 0);
   }
   if (GEN) {
     for (int idx = tid; idx < NPT; idx += NT) {
@@ -692,14 +703,16 @@ __device__ __forceinline__ bool stage_body(const StageArgs& a, int i0, int j0, c
 
 
 // Threads of a stage CTA: 256 for tiles of TR rows (two CTAs per SM), 128 for the half
-// tiles of TR / 2 rows (four CTAs per SM: while one waits for its boxes, three compute).
+// tiles of TR / 2 rows (four CTAs per SM, six with FP32 stencils: while one waits for its
+// boxes, the others compute).
 __host__ __device__ constexpr int stage_threads(int trt) { return trt == TR ? STAGE_THREADS : STAGE_THREADS / 2; }
-__host__ __device__ constexpr int stage_ctas(int trt) { return trt == TR ? 2 : 4; }
+template <typename R, int TRT>
+__host__ __device__ constexpr int stage_ctas() { return TRT == TR ? 2 : (rk_global<R, TRT>() ? 6 : 4); }
 
 // One tile per CTA; with TRT < TR (interior tiles only) CTA k takes rows (k % NH) * TRT ..
 // of tile k / NH, NH = TR / TRT.
 template <int H, bool GEN, typename SIN, typename R, int CM, int TRT = TR>
-__global__ void __launch_bounds__(stage_threads(TRT), stage_ctas(TRT))
+__global__ void __launch_bounds__(stage_threads(TRT), (stage_ctas<R, TRT>()))
     stage_kernel(const StageArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mState,
                  const __grid_constant__ CUtensorMap mQ, const __grid_constant__ CUtensorMap mU0,
                  const __grid_constant__ CUtensorMap mAcc, const __grid_constant__ CUtensorMap mB,
@@ -725,7 +738,7 @@ __global__ void __launch_bounds__(stage_threads(TRT), stage_ctas(TRT))
 // (the arguments are staged in shared memory per tile). With TRT < TR the table holds the
 // half tiles of the interior class (their own origins) and the maps their boxes.
 template <int H, bool GEN, typename SIN, typename R, int CM, int TRT = TR>
-__global__ void __launch_bounds__(stage_threads(TRT), TRT == TR ? 1 : stage_ctas(TRT))
+__global__ void __launch_bounds__(stage_threads(TRT), TRT == TR ? 1 : (stage_ctas<R, TRT>()))
     stage_kernel_batch(const StageArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
                        const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
