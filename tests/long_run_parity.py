@@ -24,7 +24,7 @@ Two modes:
     python tests/long_run_parity.py verdict --check long_run_check.json \\
         --calibration tests/golden/long_run_calibration.json --out long_run_check.json
 
-Fields: rho, V_r, V_z, T (the north_star's four), relative L2 = ||a - b|| / ||b|| over the
+Fields: rho, V_r, V_z, T, relative L2 = ||a - b|| / ||b|| over the
 grid; V_r is taken relative to the norm of V_z (V_r's own norm is the perturbation's).
 The oracle is test infrastructure: only this script runs it.
 """

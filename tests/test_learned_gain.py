@@ -12,8 +12,8 @@ same steps from the same state with the same dt sequence:
            its values kept wherever the prediction disagrees by more than the threshold.
 
 The test asserts the network's gain over the plain sensor: the learned run is cheaper per
-step and stays within the north_star's 1e-5 relative L2 of the plain run in rho and p
-after 200 steps (cost at a bounded accuracy loss). Against the held schedule it records,
+step and stays within 1e-5 relative L2 of the plain run in rho and p (the accuracy gate)
+after 200 steps: cost at a bounded accuracy loss. Against the held schedule it records,
 without asserting a direction, the accuracy and the cost (the network costs time on every
 step and is judged on the same schedule), and the fraction of judged outputs that fell
 back. The numbers are printed for the record.
