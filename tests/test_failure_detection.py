@@ -99,3 +99,36 @@ def test_wait_timeout_is_reported_and_the_context_stays_usable(name):
         assert s.compute_time_step() == dt
         s.rk4(dt)
         np.testing.assert_array_equal(s.get_state(), want)
+
+
+def test_batch_wait_timeout_is_reported_and_the_batch_recovers():
+    """The batched kernels share the bounded waits: with the limit at zero a batch step
+    reports AXJ_ERR_TIMEOUT; with the default limit and the states set again, the batch steps
+    as the same instances do one by one (physical dt, FP64)."""
+    cases = fixtures.batch_instances(3, seed=5, nz_range=(256, 384), nr_range=(96, 128), dt_mode=1)
+    singles, batched = [], []
+    for c in cases:
+        for lst in (singles, batched):
+            s = solver(c)
+            s.set_state(c["pv"], c["target"])
+            lst.append(s)
+    b = axj.AxjBatch(batched)
+    batched[0].set_wait_limit(0)
+    try:
+        with pytest.raises(axj.AxjError) as e:
+            b.run(1)
+        assert e.value.code == TIMEOUT
+    finally:
+        batched[0].set_wait_limit(-1)
+    for s, c in zip(batched, cases):
+        s.set_state(c["pv"], c["target"])
+    b.run(2)
+    for s in singles:
+        s.run(2)
+    for s, t in zip(singles, batched):
+        a, r = t.get_state(), s.get_state()
+        errs = [np.abs(a[f] - r[f]).max() / max(np.abs(r[f]).max(), 1e-300) for f in range(5)]
+        assert max(errs) <= 1e-12, errs
+    b.close()
+    for s in singles + batched:
+        s.close()
