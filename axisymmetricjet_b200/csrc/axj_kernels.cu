@@ -885,64 +885,28 @@ __device__ __forceinline__ void dt_body(const DtArgs& a, int blk, int nblk) {
   const bool phys = a.c.dt_mode == DT_PHYSICAL;
   const double sqrtTst = sqrt(*a.staleT);
   const double RePr = a.c.Re * a.c.Pr;
-  // dt_point's denominator at point p, term for term, with mu = mu_of_T(T) exact (FP64) or
-  // its FP32 estimate
-  auto denom = [&](long long p, bool exact, bool& blanked) -> double {
+  double xm = 0.0;  // maximum of the denominators (0: no unblanked point yet)
+  int bad = 0, blank = 0;
+  for (long long p = (long long)blk * DT_THREADS + threadIdx.x; p < n; p += (long long)nblk * DT_THREADS) {
     const int j = (int)(p / Nz), i = (int)(p - (long long)j * Nz);
     const long long o = (long long)j * a.g.P + i;
-    blanked = desc_blank(__ldg(a.desc + o));
-    if (blanked) return 0.0;
+    if (desc_blank(__ldg(a.desc + o))) {
+      blank = 1;
+      continue;
+    }
     const double Vr = __ldg(a.U + 1 * PL + o), Vz = __ldg(a.U + 3 * PL + o), T = __ldg(a.U + 4 * PL + o);
     const double dxidz = __ldg(a.dxidz + i), detadr = __ldg(a.detadr + j);
-    const double mu = exact ? mu_of_T<double>(T) : double(mu_of_T<float>(float(T)));
+    const double mu = mu_of_T<double>(T);
     const double beta = (3.0 / 5.0) * mu;
     const double lambda = beta - (2.0 / 3.0) * mu;
+    // dt_point's denominator, term for term
     const double inv = fabs(Vz * dxidz + Vr * detadr) + (phys ? sqrt(T) : sqrtTst) * sqrt(dxidz * dxidz + detadr * detadr);
     double mx = (lambda > mu ? lambda : mu) / a.c.Re;
     const double k = mu / RePr;
     if (k > mx) mx = k;
     const double sabs = fabs(dxidz) + fabs(detadr);
-    return inv + 2.0 * mx * (sabs * sabs);
-  };
-  // The block's largest denominator, found without T**0.666 in FP64 at every point. Pass 1
-  // forms each denominator with mu from FP32 log2/exp2 (within 1e-6 of the FP64 mu, so the
-  // denominator is within 1e-6 of its exact value, the viscous term being the only one that
-  // changes) and the block's largest estimate. Pass 2 forms the exact denominator only where
-  // the estimate is within 3e-5 of that largest estimate: the point of the exact maximum is
-  // among them, so the block's maximum is the exact one. Non-finite estimates are decided
-  // exactly in pass 1.
-  double xm = 0.0;   // exact maximum of the denominators (0: no unblanked point yet)
-  double xmf = 0.0;  // largest finite estimate
-  int bad = 0, blank = 0;
-  for (long long p = (long long)blk * DT_THREADS + threadIdx.x; p < n; p += (long long)nblk * DT_THREADS) {
-    bool bl;
-    const double xf = denom(p, false, bl);
-    if (bl) {
-      blank = 1;
-      continue;
-    }
-    if (isfinite(xf)) {
-      xmf = fmax(xmf, xf);
-    } else {
-      const double x = denom(p, true, bl);
-      if (!isfinite(x)) bad = 1;  // NaN, or an infinite input (which would give dt = 0)
-      xm = fmax(xm, x);
-    }
-  }
-  __shared__ double sthr[DT_THREADS / 32];
-  xmf = warp_max(xmf);
-  if ((threadIdx.x & 31) == 0) sthr[threadIdx.x >> 5] = xmf;
-  __syncthreads();
-  double thr = sthr[0];
-#pragma unroll
-  for (int q = 1; q < DT_THREADS / 32; ++q) thr = fmax(thr, sthr[q]);
-  thr = thr * (1.0 - 3e-5);
-  for (long long p = (long long)blk * DT_THREADS + threadIdx.x; p < n; p += (long long)nblk * DT_THREADS) {
-    bool bl;
-    const double xf = denom(p, false, bl);
-    if (bl || !isfinite(xf) || xf < thr) continue;
-    const double x = denom(p, true, bl);
-    if (!isfinite(x)) bad = 1;
+    const double x = inv + 2.0 * mx * (sabs * sabs);
+    if (!isfinite(x)) bad = 1;  // NaN, or an infinite input (which would give dt = 0)
     xm = fmax(xm, x);
   }
   __shared__ double sred[DT_THREADS / 32];
