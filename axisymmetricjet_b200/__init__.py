@@ -78,6 +78,7 @@ def load_library():
         "axj_patches_from_records": (C.c_int, [C.POINTER(AxjBcRecord), i64, i64, i64, C.POINTER(AxjPatch),
                                                C.POINTER(i64)]),
         "axj_version": (C.c_char_p, []),
+        "axj_mu_of_T": (C.c_double, [C.c_double]),
         "axj_default_train_cfg": (None, [C.POINTER(AxjTrainCfg)]),
         "axj_mlp_init": (None, [C.POINTER(AxjMlp), i64]),
         "axj_mlp_set": (C.c_int, [h, C.POINTER(AxjMlp)]),

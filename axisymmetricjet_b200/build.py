@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libaxj.so")
 SOURCES = ["axj_api.cu", "axj_kernels.cu", "axj_mlp.cu", "axj_noalloc.cu", "axj_prep.cu"]
-HEADERS = ["axj_common.cuh", "axj_point.cuh", "axj_kernels.cuh", "axj_mlp.cuh", "axj_prep.cuh"]
+HEADERS = ["axj_common.cuh", "axj_point.cuh", "axj_pow.cuh", "axj_kernels.cuh", "axj_mlp.cuh", "axj_prep.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler",
               "-fPIC", "-shared", "-cudart", "static"]
 

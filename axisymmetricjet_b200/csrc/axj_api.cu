@@ -16,6 +16,7 @@
 #include "axj_prep.cuh"
 #include "axj_kernels.cuh"
 #include "axj_mlp.cuh"
+#include "axj_pow.cuh"
 
 using namespace axj;
 
@@ -1149,6 +1150,15 @@ void axj_default_params(axj_params* p) {
 }
 
 const char* axj_version(void) { return "axj 0.2 sm_100a fp64 mixed"; }
+
+double axj_mu_of_T(double T) {
+  static const std::vector<double> tab = [] {
+    std::vector<double> t(POW_TAB);
+    pow0666_fill(t.data());
+    return t;
+  }();
+  return pow0666(T, tab.data());
+}
 
 int axj_read_bc_file(const char* path, axj_bc_record* rec, int64_t max_records, int64_t* nrecords) {
   if (!path || !nrecords) return fail(nullptr, AXJ_ERR_ARG, "null argument");
@@ -2733,7 +2743,7 @@ void axj_batch_default_tuning(axj_batch_tuning* t) {
   std::memset(t, 0, sizeof(*t));
   t->tile_order = 0;
   t->stage_ctas_per_sm = 2;
-  t->sensor_ctas_per_sm = 2;
+  t->sensor_ctas_per_sm = 4;
   t->stage_rows = TR;
 }
 
@@ -2866,7 +2876,7 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
   if (int rc = batch_save(b, save)) return rc;
   // candidates: tile order x interior stage tile shape (32 x 16, or 32 x 8 half tiles)
   // with its persistent CTAs per SM (1 or 2 of 256 threads; 2 or 4 of 128) x persistent
-  // CTAs per SM of the interior sensor kernel
+  // CTAs per SM of the interior sensor kernel (2 or 4 of 128 threads)
   std::vector<axj_batch_tuning> cands;
   for (int o = 0; o < 2; ++o)
     for (int rows : {TR, TR / 2})
@@ -2878,7 +2888,7 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
           t.stage_rows = rows;
           // half tiles: two or four CTAs per SM (FP64), three or six (FP32 stencils)
           t.stage_ctas_per_sm = rows == TR ? sc : (b->mixed ? 3 : 2) * sc;
-          t.sensor_ctas_per_sm = se;
+          t.sensor_ctas_per_sm = 2 * se;
           if (!b->sc && se > 1) continue;
           cands.push_back(t);
         }

@@ -20,6 +20,7 @@
 
 #include "axj_kernels.cuh"
 #include "axj_point.cuh"
+#include "axj_pow.cuh"
 
 namespace axj {
 
@@ -32,6 +33,17 @@ __constant__ PatchDev cPatch[MAX_PATCHES];
 // SBP2 centred row composed with itself: the 9-point fourth-difference row (offsets -4..4)
 __constant__ double cC9[9];
 __constant__ float cC9f[9];
+// tables of the FP64 power mu = T**0.666 (axj_pow.cuh); read through the L1 cache, since
+// the points of a warp index them by their own T
+__device__ double gPowTab[POW_TAB];
+
+// mu = T**0.666 of the stage input: the table-driven FP64 power, or (FP32 stencils)
+// exp2f / log2f
+template <typename R>
+__device__ __forceinline__ R mu_k(R T) {
+  if constexpr (std::is_same<R, double>::value) return pow0666(T, gPowTab);
+  else return mu_of_T<float>(T);
+}
 
 void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const double tg[9][11],
                    const PatchDev* patches, int npatch, cudaStream_t s) {
@@ -57,6 +69,13 @@ void upload_tables(const double sbp1[9][6], const double sbp2[9][6], const doubl
   for (int k = 0; k < 9; ++k) c9f[k] = (float)c9[k];
   cudaMemcpyToSymbolAsync(cC9, c9, sizeof(double) * 9, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(cC9f, c9f, sizeof(float) * 9, 0, cudaMemcpyHostToDevice, s);
+  static double pw[POW_TAB];
+  static bool pw_done = false;
+  if (!pw_done) {
+    pow0666_fill(pw);
+    pw_done = true;
+  }
+  cudaMemcpyToSymbolAsync(gPowTab, pw, sizeof pw, 0, cudaMemcpyHostToDevice, s);
 }
 
 // Round-to-nearest arithmetic that the compiler may not contract into an FMA; used
@@ -343,7 +362,7 @@ __device__ __forceinline__ bool stage_compute(const StageArgs& a, int i0, int j0
       const int rr = idx / RZ, rz = idx - rr * RZ;
       const bool cross = (rr >= H && rr < H + TRT && rz >= HZ - H && rz < HZ + TZ + H) || (rz >= HZ && rz < HZ + TZ);
       if (!cross) continue;
-      const double mu = double(mu_of_T<R>(R(sU[4 * NPT + idx])));
+      const double mu = double(mu_k<R>(R(sU[4 * NPT + idx])));
       vmu[k] = mu;
       if (rr >= H && rr < H + TRT && rz >= HZ && rz < HZ + TZ) sMu0[(rr - H) * TZ + (rz - HZ)] = mu;
       if (sc) {
@@ -876,19 +895,28 @@ __device__ __forceinline__ double warp_min(double v) {
 // The minimum of dt = CFL / x over the points is CFL / (maximum of x): division by a
 // positive x is monotonic and correctly rounded, so the two agree exactly; the kernel
 // reduces x and divides once. Likewise max(mu/Re, lambda/Re) = max(mu, lambda)/Re. The
-// stale T's square root is formed once. Blanked points contribute dt = 100
-// (ModInputOutput.f90:398-400).
+// divisions by Re and Re Pr are products with the reciprocals (within an ulp of the
+// quotients). The stale T's square root is formed once. Blanked points contribute dt = 100
+// (ModInputOutput.f90:398-400). A thread's (i, j) advances by the grid stride without a
+// division per point.
 __device__ __forceinline__ void dt_body(const DtArgs& a, int blk, int nblk) {
   const int Nz = a.g.Nz, Nr = a.g.Nr;
   const long long n = (long long)Nz * Nr;
   const long long PL = a.g.plane;
   const bool phys = a.c.dt_mode == DT_PHYSICAL;
   const double sqrtTst = sqrt(*a.staleT);
-  const double RePr = a.c.Re * a.c.Pr;
+  const double inv_Re = 1.0 / a.c.Re, inv_RePr = 1.0 / (a.c.Re * a.c.Pr);
   double xm = 0.0;  // maximum of the denominators (0: no unblanked point yet)
   int bad = 0, blank = 0;
-  for (long long p = (long long)blk * DT_THREADS + threadIdx.x; p < n; p += (long long)nblk * DT_THREADS) {
-    const int j = (int)(p / Nz), i = (int)(p - (long long)j * Nz);
+  const long long stride = (long long)nblk * DT_THREADS;
+  const int sj = (int)(stride / Nz), si = (int)(stride - (long long)sj * Nz);
+  long long p = (long long)blk * DT_THREADS + threadIdx.x;
+  int j = (int)(p / Nz), i = (int)(p - (long long)j * Nz);
+  for (; p < n; p += stride, i += si, j += sj) {
+    if (i >= Nz) {  // i + si < 2 Nz: one carry at most
+      i -= Nz;
+      ++j;
+    }
     const long long o = (long long)j * a.g.P + i;
     if (desc_blank(__ldg(a.desc + o))) {
       blank = 1;
@@ -896,13 +924,13 @@ __device__ __forceinline__ void dt_body(const DtArgs& a, int blk, int nblk) {
     }
     const double Vr = __ldg(a.U + 1 * PL + o), Vz = __ldg(a.U + 3 * PL + o), T = __ldg(a.U + 4 * PL + o);
     const double dxidz = __ldg(a.dxidz + i), detadr = __ldg(a.detadr + j);
-    const double mu = mu_of_T<double>(T);
+    const double mu = mu_k<double>(T);
     const double beta = (3.0 / 5.0) * mu;
     const double lambda = beta - (2.0 / 3.0) * mu;
     // dt_point's denominator, term for term
     const double inv = fabs(Vz * dxidz + Vr * detadr) + (phys ? sqrt(T) : sqrtTst) * sqrt(dxidz * dxidz + detadr * detadr);
-    double mx = (lambda > mu ? lambda : mu) / a.c.Re;
-    const double k = mu / RePr;
+    double mx = (lambda > mu ? lambda : mu) * inv_Re;
+    const double k = mu * inv_RePr;
     if (k > mx) mx = k;
     const double sabs = fabs(dxidz) + fabs(detadr);
     const double x = inv + 2.0 * mx * (sabs * sabs);
@@ -1050,8 +1078,9 @@ struct SensSmem {
 };
 
 // Threads of a sensor tile CTA: general tiles (one CTA per SM, bound by shared memory)
-// take 512 so the SM has 16 warps to hide latency with; interior tiles 256.
-__host__ __device__ constexpr int sens_threads(bool gen) { return gen ? 512 : STAGE_THREADS; }
+// take 512 so the SM has 16 warps to hide latency with; interior tiles 128 (a 2 x 2
+// block of points per thread in the fourth differences; four CTAs per SM).
+__host__ __device__ constexpr int sens_threads(bool gen) { return gen ? 512 : 128; }
 
 template <typename R>
 __device__ __forceinline__ R sqrt_t(R x) { return sqrt(x); }
@@ -1180,71 +1209,106 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   phase ^= 1u;
 
   // ---- phase 2: S and dilatation on the cross of the S region (reach HS either way);
-  // f_sw on the tile. Interior tiles: horizontal pairs of points (S columns sz, sz + 1 with
-  // sz even) whose stencil windows come in pair loads; the arithmetic per point is the
-  // general loop's.
+  // f_sw on the tile. Interior tiles: 2 x 2 blocks of S points (rows sr, sr + 1, columns
+  // sz, sz + 1; sr, sz even) over the z arm (the tile rows, TZ + 2 HS columns) and the r
+  // arm (HS rows either side, the tile columns). Each block row's z windows come in three
+  // pair loads per field, which also hold the block's own values; its r windows need the
+  // rows sr - 2, sr - 1, sr + 2, sr + 3 besides. The arithmetic per point is the general
+  // loop's (dot_c1's order, the zero middle weight left out). Points off the cross are
+  // never read.
   if constexpr (!GEN) {
-    static_assert(SZ % 2 == 0 && VZ % 2 == 0 && HSZ % 2 == 0 && HVZ % 2 == 0 && HS % 2 == 0 && TZ % 2 == 0,
+    static_assert(SZ % 2 == 0 && VZ % 2 == 0 && HSZ % 2 == 0 && HVZ % 2 == 0 && HS % 2 == 0 && TZ % 2 == 0 &&
+                      TR % 2 == 0,
                   "pair loads need even offsets");
-    for (int pp = tid; pp < NS / 2; pp += NT) {
-      const int sr = pp / (SZ / 2), sz = 2 * (pp - sr * (SZ / 2));
-      const bool zarm = sr >= HS && sr < HS + TR && sz >= HSZ - HS && sz < HSZ + TZ + HS;
+    constexpr int ZBW = (TZ + 2 * HS) / 2;        // blocks per z-arm row pair
+    constexpr int NZB = (TR / 2) * ZBW;           // z-arm blocks
+    constexpr int NRB = HS * (TZ / 2);            // r-arm blocks (2 HS rows, in pairs)
+    const R k0 = tabv<R, 1>(4, 0), k1 = tabv<R, 1>(4, 1), k3 = tabv<R, 1>(4, 3), k4 = tabv<R, 1>(4, 4);
+    for (int bq = tid; bq < NZB + NRB; bq += NT) {
+      int sr, sz;
+      if (bq < NZB) {
+        const int br = bq / ZBW;
+        sr = HS + 2 * br;
+        sz = HSZ - HS + 2 * (bq - br * ZBW);
+      } else {
+        const int k = bq - NZB, br = k / (TZ / 2);
+        sr = 2 * br < HS ? 2 * br : 2 * br + TR;
+        sz = HSZ + 2 * (k - br * (TZ / 2));
+      }
+      const bool zarm = bq < NZB;
       const bool rarm = sz >= HSZ && sz < HSZ + TZ;
-      R S[2] = {R(0), R(0)}, dil[2] = {R(0), R(0)};
-      if (zarm || rarm) {
-        const int j = j0 - HS + sr;
-        const int vidx = (sr + HV - HS) * VZ + (sz + HVZ - HSZ);
-        const R k0 = tabv<R, 1>(4, 0), k1 = tabv<R, 1>(4, 1), k3 = tabv<R, 1>(4, 3), k4 = tabv<R, 1>(4, 4);
-        // the centred SBP1 row at both points, accumulated pair load by pair load in dot_c1's
-        // order (offsets -2, -1, +1, +2 of each point's own column or row)
-        auto zpair = [&](const SIN* row, R& p0, R& p1, R& c0, R& c1v) {
-          SIN u, v;
-          ld_pair(row - 2, u, v);  // columns -2, -1
-          p0 = k0 * R(u);
-          p0 = p0 + k1 * R(v);
-          p1 = k0 * R(v);
-          ld_pair(row, u, v);      // columns 0, +1 (the points themselves)
-          c0 = R(u);
-          c1v = R(v);
-          p0 = p0 + k3 * R(v);
-          p1 = p1 + k1 * R(u);
-          ld_pair(row + 2, u, v);  // columns +2, +3
-          p0 = p0 + k4 * R(u);
-          p1 = p1 + k3 * R(u);
-          p1 = p1 + k4 * R(v);
-        };
-        auto rpair = [&](const SIN* col, R& p0, R& p1) {
-          SIN u, v;
-          ld_pair(col - 2 * VZ, u, v);
-          p0 = k0 * R(u);
-          p1 = k0 * R(v);
-          ld_pair(col - VZ, u, v);
-          p0 = p0 + k1 * R(u);
-          p1 = p1 + k1 * R(v);
-          ld_pair(col + VZ, u, v);
-          p0 = p0 + k3 * R(u);
-          p1 = p1 + k3 * R(v);
-          ld_pair(col + 2 * VZ, u, v);
-          p0 = p0 + k4 * R(u);
-          p1 = p1 + k4 * R(v);
-        };
-        R zr0, zr1, zz0, zz1, rr0, rr1, rz0, rz1, vc0, vc1, wc0, wc1;
-        zpair(sVr + vidx, zr0, zr1, vc0, vc1);
-        zpair(sVz + vidx, zz0, zz1, wc0, wc1);
-        rpair(sVr + vidx, rr0, rr1);
-        rpair(sVz + vidx, rz0, rz1);
-        const R gz[2][2] = {{zr0, zr1}, {zz0, zz1}}, gr[2][2] = {{rr0, rr1}, {rz0, rz1}};
-        const R vrc[2] = {vc0, vc1};
-        const R er = R(sMr[sr]), ir = R(sIr[sr]);
+      const int vidx = (sr + HV - HS) * VZ + (sz + HVZ - HSZ);
+      // z: the centred SBP1 row at both points of a block row, accumulated pair load by pair
+      // load (offsets -2, -1, +1, +2 of each point's own column); c0, c1 the points' values
+      auto zpair = [&](const SIN* row, R& p0, R& p1, R& c0, R& c1v) {
+        SIN u, v;
+        ld_pair(row - 2, u, v);  // columns -2, -1
+        p0 = k0 * R(u);
+        p0 = p0 + k1 * R(v);
+        p1 = k0 * R(v);
+        ld_pair(row, u, v);      // columns 0, +1 (the points themselves)
+        c0 = R(u);
+        c1v = R(v);
+        p0 = p0 + k3 * R(v);
+        p1 = p1 + k1 * R(u);
+        ld_pair(row + 2, u, v);  // columns +2, +3
+        p0 = p0 + k4 * R(u);
+        p1 = p1 + k3 * R(u);
+        p1 = p1 + k4 * R(v);
+      };
+      // r: both block rows from rows sr - 2, sr - 1, sr + 2, sr + 3 and the block's own
+      // values (ce[w][h] at row sr + w)
+      auto rblock = [&](const SIN* col, const R ce[2][2], R g[2][2]) {
+        SIN u, v;
+        R m2[2], m1[2], p2[2], p3[2];
+        ld_pair(col - 2 * VZ, u, v);
+        m2[0] = R(u);
+        m2[1] = R(v);
+        ld_pair(col - VZ, u, v);
+        m1[0] = R(u);
+        m1[1] = R(v);
+        ld_pair(col + 2 * VZ, u, v);
+        p2[0] = R(u);
+        p2[1] = R(v);
+        ld_pair(col + 3 * VZ, u, v);
+        p3[0] = R(u);
+        p3[1] = R(v);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          R a0 = k0 * m2[h];
+          a0 = a0 + k1 * m1[h];
+          a0 = a0 + k3 * ce[1][h];
+          a0 = a0 + k4 * p2[h];
+          g[0][h] = a0;
+          R a1 = k0 * m1[h];
+          a1 = a1 + k1 * ce[0][h];
+          a1 = a1 + k3 * p2[h];
+          a1 = a1 + k4 * p3[h];
+          g[1][h] = a1;
+        }
+      };
+      R gzr[2][2], gzz[2][2], grr[2][2], grz[2][2], vr[2][2], vz[2][2];
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        zpair(sVr + vidx + w * VZ, gzr[w][0], gzr[w][1], vr[w][0], vr[w][1]);
+        zpair(sVz + vidx + w * VZ, gzz[w][0], gzz[w][1], vz[w][0], vz[w][1]);
+      }
+      rblock(sVr + vidx, vr, grr);
+      rblock(sVz + vidx, vz, grz);
+#pragma unroll
+      for (int w = 0; w < 2; ++w) {
+        const int j = j0 - HS + sr + w;
+        const R er = R(sMr[sr + w]), ir = R(sIr[sr + w]);
+        R S[2], dil[2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const R xz = R(sMz[sz + h]);
-          const R dVrdz = gz[0][h] * xz;
-          const R dVzdz = gz[1][h] * xz;
-          const R dVrdr = gr[0][h] * er;
-          const R dVzdr = gr[1][h] * er;
+          const R dVrdz = gzr[w][h] * xz;
+          const R dVzdz = gzz[w][h] * xz;
+          const R dVrdr = grr[w][h] * er;
+          const R dVzdr = grz[w][h] * er;
           // V_r / r as V_r * (1/r) (the reference divides; the two differ by rounding)
-          const R vr_r = vrc[h] * ir;
+          const R vr_r = vr[w][h] * ir;
           R d;
           if (j == 0) d = R(2.0) * dVrdr + dVzdz;
           else d = dVrdr + vr_r + dVzdz;
@@ -1258,12 +1322,12 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
             const R vort = fabs(dVrdz - dVzdr);
             const R Hm = (R(-1.0) * d < R(0)) ? R(0) : R(1);
             const R eps = R((double)1e-15f);  // single-precision literal of the reference (:202)
-            sFsw[(sr - HS) * TZ + (sz + h - HSZ)] = Hm * (d * d) / (d * d + vort * vort + eps);
+            sFsw[(sr + w - HS) * TZ + (sz + h - HSZ)] = Hm * (d * d) / (d * d + vort * vort + eps);
           }
         }
+        st_pair(sS + (sr + w) * SZ + sz, S[0], S[1]);
+        st_pair(sD + (sr + w) * SZ + sz, dil[0], dil[1]);
       }
-      st_pair(sS + sr * SZ + sz, S[0], S[1]);
-      st_pair(sD + sr * SZ + sz, dil[0], dil[1]);
     }
   } else
   for (int idx = tid; idx < NS; idx += NT) {
@@ -1316,93 +1380,123 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   auto ppoint = [](int t, int q) { return (t >> 5) * (TZ * PPT) + q * TZ + (t & 31); };
   R d4z[3][PPT], d4r[3][PPT];
   if constexpr (!GEN) {
-    // horizontal pairs (columns c, c + 1, c even), every window in pair loads, then the
-    // quantities of both points (cC9 on each point's 9 values, in c9dot's order)
-    static_assert(NT * 2 == TZ * TR, "one pair of points per thread");
-    const int r = tid / (TZ / 2), c = 2 * (tid - r * (TZ / 2));
+    // 2 x 2 blocks of points (rows r, r + 1 and columns c, c + 1; r, c even), every window
+    // in pair loads: along z each block row's five pairs (columns c - 4 .. c + 5) serve its
+    // two points, along r each of the ten rows r - 4 .. r + 5 serves the block rows it
+    // reaches. Every point's sum keeps c9dot's order (taps left to right). The quantities
+    // of a field leave as soon as its sums are complete.
+    static_assert(NT * 4 == TZ * TR, "one 2 x 2 block of points per thread");
+    const int r = 2 * (tid / (TZ / 2)), c = 2 * (tid - (tid / (TZ / 2)) * (TZ / 2));
     const int sidx = (HS + r) * SZ + (HSZ + c);
-    R qz[3][2], qr[3][2], Tc[2];
     const R* c9 = std::is_same<R, float>::value ? reinterpret_cast<const R*>(cC9f) : reinterpret_cast<const R*>(cC9);
-    // cC9 at both points, accumulated pair load by pair load in c9dot's order: along z the
-    // pair loads cover columns c - 4 .. c + 5 (point 0 takes columns -4..4, point 1 -3..5),
-    // along r each row's pair serves both points
+    R zs[2][2], rs[2][2], Tc[2][2];
     auto four = [&](const auto* base, int f) {
       using E = std::remove_cv_t<std::remove_reference_t<decltype(base[0])>>;
-      R z0 = R(0), z1 = R(0), r0 = R(0), r1 = R(0);
 #pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        R u, v;
-        {
-          E uu, vv;
-          ld_pair(base + sidx - 4 + 2 * q, uu, vv);
-          u = R(uu);
-          v = R(vv);
+      for (int w = 0; w < 2; ++w) {
+        R z0 = R(0), z1 = R(0);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+          R u, v;
+          {
+            E uu, vv;
+            ld_pair(base + sidx + w * SZ - 4 + 2 * q, uu, vv);
+            u = R(uu);
+            v = R(vv);
+          }
+          const int m = 2 * q;  // u is column m - 4, v column m - 3
+          if (q == 0) {
+            z0 = c9[0] * u;
+            z0 = z0 + c9[1] * v;
+            z1 = c9[0] * v;
+          } else if (q < 4) {
+            z0 = z0 + c9[m] * u;
+            z0 = z0 + c9[m + 1] * v;
+            z1 = z1 + c9[m - 1] * u;
+            z1 = z1 + c9[m] * v;
+          } else {
+            z0 = z0 + c9[8] * u;
+            z1 = z1 + c9[7] * u;
+            z1 = z1 + c9[8] * v;
+          }
+          if (f == 1 && q == 2) {
+            Tc[w][0] = u;
+            Tc[w][1] = v;
+          }
         }
-        const int m = 2 * q;  // u is column m - 4, v column m - 3
-        if (q == 0) {
-          z0 = c9[0] * u;
-          z0 = z0 + c9[1] * v;
-          z1 = c9[0] * v;
-        } else if (q < 4) {
-          z0 = z0 + c9[m] * u;
-          z0 = z0 + c9[m + 1] * v;
-          z1 = z1 + c9[m - 1] * u;
-          z1 = z1 + c9[m] * v;
-        } else {
-          z0 = z0 + c9[8] * u;
-          z1 = z1 + c9[7] * u;
-          z1 = z1 + c9[8] * v;
-        }
-        if (f == 1 && q == 2) {
-          Tc[0] = u;
-          Tc[1] = v;
-        }
+        zs[w][0] = z0;
+        zs[w][1] = z1;
       }
 #pragma unroll
-      for (int m = 0; m < 9; ++m) {
+      for (int m = 0; m < 10; ++m) {
         E uu, vv;
         ld_pair(base + sidx + (m - 4) * SZ, uu, vv);
+        const R u = R(uu), v = R(vv);
         if (m == 0) {
-          r0 = c9[0] * R(uu);
-          r1 = c9[0] * R(vv);
-        } else {
-          r0 = r0 + c9[m] * R(uu);
-          r1 = r1 + c9[m] * R(vv);
+          rs[0][0] = c9[0] * u;
+          rs[0][1] = c9[0] * v;
+        } else if (m < 9) {
+          rs[0][0] = rs[0][0] + c9[m] * u;
+          rs[0][1] = rs[0][1] + c9[m] * v;
+        }
+        if (m == 1) {
+          rs[1][0] = c9[0] * u;
+          rs[1][1] = c9[0] * v;
+        } else if (m > 1) {
+          rs[1][0] = rs[1][0] + c9[m - 1] * u;
+          rs[1][1] = rs[1][1] + c9[m - 1] * v;
         }
       }
-      qz[f][0] = z0;
-      qz[f][1] = z1;
-      qr[f][0] = r0;
-      qr[f][1] = r1;
     };
-    four(sS, 0);
-    four(sT, 1);
-    four(sD, 2);
     // ---- quantities to be filtered (ComputeTobeFilteredQuantities :204-215)
     const long long o = (long long)(j0 + r) * g.P + (i0 + c);
-    R dzp[2], rho[2], fsw[2];
+    R dzp[2], rho[2][2], fsw[2][2];
     {
       double a0, a1;
       ld_pair(sDzv + c, a0, a1);
       dzp[0] = R(a0);
       dzp[1] = R(a1);
-      SIN r0, r1;
-      ld_pair(sRho + r * TZ + c, r0, r1);
-      rho[0] = R(r0);
-      rho[1] = R(r1);
-      ld_pair(sFsw + r * TZ + c, fsw[0], fsw[1]);
-    }
-    const R dr = R(sDrv[r]);
-    double out[3][2];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const R dz = dzp[h];
-      out[0][h] = double(rho[h] * fabs((qz[0][h] * (dz * dz) + qr[0][h] * (dr * dr))));
-      out[1][h] = double(rho[h] * fsw[h] * fabs((qz[2][h] * (dz * dz) + qr[2][h] * (dr * dr))));
-      out[2][h] = double(rho[h] / (R(a.c.gam) * sqrt_t<R>(Tc[h])) * fabs((qz[1][h] * dz + qr[1][h] * dr)));
+      for (int w = 0; w < 2; ++w) {
+        SIN r0, r1;
+        ld_pair(sRho + (r + w) * TZ + c, r0, r1);
+        rho[w][0] = R(r0);
+        rho[w][1] = R(r1);
+        ld_pair(sFsw + (r + w) * TZ + c, fsw[w][0], fsw[w][1]);
+      }
     }
+    const R drw[2] = {R(sDrv[r]), R(sDrv[r + 1])};
+    double out[2][2];
+    four(sS, 0);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) st_pair(a.Q + q * g.plane + o, out[q][0], out[q][1]);
+    for (int w = 0; w < 2; ++w)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const R dz = dzp[h], dr = drw[w];
+        out[w][h] = double(rho[w][h] * fabs((zs[w][h] * (dz * dz) + rs[w][h] * (dr * dr))));
+      }
+#pragma unroll
+    for (int w = 0; w < 2; ++w) st_pair(a.Q + o + w * g.P, out[w][0], out[w][1]);
+    four(sD, 2);
+#pragma unroll
+    for (int w = 0; w < 2; ++w)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const R dz = dzp[h], dr = drw[w];
+        out[w][h] = double(rho[w][h] * fsw[w][h] * fabs((zs[w][h] * (dz * dz) + rs[w][h] * (dr * dr))));
+      }
+#pragma unroll
+    for (int w = 0; w < 2; ++w) st_pair(a.Q + g.plane + o + w * g.P, out[w][0], out[w][1]);
+    four(sT, 1);
+#pragma unroll
+    for (int w = 0; w < 2; ++w)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const R dz = dzp[h], dr = drw[w];
+        out[w][h] = double(rho[w][h] / (R(a.c.gam) * sqrt_t<R>(Tc[w][h])) * fabs((zs[w][h] * dz + rs[w][h] * dr)));
+      }
+#pragma unroll
+    for (int w = 0; w < 2; ++w) st_pair(a.Q + 2 * g.plane + o + w * g.P, out[w][0], out[w][1]);
     return true;
   } else {
 #pragma unroll
@@ -1488,7 +1582,7 @@ __global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 4)
 // Batched form: persistent loop over (i0, j0, instance) tiles; kmaps = indices of the
 // V, T and rho maps in each instance's block of nmaps maps.
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(sens_threads(GEN))
+__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 4)
     sensor_tile_kernel_batch(const SensorArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
                              const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1597,7 +1691,7 @@ static void launch_sensor_tiles(const SensorArgs& a, const SideStream& side, cud
                                                                                             *a.mt_gen, *a.mrho);
   if (a.ntiles_int > 0)
     sensor_tile_kernel<SENS_HS_INT, H_INT, false, SIN, R>
-        <<<a.ntiles_int, STAGE_THREADS, SI::bytes(false), s>>>(a, a.tiles_int, *a.mv_int, *a.mt_int, *a.mrho);
+        <<<a.ntiles_int, sens_threads(false), SI::bytes(false), s>>>(a, a.tiles_int, *a.mv_int, *a.mt_int, *a.mrho);
 }
 
 __global__ void sensor_rfilter_kernel(const SensorArgs a) {
@@ -2054,7 +2148,7 @@ __device__ __forceinline__ void zr_body(const ZrArgs& a, const CUtensorMap* pQ, 
         const int row = qd / ZRK_BZ, p = qd - row * ZRK_BZ;
         const int j = j0 + row, i = ZRK_BZ * m + p;
         if (qd >= ZRK_RB * ZRK_BZ || j >= Nr || i < zs || i >= ze) continue;
-        const double mu = double(mu_of_T<R>(R(tb[qd])));
+        const double mu = double(mu_k<R>(R(tb[qd])));
         const int rw = rcb[qd];
         double fv[3] = {0.0, 0.0, 0.0};
         // column of this point in the transposed block: row j0 + row is Z row row + ZRK_HR
@@ -2418,7 +2512,7 @@ static void launch_sensor_tiles_batch(const SensorArgs* argv, const BatchTiles& 
         <<<tgen.grid, sens_threads(true), SG::bytes(true), side.stream ? side.stream : s>>>(
             argv, tgen.tiles, tgen.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 1), bmap_sensT(kin, 1), bmap_rho(kin), 0));
   if (tint.ntiles > 0)
-    sensor_tile_kernel_batch<SENS_HS_INT, H_INT, false, SIN, R><<<tint.grid, STAGE_THREADS, SI::bytes(false), s>>>(
+    sensor_tile_kernel_batch<SENS_HS_INT, H_INT, false, SIN, R><<<tint.grid, sens_threads(false), SI::bytes(false), s>>>(
         argv, tint.tiles, tint.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 0), bmap_sensT(kin, 0), bmap_rho(kin), 0));
 }
 

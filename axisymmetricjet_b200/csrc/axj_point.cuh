@@ -121,7 +121,9 @@ AXJ_HD void rhs_viscous(const PrimT<R>& q, const DerivT<R>& d, R onebyr, R inv_r
                 (d.dVrdz + d.dVzdr) * (d.dVzdr + d.dVrdz));
 }
 
-// mu = T**0.666 (ModAssign.f90:20) as exp2(0.666 log2 T): within a few ulp of pow.
+// mu = T**0.666 (ModAssign.f90:20) as exp2(0.666 log2 T): within a few ulp of pow. The
+// FP32 stencils and the allocation-free dt use it; the FP64 kernels use the table-driven
+// pow0666 (axj_pow.cuh).
 template <typename R>
 AXJ_HD R mu_of_T(R T);
 template <>

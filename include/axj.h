@@ -321,7 +321,7 @@ typedef struct axj_batch axj_batch;
 typedef struct axj_batch_tuning {
   int64_t tile_order;          /* 0: instance after instance; 1: round-robin over instances */
   int64_t stage_ctas_per_sm;   /* persistent CTAs per SM of the interior stage kernel (2) */
-  int64_t sensor_ctas_per_sm;  /* persistent CTAs per SM of the interior sensor kernel (2) */
+  int64_t sensor_ctas_per_sm;  /* persistent CTAs per SM of the interior sensor kernel (4) */
   int64_t stage_rows;          /* rows of the interior stage tiles' CTAs: 16 (32 x 16 tiles, default) or 8 */
   int64_t reserved[4];
 } axj_batch_tuning;
@@ -395,6 +395,11 @@ int axj_prep_maps(const axj_patch* patches, int64_t npatch, int64_t Nz, int64_t 
  * (ModOperator.f90:5-121): SBP1(0:8,0:5) and SBP2(0:8,0:5) into sbp1[54] and sbp2[54],
  * TGfilt(0:8,0:10) into tgfilt[99], row-major (row = the SBP row). */
 int axj_operator_tables(double* sbp1, double* sbp2, double* tgfilt);
+
+/* mu = T**0.666 (ModAssign.f90:20, Tvec**0.666D0) as the FP64 kernels form it: a
+ * table-driven power within 1 ulp of the correctly rounded result for T in [2^-16, 2^16),
+ * evaluated on the host with the device's operations (the same bits). */
+double axj_mu_of_T(double T);
 
 /* Library build information, e.g. "axj 0.1 sm_100a". */
 const char* axj_version(void);
