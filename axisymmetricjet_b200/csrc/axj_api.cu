@@ -2876,7 +2876,8 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
   if (int rc = batch_save(b, save)) return rc;
   // candidates: tile order x interior stage tile shape (32 x 16, or 32 x 8 half tiles)
   // with its persistent CTAs per SM (1 or 2 of 256 threads; 2 or 4 of 128) x persistent
-  // CTAs per SM of the interior sensor kernel (2 or 4 of 128 threads)
+  // CTAs per SM of the interior sensor kernel (4 or 6 of 128 threads: four fit an SM with
+  // FP64 boxes, six with FP32 ones)
   std::vector<axj_batch_tuning> cands;
   for (int o = 0; o < 2; ++o)
     for (int rows : {TR, TR / 2})
@@ -2888,7 +2889,7 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
           t.stage_rows = rows;
           // half tiles: two or four CTAs per SM (FP64), three or six (FP32 stencils)
           t.stage_ctas_per_sm = rows == TR ? sc : (b->mixed ? 3 : 2) * sc;
-          t.sensor_ctas_per_sm = 2 * se;
+          t.sensor_ctas_per_sm = 2 + 2 * se;
           if (!b->sc && se > 1) continue;
           cands.push_back(t);
         }
