@@ -1969,11 +1969,12 @@ constexpr int ZRK_ZP = ZRK_NR + 1;
 
 template <typename SIN>
 struct ZrSmem {
-  static constexpr size_t qbytes = (size_t)ZRK_LANES * ZRK_QROW;           // 19968
-  static constexpr size_t qslot = (qbytes + 1023) / 1024 * 1024;           // 20480
+  static constexpr size_t qbytes = (size_t)ZRK_LANES * ZRK_QROW;
+  static constexpr size_t qslot = (qbytes + 1023) / 1024 * 1024;
+  static constexpr size_t zslot = ((size_t)3 * ZRK_BZ * ZRK_ZP * sizeof(double) + 1023) / 1024 * 1024;
   static constexpr size_t oQ = 0;                                            // [2] Q blocks (swizzled)
   static constexpr size_t oZ = 2 * qslot;                                    // z-filtered block [3][16][ZRK_ZP]
-  static constexpr size_t oZc = oZ + qslot;                                  // [2][ZRK_NR][16] z row codes
+  static constexpr size_t oZc = oZ + zslot;                                  // [2][ZRK_NR][16] z row codes
   static constexpr size_t zcbytes = (size_t)ZRK_NR * ZRK_BZ;
   static constexpr size_t oT = oZc + 2 * 1024;                               // [2][ZRK_RB][16] T
   static constexpr size_t tbytes = (size_t)ZRK_RB * ZRK_BZ * sizeof(SIN);
@@ -1982,6 +1983,7 @@ struct ZrSmem {
   static constexpr size_t oW = oRc + 2 * 512;                                // [10][21] padded TG rows
   static constexpr size_t bytes = oW + 10 * 21 * sizeof(double) + 1024;      // + alignment slack
   static constexpr uint32_t tx = (uint32_t)(qbytes + zcbytes + tbytes + rcbytes);
+  static_assert(zcbytes <= 1024 && rcbytes <= 512, "code slots");
 };
 
 // The fused z/r filter for the CTA (bx, by): z positions bx * a.seg .., rows by * ZRK_RB ..

@@ -165,7 +165,7 @@ cudaError_t launch_sensor_tiles_only(const SensorArgs& a, const SideStream& side
 // mu_eff, beta = 0.6 mu + beta*, kappa_eff of the stage input. A CTA of ZRK_THREADS
 // threads owns seg z positions (a multiple of ZRK_BZ) and ZRK_RB rows.
 constexpr int ZRK_BZ = 16;                    // z positions per block (one 128-byte row of doubles)
-constexpr int ZRK_RB = 32;                    // rows per CTA
+constexpr int ZRK_RB = 30;                    // rows per CTA (30 x 16 points: three per thread)
 constexpr int ZRK_HR = 10;                    // r reach of the TG boundary rows
 constexpr int ZRK_NR = ZRK_RB + 2 * ZRK_HR;   // rows of the z recurrence per CTA
 constexpr int ZRK_THREADS = 160;

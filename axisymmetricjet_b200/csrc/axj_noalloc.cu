@@ -18,6 +18,7 @@
 #include "axj_common.cuh"
 #include "axj_kernels.cuh"
 #include "axj_point.cuh"
+#include "axj_pow.cuh"
 
 namespace {
 
@@ -31,6 +32,9 @@ constexpr int NA_BAD = NA_MAX_BLOCKS + 1;             // slot of the non-finite 
 // kept in the slots after them. Every call shares it and it keeps the last call's
 // contents; each call clears the two words before its kernel runs.
 static __device__ __align__(256) double g_dt_scratch[NA_MAX_BLOCKS + 2];
+// the tables of the FP64 power mu = T**0.666 (axj_pow.cuh), written by the first call on
+// each device
+static __device__ double g_na_pow[axj::POW_TAB];
 
 __device__ __forceinline__ double na_warp_min(double v) {
 #pragma unroll
@@ -57,8 +61,8 @@ __global__ void __launch_bounds__(NA_THREADS)
       v = 100.0;
     } else {
       const double Vr = __ldg(U + 1 * plane + o), Vz = __ldg(U + 3 * plane + o), T = __ldg(U + 4 * plane + o);
-      // mu = T**0.666 (AssignValues) by the same definition as the handle-based dt kernel
-      const double mu = axj::mu_of_T<double>(T);
+      // mu = T**0.666 (AssignValues) from the table-driven power of the handle-based kernels
+      const double mu = axj::pow0666(T, g_na_pow);
       const double beta = (3.0 / 5.0) * mu;
       const double lambda = beta - (2.0 / 3.0) * mu;
       const bool phys = c.dt_mode == axj::DT_PHYSICAL;
@@ -136,10 +140,13 @@ extern "C" int axj_compute_dt_noalloc(const double* d_pv, int64_t pitch, int64_t
   {
     std::lock_guard<std::mutex> g(g_na_lock);
     if (!g_na_ptr[dev]) {
-      cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&g_na_ptr[dev]), g_dt_scratch);
+      static double tab[axj::POW_TAB];
+      axj::pow0666_fill(tab);
+      cudaError_t e = cudaMemcpyToSymbol(g_na_pow, tab, sizeof tab);
+      if (e == cudaSuccess) e = cudaGetSymbolAddress(reinterpret_cast<void**>(&g_na_ptr[dev]), g_dt_scratch);
       if (e != cudaSuccess) {
         g_na_ptr[dev] = nullptr;
-        std::snprintf(msg, sizeof(msg), "axj_compute_dt_noalloc: cudaGetSymbolAddress failed: %s",
+        std::snprintf(msg, sizeof(msg), "axj_compute_dt_noalloc: device set-up failed: %s",
                       cudaGetErrorString(e));
         axj::set_global_error(msg);
         return AXJ_ERR_CUDA;

@@ -237,8 +237,9 @@ int axj_sensor(axj_handle* h, const double* pv, double* mustar, double* betastar
  *            is not blanked holds a non-finite V_r, V_z or T, or gives a NaN dt); stream is a cudaStream_t (NULL: legacy default stream)
  * At most 16,777,216 points (Nz*Nr); larger grids return AXJ_ERR_ARG with a message in
  * axj_last_error(NULL). The call is asynchronous on `stream`. The first call on a device
- * looks up the scratch array's device address with that device current; make that first
- * call before any stream capture. Calls share the scratch, so calls that overlap on the
+ * writes the tables of mu = T**0.666 (a synchronous copy into the library's own device
+ * array, no allocation) and looks up the scratch array's device address with that device
+ * current; make that first call before any stream capture. Calls share the scratch, so calls that overlap on the
  * GPU (different streams, no ordering) race with each other. */
 int axj_compute_dt_noalloc(const double* d_pv, int64_t pitch, int64_t Nz, int64_t Nr, const double* d_dxidz,
                            const double* d_detadr, const double* d_ibval, const axj_params* params, double stale_T,

@@ -19,7 +19,8 @@ from axisymmetricjet_b200 import fixtures
 
 pytestmark = pytest.mark.gpu
 
-REL = 1e-14  # both compute the same per-point values by the same formulas; the minimum is exact
+REL = 1e-14  # the same per-point formulas (the handle's kernel multiplies by 1/Re where this one
+             # divides: an ulp at most); the minimum is exact
 PAD = 24     # caller arrays with a row pitch of Nz + PAD
 
 
