@@ -128,11 +128,13 @@ def default_train_cfg(**overrides):
 
 class AxjBatchTuning(C.Structure):
     _fields_ = [("tile_order", C.c_int64), ("stage_ctas_per_sm", C.c_int64), ("sensor_ctas_per_sm", C.c_int64),
-                ("stage_rows", C.c_int64), ("reserved", C.c_int64 * 4)]
+                ("stage_rows", C.c_int64), ("general_ctas_per_sm", C.c_int64), ("general_serial", C.c_int64),
+                ("reserved", C.c_int64 * 2)]
 
     def to_dict(self):
         return {"tile_order": self.tile_order, "stage_ctas_per_sm": self.stage_ctas_per_sm,
-                "sensor_ctas_per_sm": self.sensor_ctas_per_sm, "stage_rows": self.stage_rows}
+                "sensor_ctas_per_sm": self.sensor_ctas_per_sm, "stage_rows": self.stage_rows,
+                "general_ctas_per_sm": self.general_ctas_per_sm, "general_serial": self.general_serial}
 
 
 def default_params(**overrides):

@@ -2450,12 +2450,14 @@ int batch_stage(axj_batch* b, int bin, int bout, int stage, bool judge) {
   const int rows = (int)b->tune.stage_rows;
   const BatchTiles sti = rows == TR / 2 ? btiles(b, b->st_half, b->h_st_half, b->tune.stage_ctas_per_sm)
                                         : btiles(b, b->st_int, b->h_st_int, b->tune.stage_ctas_per_sm);
-  const BatchTiles stg = btiles(b, b->st_gen, b->h_st_gen, 1);
+  const BatchTiles stg = btiles(b, b->st_gen, b->h_st_gen, std::max<int64_t>(1, b->tune.general_ctas_per_sm));
   const BatchTiles sei = btiles(b, b->se_int, b->h_se_int, b->tune.sensor_ctas_per_sm);
   const BatchTiles seg = btiles(b, b->se_gen, b->h_se_gen, 1);
+  // general tiles beside the interior launches (side stream) or on the batch's stream
+  const SideStream gside = b->tune.general_serial ? SideStream{nullptr, nullptr, nullptr} : b->side;
   auto sensor = [&](bool rfilter) -> int {
     BATCH_CUDA(b, launch_sensor_batch(b->sens_argv[bin], b->a0_sens[bin], sei, seg, b->maps, bin, b->zrows, b->nzrows,
-                                      b->zthreads, b->zsmem, rfilter, b->n, b->max_pts, b->side, b->stream));
+                                      b->zthreads, b->zsmem, rfilter, b->n, b->max_pts, gside, b->stream));
     return AXJ_OK;
   };
   if (lrn) {
@@ -2476,12 +2478,12 @@ int batch_stage(axj_batch* b, int bin, int bout, int stage, bool judge) {
   } else if (b->sc) {
     // the plain sensor: sensor tiles, then the fused z/r filter into the coefficient planes
     BATCH_CUDA(b, launch_sensor_batch(b->sens_argv[bin], b->a0_sens[bin], sei, seg, b->maps, bin, nullptr, 0,
-                                      b->zthreads, b->zsmem, false, b->n, b->max_pts, b->side, b->stream));
+                                      b->zthreads, b->zsmem, false, b->n, b->max_pts, gside, b->stream));
     BATCH_CUDA(b, launch_zr_batch(b->zr_argv, b->zr_items, b->nzr_items, b->maps, bin, b->mixed, buf_f32(bin),
                                   b->stream));
   }
   const int L = lrn ? CM_LRN : (b->sc ? CM_PRE : CM_FILT);
-  BATCH_CUDA(b, launch_stage_batch(b->stage_argv[L][stage], b->a0_stage[L][stage], sti, stg, b->maps, bin, b->side,
+  BATCH_CUDA(b, launch_stage_batch(b->stage_argv[L][stage], b->a0_stage[L][stage], sti, stg, b->maps, bin, gside,
                                    b->stream, rows));
   return AXJ_OK;
 }
@@ -2745,6 +2747,8 @@ void axj_batch_default_tuning(axj_batch_tuning* t) {
   t->stage_ctas_per_sm = 2;
   t->sensor_ctas_per_sm = 4;
   t->stage_rows = TR;
+  t->general_ctas_per_sm = 1;
+  t->general_serial = 0;
 }
 
 int axj_batch_create(axj_handle* const* handles, int64_t n, axj_batch** out) {
@@ -2815,7 +2819,8 @@ int axj_batch_create(axj_handle* const* handles, int64_t n, axj_batch** out) {
 int axj_batch_set_tuning(axj_batch* b, const axj_batch_tuning* t) {
   if (!b || !t) return bfail(b, AXJ_ERR_ARG, "null argument");
   if (t->tile_order < 0 || t->tile_order > 1 || t->stage_ctas_per_sm < 1 || t->stage_ctas_per_sm > 8 ||
-      t->sensor_ctas_per_sm < 1 || t->sensor_ctas_per_sm > 8 || (t->stage_rows != TR && t->stage_rows != TR / 2))
+      t->sensor_ctas_per_sm < 1 || t->sensor_ctas_per_sm > 8 || (t->stage_rows != TR && t->stage_rows != TR / 2) ||
+      t->general_ctas_per_sm < 0 || t->general_ctas_per_sm > 2 || t->general_serial < 0 || t->general_serial > 1)
     return bfail(b, AXJ_ERR_ARG, "tuning out of range");
   BATCH_CUDA(b, cudaSetDevice(b->device));
   BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
@@ -2896,10 +2901,11 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
   double best = 1e300;
   axj_batch_tuning best_t = b->tune;
   int k = 0;
-  for (const axj_batch_tuning& t : cands) {
+  // one trial: set t, warm up (captures the graphs), time, undo the steps
+  auto trial = [&](const axj_batch_tuning& t) -> int {
     int rc = axj_batch_set_tuning(b, &t);
     double ms = 0.0;
-    if (rc == AXJ_OK) rc = axj_batch_run(b, 1);  // warm-up (captures the graphs)
+    if (rc == AXJ_OK) rc = axj_batch_run(b, 1);
     if (rc == AXJ_OK) rc = axj_batch_run_timed(b, steps_per_trial, &ms);
     if (rc != AXJ_OK) {
       batch_restore(b, save);
@@ -2912,7 +2918,18 @@ int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* 
       best_t = t;
     }
     if (int r2 = batch_restore(b, save)) return r2;
-    if (int r3 = batch_save(b, save)) return r3;
+    return batch_save(b, save);
+  };
+  for (const axj_batch_tuning& t : cands)
+    if (int rc = trial(t)) return rc;
+  // then the fastest with the general stage tiles at two CTAs per SM and / or on the
+  // batch's stream after the interior tiles
+  const axj_batch_tuning main_best = best_t;
+  for (int g = 1; g < 4; ++g) {
+    axj_batch_tuning t = main_best;
+    t.general_ctas_per_sm = (g & 1) ? 2 : 1;
+    t.general_serial = (g & 2) ? 1 : 0;
+    if (int rc = trial(t)) return rc;
   }
   for (void* p : save.u0) cudaFree(p);
   save.u0.clear();

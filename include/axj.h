@@ -324,7 +324,10 @@ typedef struct axj_batch_tuning {
   int64_t stage_ctas_per_sm;   /* persistent CTAs per SM of the interior stage kernel (2) */
   int64_t sensor_ctas_per_sm;  /* persistent CTAs per SM of the interior sensor kernel (4) */
   int64_t stage_rows;          /* rows of the interior stage tiles' CTAs: 16 (32 x 16 tiles, default) or 8 */
-  int64_t reserved[4];
+  int64_t general_ctas_per_sm; /* persistent CTAs per SM of the general stage kernel: 1 (default; 0 = 1) or 2 */
+  int64_t general_serial;      /* 0: general tiles on a side stream beside the interior launches (default);
+                                  1: on the batch's stream with them */
+  int64_t reserved[2];
 } axj_batch_tuning;
 
 void axj_batch_default_tuning(axj_batch_tuning* t);
@@ -336,9 +339,10 @@ int axj_batch_run_timed(axj_batch* b, int64_t nsteps, double* ms);
 int axj_batch_set_tuning(axj_batch* b, const axj_batch_tuning* t);
 int axj_batch_get_tuning(axj_batch* b, axj_batch_tuning* t);
 /* Autotuner: times steps_per_trial batch steps for every candidate tuning (tile order x
- * interior stage tile shape 32 x 16 or 32 x 8 with its CTAs per SM x sensor CTAs per SM),
- * keeps the fastest and returns it in *chosen; trial_ms (nullable, room for 16) receives
- * each trial's time. The trial steps are undone: the instances' solutions,
+ * interior stage tile shape 32 x 16 or 32 x 8 with its CTAs per SM x sensor CTAs per SM:
+ * 16 trials), then, from the fastest, the general tiles' CTAs per SM and stream (3 more
+ * trials); keeps the fastest and returns it in *chosen; trial_ms (nullable, room for 19)
+ * receives each trial's time. The trial steps are undone: the instances' solutions,
  * times and iteration counters are restored (the learned sensor re-judges). */
 int axj_batch_autotune(axj_batch* b, int64_t steps_per_trial, axj_batch_tuning* chosen, double* trial_ms,
                        int64_t* ntrials);

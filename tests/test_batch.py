@@ -57,15 +57,16 @@ MODES = {
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode", list(MODES))
-@pytest.mark.parametrize("order,rows", [(0, 16), (1, 16), (0, 8), (1, 8)])
-def test_batch_equals_individual_runs(mode, order, rows):
+@pytest.mark.parametrize("order,rows,gen_ctas,gen_serial", [(0, 16, 1, 0), (1, 16, 2, 1), (0, 8, 2, 0), (1, 8, 1, 1)])
+def test_batch_equals_individual_runs(mode, order, rows, gen_ctas, gen_serial):
     kw = MODES[mode]
     cases = fixtures.batch_instances(3, seed=5, **SMALL, **kw)
     model = _model(cases) if mode == "mixed_learned" else None
     single = _solvers(cases, model)
     batched = _solvers(cases, model)
     b = axj.AxjBatch(batched)
-    b.set_tuning(tile_order=order, stage_ctas_per_sm=(1 + order) * (16 // rows), stage_rows=rows)
+    b.set_tuning(tile_order=order, stage_ctas_per_sm=(1 + order) * (16 // rows), stage_rows=rows,
+                 general_ctas_per_sm=gen_ctas, general_serial=gen_serial)
     steps = 7
     b.run(steps)
     for s in single:
@@ -90,7 +91,7 @@ def test_autotune_undoes_its_trials():
     ref = _solvers(cases, model)
     b = axj.AxjBatch(batched)
     chosen, trials = b.autotune(steps_per_trial=2)
-    assert len(trials) == 16 and all(t > 0 for t in trials)
+    assert len(trials) == 19 and all(t > 0 for t in trials)
     assert b.tuning() == chosen
     b.run(3)
     for s in ref:
