@@ -263,6 +263,7 @@ SensorArgs sensor_args(axj_handle* h, int b) {
   SensorArgs s;
   s.g = grid_of(h);
   s.U = buf_f32(b) ? nullptr : static_cast<const double*>(buf_ptr(h, b));
+  s.Uf = buf_f32(b) ? static_cast<const float*>(buf_ptr(h, b)) : nullptr;
   s.mv_int = &h->map_sens[b][0];
   s.mv_gen = &h->map_sens[b][1];
   s.mt_int = &h->map_sensT[b][0];

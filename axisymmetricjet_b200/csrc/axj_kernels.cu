@@ -1053,20 +1053,26 @@ struct SensSmem {
   static constexpr int DZ = TZ + 2 * HF;      // z-arm of the second derivatives: [TR][DZ]
   static constexpr int DR = TR + 2 * HF;      // r-arm: [DR][TZ]
   // byte offsets (every TMA destination 128-byte aligned): V_r, V_z [VR][VZ] each;
-  // T [SR][SZ] (TMA); S and dil [SR][SZ]; rho on the tile [TR][TZ] (TMA); arms; f_sw;
-  // descriptors. V, T, rho are in the stage-input type, the rest in the stencil type.
+  // T [SR][SZ] (TMA); S and dil [SR][SZ]; general tiles only: rho on the tile [TR][TZ]
+  // (TMA), arms, f_sw, descriptors. V, T, rho are in the stage-input type, the rest in
+  // the stencil type. Interior tiles read rho into registers and keep f_sw in the V_r
+  // box once the strain rates are formed.
   static constexpr size_t oVr = 0;
   static constexpr size_t oVz = align128(sizeof(SIN) * NV);
   static constexpr size_t oT = align128(oVz + sizeof(SIN) * NV);
   static constexpr size_t oS = align128(oT + sizeof(SIN) * NS);
   static constexpr size_t oD = align128(oS + sizeof(R) * NS);
   static constexpr size_t oRho = align128(oD + sizeof(R) * NS);
-  static constexpr size_t oD2 = align128(oRho + sizeof(SIN) * TR * TZ);
+  __host__ __device__ static constexpr size_t oD2(bool gen) {
+    return gen ? align128(oRho + sizeof(SIN) * TR * TZ) : oRho;
+  }
   // the arms exist only in general tiles (interior tiles use the composite 9-point row)
   __host__ __device__ static constexpr size_t oFsw(bool gen) {
-    return oD2 + (gen ? sizeof(R) * (TR * DZ + DR * TZ) : 0);
+    return oD2(gen) + (gen ? sizeof(R) * (TR * DZ + DR * TZ) : 0);
   }
-  __host__ __device__ static constexpr size_t oDesc(bool gen) { return align128(oFsw(gen) + sizeof(R) * TR * TZ); }
+  __host__ __device__ static constexpr size_t oDesc(bool gen) {
+    return align128(oFsw(gen) + (gen ? sizeof(R) * TR * TZ : 0));
+  }
   // metrics of the S region: dxidz on its columns [SZ], detadr and 1/r on its rows
   // [2][SR]; deltaz, deltar on the tile [TZ] + [TR]
   __host__ __device__ static constexpr size_t oMet(bool gen) {
@@ -1074,7 +1080,9 @@ struct SensSmem {
   }
   static constexpr int NMET = SZ + 2 * SR + TZ + TR;
   __host__ __device__ static constexpr size_t bytes(bool gen) { return align128(oMet(gen) + sizeof(double) * NMET); }
-  static constexpr uint32_t tx_bytes = sizeof(SIN) * (2 * NV + NS + TR * TZ);
+  __host__ __device__ static constexpr uint32_t tx_bytes(bool gen) {
+    return sizeof(SIN) * (2 * NV + NS + (gen ? TR * TZ : 0));
+  }
 };
 
 // Threads of a sensor tile CTA: general tiles (one CTA per SM, bound by shared memory)
@@ -1143,9 +1151,10 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   R* sS = reinterpret_cast<R*>(smem_raw + SM::oS);         // [SR][SZ]
   R* sD = reinterpret_cast<R*>(smem_raw + SM::oD);         // [SR][SZ]
   SIN* sRho = reinterpret_cast<SIN*>(smem_raw + SM::oRho); // [TR][TZ]
-  R* sd2z = reinterpret_cast<R*>(smem_raw + SM::oD2);      // [TR][DZ] (general tiles)
+  R* sd2z = reinterpret_cast<R*>(smem_raw + SM::oD2(GEN)); // [TR][DZ] (general tiles)
   R* sd2r = sd2z + TR * DZ;                                 // [DR][TZ] (general tiles)
-  R* sFsw = reinterpret_cast<R*>(smem_raw + SM::oFsw(GEN)); // [TR][TZ]
+  // f_sw [TR][TZ]: its own buffer (general tiles), the V_r box after phase 2 (interior)
+  R* sFsw = reinterpret_cast<R*>(smem_raw + (GEN ? SM::oFsw(GEN) : SM::oVr));
   uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
   double* sMz = reinterpret_cast<double*>(smem_raw + SM::oMet(GEN));  // dxidz, column i0 - HSZ + k
   double* sMr = sMz + SZ;                                               // detadr, row j0 - HS + k
@@ -1172,11 +1181,26 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   __syncthreads();
   if (tid == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&bar, SM::tx_bytes);
+    mbar_expect_tx(&bar, SM::tx_bytes(GEN));
     tma_load_3d(sVr, mV, i0 - HVZ, j0 - HV, 1, &bar);
     tma_load_3d(sVz, mV, i0 - HVZ, j0 - HV, 3, &bar);
     tma_load_3d(sT, mT, i0 - HSZ, j0 - HS, 4, &bar);
-    tma_load_3d(sRho, mRho, i0, j0, 0, &bar);
+    if (GEN) tma_load_3d(sRho, mRho, i0, j0, 0, &bar);
+  }
+  // interior tiles: rho of the thread's 2 x 2 block of phase 3 (rows r, r + 1, columns
+  // c, c + 1) into registers now, from the stage input (the tile lies inside the grid)
+  SIN rho_pf[2][2];
+  if constexpr (!GEN) {
+    const int r = 2 * (tid / (TZ / 2)), c = 2 * (tid - (tid / (TZ / 2)) * (TZ / 2));
+    const SIN* rho0 = std::is_same<SIN, float>::value ? reinterpret_cast<const SIN*>(a.Uf)
+                                                       : reinterpret_cast<const SIN*>(a.U);
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+      const typename Pair2<SIN>::t v =
+          __ldg(reinterpret_cast<const typename Pair2<SIN>::t*>(rho0 + (long long)(j0 + r + w) * g.P + (i0 + c)));
+      rho_pf[w][0] = v.x;
+      rho_pf[w][1] = v.y;
+    }
   }
   if (GEN) {
     for (int idx = tid; idx < NV; idx += NT) {
@@ -1208,6 +1232,8 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   }
   phase ^= 1u;
 
+  R fkeep[2][2][2];     // interior tiles: f_sw of the thread's (up to two) blocks
+  int fidx[2] = {-1, -1};  // their first point in the [TR][TZ] f_sw layout (-1: none)
   // ---- phase 2: S and dilatation on the cross of the S region (reach HS either way);
   // f_sw on the tile. Interior tiles: 2 x 2 blocks of S points (rows sr, sr + 1, columns
   // sz, sz + 1; sr, sz even) over the z arm (the tile rows, TZ + 2 HS columns) and the r
@@ -1224,7 +1250,11 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     constexpr int NZB = (TR / 2) * ZBW;           // z-arm blocks
     constexpr int NRB = HS * (TZ / 2);            // r-arm blocks (2 HS rows, in pairs)
     const R k0 = tabv<R, 1>(4, 0), k1 = tabv<R, 1>(4, 1), k3 = tabv<R, 1>(4, 3), k4 = tabv<R, 1>(4, 4);
-    for (int bq = tid; bq < NZB + NRB; bq += NT) {
+    static_assert(NZB + NRB <= 2 * NT, "two blocks per thread at most");
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int bq = tid + u * NT;
+      if (bq >= NZB + NRB) break;
       int sr, sz;
       if (bq < NZB) {
         const int br = bq / ZBW;
@@ -1322,7 +1352,9 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
             const R vort = fabs(dVrdz - dVzdr);
             const R Hm = (R(-1.0) * d < R(0)) ? R(0) : R(1);
             const R eps = R((double)1e-15f);  // single-precision literal of the reference (:202)
-            sFsw[(sr + w - HS) * TZ + (sz + h - HSZ)] = Hm * (d * d) / (d * d + vort * vort + eps);
+            // kept in registers: the V_r box that holds f_sw is still being read
+            fkeep[u][w][h] = Hm * (d * d) / (d * d + vort * vort + eps);
+            fidx[u] = (sr - HS) * TZ + (sz - HSZ);
           }
         }
         st_pair(sS + (sr + w) * SZ + sz, S[0], S[1]);
@@ -1367,6 +1399,16 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     sD[idx] = dil;
   }
   __syncthreads();
+  if constexpr (!GEN) {
+    // every thread is done with the V boxes: f_sw into the V_r box
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (fidx[u] < 0) continue;
+#pragma unroll
+      for (int w = 0; w < 2; ++w) st_pair(sFsw + fidx[u] + w * TZ, fkeep[u][w][0], fkeep[u][w][1]);
+    }
+    __syncthreads();
+  }
 
   // ---- phases 3-4 per field: fourth derivatives at the tile points (kept in registers:
   // 2 points per thread). Interior tiles: SBP2 of SBP2 with the centred row both times is
@@ -1458,10 +1500,8 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
       dzp[1] = R(a1);
 #pragma unroll
       for (int w = 0; w < 2; ++w) {
-        SIN r0, r1;
-        ld_pair(sRho + (r + w) * TZ + c, r0, r1);
-        rho[w][0] = R(r0);
-        rho[w][1] = R(r1);
+        rho[w][0] = R(rho_pf[w][0]);
+        rho[w][1] = R(rho_pf[w][1]);
         ld_pair(sFsw + (r + w) * TZ + c, fsw[w][0], fsw[w][1]);
       }
     }
@@ -1565,7 +1605,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
 }
 
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 4)
+__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 5)
     sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mV,
                        const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
   extern __shared__ __align__(128) unsigned char smem_raw[];

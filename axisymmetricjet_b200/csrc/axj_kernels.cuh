@@ -93,7 +93,8 @@ struct DtArgs {
 // Shock-capturing sensor chain (ModShockCapturing.f90:5-106).
 struct SensorArgs {
   Grid g;
-  const double* U;       // stage input state
+  const double* U;       // stage input state (FP64 inputs; else null)
+  const float* Uf;       // stage input state (FP32 inputs; else null)
   const uint32_t* desc;
   const double* dxidz;
   const double* detadr;
