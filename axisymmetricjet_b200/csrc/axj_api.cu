@@ -1472,7 +1472,7 @@ int axj_create(const axj_params* prm, int64_t Nz, int64_t Nr, const double* zvec
   h->flags = dalloc<int>(h, 1, &rc);
 
   h->counter = dalloc<unsigned int>(h, 1, &rc);
-  h->dt_blocks = 148 * 4;
+  h->dt_blocks = dt_grid_blocks();
   h->partial = dalloc<double>(h, h->dt_blocks, &rc);
   h->tiles_int = dalloc<int2>(h, std::max<size_t>(tint.size(), 1), &rc);
   h->tiles_gen = dalloc<int2>(h, std::max<size_t>(tgen.size(), 1), &rc);

@@ -1006,6 +1006,17 @@ cudaError_t launch_harmonic_phase(const double* time, const double* dt, double o
   return cudaGetLastError();
 }
 
+// Blocks of the dt kernel for the current device: as many as are resident at once (one
+// wave, every SM full), so that every thread's loads are in flight together.
+int dt_grid_blocks() {
+  int dev = 0, nsm = 148, per_sm = 4;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dt_kernel, DT_THREADS, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 4;
+  return nsm * per_sm;
+}
+
 cudaError_t launch_dt(const DtArgs& a, int nblocks, cudaStream_t s) {
   dt_kernel<<<nblocks, DT_THREADS, 0, s>>>(a);
   return cudaGetLastError();

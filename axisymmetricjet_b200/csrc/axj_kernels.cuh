@@ -151,6 +151,7 @@ void stage_boxes(bool gen, bool mixed, int* halo_w, int* halo_h, int* q_h, int* 
 // V_r / V_z box vw x vh, temperature box tw x th (rho uses the stage tile box).
 void sensor_boxes(bool gen, bool mixed, int* vw, int* vh, int* tw, int* th);
 cudaError_t launch_dt(const DtArgs& a, int nblocks, cudaStream_t s);
+int dt_grid_blocks();
 // cos(omega t_s) of the harmonic forcing: rhs_mode != 0: out[0] at t = *time; else
 // out[s], s = 1..4, at t_s = (*time - *dt) + c_s * *dt (the device time is t_n + dt).
 cudaError_t launch_harmonic_phase(const double* time, const double* dt, double omega, int rhs_mode, double* out,
