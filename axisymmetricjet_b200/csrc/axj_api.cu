@@ -116,7 +116,6 @@ struct axj_handle {
   CUtensorMap map_u0_tile, map_acc_tile, map_b_tile;
   CUtensorMap map_sens[5][2];  // sensor V boxes of the stage buffers x {interior, general}
   CUtensorMap map_sensT[5][2]; // sensor temperature boxes
-  CUtensorMap map_rho[5];      // density tile boxes
   // fused z/r filter: Q blocks, z and r code blocks, temperature blocks of the stage
   // buffers; the coefficient planes it writes, as boxes of the two tile classes
   CUtensorMap map_zrQ, map_zrZc, map_zrRc, map_zrT[5];
@@ -268,7 +267,6 @@ SensorArgs sensor_args(axj_handle* h, int b) {
   s.mv_gen = &h->map_sens[b][1];
   s.mt_int = &h->map_sensT[b][0];
   s.mt_gen = &h->map_sensT[b][1];
-  s.mrho = &h->map_rho[b];
   s.desc = h->desc;
   s.dxidz = h->dxidz;
   s.detadr = h->detadr;
@@ -446,10 +444,6 @@ int build_maps(axj_handle* h) {
   }
   int hw, hh, qh, tw, th;
   stage_boxes(false, h->mixed, &hw, &hh, &qh, &tw, &th, nullptr);
-  for (int b = 0; b < nb; ++b) {
-    int rc = make_map(h, &h->map_rho[b], buf_ptr(h, b), 5, tw, th, 1, buf_f32(b));
-    if (rc != AXJ_OK) return rc;
-  }
   int rc = make_map(h, &h->map_u0_tile, h->U0, 5, tw, th, 5);
   if (rc != AXJ_OK) return rc;
   rc = make_map(h, &h->map_b_tile, h->B, 5, tw, th, 5);
@@ -2601,7 +2595,6 @@ int batch_build_tables(axj_batch* b) {
       m[bmap_coef(1)] = h->map_coef[1];
       m[bmap_coef(2)] = h->map_coefH;
     }
-    for (int bf = 0; bf < NBUF; ++bf) m[bmap_rho(bf)] = h->map_rho[bf < nb ? bf : 0];
   }
   {
     void* p = nullptr;

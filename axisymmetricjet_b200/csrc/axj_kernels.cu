@@ -1064,26 +1064,19 @@ struct SensSmem {
   static constexpr int DZ = TZ + 2 * HF;      // z-arm of the second derivatives: [TR][DZ]
   static constexpr int DR = TR + 2 * HF;      // r-arm: [DR][TZ]
   // byte offsets (every TMA destination 128-byte aligned): V_r, V_z [VR][VZ] each;
-  // T [SR][SZ] (TMA); S and dil [SR][SZ]; general tiles only: rho on the tile [TR][TZ]
-  // (TMA), arms, f_sw, descriptors. V, T, rho are in the stage-input type, the rest in
-  // the stencil type. Interior tiles read rho into registers and keep f_sw in the V_r
-  // box once the strain rates are formed.
+  // T [SR][SZ] (TMA); S and dil [SR][SZ]; general tiles: descriptors [VR][VZ]. V and T
+  // are in the stage-input type, the rest in the stencil type. Once phase 2 has formed the
+  // strain rates the V boxes are spent: f_sw [TR][TZ] then lives in the V_r box (interior
+  // tiles) or the V_z box (general tiles), and the general tiles' second derivatives on the
+  // arms ([TR][DZ] + [DR][TZ]) in the V_r box. rho is read from the stage input.
   static constexpr size_t oVr = 0;
   static constexpr size_t oVz = align128(sizeof(SIN) * NV);
   static constexpr size_t oT = align128(oVz + sizeof(SIN) * NV);
   static constexpr size_t oS = align128(oT + sizeof(SIN) * NS);
   static constexpr size_t oD = align128(oS + sizeof(R) * NS);
-  static constexpr size_t oRho = align128(oD + sizeof(R) * NS);
-  __host__ __device__ static constexpr size_t oD2(bool gen) {
-    return gen ? align128(oRho + sizeof(SIN) * TR * TZ) : oRho;
-  }
-  // the arms exist only in general tiles (interior tiles use the composite 9-point row)
-  __host__ __device__ static constexpr size_t oFsw(bool gen) {
-    return oD2(gen) + (gen ? sizeof(R) * (TR * DZ + DR * TZ) : 0);
-  }
-  __host__ __device__ static constexpr size_t oDesc(bool gen) {
-    return align128(oFsw(gen) + (gen ? sizeof(R) * TR * TZ : 0));
-  }
+  static_assert(sizeof(R) * (TR * DZ + DR * TZ) <= sizeof(SIN) * NV && sizeof(R) * TR * TZ <= sizeof(SIN) * NV,
+                "the arms and f_sw fit in a spent V box");
+  __host__ __device__ static constexpr size_t oDesc(bool gen) { return align128(oD + sizeof(R) * NS); }
   // metrics of the S region: dxidz on its columns [SZ], detadr and 1/r on its rows
   // [2][SR]; deltaz, deltar on the tile [TZ] + [TR]
   __host__ __device__ static constexpr size_t oMet(bool gen) {
@@ -1091,9 +1084,7 @@ struct SensSmem {
   }
   static constexpr int NMET = SZ + 2 * SR + TZ + TR;
   __host__ __device__ static constexpr size_t bytes(bool gen) { return align128(oMet(gen) + sizeof(double) * NMET); }
-  __host__ __device__ static constexpr uint32_t tx_bytes(bool gen) {
-    return sizeof(SIN) * (2 * NV + NS + (gen ? TR * TZ : 0));
-  }
+  static constexpr uint32_t tx_bytes = sizeof(SIN) * (2 * NV + NS);
 };
 
 // Threads of a sensor tile CTA: general tiles (one CTA per SM, bound by shared memory)
@@ -1150,7 +1141,7 @@ __device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
 // One sensor tile (i0, j0); false if a bounded wait gave up.
 template <int HS, int HF, bool GEN, typename SIN, typename R>
 __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0, const CUtensorMap* mV,
-                                            const CUtensorMap* mT, const CUtensorMap* mRho, unsigned char* smem_raw,
+                                            const CUtensorMap* mT, unsigned char* smem_raw,
                                             uint64_t& bar, uint32_t& phase) {
   using SM = SensSmem<HS, HF, SIN, R>;
   constexpr int NT = sens_threads(GEN);
@@ -1161,11 +1152,12 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   SIN* sT = reinterpret_cast<SIN*>(smem_raw + SM::oT);     // [SR][SZ]
   R* sS = reinterpret_cast<R*>(smem_raw + SM::oS);         // [SR][SZ]
   R* sD = reinterpret_cast<R*>(smem_raw + SM::oD);         // [SR][SZ]
-  SIN* sRho = reinterpret_cast<SIN*>(smem_raw + SM::oRho); // [TR][TZ]
-  R* sd2z = reinterpret_cast<R*>(smem_raw + SM::oD2(GEN)); // [TR][DZ] (general tiles)
-  R* sd2r = sd2z + TR * DZ;                                 // [DR][TZ] (general tiles)
-  // f_sw [TR][TZ]: its own buffer (general tiles), the V_r box after phase 2 (interior)
-  R* sFsw = reinterpret_cast<R*>(smem_raw + (GEN ? SM::oFsw(GEN) : SM::oVr));
+  R* sd2z = reinterpret_cast<R*>(smem_raw + SM::oVr);      // [TR][DZ] (general tiles, phase 3)
+  R* sd2r = sd2z + TR * DZ;                                 // [DR][TZ] (general tiles, phase 3)
+  // f_sw [TR][TZ] in a spent V box (after phase 2): V_z (general tiles) or V_r (interior)
+  R* sFsw = reinterpret_cast<R*>(smem_raw + (GEN ? SM::oVz : SM::oVr));
+  const SIN* rho0 = std::is_same<SIN, float>::value ? reinterpret_cast<const SIN*>(a.Uf)
+                                                     : reinterpret_cast<const SIN*>(a.U);  // rho plane
   uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
   double* sMz = reinterpret_cast<double*>(smem_raw + SM::oMet(GEN));  // dxidz, column i0 - HSZ + k
   double* sMr = sMz + SZ;                                               // detadr, row j0 - HS + k
@@ -1192,19 +1184,16 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   __syncthreads();
   if (tid == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&bar, SM::tx_bytes(GEN));
+    mbar_expect_tx(&bar, SM::tx_bytes);
     tma_load_3d(sVr, mV, i0 - HVZ, j0 - HV, 1, &bar);
     tma_load_3d(sVz, mV, i0 - HVZ, j0 - HV, 3, &bar);
     tma_load_3d(sT, mT, i0 - HSZ, j0 - HS, 4, &bar);
-    if (GEN) tma_load_3d(sRho, mRho, i0, j0, 0, &bar);
   }
   // interior tiles: rho of the thread's 2 x 2 block of phase 3 (rows r, r + 1, columns
   // c, c + 1) into registers now, from the stage input (the tile lies inside the grid)
   SIN rho_pf[2][2];
   if constexpr (!GEN) {
     const int r = 2 * (tid / (TZ / 2)), c = 2 * (tid - (tid / (TZ / 2)) * (TZ / 2));
-    const SIN* rho0 = std::is_same<SIN, float>::value ? reinterpret_cast<const SIN*>(a.Uf)
-                                                       : reinterpret_cast<const SIN*>(a.U);
 #pragma unroll
     for (int w = 0; w < 2; ++w) {
       const typename Pair2<SIN>::t v =
@@ -1245,6 +1234,11 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
 
   R fkeep[2][2][2];     // interior tiles: f_sw of the thread's (up to two) blocks
   int fidx[2] = {-1, -1};  // their first point in the [TR][TZ] f_sw layout (-1: none)
+  constexpr int NSIT = (NS + NT - 1) / NT;  // general tiles: S points per thread
+  R fkg[GEN ? NSIT : 1];                    // general tiles: f_sw of the thread's tile points
+  int fig[GEN ? NSIT : 1];                  // their index in the f_sw layout (-1: none)
+#pragma unroll
+  for (int u = 0; u < (GEN ? NSIT : 1); ++u) fig[u] = -1;
   // ---- phase 2: S and dilatation on the cross of the S region (reach HS either way);
   // f_sw on the tile. Interior tiles: 2 x 2 blocks of S points (rows sr, sr + 1, columns
   // sz, sz + 1; sr, sz even) over the z arm (the tile rows, TZ + 2 HS columns) and the r
@@ -1372,8 +1366,11 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
         st_pair(sD + (sr + w) * SZ + sz, dil[0], dil[1]);
       }
     }
-  } else
-  for (int idx = tid; idx < NS; idx += NT) {
+  } else {
+#pragma unroll
+  for (int u = 0; u < NSIT; ++u) {
+    const int idx = tid + u * NT;
+    if (idx >= NS) break;
     const int sr = idx / SZ, sz = idx - sr * SZ;
     const bool zarm = sr >= HS && sr < HS + TR && sz >= HSZ - HS && sz < HSZ + TZ + HS;
     const bool rarm = sz >= HSZ && sz < HSZ + TZ;
@@ -1403,13 +1400,23 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
         const R vort = fabs(dVrdz - dVzdr);
         const R Hm = (R(-1.0) * dil < R(0)) ? R(0) : R(1);
         const R eps = R((double)1e-15f);  // single-precision literal of the reference (:202)
-        sFsw[(sr - HS) * TZ + (sz - HSZ)] = Hm * (dil * dil) / (dil * dil + vort * vort + eps);
+        // kept in registers: the V_z box that holds f_sw is still being read
+        fkg[u] = Hm * (dil * dil) / (dil * dil + vort * vort + eps);
+        fig[u] = (sr - HS) * TZ + (sz - HSZ);
       }
     }
     sS[idx] = S;
     sD[idx] = dil;
   }
+  }
   __syncthreads();
+  if constexpr (GEN) {
+    // every thread is done with the V boxes: f_sw into the V_z box
+#pragma unroll
+    for (int u = 0; u < NSIT; ++u)
+      if (fig[u] >= 0) sFsw[fig[u]] = fkg[u];
+    __syncthreads();
+  }
   if constexpr (!GEN) {
     // every thread is done with the V boxes: f_sw into the V_r box
 #pragma unroll
@@ -1604,7 +1611,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
     if (!inside(i, j) || r >= nrow) continue;
     const long long o = (long long)j * g.P + i;
     const R dz = R(sDzv[c]), dr = R(sDrv[r]);
-    const R rho = R(sRho[r * TZ + c]);
+    const R rho = R(rho0[o]);
     const R T = R(sT[(HS + r) * SZ + HSZ + c]);
     const R fsw = sFsw[r * TZ + c];
     a.Q[o] = double(rho * fabs((d4z[0][q] * (dz * dz) + d4r[0][q] * (dr * dr))));
@@ -1616,9 +1623,9 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
 }
 
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 5)
+__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 2 : 5)
     sensor_tile_kernel(const SensorArgs a, const int2* __restrict__ tiles, const __grid_constant__ CUtensorMap mV,
-                       const __grid_constant__ CUtensorMap mT, const __grid_constant__ CUtensorMap mRho) {
+                       const __grid_constant__ CUtensorMap mT) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar;
   if (threadIdx.x == 0) {
@@ -1627,13 +1634,13 @@ __global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 5)
   }
   uint32_t phase = 0;
   const int2 t0 = tiles[blockIdx.x];
-  sensor_body<HS, HF, GEN, SIN, R>(a, t0.x, t0.y, &mV, &mT, &mRho, smem_raw, bar, phase);
+  sensor_body<HS, HF, GEN, SIN, R>(a, t0.x, t0.y, &mV, &mT, smem_raw, bar, phase);
 }
 
 // Batched form: persistent loop over (i0, j0, instance) tiles; kmaps = indices of the
-// V, T and rho maps in each instance's block of nmaps maps.
+// V and T maps in each instance's block of nmaps maps.
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 4)
+__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 5)
     sensor_tile_kernel_batch(const SensorArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
                              const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1652,7 +1659,7 @@ __global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 4)
       reinterpret_cast<unsigned long long*>(&sa)[k] = reinterpret_cast<const unsigned long long*>(argv + tt.z)[k];
     __syncthreads();
     const CUtensorMap* m = mapv + (size_t)tt.z * nmaps;
-    if (!sensor_body<HS, HF, GEN, SIN, R>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, m + kmaps.z, smem_raw, bar, phase))
+    if (!sensor_body<HS, HF, GEN, SIN, R>(sa, tt.x, tt.y, m + kmaps.x, m + kmaps.y, smem_raw, bar, phase))
       return;
   }
 }
@@ -1739,10 +1746,10 @@ static void launch_sensor_tiles(const SensorArgs& a, const SideStream& side, cud
   if (a.ntiles_gen > 0)
     sensor_tile_kernel<SENS_HS_GEN, H_GEN, true, SIN, R><<<a.ntiles_gen, sens_threads(true), SG::bytes(true),
                                                            side.stream ? side.stream : s>>>(a, a.tiles_gen, *a.mv_gen,
-                                                                                            *a.mt_gen, *a.mrho);
+                                                                                            *a.mt_gen);
   if (a.ntiles_int > 0)
     sensor_tile_kernel<SENS_HS_INT, H_INT, false, SIN, R>
-        <<<a.ntiles_int, sens_threads(false), SI::bytes(false), s>>>(a, a.tiles_int, *a.mv_int, *a.mt_int, *a.mrho);
+        <<<a.ntiles_int, sens_threads(false), SI::bytes(false), s>>>(a, a.tiles_int, *a.mv_int, *a.mt_int);
 }
 
 __global__ void sensor_rfilter_kernel(const SensorArgs a) {
@@ -2563,10 +2570,10 @@ static void launch_sensor_tiles_batch(const SensorArgs* argv, const BatchTiles& 
   if (tgen.ntiles > 0)
     sensor_tile_kernel_batch<SENS_HS_GEN, H_GEN, true, SIN, R>
         <<<tgen.grid, sens_threads(true), SG::bytes(true), side.stream ? side.stream : s>>>(
-            argv, tgen.tiles, tgen.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 1), bmap_sensT(kin, 1), bmap_rho(kin), 0));
+            argv, tgen.tiles, tgen.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 1), bmap_sensT(kin, 1), 0, 0));
   if (tint.ntiles > 0)
     sensor_tile_kernel_batch<SENS_HS_INT, H_INT, false, SIN, R><<<tint.grid, sens_threads(false), SI::bytes(false), s>>>(
-        argv, tint.tiles, tint.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 0), bmap_sensT(kin, 0), bmap_rho(kin), 0));
+        argv, tint.tiles, tint.ntiles, mapv, NM_BATCH, make_int4(bmap_sens(kin, 0), bmap_sensT(kin, 0), 0, 0));
 }
 
 cudaError_t launch_sensor_batch(const SensorArgs* argv, const SensorArgs& a0, const BatchTiles& tint,

@@ -110,8 +110,7 @@ struct SensorArgs {
   const CUtensorMap* mv_int;   // TMA maps of the stage input for the two sensor tile classes:
   const CUtensorMap* mv_gen;   //   V_r / V_z boxes,
   const CUtensorMap* mt_int;   //   temperature boxes,
-  const CUtensorMap* mt_gen;
-  const CUtensorMap* mrho;     //   and the density tile box
+  const CUtensorMap* mt_gen;   // (rho is read from the stage input: U / Uf)
   const unsigned char* zcode;  // z stencil code per point (9 = blanked), pitch P
   int* flags;
   double* Q;             // 3 planes: mustarQuantity, betastarQuantity, kappastarQuantity
@@ -214,24 +213,22 @@ constexpr int DT_THREADS = 256;
 //   pv_old tile box, running-sum tile box:         14, 15
 //   sensor V box of buffer b, class cls:           16 + b * 2 + cls  (16..25)
 //   sensor temperature box of buffer b, class cls: 26 + b * 2 + cls  (26..35)
-//   density tile box of buffer b:                  36 + b            (36..40)
-//   interior half tiles (TR / 2 rows): state box of buffer b 41 + b (41..45), z-filtered
-//   coefficient box 46, final-coefficient box 47, pv_old and running-sum tile boxes 48, 49
-//   fused z/r filter: Q blocks 50, z and r code blocks 51, 52, temperature blocks of
-//   buffer b 53 + b (53..57); its coefficient planes as boxes of the interior, general and
-//   half tiles 58, 59, 60
-constexpr int NM_BATCH = 61;
+//   interior half tiles (TR / 2 rows): state box of buffer b 36 + b (36..40), z-filtered
+//   coefficient box 41, final-coefficient box 42, pv_old and running-sum tile boxes 43, 44
+//   fused z/r filter: Q blocks 45, z and r code blocks 46, 47, temperature blocks of
+//   buffer b 48 + b (48..52); its coefficient planes as boxes of the interior, general and
+//   half tiles 53, 54, 55
+constexpr int NM_BATCH = 56;
 inline int bmap_state(int b, int cls) { return b * 2 + cls; }
 inline int bmap_star(int cls, bool lrn) { return (lrn ? 12 : 10) + cls; }
 inline int bmap_sens(int b, int cls) { return 16 + b * 2 + cls; }
 inline int bmap_sensT(int b, int cls) { return 26 + b * 2 + cls; }
-inline int bmap_rho(int b) { return 36 + b; }
-inline int bmap_stateH(int b) { return 41 + b; }
-inline int bmap_starH(bool lrn) { return lrn ? 47 : 46; }
-constexpr int bmap_u0H = 48, bmap_accH = 49;
-constexpr int bmap_zrQ = 50, bmap_zrZc = 51, bmap_zrRc = 52;
-inline int bmap_zrT(int b) { return 53 + b; }
-inline int bmap_coef(int cls) { return 58 + cls; }  // cls 0 interior, 1 general, 2 half tiles
+inline int bmap_stateH(int b) { return 36 + b; }
+inline int bmap_starH(bool lrn) { return lrn ? 42 : 41; }
+constexpr int bmap_u0H = 43, bmap_accH = 44;
+constexpr int bmap_zrQ = 45, bmap_zrZc = 46, bmap_zrRc = 47;
+inline int bmap_zrT(int b) { return 48 + b; }
+inline int bmap_coef(int cls) { return 53 + cls; }  // cls 0 interior, 1 general, 2 half tiles
 
 struct BatchTiles {
   const int4* tiles;  // (i0, j0, instance, 0)
