@@ -2447,7 +2447,7 @@ int batch_stage(axj_batch* b, int bin, int bout, int stage, bool judge) {
                                         : btiles(b, b->st_int, b->h_st_int, b->tune.stage_ctas_per_sm);
   const BatchTiles stg = btiles(b, b->st_gen, b->h_st_gen, std::max<int64_t>(1, b->tune.general_ctas_per_sm));
   const BatchTiles sei = btiles(b, b->se_int, b->h_se_int, b->tune.sensor_ctas_per_sm);
-  const BatchTiles seg = btiles(b, b->se_gen, b->h_se_gen, 1);
+  const BatchTiles seg = btiles(b, b->se_gen, b->h_se_gen, 2);
   // general tiles beside the interior launches (side stream) or on the batch's stream
   const SideStream gside = b->tune.general_serial ? SideStream{nullptr, nullptr, nullptr} : b->side;
   auto sensor = [&](bool rfilter) -> int {

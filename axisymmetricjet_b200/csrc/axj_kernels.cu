@@ -1640,7 +1640,7 @@ __global__ void __launch_bounds__(sens_threads(GEN), GEN ? 2 : 5)
 // Batched form: persistent loop over (i0, j0, instance) tiles; kmaps = indices of the
 // V and T maps in each instance's block of nmaps maps.
 template <int HS, int HF, bool GEN, typename SIN, typename R>
-__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 1 : 5)
+__global__ void __launch_bounds__(sens_threads(GEN), GEN ? 2 : 5)
     sensor_tile_kernel_batch(const SensorArgs* __restrict__ argv, const int4* __restrict__ tiles, int ntiles,
                              const CUtensorMap* __restrict__ mapv, int nmaps, int4 kmaps) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
