@@ -1076,20 +1076,20 @@ struct SensSmem {
   static constexpr size_t oD = align128(oS + sizeof(R) * NS);
   static_assert(sizeof(R) * (TR * DZ + DR * TZ) <= sizeof(SIN) * NV && sizeof(R) * TR * TZ <= sizeof(SIN) * NV,
                 "the arms and f_sw fit in a spent V box");
-  __host__ __device__ static constexpr size_t oDesc(bool gen) { return align128(oD + sizeof(R) * NS); }
+  static constexpr size_t oDesc = align128(oD + sizeof(R) * NS);
   // metrics of the S region: dxidz on its columns [SZ], detadr and 1/r on its rows
   // [2][SR]; deltaz, deltar on the tile [TZ] + [TR]
   __host__ __device__ static constexpr size_t oMet(bool gen) {
-    return align128(oDesc(gen) + (gen ? sizeof(uint32_t) * NV : 0));
+    return align128(oDesc + (gen ? sizeof(uint32_t) * NV : 0));
   }
   static constexpr int NMET = SZ + 2 * SR + TZ + TR;
   __host__ __device__ static constexpr size_t bytes(bool gen) { return align128(oMet(gen) + sizeof(double) * NMET); }
   static constexpr uint32_t tx_bytes = sizeof(SIN) * (2 * NV + NS);
 };
 
-// Threads of a sensor tile CTA: general tiles (one CTA per SM, bound by shared memory)
-// take 512 so the SM has 16 warps to hide latency with; interior tiles 128 (a 2 x 2
-// block of points per thread in the fourth differences; four CTAs per SM).
+// Threads of a sensor tile CTA: general tiles 512, one point per thread in the stencil
+// phases (two CTAs per SM at 105 KB of shared memory and 64 registers); interior tiles
+// 128, a 2 x 2 block of points per thread (five CTAs per SM at 44 KB).
 __host__ __device__ constexpr int sens_threads(bool gen) { return gen ? 512 : 128; }
 
 template <typename R>
@@ -1158,7 +1158,7 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   R* sFsw = reinterpret_cast<R*>(smem_raw + (GEN ? SM::oVz : SM::oVr));
   const SIN* rho0 = std::is_same<SIN, float>::value ? reinterpret_cast<const SIN*>(a.Uf)
                                                      : reinterpret_cast<const SIN*>(a.U);  // rho plane
-  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc(GEN));
+  uint32_t* sDesc = reinterpret_cast<uint32_t*>(smem_raw + SM::oDesc);
   double* sMz = reinterpret_cast<double*>(smem_raw + SM::oMet(GEN));  // dxidz, column i0 - HSZ + k
   double* sMr = sMz + SZ;                                               // detadr, row j0 - HS + k
   double* sIr = sMr + SM::SR;                                           // 1/r (0 on the axis row)
@@ -1429,7 +1429,8 @@ __device__ __forceinline__ bool sensor_body(const SensorArgs& a, int i0, int j0,
   }
 
   // ---- phases 3-4 per field: fourth derivatives at the tile points (kept in registers:
-  // 2 points per thread). Interior tiles: SBP2 of SBP2 with the centred row both times is
+  // PPT points per thread, 4 in interior tiles, 1 in general tiles, the general tiles'
+  // arms in the spent V_r box). Interior tiles: SBP2 of SBP2 with the centred row both times is
   // the 9-point row cC9 = c * c (c the centred SBP2 row), applied to S, T, the dilatation
   // directly (one rounding per product instead of two stencil passes: the difference is
   // rounding only). General tiles: second derivatives on the arms with each arm point's
