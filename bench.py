@@ -361,7 +361,8 @@ def main():
 def time_batched(args, rank):
     """The batched form of uneven jets: 64 instances (Nz in [256, 2048], Nr in [96, 384],
     Mach in [0.9, 1.5], Re in [1000, 5000], harmonic inflow forcing) in one persistent launch
-    per kernel, mixed precision, autotuned (tile order, stage tile shape, CTAs per SM),
+    per kernel, mixed precision, autotuned (tile order, stage tile shape, CTAs per SM, the
+    general tiles' CTAs per SM and stream),
     graph-captured steps; against the same instances one after another on the plain FP64
     path, with each instance's relative L2 error of rho and p against its FP64 run after the
     same number of steps. Forms: the learned sensor judged every 50 steps (the plain sensor
